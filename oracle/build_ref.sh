@@ -1,0 +1,31 @@
+#!/usr/bin/env bash
+# Compile the reference's own C extension (`pyvl.cvl`) from its sources, where they
+# lie, into oracle/_ref/.  Test infrastructure only: the product never loads it.
+#
+# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default: /root/reference)
+#
+# The output, oracle/_ref/cvl<EXT_SUFFIX>, is the unmodified reference induction,
+# topology and line-force code (src/core/*.c + src/*.c, built the way the
+# reference's CMakeLists.txt:60-95 builds it, plus -O3 -fopenmp).  It is git-ignored
+# and travels to the GPU host as a prebuilt file; nothing here needs the reference
+# tree at run time.
+set -euo pipefail
+REF="${1:-/root/reference}"
+HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+OUT="$HERE/_ref"
+PY="${PYTHON:-python3}"
+if [ ! -d "$REF/src/core" ]; then
+  echo "reference sources not found under $REF" >&2
+  exit 1
+fi
+EXT_SUFFIX="$($PY -c 'import sysconfig;print(sysconfig.get_config_var("EXT_SUFFIX"))')"
+PY_INC="$($PY -c 'import sysconfig;print(sysconfig.get_paths()["include"])')"
+NP_INC="$($PY -c 'import numpy;print(numpy.get_include())')"
+mkdir -p "$OUT"
+gcc -O3 -fopenmp -fPIC -shared -std=c17 -DCVL_ASSERTS \
+  -I"$PY_INC" -I"$NP_INC" \
+  "$REF"/src/module.c "$REF"/src/allocator.c "$REF"/src/geoidobject.c \
+  "$REF"/src/lineobject.c "$REF"/src/surfaceobject.c "$REF"/src/meshobject.c \
+  "$REF"/src/referenceframeobject.c "$REF"/src/core/*.c \
+  -o "$OUT/cvl$EXT_SUFFIX" -lm
+echo "built $OUT/cvl$EXT_SUFFIX"
