@@ -1,0 +1,263 @@
+/*
+ * pyvl_b200 -- C ABI of the B200-native UVLM hot path (libpvl_b200.so).
+ *
+ * Plain pointers and sizes only.  Every entry point returns an int status (PVL_OK = 0,
+ * negative on failure; pvl_last_error() gives the message of the calling thread's last
+ * failure).  "Device" arguments are CUDA device pointers; `stream` is a cudaStream_t
+ * passed as void* (NULL = legacy default stream).  Device entry points only enqueue
+ * work: they never synchronise and never allocate; scratch memory comes from the
+ * caller through (ws, ws_bytes) pairs sized by the matching *_workspace() query.
+ *
+ * Geometry ids follow the reference's geo_id_t (src/core/common.h:46-56): bits 0-30
+ * index, bit 31 = reversed orientation; PVL_INVALID_ID = 0x7FFFFFFF.  A mesh is the
+ * reference's mesh_t CSR (src/core/mesh.h:130-139): lines (n_lines x 2 uint32, point
+ * ids), surface_offsets (n_surfaces + 1 uint32), surface_lines (geo ids of lines).
+ * Point arrays are (n, 3) float64 row-major like the reference's real3_t arrays.
+ *
+ * Each declaration names the reference routine it replaces (file:line within the
+ * reference project).
+ */
+#ifndef PVL_B200_H
+#define PVL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    PVL_OK = 0,
+    PVL_ERR_ARG = -1,           /* invalid argument (the reference raises ValueError/TypeError) */
+    PVL_ERR_CUDA = -2,          /* CUDA runtime error */
+    PVL_ERR_ALLOC = -3,         /* workspace too small / host allocation failed */
+    PVL_ERR_SINGULAR = -4,      /* exactly zero pivot met by the LU factorisation */
+    PVL_ERR_NOT_CONVERGED = -5, /* an iterative solve missed its tolerance */
+    PVL_ERR_TOPOLOGY = -6,      /* topology construction failed (RuntimeError in the reference) */
+    PVL_ERR_TIMEOUT = -7        /* a device-side wait gave up (bounded spin) */
+};
+
+enum { PVL_F64 = 0, PVL_F32 = 1 };
+
+#define PVL_INVALID_ID 0x7FFFFFFFu
+
+/* Message of the calling thread's most recent failure ("" if none). */
+const char* pvl_last_error(void);
+/* ABI version (major * 100 + minor). */
+int pvl_version(void);
+
+/* ------------------------------------------------------------------ host topology */
+
+/* Element connectivity -> unique lines + signed ring->line CSR.
+ * Replaces mesh_from_elements (src/core/mesh.c:175-247) and the validation of
+ * Mesh.__new__ (src/meshobject.c:41-116): every element needs >= 3 points and point ids
+ * may not exceed n_points (the reference's own bound, meshobject.c:90).  Line numbering
+ * and orientation bits are identical to the reference's (first appearance order).
+ * lines_out: 2 * sum(counts) uint32; surface_lines_out: sum(counts); offsets_out:
+ * n_elements + 1.  Runs in O(sum(counts)) with a hash of unordered node pairs. */
+int pvl_mesh_from_elements(uint32_t n_points, uint32_t n_elements, const uint32_t* counts,
+                           const uint32_t* flat_points, uint32_t* lines_out,
+                           uint32_t* surface_lines_out, uint32_t* offsets_out,
+                           uint32_t* n_lines_out);
+
+/* Dual mesh: dual line i = the rings on either side of primal line i (slot 0: ring holding
+ * it reversed, slot 1: ring holding it forward; INVALID_ID where missing); dual surface p =
+ * the lines touching primal point p (orientation 0 where p is the line's first point).
+ * Replaces mesh_dual_from_primal (src/core/mesh.c:70-173), O(total) instead of O(L*S).
+ * dual_lines_out: 2 * n_lines; dual_offsets_out: n_points + 1;
+ * dual_surface_lines_out: 2 * n_lines. */
+int pvl_mesh_dual(uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
+                  uint32_t n_surfaces, const uint32_t* surface_offsets,
+                  const uint32_t* surface_lines, uint32_t* dual_lines_out,
+                  uint32_t* dual_offsets_out, uint32_t* dual_surface_lines_out);
+
+/* Mesh -> element connectivity (point counts and flattened loops).
+ * Replaces mesh_to_elements (src/core/mesh.c:249-301).  counts_out: n_surfaces;
+ * flat_out: surface_offsets[n_surfaces]. */
+int pvl_mesh_to_elements(uint32_t n_surfaces, const uint32_t* surface_offsets,
+                         const uint32_t* surface_lines, const uint32_t* lines,
+                         uint32_t* counts_out, uint32_t* flat_out);
+
+/* Inverse of the ring->line CSR: for each line the signed ids of the rings that hold it
+ * (bit 31 set where the ring holds the line reversed), rings in ascending order.  Used to
+ * turn ring circulations into line circulations.  No reference counterpart; it is the
+ * transpose of the CSR the reference reduces over (src/core/flow_solver.c:141-205).
+ * map_offsets_out: n_lines + 1; map_entries_out: surface_offsets[n_surfaces]. */
+int pvl_line_ring_map(uint32_t n_lines, uint32_t n_surfaces, const uint32_t* surface_offsets,
+                      const uint32_t* surface_lines, uint32_t* map_offsets_out,
+                      uint32_t* map_entries_out);
+
+/* ------------------------------------------------------------------ device geometry */
+
+/* Unit ring normals (n_surfaces, 3).  Replaces surface_normal (src/core/mesh.c:48-68) as
+ * called by Mesh.surface_normal (src/meshobject.c:956-1008). */
+int pvl_surface_normal(uint32_t n_surfaces, const uint32_t* surface_offsets,
+                       const uint32_t* surface_lines, const uint32_t* lines,
+                       const double* positions, double* out, void* stream);
+
+/* Per-ring mean of a per-point vec3 (n_surfaces, 3).  Replaces surface_center
+ * (src/core/mesh.c:24-46) as called by Mesh.surface_average_vec3 (src/meshobject.c:1010-1062). */
+int pvl_surface_average(uint32_t n_surfaces, const uint32_t* surface_offsets,
+                        const uint32_t* surface_lines, const uint32_t* lines,
+                        const double* values, double* out, void* stream);
+
+/* No-penetration right-hand side b_i = n_i . (-(U_i - v_i)) with U_i = flow[i] when
+ * flow != NULL else (ux, uy, uz); cp_velocity may be NULL (zero).
+ * Replaces python/pyvl/solver.py:199-206. */
+int pvl_rhs(uint32_t n, const double* normals, const double* flow, double ux, double uy,
+            double uz, const double* cp_velocity, double* rhs_out, void* stream);
+
+/* ------------------------------------------------------------------ induction */
+
+/* Scratch for the segment table of n_lines segments at `precision`. */
+size_t pvl_segments_workspace(uint32_t n_lines, int precision);
+
+/* Line induction matrix (n_cp, n_lines, 3) float64: every (segment, point) pair.
+ * Replaces compute_line_induction (src/core/flow_solver.c:86-139) as called by
+ * Mesh.line_induction_matrix (src/meshobject.c:1232-1286). */
+int pvl_line_induction(uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
+                       const double* positions, uint32_t n_cp, const double* cps, double tol,
+                       double* out, void* ws, size_t ws_bytes, void* stream);
+
+/* Ring induction matrix (n_cp, n_surfaces, 3) float64, fused pair + signed ring sum (no
+ * line buffer).  Replaces Mesh.induction_matrix (src/meshobject.c:475-556):
+ * compute_line_induction + line_induction_to_surface_induction (flow_solver.c:141-172). */
+int pvl_induction_matrix(uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
+                         const double* positions, uint32_t n_surfaces,
+                         const uint32_t* surface_offsets, const uint32_t* surface_lines,
+                         uint32_t n_cp, const double* cps, double tol, double* out, void* ws,
+                         size_t ws_bytes, void* stream);
+
+/* Normal ring induction matrix out[i * ld + j] = n_i . sum_{k in ring j} +-u_k(cp_i),
+ * fused (no line buffer); `out_precision` selects float64 or float32 output and
+ * arithmetic.  Replaces Mesh.induction_matrix3 (src/meshobject.c:384-473):
+ * compute_line_induction + line_induction_to_normal_surface_induction
+ * (flow_solver.c:174-205). */
+int pvl_induction_normal(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
+                         const double* positions, uint32_t n_surfaces,
+                         const uint32_t* surface_offsets, const uint32_t* surface_lines,
+                         uint32_t n_cp, const double* cps, const double* normals, double tol,
+                         void* out, uint32_t ld, void* ws, size_t ws_bytes, void* stream);
+
+/* Scratch for pvl_line_velocity. */
+size_t pvl_line_velocity_workspace(uint32_t n_lines, uint32_t n_pts, int precision);
+
+/* Velocity induced at points by segments carrying circulations:
+ *   v(p) = sum_k gamma_k u_k(p)   (line_gamma == NULL: gamma_k = 1)
+ * and, with normals != NULL, the projection n_p . v(p).  out is (n_pts, 3) or (n_pts,);
+ * out = beta * out + alpha * v.  This is the contraction sum_j K_ij Gamma_j the reference
+ * forms from a materialised (n_pts, n_surfaces, 3) matrix and numpy's vecdot
+ * (python/pyvl/wake_models.py:125-126, 170-175, 219-223; solver.py:274-279), evaluated
+ * per segment with gamma_k = sum of the signed ring circulations of the rings holding k. */
+int pvl_line_velocity(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
+                      const double* positions, const double* line_gamma, uint32_t n_pts,
+                      const double* pts, const double* normals, double tol, double alpha,
+                      double beta, double* out, void* ws, size_t ws_bytes, void* stream);
+
+/* Line circulations gamma_line[k] = sum over the rings holding line k of +-gamma_ring
+ * (sign from the orientation bit).  With ring_period > 0, rings whose index is a multiple
+ * of ring_period are skipped (the implicit first wake row).  Uses pvl_line_ring_map. */
+int pvl_line_circulation(uint32_t n_lines, const uint32_t* map_offsets,
+                         const uint32_t* map_entries, const double* ring_gamma,
+                         uint32_t ring_period, double* line_gamma_out, void* stream);
+
+/* ------------------------------------------------------------------ free wake */
+
+/* Fold the implicit wake row into the system matrix:
+ *   A[:, adj[s,1]] -= implicit[:, s];  A[:, adj[s,0]] += implicit[:, s]
+ * for s = 0..n_shed-1 in order, INVALID_ID sides skipped.  implicit is (n_cp, n_shed).
+ * Replaces python/pyvl/wake_models.py:204-216. */
+int pvl_wake_fold_implicit(uint32_t n_cp, uint32_t n_shed, const double* implicit,
+                           const uint32_t* adjacent, double* A, uint32_t lda, void* stream);
+
+/* Velocity of the wake nodes that advect this step: for every (s, side) and row
+ * i < complete_rows, node_vel[(s*2 + side)*complete_rows + i] = U_inf + sum_k gamma_k u_k(node)
+ * with the body segments (lines, positions, line_gamma).  wake_pos is (n_shed, 2,
+ * line_rows + 1, 3).  Replaces the per-row loop of python/pyvl/wake_models.py:120-126
+ * (FlowConditions.get_velocity + induction_matrix @ circulation) for a uniform U_inf. */
+size_t pvl_wake_node_velocity_workspace(uint32_t n_lines, uint32_t n_shed, uint32_t complete_rows,
+                                        int precision);
+int pvl_wake_node_velocity(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
+                           const double* positions, const double* line_gamma, uint32_t n_shed,
+                           uint32_t line_rows, uint32_t complete_rows, const double* wake_pos,
+                           double ux, double uy, double uz, double tol, double* node_vel, void* ws,
+                           size_t ws_bytes, void* stream);
+
+/* Advance wake node rows (explicit Euler) from `old_pos` into `new_pos` (both
+ * (n_shed, 2, line_rows + 1, 3)): new[:, :, i+1] = old[:, :, i] + node_vel[:, :, i] * dt for
+ * i < complete_rows; row 0 pinned to the bordering body nodes; rows beyond complete_rows
+ * collapsed onto row complete_rows.  node_vel is (n_shed, 2, complete_rows, 3) and already
+ * holds U_inf + body induction.  Replaces python/pyvl/wake_models.py:113-137. */
+int pvl_wake_advect(uint32_t n_shed, uint32_t line_rows, uint32_t complete_rows,
+                    const double* old_pos, const double* node_vel, double dt,
+                    const double* body_positions, const uint32_t* bordering_nodes,
+                    double* new_pos, void* stream);
+
+/* Shift wake circulations one row back and shed the new first row
+ *   circ[:, 0] = gamma[adj[:,1]] - gamma[adj[:,0]]   (INVALID_ID sides skipped)
+ * into new_circ (n_shed, line_rows) from old_circ.  Replaces wake_models.py:139-151. */
+int pvl_wake_shed(uint32_t n_shed, uint32_t line_rows, const double* old_circ,
+                  const uint32_t* adjacent, const double* gamma, double* new_circ, void* stream);
+
+/* ------------------------------------------------------------------ dense solve */
+
+/* Scratch for pvl_lu_factor / pvl_lu_solve. */
+size_t pvl_lu_workspace(uint32_t n);
+size_t pvl_lu_solve_workspace(uint32_t n);
+
+/* In-place LU with partial pivoting of the row-major n x n matrix A (leading dimension
+ * lda): P A = L U with unit-lower L.  ipiv (device int32, 2n entries) receives in its first
+ * n entries the LAPACK interchange sequence (ipiv[k] = row swapped with row k, 0-based) and
+ * in the next n the resulting row permutation (row i of P A is row perm[i] of A).  info
+ * (device int32) receives 0, or k+1 when U[k,k] == 0 (getrf convention).  FP64 throughout;
+ * the pivots are exactly those of partial pivoting (first maximal |entry| per column).
+ * Replaces scipy.linalg.lu_factor (python/pyvl/solver.py:223). */
+int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv, int32_t* info, void* ws,
+                  size_t ws_bytes, void* stream);
+
+/* Solve A x = b in place in b (device, n) with the factors and ipiv of pvl_lu_factor.  err
+ * (device int32) receives 0, or 1 if a wait between row blocks timed out.
+ * Replaces scipy.linalg.lu_solve (python/pyvl/solver.py:227). */
+int pvl_lu_solve(uint32_t n, const double* LU, uint32_t lda, const int32_t* ipiv, double* b,
+                 int32_t* err, void* ws, size_t ws_bytes, void* stream);
+
+/* Remove the mean of x over each group g: x[off[g]:off[g+1]] -= mean.  Replaces the
+ * closed-body constraint of python/pyvl/solver.py:229-233. */
+int pvl_group_mean_remove(uint32_t n_groups, const uint32_t* group_offsets, double* x,
+                          void* stream);
+
+/* Border an n x n system for zero-mean circulation on m groups: with A of leading
+ * dimension lda >= n + m, sets A[i, n+g] = A[n+g, i] = 1 for i in group g, zero elsewhere
+ * in the border, and rhs[n+g] = 0.  The bordered system is the well-posed form of the
+ * reference's closed-body constraint (solver.py:229-233). */
+int pvl_border_groups(uint32_t n, uint32_t m, const uint32_t* group_offsets, double* A,
+                      uint32_t lda, double* rhs, void* stream);
+
+/* ------------------------------------------------------------------ forces */
+
+/* Kutta-Joukowski line forces F_k = (r_end - r_begin) x (0.5 c_k (v_p1 + v_p2)),
+ * c_k = circ[dual.p1] - circ[dual.p2] (INVALID sides skipped); circ is the ring
+ * circulation divided by 2 pi.  Replaces Mesh.line_forces (src/meshobject.c:1288-1396). */
+int pvl_line_forces(uint32_t n_lines, const uint32_t* primal_lines, const uint32_t* dual_lines,
+                    const double* circ, const double* positions, const double* velocity,
+                    double* out, void* stream);
+
+/* ------------------------------------------------------------------ measurement */
+
+/* Number of kernels this library has enqueued since it was loaded (all threads).  No
+ * reference counterpart: it lets a benchmark state how many of the library's kernels ran. */
+unsigned long long pvl_launch_count(void);
+
+/* Enqueue a kernel of n_blocks x 256 threads, each running 8 independent FMA chains of
+ * `iters` steps in `precision`; returns the exact FLOP count it performs (2 per FMA), or a
+ * negative value on error.  `sink` is a device buffer of n_blocks elements (never written in
+ * practice).  Timing it with events gives the non-tensor FMA peak of the GPU.  No reference
+ * counterpart (measurement helper). */
+double pvl_fma_probe(int precision, uint32_t n_blocks, uint32_t iters, void* sink, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PVL_B200_H */

@@ -1,0 +1,663 @@
+// Segment -> point induction kernels for sm_100a.
+//
+// The reference evaluates every (line, point) pair into a 24 B/pair line buffer and then
+// reduces it per ring (src/core/flow_solver.c:86-205).  Here no line buffer exists:
+//  * ring matrices (normal or vector) evaluate each ring's segments in the thread that
+//    owns the (point, ring) entry and store the entry once, coalesced along the row;
+//  * contractions with circulations (velocities, the explicit wake term) become an
+//    N-body sweep: points live in registers, segments stream through shared memory in
+//    tiles, each segment carries its line circulation, and partial sums over segment
+//    ranges are reduced deterministically in a second pass.
+// All pair arithmetic is pvl::segment_induction (pvl_common.cuh).
+#include <algorithm>
+#include <cstdint>
+
+#include "pvl_common.cuh"
+
+using pvl::Segment;
+using pvl::Vec3;
+
+namespace {
+
+constexpr int kSegTile = 128;   // segments per shared-memory tile
+constexpr int kSumThreads = 128;
+constexpr int kSumPPT = 2;      // points per thread in the N-body sweep
+constexpr int kRingThreads = 128;
+constexpr int kRingCPB = 8;     // control points per CTA row-block in ring matrices
+
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+template <typename T>
+__global__ void prep_segments_kernel(uint32_t n_points, uint32_t n_lines, const uint32_t* __restrict__ lines,
+                                     const double* __restrict__ pos, const double* __restrict__ line_gamma,
+                                     double tol, Segment<T>* __restrict__ seg)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_lines)
+        return;
+    const uint32_t a = PVL_IDX(lines[2 * i]), b = PVL_IDX(lines[2 * i + 1]);
+    Segment<T> s;
+    if (a >= n_points || b >= n_points) {
+        s.r1x = s.r1y = s.r1z = s.r2x = s.r2y = s.r2z = s.dx = s.dy = s.dz = T(0);
+        s.len = T(-1);
+        s.gamma = T(0);
+        s.pad = T(0);
+        seg[i] = s;
+        return;
+    }
+    const double r1x = pos[3 * (size_t)a], r1y = pos[3 * (size_t)a + 1], r1z = pos[3 * (size_t)a + 2];
+    const double r2x = pos[3 * (size_t)b], r2y = pos[3 * (size_t)b + 1], r2z = pos[3 * (size_t)b + 2];
+    double dx = r2x - r1x, dy = r2y - r1y, dz = r2z - r1z;
+    const double len = sqrt(dx * dx + dy * dy + dz * dz);
+    dx /= len;
+    dy /= len;
+    dz /= len;
+    s.r1x = T(r1x);
+    s.r1y = T(r1y);
+    s.r1z = T(r1z);
+    s.r2x = T(r2x);
+    s.r2y = T(r2y);
+    s.r2z = T(r2z);
+    s.dx = T(dx);
+    s.dy = T(dy);
+    s.dz = T(dz);
+    // src/core/flow_solver.c:107-112: a segment shorter than tol induces nothing.
+    s.len = (len < tol) ? T(-1) : T(len);
+    s.gamma = line_gamma ? T(line_gamma[i]) : T(1);
+    s.pad = T(0);
+    seg[i] = s;
+}
+
+template <typename T>
+__device__ __forceinline__ Vec3<T> ring_sum(const uint32_t* __restrict__ sl, uint32_t k0, uint32_t k1,
+                                            uint32_t n_lines, const Segment<T>* __restrict__ seg, T px, T py,
+                                            T pz, T tol2)
+{
+    Vec3<T> acc{T(0), T(0), T(0)};
+    for (uint32_t k = k0; k < k1; ++k) {
+        const uint32_t g = sl[k];
+        const uint32_t l = PVL_IDX(g);
+        if (l >= n_lines)
+            continue;
+        // reversed lines are subtracted (src/core/flow_solver.c:192-199)
+        pvl::segment_induction(seg[l], px, py, pz, tol2, PVL_REV(g) ? T(-1) : T(1), acc);
+    }
+    return acc;
+}
+
+// out[i*ld + j] = n_i . sum_{k in ring j} +-u_k(cp_i)        (MODE 0, OutT = T or float)
+// out[(i*n_surfaces + j)*3 + c] = sum_{k in ring j} +-u_k     (MODE 1, OutT = double)
+template <typename T, typename OutT, int MODE>
+__global__ void __launch_bounds__(kRingThreads) ring_matrix_kernel(
+    uint32_t n_surfaces, const uint32_t* __restrict__ off, const uint32_t* __restrict__ sl, uint32_t n_lines,
+    const Segment<T>* __restrict__ seg, uint32_t n_cp, const double* __restrict__ cps,
+    const double* __restrict__ normals, T tol2, OutT* __restrict__ out, uint32_t ld)
+{
+    __shared__ T s_p[kRingCPB][3];
+    __shared__ T s_n[kRingCPB][3];
+    const uint32_t i0 = blockIdx.y * kRingCPB;
+    if (threadIdx.x < kRingCPB * 3) {
+        const uint32_t c = threadIdx.x / 3, e = threadIdx.x % 3;
+        const uint32_t i = i0 + c;
+        s_p[c][e] = i < n_cp ? T(cps[3 * (size_t)i + e]) : T(0);
+        s_n[c][e] = (MODE == 0 && i < n_cp) ? T(normals[3 * (size_t)i + e]) : T(0);
+    }
+    __syncthreads();
+    const uint32_t j = blockIdx.x * kRingThreads + threadIdx.x;
+    if (j >= n_surfaces)
+        return;
+    const uint32_t k0 = off[j], k1 = off[j + 1];
+#pragma unroll 1
+    for (int c = 0; c < kRingCPB; ++c) {
+        const uint32_t i = i0 + c;
+        if (i >= n_cp)
+            break;
+        const Vec3<T> v = ring_sum(sl, k0, k1, n_lines, seg, s_p[c][0], s_p[c][1], s_p[c][2], tol2);
+        if (MODE == 0) {
+            out[(size_t)i * ld + j] = OutT(v.x * s_n[c][0] + v.y * s_n[c][1] + v.z * s_n[c][2]);
+        } else {
+            OutT* o = out + 3 * ((size_t)i * n_surfaces + j);
+            o[0] = OutT(v.x);
+            o[1] = OutT(v.y);
+            o[2] = OutT(v.z);
+        }
+    }
+}
+
+// out[(i*n_lines + l)*3 + c] = u_l(cp_i)
+__global__ void __launch_bounds__(kRingThreads) line_matrix_kernel(uint32_t n_lines,
+                                                                   const Segment<double>* __restrict__ seg,
+                                                                   uint32_t n_cp, const double* __restrict__ cps,
+                                                                   double tol2, double* __restrict__ out)
+{
+    __shared__ double s_p[kRingCPB][3];
+    const uint32_t i0 = blockIdx.y * kRingCPB;
+    if (threadIdx.x < kRingCPB * 3) {
+        const uint32_t c = threadIdx.x / 3, e = threadIdx.x % 3;
+        s_p[c][e] = (i0 + c) < n_cp ? cps[3 * (size_t)(i0 + c) + e] : 0.0;
+    }
+    __syncthreads();
+    const uint32_t l = blockIdx.x * kRingThreads + threadIdx.x;
+    if (l >= n_lines)
+        return;
+    const Segment<double> s = seg[l];
+    for (int c = 0; c < kRingCPB; ++c) {
+        const uint32_t i = i0 + c;
+        if (i >= n_cp)
+            break;
+        Vec3<double> acc{0.0, 0.0, 0.0};
+        pvl::segment_induction(s, s_p[c][0], s_p[c][1], s_p[c][2], tol2, 1.0, acc);
+        double* o = out + 3 * ((size_t)i * n_lines + l);
+        o[0] = acc.x;
+        o[1] = acc.y;
+        o[2] = acc.z;
+    }
+}
+
+// N-body sweep: partial[(split*n_pts + p)*3 + c] = sum over this split's segments of gamma_k u_k(p).
+// Point p of the sweep is pts[(p / group) * stride + p % group]: group == stride == n_pts
+// is a plain array; group = complete rows, stride = rows + 1 walks the advecting wake rows.
+template <typename T>
+__global__ void __launch_bounds__(kSumThreads) line_sum_kernel(const Segment<T>* __restrict__ seg, uint32_t n_lines,
+                                                               uint32_t lines_per_split,
+                                                               const double* __restrict__ pts, uint32_t n_pts,
+                                                               uint32_t group, uint32_t stride, T tol2,
+                                                               T* __restrict__ partial)
+{
+    __shared__ Segment<T> s_seg[kSegTile];
+    const uint32_t split = blockIdx.y;
+    const uint32_t l_begin = split * lines_per_split;
+    const uint32_t l_end = min(n_lines, l_begin + lines_per_split);
+    T px[kSumPPT], py[kSumPPT], pz[kSumPPT];
+    Vec3<T> acc[kSumPPT];
+#pragma unroll
+    for (int t = 0; t < kSumPPT; ++t) {
+        const uint32_t p = blockIdx.x * (kSumThreads * kSumPPT) + t * kSumThreads + threadIdx.x;
+        const bool ok = p < n_pts;
+        const size_t q = ok ? (size_t)(p / group) * stride + p % group : 0;
+        px[t] = ok ? T(pts[3 * q]) : T(0);
+        py[t] = ok ? T(pts[3 * q + 1]) : T(0);
+        pz[t] = ok ? T(pts[3 * q + 2]) : T(0);
+        acc[t] = Vec3<T>{T(0), T(0), T(0)};
+    }
+    for (uint32_t l0 = l_begin; l0 < l_end; l0 += kSegTile) {
+        const uint32_t l = l0 + threadIdx.x;
+        if (threadIdx.x < kSegTile && l < l_end)
+            s_seg[threadIdx.x] = seg[l];
+        __syncthreads();
+        const int cnt = (int)min((uint32_t)kSegTile, l_end - l0);
+#pragma unroll 1
+        for (int k = 0; k < cnt; ++k) {
+            const Segment<T> s = s_seg[k];
+#pragma unroll
+            for (int t = 0; t < kSumPPT; ++t)
+                pvl::segment_induction(s, px[t], py[t], pz[t], tol2, s.gamma, acc[t]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int t = 0; t < kSumPPT; ++t) {
+        const uint32_t p = blockIdx.x * (kSumThreads * kSumPPT) + t * kSumThreads + threadIdx.x;
+        if (p < n_pts) {
+            T* o = partial + 3 * ((size_t)split * n_pts + p);
+            o[0] = acc[t].x;
+            o[1] = acc[t].y;
+            o[2] = acc[t].z;
+        }
+    }
+}
+
+// out = beta * out + alpha * v (+ (ux, uy, uz) for vector output), v = sum of the partials.
+template <typename T>
+__global__ void reduce_partials_kernel(uint32_t n_pts, uint32_t n_split, const T* __restrict__ partial,
+                                       const double* __restrict__ normals, double alpha, double beta, double ux,
+                                       double uy, double uz, double* __restrict__ out)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n_pts)
+        return;
+    double vx = 0, vy = 0, vz = 0;
+    for (uint32_t s = 0; s < n_split; ++s) {
+        const T* q = partial + 3 * ((size_t)s * n_pts + p);
+        vx += double(q[0]);
+        vy += double(q[1]);
+        vz += double(q[2]);
+    }
+    if (normals) {
+        const double v = vx * normals[3 * (size_t)p] + vy * normals[3 * (size_t)p + 1] + vz * normals[3 * (size_t)p + 2];
+        out[p] = beta == 0.0 ? alpha * v : beta * out[p] + alpha * v;
+    } else {
+        double* o = out + 3 * (size_t)p;
+        if (beta == 0.0) {
+            o[0] = ux + alpha * vx;
+            o[1] = uy + alpha * vy;
+            o[2] = uz + alpha * vz;
+        } else {
+            o[0] = beta * o[0] + (ux + alpha * vx);
+            o[1] = beta * o[1] + (uy + alpha * vy);
+            o[2] = beta * o[2] + (uz + alpha * vz);
+        }
+    }
+}
+
+__global__ void line_circulation_kernel(uint32_t n_lines, const uint32_t* __restrict__ map_off,
+                                        const uint32_t* __restrict__ map_ent, const double* __restrict__ ring_gamma,
+                                        uint32_t ring_period, double* __restrict__ out)
+{
+    const uint32_t l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= n_lines)
+        return;
+    double g = 0.0;
+    for (uint32_t k = map_off[l]; k < map_off[l + 1]; ++k) {
+        const uint32_t e = map_ent[k];
+        const uint32_t r = PVL_IDX(e);
+        if (ring_period && (r % ring_period) == 0)
+            continue;
+        g += PVL_REV(e) ? -ring_gamma[r] : ring_gamma[r];
+    }
+    out[l] = g;
+}
+
+__device__ __forceinline__ void load3(const double* p, uint32_t i, double& x, double& y, double& z)
+{
+    x = p[3 * (size_t)i];
+    y = p[3 * (size_t)i + 1];
+    z = p[3 * (size_t)i + 2];
+}
+
+// src/core/mesh.c:48-68 (direction of an oriented line: mesh.c:14-22)
+__global__ void surface_normal_kernel(uint32_t n_surfaces, const uint32_t* __restrict__ off,
+                                      const uint32_t* __restrict__ sl, const uint32_t* __restrict__ lines,
+                                      const double* __restrict__ pos, double* __restrict__ out)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_surfaces)
+        return;
+    const uint32_t k0 = off[s], k1 = off[s + 1];
+    auto dir = [&](uint32_t g, double& x, double& y, double& z) {
+        double ax, ay, az, bx, by, bz;
+        load3(pos, PVL_IDX(lines[2 * PVL_IDX(g)]), ax, ay, az);
+        load3(pos, PVL_IDX(lines[2 * PVL_IDX(g) + 1]), bx, by, bz);
+        if (PVL_REV(g)) {
+            x = bx - ax; y = by - ay; z = bz - az;
+        } else {
+            x = ax - bx; y = ay - by; z = az - bz;
+        }
+    };
+    double ox = 0, oy = 0, oz = 0, d1x, d1y, d1z;
+    dir(sl[k0], d1x, d1y, d1z);
+    const double d0x = d1x, d0y = d1y, d0z = d1z;
+    for (uint32_t k = k0 + 1; k < k1; ++k) {
+        double d2x, d2y, d2z;
+        dir(sl[k], d2x, d2y, d2z);
+        ox += d2y * d1z - d2z * d1y;
+        oy += d2z * d1x - d2x * d1z;
+        oz += d2x * d1y - d2y * d1x;
+        d1x = d2x; d1y = d2y; d1z = d2z;
+    }
+    ox += d0y * d1z - d0z * d1y;
+    oy += d0z * d1x - d0x * d1z;
+    oz += d0x * d1y - d0y * d1x;
+    const double inv = 1.0 / sqrt(ox * ox + oy * oy + oz * oz);
+    out[3 * (size_t)s] = ox * inv;
+    out[3 * (size_t)s + 1] = oy * inv;
+    out[3 * (size_t)s + 2] = oz * inv;
+}
+
+// src/core/mesh.c:24-46
+__global__ void surface_average_kernel(uint32_t n_surfaces, const uint32_t* __restrict__ off,
+                                       const uint32_t* __restrict__ sl, const uint32_t* __restrict__ lines,
+                                       const double* __restrict__ val, double* __restrict__ out)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_surfaces)
+        return;
+    double ax = 0, ay = 0, az = 0;
+    for (uint32_t k = off[s]; k < off[s + 1]; ++k) {
+        const uint32_t g = sl[k];
+        const uint32_t pt = PVL_REV(g) ? lines[2 * PVL_IDX(g) + 1] : lines[2 * PVL_IDX(g)];
+        double x, y, z;
+        load3(val, PVL_IDX(pt), x, y, z);
+        ax += x; ay += y; az += z;
+    }
+    const double div = 1.0 / double(off[s + 1] - off[s]);
+    out[3 * (size_t)s] = ax * div;
+    out[3 * (size_t)s + 1] = ay * div;
+    out[3 * (size_t)s + 2] = az * div;
+}
+
+// python/pyvl/solver.py:199-206
+__global__ void rhs_kernel(uint32_t n, const double* __restrict__ normals, const double* __restrict__ flow, double ux,
+                           double uy, double uz, const double* __restrict__ cpv, double* __restrict__ rhs)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    double ex = flow ? flow[3 * (size_t)i] : ux, ey = flow ? flow[3 * (size_t)i + 1] : uy,
+           ez = flow ? flow[3 * (size_t)i + 2] : uz;
+    if (cpv) {
+        ex -= cpv[3 * (size_t)i];
+        ey -= cpv[3 * (size_t)i + 1];
+        ez -= cpv[3 * (size_t)i + 2];
+    }
+    rhs[i] = normals[3 * (size_t)i] * -ex + normals[3 * (size_t)i + 1] * -ey + normals[3 * (size_t)i + 2] * -ez;
+}
+
+// src/meshobject.c:1368-1393
+__global__ void line_forces_kernel(uint32_t n_lines, const uint32_t* __restrict__ pl, const uint32_t* __restrict__ dl,
+                                   const double* __restrict__ circ, const double* __restrict__ pos,
+                                   const double* __restrict__ vel, double* __restrict__ out)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_lines)
+        return;
+    const uint32_t p1 = PVL_IDX(pl[2 * i]), p2 = PVL_IDX(pl[2 * i + 1]);
+    const uint32_t d1 = PVL_IDX(dl[2 * i]), d2 = PVL_IDX(dl[2 * i + 1]);
+    double ax, ay, az, bx, by, bz;
+    load3(pos, p1, ax, ay, az);
+    load3(pos, p2, bx, by, bz);
+    const double rx = bx - ax, ry = by - ay, rz = bz - az;
+    double c = 0.0;
+    if (d1 != PVL_INVALID)
+        c += circ[d1];
+    if (d2 != PVL_INVALID)
+        c -= circ[d2];
+    double v1x, v1y, v1z, v2x, v2y, v2z;
+    load3(vel, p1, v1x, v1y, v1z);
+    load3(vel, p2, v2x, v2y, v2z);
+    const double k = 0.5 * c;
+    const double wx = (v1x + v2x) * k, wy = (v1y + v2y) * k, wz = (v1z + v2z) * k;
+    out[3 * (size_t)i] = ry * wz - rz * wy;
+    out[3 * (size_t)i + 1] = rz * wx - rx * wz;
+    out[3 * (size_t)i + 2] = rx * wy - ry * wx;
+}
+
+inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+template <typename T>
+int prep_segments(uint32_t n_points, uint32_t n_lines, const uint32_t* lines, const double* positions,
+                  const double* line_gamma, double tol, Segment<T>* seg, cudaStream_t st)
+{
+    if (n_lines == 0)
+        return PVL_OK;
+    prep_segments_kernel<T><<<blocks_for(n_lines, 256), 256, 0, st>>>(n_points, n_lines, lines, positions, line_gamma,
+                                                                       tol, seg);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+// Number of segment ranges the N-body sweep is split into: enough CTAs to fill the
+// 148 SMs several times over, at least two tiles of segments per range.
+uint32_t sum_splits(uint32_t n_lines, uint32_t n_pts)
+{
+    const uint64_t ctas_x = (n_pts + kSumThreads * kSumPPT - 1) / (kSumThreads * kSumPPT);
+    const uint64_t want = 148ull * 8;
+    uint64_t s = (want + ctas_x - 1) / std::max<uint64_t>(ctas_x, 1);
+    const uint64_t max_s = std::max<uint64_t>(1, (n_lines + 2 * kSegTile - 1) / (2 * kSegTile));
+    s = std::min(std::max<uint64_t>(s, 1), max_s);
+    return (uint32_t)std::min<uint64_t>(s, 65535);
+}
+
+int check_stream_args(const void* p, const char* what)
+{
+    if (!p)
+        return pvl_fail(PVL_ERR_ARG, "%s is NULL", what);
+    return PVL_OK;
+}
+
+}  // namespace
+
+#define PVL_REQUIRE(ptr)                                 \
+    do {                                                 \
+        int _r = check_stream_args((ptr), #ptr);         \
+        if (_r)                                          \
+            return _r;                                   \
+    } while (0)
+
+extern "C" size_t pvl_segments_workspace(uint32_t n_lines, int precision)
+{
+    return align256((size_t)n_lines * (precision == PVL_F32 ? sizeof(Segment<float>) : sizeof(Segment<double>)));
+}
+
+extern "C" int pvl_surface_normal(uint32_t n_surfaces, const uint32_t* off, const uint32_t* sl, const uint32_t* lines,
+                                  const double* positions, double* out, void* stream)
+{
+    if (n_surfaces == 0)
+        return PVL_OK;
+    PVL_REQUIRE(off); PVL_REQUIRE(sl); PVL_REQUIRE(lines); PVL_REQUIRE(positions); PVL_REQUIRE(out);
+    surface_normal_kernel<<<blocks_for(n_surfaces, 128), 128, 0, (cudaStream_t)stream>>>(n_surfaces, off, sl, lines,
+                                                                                         positions, out);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_surface_average(uint32_t n_surfaces, const uint32_t* off, const uint32_t* sl, const uint32_t* lines,
+                                   const double* values, double* out, void* stream)
+{
+    if (n_surfaces == 0)
+        return PVL_OK;
+    PVL_REQUIRE(off); PVL_REQUIRE(sl); PVL_REQUIRE(lines); PVL_REQUIRE(values); PVL_REQUIRE(out);
+    surface_average_kernel<<<blocks_for(n_surfaces, 128), 128, 0, (cudaStream_t)stream>>>(n_surfaces, off, sl, lines,
+                                                                                          values, out);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_rhs(uint32_t n, const double* normals, const double* flow, double ux, double uy, double uz,
+                       const double* cp_velocity, double* rhs_out, void* stream)
+{
+    if (n == 0)
+        return PVL_OK;
+    PVL_REQUIRE(normals); PVL_REQUIRE(rhs_out);
+    rhs_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(n, normals, flow, ux, uy, uz, cp_velocity,
+                                                                     rhs_out);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_line_induction(uint32_t n_points, uint32_t n_lines, const uint32_t* lines, const double* positions,
+                                  uint32_t n_cp, const double* cps, double tol, double* out, void* ws,
+                                  size_t ws_bytes, void* stream)
+{
+    if (n_lines == 0 || n_cp == 0)
+        return PVL_OK;
+    PVL_REQUIRE(lines); PVL_REQUIRE(positions); PVL_REQUIRE(cps); PVL_REQUIRE(out); PVL_REQUIRE(ws);
+    if (ws_bytes < pvl_segments_workspace(n_lines, PVL_F64))
+        return pvl_fail(PVL_ERR_ALLOC, "pvl_line_induction: workspace %zu < %zu", ws_bytes,
+                        pvl_segments_workspace(n_lines, PVL_F64));
+    cudaStream_t st = (cudaStream_t)stream;
+    auto* seg = static_cast<Segment<double>*>(ws);
+    if (int r = prep_segments<double>(n_points, n_lines, lines, positions, nullptr, tol, seg, st))
+        return r;
+    dim3 grid(blocks_for(n_lines, kRingThreads), blocks_for(n_cp, kRingCPB));
+    if (grid.y > 65535)
+        return pvl_fail(PVL_ERR_ARG, "pvl_line_induction: too many points (%u)", n_cp);
+    line_matrix_kernel<<<grid, kRingThreads, 0, st>>>(n_lines, seg, n_cp, cps, tol * tol, out);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_induction_matrix(uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
+                                    const double* positions, uint32_t n_surfaces, const uint32_t* off,
+                                    const uint32_t* sl, uint32_t n_cp, const double* cps, double tol, double* out,
+                                    void* ws, size_t ws_bytes, void* stream)
+{
+    if (n_surfaces == 0 || n_cp == 0)
+        return PVL_OK;
+    PVL_REQUIRE(lines); PVL_REQUIRE(positions); PVL_REQUIRE(off); PVL_REQUIRE(sl); PVL_REQUIRE(cps);
+    PVL_REQUIRE(out); PVL_REQUIRE(ws);
+    if (ws_bytes < pvl_segments_workspace(n_lines, PVL_F64))
+        return pvl_fail(PVL_ERR_ALLOC, "pvl_induction_matrix: workspace too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    auto* seg = static_cast<Segment<double>*>(ws);
+    if (int r = prep_segments<double>(n_points, n_lines, lines, positions, nullptr, tol, seg, st))
+        return r;
+    dim3 grid(blocks_for(n_surfaces, kRingThreads), blocks_for(n_cp, kRingCPB));
+    if (grid.y > 65535)
+        return pvl_fail(PVL_ERR_ARG, "pvl_induction_matrix: too many points (%u)", n_cp);
+    ring_matrix_kernel<double, double, 1><<<grid, kRingThreads, 0, st>>>(n_surfaces, off, sl, n_lines, seg, n_cp, cps,
+                                                                         nullptr, tol * tol, out, 0);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_induction_normal(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
+                                    const double* positions, uint32_t n_surfaces, const uint32_t* off,
+                                    const uint32_t* sl, uint32_t n_cp, const double* cps, const double* normals,
+                                    double tol, void* out, uint32_t ld, void* ws, size_t ws_bytes, void* stream)
+{
+    if (n_surfaces == 0 || n_cp == 0)
+        return PVL_OK;
+    PVL_REQUIRE(lines); PVL_REQUIRE(positions); PVL_REQUIRE(off); PVL_REQUIRE(sl); PVL_REQUIRE(cps);
+    PVL_REQUIRE(normals); PVL_REQUIRE(out); PVL_REQUIRE(ws);
+    if (precision != PVL_F64 && precision != PVL_F32)
+        return pvl_fail(PVL_ERR_ARG, "pvl_induction_normal: unknown precision %d", precision);
+    if (ld < n_surfaces)
+        return pvl_fail(PVL_ERR_ARG, "pvl_induction_normal: ld %u < n_surfaces %u", ld, n_surfaces);
+    if (ws_bytes < pvl_segments_workspace(n_lines, precision))
+        return pvl_fail(PVL_ERR_ALLOC, "pvl_induction_normal: workspace too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    dim3 grid(blocks_for(n_surfaces, kRingThreads), blocks_for(n_cp, kRingCPB));
+    if (grid.y > 65535)
+        return pvl_fail(PVL_ERR_ARG, "pvl_induction_normal: too many points (%u)", n_cp);
+    if (precision == PVL_F64) {
+        auto* seg = static_cast<Segment<double>*>(ws);
+        if (int r = prep_segments<double>(n_points, n_lines, lines, positions, nullptr, tol, seg, st))
+            return r;
+        ring_matrix_kernel<double, double, 0><<<grid, kRingThreads, 0, st>>>(
+            n_surfaces, off, sl, n_lines, seg, n_cp, cps, normals, tol * tol, static_cast<double*>(out), ld);
+    } else {
+        auto* seg = static_cast<Segment<float>*>(ws);
+        if (int r = prep_segments<float>(n_points, n_lines, lines, positions, nullptr, tol, seg, st))
+            return r;
+        ring_matrix_kernel<float, float, 0><<<grid, kRingThreads, 0, st>>>(
+            n_surfaces, off, sl, n_lines, seg, n_cp, cps, normals, float(tol * tol), static_cast<float*>(out), ld);
+    }
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" size_t pvl_line_velocity_workspace(uint32_t n_lines, uint32_t n_pts, int precision)
+{
+    const size_t el = precision == PVL_F32 ? sizeof(float) : sizeof(double);
+    return pvl_segments_workspace(n_lines, precision) + align256((size_t)sum_splits(n_lines, n_pts) * n_pts * 3 * el);
+}
+
+namespace {
+
+// Shared driver of the N-body sweep: segment table, split sweep, deterministic reduction.
+int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines, const double* positions,
+                 const double* line_gamma, uint32_t n_pts, const double* pts, uint32_t group, uint32_t stride,
+                 const double* normals, double tol, double alpha, double beta, double ux, double uy, double uz,
+                 double* out, void* ws, size_t ws_bytes, cudaStream_t st, const char* who)
+{
+    if (precision != PVL_F64 && precision != PVL_F32)
+        return pvl_fail(PVL_ERR_ARG, "%s: unknown precision %d", who, precision);
+    if (n_lines == 0) {
+        reduce_partials_kernel<double><<<blocks_for(n_pts, 256), 256, 0, st>>>(n_pts, 0, nullptr, normals, alpha,
+                                                                               beta, ux, uy, uz, out);
+        PVL_LAUNCH_CHECK();
+        return PVL_OK;
+    }
+    if (!lines || !positions || !ws)
+        return pvl_fail(PVL_ERR_ARG, "%s: null pointer argument", who);
+    if (ws_bytes < pvl_line_velocity_workspace(n_lines, n_pts, precision))
+        return pvl_fail(PVL_ERR_ALLOC, "%s: workspace %zu < %zu", who, ws_bytes,
+                        pvl_line_velocity_workspace(n_lines, n_pts, precision));
+    const uint32_t n_split = sum_splits(n_lines, n_pts);
+    const uint32_t per = (n_lines + n_split - 1) / n_split;
+    const uint32_t n_split_used = (n_lines + per - 1) / per;
+    dim3 grid(blocks_for(n_pts, kSumThreads * kSumPPT), n_split_used);
+    char* base = static_cast<char*>(ws);
+    if (precision == PVL_F64) {
+        auto* seg = reinterpret_cast<Segment<double>*>(base);
+        auto* part = reinterpret_cast<double*>(base + pvl_segments_workspace(n_lines, PVL_F64));
+        if (int r = prep_segments<double>(n_points, n_lines, lines, positions, line_gamma, tol, seg, st))
+            return r;
+        line_sum_kernel<double><<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride,
+                                                              tol * tol, part);
+        PVL_LAUNCH_CHECK();
+        reduce_partials_kernel<double><<<blocks_for(n_pts, 256), 256, 0, st>>>(n_pts, n_split_used, part, normals,
+                                                                               alpha, beta, ux, uy, uz, out);
+    } else {
+        auto* seg = reinterpret_cast<Segment<float>*>(base);
+        auto* part = reinterpret_cast<float*>(base + pvl_segments_workspace(n_lines, PVL_F32));
+        if (int r = prep_segments<float>(n_points, n_lines, lines, positions, line_gamma, tol, seg, st))
+            return r;
+        line_sum_kernel<float><<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride,
+                                                             float(tol * tol), part);
+        PVL_LAUNCH_CHECK();
+        reduce_partials_kernel<float><<<blocks_for(n_pts, 256), 256, 0, st>>>(n_pts, n_split_used, part, normals,
+                                                                              alpha, beta, ux, uy, uz, out);
+    }
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+}  // namespace
+
+extern "C" int pvl_line_velocity(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
+                                 const double* positions, const double* line_gamma, uint32_t n_pts, const double* pts,
+                                 const double* normals, double tol, double alpha, double beta, double* out, void* ws,
+                                 size_t ws_bytes, void* stream)
+{
+    if (n_pts == 0)
+        return PVL_OK;
+    PVL_REQUIRE(pts); PVL_REQUIRE(out);
+    return run_line_sum(precision, n_points, n_lines, lines, positions, line_gamma, n_pts, pts, n_pts, n_pts, normals,
+                        tol, alpha, beta, 0.0, 0.0, 0.0, out, ws, ws_bytes, (cudaStream_t)stream,
+                        "pvl_line_velocity");
+}
+
+extern "C" size_t pvl_wake_node_velocity_workspace(uint32_t n_lines, uint32_t n_shed, uint32_t complete_rows,
+                                                   int precision)
+{
+    return pvl_line_velocity_workspace(n_lines, 2 * n_shed * complete_rows, precision);
+}
+
+extern "C" int pvl_wake_node_velocity(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
+                                      const double* positions, const double* line_gamma, uint32_t n_shed,
+                                      uint32_t line_rows, uint32_t complete_rows, const double* wake_pos, double ux,
+                                      double uy, double uz, double tol, double* node_vel, void* ws, size_t ws_bytes,
+                                      void* stream)
+{
+    if (n_shed == 0 || complete_rows == 0)
+        return PVL_OK;
+    if (complete_rows > line_rows)
+        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity: complete_rows %u > line_rows %u", complete_rows,
+                        line_rows);
+    PVL_REQUIRE(wake_pos); PVL_REQUIRE(node_vel);
+    const uint64_t n_pts = 2ull * n_shed * complete_rows;
+    if (n_pts > 0xFFFFFFFFull)
+        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity: too many nodes");
+    return run_line_sum(precision, n_points, n_lines, lines, positions, line_gamma, (uint32_t)n_pts, wake_pos,
+                        complete_rows, line_rows + 1, nullptr, tol, 1.0, 0.0, ux, uy, uz, node_vel, ws, ws_bytes,
+                        (cudaStream_t)stream, "pvl_wake_node_velocity");
+}
+
+extern "C" int pvl_line_circulation(uint32_t n_lines, const uint32_t* map_offsets, const uint32_t* map_entries,
+                                    const double* ring_gamma, uint32_t ring_period, double* line_gamma_out,
+                                    void* stream)
+{
+    if (n_lines == 0)
+        return PVL_OK;
+    PVL_REQUIRE(map_offsets); PVL_REQUIRE(map_entries); PVL_REQUIRE(ring_gamma); PVL_REQUIRE(line_gamma_out);
+    line_circulation_kernel<<<blocks_for(n_lines, 256), 256, 0, (cudaStream_t)stream>>>(
+        n_lines, map_offsets, map_entries, ring_gamma, ring_period, line_gamma_out);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_line_forces(uint32_t n_lines, const uint32_t* primal_lines, const uint32_t* dual_lines,
+                               const double* circ, const double* positions, const double* velocity, double* out,
+                               void* stream)
+{
+    if (n_lines == 0)
+        return PVL_OK;
+    PVL_REQUIRE(primal_lines); PVL_REQUIRE(dual_lines); PVL_REQUIRE(circ); PVL_REQUIRE(positions);
+    PVL_REQUIRE(velocity); PVL_REQUIRE(out);
+    line_forces_kernel<<<blocks_for(n_lines, 256), 256, 0, (cudaStream_t)stream>>>(n_lines, primal_lines, dual_lines,
+                                                                                   circ, positions, velocity, out);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}

@@ -1,0 +1,674 @@
+// Dense FP64 LU with partial pivoting (GEPP) and the matching solve, for the row-major
+// system matrix the induction kernels write.  Replaces the reference's
+// scipy.linalg.lu_factor / lu_solve (python/pyvl/solver.py:223-227).
+//
+// Right-looking blocked factorisation, panel width NB = 64.  Per panel (k0, nb):
+//   1. panel_spec_kernel -- speculative factorisation of the whole panel with the diagonal as
+//      pivot.  Every CTA factors the same nb x nb top block (one row per thread, rows held in
+//      registers) together with its own 64 rows below it, so no CTA waits for another.  Per
+//      column it records the largest |entry| below the diagonal at the moment the column is
+//      eliminated.
+//   2. panel_pivot_kernel -- one CTA: if every diagonal entry is non-zero and no entry below
+//      it is larger, partial pivoting would have chosen exactly these pivots (LAPACK's idamax
+//      returns the first maximal entry and the diagonal comes first), so the speculative
+//      factors ARE the GEPP factors: commit them with identity pivots.  Otherwise restore the
+//      panel from the backup and factor it with explicit partial pivoting in getf2 order.
+//   3. trsm_kernel -- applies the panel's interchanges to the other columns and forms
+//      U12 = L11^-1 A12 (one column per thread, held in registers).
+//   4. gemm_update_kernel -- A22 -= L21 U12, FP64, 128 x 128 tiles, 8 x 8 outputs per thread,
+//      128-bit conflict-free shared loads.
+// Diagonally dominant systems (the vortex-ring matrices are close to -2 pi I) take the
+// speculative path on every panel; a bordered closed-body system falls back on the panel
+// holding the zero-diagonal border.
+//
+// The solve runs two wavefront kernels (forward with unit-lower L, backward with U) over
+// row blocks, one CTA per block, co-resident through a cooperative launch; each CTA stages
+// its diagonal block in shared memory before waiting, and every wait on an earlier block is
+// bounded and reports a time-out through a device error word.
+#include <algorithm>
+#include <cstdint>
+
+#include "pvl_common.cuh"
+
+namespace {
+
+constexpr int NB = 64;               // panel width
+constexpr int kSlabRows = 64;        // rows below the top block per CTA in panel_spec_kernel
+constexpr int kGemmTile = 128;       // trailing update tile (M and N)
+constexpr int kGemmThreads = 256;    // 16 x 16 threads, 8 x 8 outputs each
+constexpr int kRB = 64;              // rows per block in the wavefront solves
+constexpr int kSolveThreads = 256;
+constexpr long long kSpinLimit = 20000000;  // bounded waits: ~2 s at 100 ns per poll
+
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+struct LuWs {
+    double* backup;         // (n, NB) copy of the current panel before speculation
+    double* top_out;        // (NB, NB) speculative top block
+    unsigned long long* colmax;  // (n_slab_ctas + 1, NB) |x| maxima as ordered bit patterns
+    int32_t* ok;            // per panel: speculative factors accepted
+    int32_t* flags;         // wavefront flags (solve)
+    double* tmp;            // (n) solve vector
+};
+
+uint32_t slab_ctas(uint32_t n) { return (n + kSlabRows - 1) / kSlabRows + 1; }
+
+size_t lu_ws_bytes(uint32_t n)
+{
+    return align256((size_t)n * NB * sizeof(double)) + align256((size_t)NB * NB * sizeof(double)) +
+           align256((size_t)slab_ctas(n) * NB * sizeof(unsigned long long)) +
+           align256(((size_t)n / NB + 2) * sizeof(int32_t)) + align256(((size_t)n / kRB + 2) * sizeof(int32_t)) +
+           align256((size_t)n * sizeof(double));
+}
+
+LuWs carve(void* ws, uint32_t n)
+{
+    char* p = static_cast<char*>(ws);
+    LuWs w;
+    w.backup = reinterpret_cast<double*>(p);
+    p += align256((size_t)n * NB * sizeof(double));
+    w.top_out = reinterpret_cast<double*>(p);
+    p += align256((size_t)NB * NB * sizeof(double));
+    w.colmax = reinterpret_cast<unsigned long long*>(p);
+    p += align256((size_t)slab_ctas(n) * NB * sizeof(unsigned long long));
+    w.ok = reinterpret_cast<int32_t*>(p);
+    p += align256(((size_t)n / NB + 2) * sizeof(int32_t));
+    w.flags = reinterpret_cast<int32_t*>(p);
+    p += align256(((size_t)n / kRB + 2) * sizeof(int32_t));
+    w.tmp = reinterpret_cast<double*>(p);
+    return w;
+}
+
+// |x| as an integer whose order matches the order of non-negative doubles.
+__device__ __forceinline__ unsigned long long abs_bits(double x)
+{
+    return (unsigned long long)__double_as_longlong(fabs(x));
+}
+
+__global__ void init_perm_kernel(uint32_t n, int32_t* __restrict__ perm)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        perm[i] = (int32_t)i;
+}
+
+// ---------------------------------------------------------------- 1+2. speculative panel
+// grid.x = max(1, ceil(below / kSlabRows)); 128 threads: threads 0..63 hold the 64 rows of
+// the top block (every CTA factors the same top block, so no CTA waits for another), threads
+// 64..127 hold this CTA's rows below it.  Each thread keeps its row in registers (columns
+// beyond nb are zero; missing top rows are unit rows) and eliminates column j with the row
+// that thread j publishes in shared memory -- the recurrence of getf2 without interchanges.
+// Per column, the largest |entry| on or below the diagonal row before elimination is reduced
+// per warp into shared memory.  Slab rows are backed up and overwritten in place; the
+// factored top block goes to `top_out` (committed by panel_pivot_kernel) so that no CTA can
+// read a half-written top block.
+__global__ void __launch_bounds__(2 * kSlabRows) panel_spec_kernel(uint32_t n, uint32_t k0, uint32_t nb,
+                                                                   double* __restrict__ A, uint32_t lda,
+                                                                   double* __restrict__ backup,
+                                                                   double* __restrict__ top_out,
+                                                                   unsigned long long* __restrict__ colmax)
+{
+    __shared__ double U[NB][NB + 1];
+    __shared__ unsigned long long cm[4][NB];
+    const uint32_t tid = threadIdx.x;
+    const bool is_top = tid < NB;
+    const uint32_t lane = tid & 31, warp = tid >> 5;
+    const uint32_t r_begin = k0 + nb + blockIdx.x * kSlabRows;
+    // global row of this thread (top: k0 + tid, slab: r_begin + tid - 64)
+    const uint32_t grow = is_top ? k0 + tid : r_begin + (tid - NB);
+    const bool valid = is_top ? tid < nb : grow < n;
+    double row[NB];
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+        double v = 0.0;
+        if (valid && (uint32_t)c < nb)
+            v = A[(size_t)grow * lda + k0 + c];
+        else if (is_top && !valid && (uint32_t)c == tid)
+            v = 1.0;  // unit row standing in for a missing top row
+        row[c] = v;
+    }
+    if (!is_top && valid)
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+            if ((uint32_t)c < nb)
+                backup[(size_t)(grow - k0) * NB + c] = row[c];
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+        if (tid == (uint32_t)j) {
+#pragma unroll
+            for (int c = j; c < NB; ++c)
+                U[j][c] = row[c];
+        }
+        __syncthreads();
+        const bool act = is_top ? tid > (uint32_t)j : valid;
+        const double v = row[j];
+        unsigned long long m = act ? abs_bits(v) : 0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0)
+            cm[warp][j] = m;
+        if (act) {
+            const double x = v / U[j][j];
+            row[j] = x;
+#pragma unroll
+            for (int c = j + 1; c < NB; ++c)
+                row[c] -= x * U[j][c];
+        }
+    }
+    __syncthreads();
+    if (is_top) {
+        if (blockIdx.x == 0 && valid)
+#pragma unroll
+            for (int c = 0; c < NB; ++c)
+                if ((uint32_t)c < nb)
+                    top_out[(size_t)tid * NB + c] = row[c];
+    } else if (valid) {
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+            if ((uint32_t)c < nb)
+                A[(size_t)grow * lda + k0 + c] = row[c];
+    }
+    if (tid < NB)
+        colmax[(size_t)blockIdx.x * NB + tid] =
+            max(max(cm[0][tid], cm[1][tid]), max(cm[2][tid], cm[3][tid]));
+}
+
+// ---------------------------------------------------------------- 3. accept or pivot
+__global__ void __launch_bounds__(1024) panel_pivot_kernel(uint32_t n, uint32_t k0, uint32_t nb, double* __restrict__ A,
+                                                           uint32_t lda, const double* __restrict__ backup,
+                                                           const double* __restrict__ top_out,
+                                                           const unsigned long long* __restrict__ colmax,
+                                                           uint32_t n_cm, int32_t* __restrict__ ok,
+                                                           uint32_t panel, int32_t* __restrict__ ipiv,
+                                                           int32_t* __restrict__ perm, int32_t* __restrict__ info)
+{
+    __shared__ int bad;
+    __shared__ double s_val[32];
+    __shared__ uint32_t s_idx[32];
+    __shared__ uint32_t s_piv;
+    __shared__ double s_prow[NB];
+    if (threadIdx.x == 0)
+        bad = 0;
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
+        unsigned long long m = 0;
+        for (uint32_t c = 0; c < n_cm; ++c)
+            m = max(m, colmax[(size_t)c * NB + j]);
+        const double d = top_out[(size_t)j * NB + j];
+        // m is the largest |entry| strictly below the diagonal; speculation holds iff it is
+        // not larger than |d| (a tie keeps the diagonal, as idamax does).  Zero or NaN
+        // pivots reject.
+        if (!(fabs(d) > 0.0) || abs_bits(d) < m)
+            atomicOr(&bad, 1);
+    }
+    __syncthreads();
+    if (!bad) {
+        if (threadIdx.x == 0)
+            ok[panel] = 1;
+        for (uint32_t t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+            const uint32_t r = t / nb, c = t % nb;
+            A[(size_t)(k0 + r) * lda + k0 + c] = top_out[(size_t)r * NB + c];
+        }
+        for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x)
+            ipiv[k0 + j] = (int32_t)(k0 + j);
+        return;
+    }
+    if (threadIdx.x == 0)
+        ok[panel] = 0;
+    // the top block of A was never written; restore the rows below it, then LAPACK getf2:
+    // first row of maximal |a|, swap, scale, update
+    for (size_t t = threadIdx.x; t < (size_t)(n - k0 - nb) * nb; t += blockDim.x) {
+        const uint32_t r = (uint32_t)(t / nb) + nb, c = (uint32_t)(t % nb);
+        A[(size_t)(k0 + r) * lda + k0 + c] = backup[(size_t)r * NB + c];
+    }
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t j = 0; j < nb; ++j) {
+        const uint32_t col = k0 + j;
+        double best = -1.0;
+        uint32_t bidx = 0xFFFFFFFFu;
+        for (uint32_t r = col + threadIdx.x; r < n; r += blockDim.x) {
+            const double v = fabs(A[(size_t)r * lda + col]);
+            if (v > best) {
+                best = v;
+                bidx = r;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+            const uint32_t oi = __shfl_xor_sync(0xffffffffu, bidx, o);
+            if (ov > best || (ov == best && oi < bidx)) {
+                best = ov;
+                bidx = oi;
+            }
+        }
+        if (lane == 0) {
+            s_val[warp] = best;
+            s_idx[warp] = bidx;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double b = -1.0;
+            uint32_t bi = col;
+            for (uint32_t w = 0; w < blockDim.x / 32; ++w)
+                if (s_val[w] > b || (s_val[w] == b && s_idx[w] < bi)) {
+                    b = s_val[w];
+                    bi = s_idx[w];
+                }
+            s_piv = bi;
+            ipiv[col] = (int32_t)bi;
+            if (bi != col) {
+                const int32_t t = perm[col];
+                perm[col] = perm[bi];
+                perm[bi] = t;
+            }
+        }
+        __syncthreads();
+        const uint32_t p = s_piv;
+        if (p != col)
+            for (uint32_t c = threadIdx.x; c < nb; c += blockDim.x) {
+                const double a = A[(size_t)col * lda + k0 + c];
+                A[(size_t)col * lda + k0 + c] = A[(size_t)p * lda + k0 + c];
+                A[(size_t)p * lda + k0 + c] = a;
+            }
+        __syncthreads();
+        for (uint32_t c = threadIdx.x; c < nb; c += blockDim.x)
+            s_prow[c] = A[(size_t)col * lda + k0 + c];
+        __syncthreads();
+        const double piv = s_prow[j];
+        if (piv == 0.0) {
+            if (threadIdx.x == 0)
+                atomicCAS(info, 0, (int32_t)(col + 1));
+            __syncthreads();
+            continue;
+        }
+        for (uint32_t r = col + 1 + threadIdx.x; r < n; r += blockDim.x) {
+            double* row = A + (size_t)r * lda + k0;
+            const double l = row[j] / piv;
+            row[j] = l;
+            for (uint32_t c = j + 1; c < nb; ++c)
+                row[c] -= l * s_prow[c];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- 3. swaps + U12
+// One thread per column outside the panel: apply the panel's interchanges (if any); columns
+// right of the panel then solve L11 x = a (unit lower).  The 64 x 128 column block is staged
+// through shared memory with coalesced row accesses; each thread keeps its column in
+// registers during the substitution.
+constexpr int kTrsmCols = 128;
+
+__global__ void __launch_bounds__(kTrsmCols, 1) trsm_kernel(uint32_t n, uint32_t k0, uint32_t nb,
+                                                            double* __restrict__ A, uint32_t lda,
+                                                            const int32_t* __restrict__ ok, uint32_t panel,
+                                                            const int32_t* __restrict__ ipiv)
+{
+    extern __shared__ double tsm[];
+    double(*L)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(tsm);                   // [NB][NB + 1]
+    double(*X)[kTrsmCols + 1] = reinterpret_cast<double(*)[kTrsmCols + 1]>(tsm + NB * (NB + 1));  // [NB][129]
+    const bool swapped = !ok[panel];
+    const uint32_t t = blockIdx.x * kTrsmCols + threadIdx.x;
+    const uint32_t n_out = n - nb;
+    const uint32_t col = t < k0 ? t : t + nb;
+    if (t < n_out && swapped)
+        for (uint32_t j = 0; j < nb; ++j) {
+            const uint32_t r1 = k0 + j, r2 = (uint32_t)ipiv[k0 + j];
+            if (r1 != r2) {
+                const double a = A[(size_t)r1 * lda + col];
+                A[(size_t)r1 * lda + col] = A[(size_t)r2 * lda + col];
+                A[(size_t)r2 * lda + col] = a;
+            }
+        }
+    // the columns right of the panel start at k0 + nb; this CTA's first such column:
+    const uint32_t c_first = blockIdx.x * kTrsmCols;  // in t-space
+    if (c_first + kTrsmCols <= k0 || c_first >= n_out)
+        return;  // CTA-uniform: only left-of-panel columns (already swapped) or none
+    __syncthreads();  // swaps of this CTA's columns are visible before staging
+    for (uint32_t e = threadIdx.x; e < NB * NB; e += kTrsmCols) {
+        const uint32_t r = e / NB, c = e % NB;
+        L[r][c] = (r < nb && c < nb) ? A[(size_t)(k0 + r) * lda + k0 + c] : 0.0;
+    }
+    for (uint32_t e = threadIdx.x; e < NB * kTrsmCols; e += kTrsmCols) {
+        const uint32_t r = e / kTrsmCols, c = e % kTrsmCols;
+        const uint32_t tt = c_first + c;
+        const uint32_t cc = tt < k0 ? tt : tt + nb;
+        X[r][c] = (r < nb && tt < n_out && cc >= k0 + nb) ? A[(size_t)(k0 + r) * lda + cc] : 0.0;
+    }
+    __syncthreads();
+    double x[NB];
+#pragma unroll
+    for (int r = 0; r < NB; ++r)
+        x[r] = X[r][threadIdx.x];
+#pragma unroll
+    for (int q = 0; q < NB - 1; ++q) {
+        const double xq = x[q];
+#pragma unroll
+        for (int r = q + 1; r < NB; ++r)
+            x[r] -= L[r][q] * xq;
+    }
+#pragma unroll
+    for (int r = 0; r < NB; ++r)
+        X[r][threadIdx.x] = x[r];
+    __syncthreads();
+    for (uint32_t e = threadIdx.x; e < NB * kTrsmCols; e += kTrsmCols) {
+        const uint32_t r = e / kTrsmCols, c = e % kTrsmCols;
+        const uint32_t tt = c_first + c;
+        const uint32_t cc = tt < k0 ? tt : tt + nb;
+        if (r >= 1 && r < nb && tt < n_out && cc >= k0 + nb)
+            A[(size_t)(k0 + r) * lda + cc] = X[r][c];
+    }
+}
+
+// ---------------------------------------------------------------- 4. trailing update
+// A22 -= L21 U12 (FP64, K = nb <= 64): 128 x 128 tile per CTA, 16 x 16 threads.  Thread
+// (ty, tx) owns rows {2ty, 2ty+1} + 32 p and columns {2tx, 2tx+1} + 32 q (p, q = 0..3).
+// L21 is staged row-major (row stride 66 doubles: conflict-free stores, 16-byte aligned rows)
+// and read two k at a time per row (each load is a broadcast: two rows per warp); U12 is
+// staged row-major and read as 16 consecutive pairs per half-warp (conflict-free).  Per two
+// k steps: 16 128-bit shared loads for 128 FMAs.
+constexpr int kAStride = NB + 2;
+
+__global__ void __launch_bounds__(kGemmThreads) gemm_update_kernel(uint32_t n, uint32_t k0, uint32_t nb,
+                                                                   double* __restrict__ A, uint32_t lda)
+{
+    extern __shared__ double2 gsm2[];
+    double* As = reinterpret_cast<double*>(gsm2);   // [kGemmTile][kAStride]: As[i][k] = L21[i][k]
+    double* Bs = As + kGemmTile * kAStride;         // [NB][kGemmTile]:       Bs[k][j] = U12[k][j]
+    const uint32_t base = k0 + nb;
+    const uint32_t i0 = base + blockIdx.y * kGemmTile, j0 = base + blockIdx.x * kGemmTile;
+    const uint32_t tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    for (uint32_t t = threadIdx.x; t < kGemmTile * NB; t += kGemmThreads) {
+        const uint32_t i = t / NB, k = t % NB;
+        As[i * kAStride + k] = (i0 + i < n && k < nb) ? A[(size_t)(i0 + i) * lda + k0 + k] : 0.0;
+    }
+    for (uint32_t t = threadIdx.x; t < NB * kGemmTile; t += kGemmThreads) {
+        const uint32_t k = t / kGemmTile, j = t % kGemmTile;
+        Bs[k * kGemmTile + j] = (j0 + j < n && k < nb) ? A[(size_t)(k0 + k) * lda + j0 + j] : 0.0;
+    }
+    __syncthreads();
+    double acc[8][8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+            acc[r][c] = 0.0;
+    const double2* A2 = reinterpret_cast<const double2*>(As);
+    const double2* B2 = reinterpret_cast<const double2*>(Bs);
+#pragma unroll 1
+    for (uint32_t k = 0; k < NB; k += 2) {
+        double2 a[8];
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                a[2 * p + h] = A2[((2 * ty + 32 * p + h) * kAStride + k) / 2];
+#pragma unroll
+        for (int kk = 0; kk < 2; ++kk) {
+            double b[8];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const double2 vb = B2[((k + kk) * kGemmTile + 2 * tx + 32 * q) / 2];
+                b[2 * q] = vb.x;
+                b[2 * q + 1] = vb.y;
+            }
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const double ar = kk ? a[r].y : a[r].x;
+#pragma unroll
+                for (int c = 0; c < 8; ++c)
+                    acc[r][c] = fma(ar, b[c], acc[r][c]);
+            }
+        }
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const uint32_t i = i0 + 2 * ty + 32 * p + h;
+            if (i >= n)
+                continue;
+            double* crow = A + (size_t)i * lda;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t j = j0 + 2 * tx + 32 * q;
+                if (j + 1 < n && ((lda & 1u) == 0)) {
+                    double2* c2 = reinterpret_cast<double2*>(crow + j);
+                    double2 v = *c2;
+                    v.x -= acc[2 * p + h][2 * q];
+                    v.y -= acc[2 * p + h][2 * q + 1];
+                    *c2 = v;
+                } else {
+                    if (j < n)
+                        crow[j] -= acc[2 * p + h][2 * q];
+                    if (j + 1 < n)
+                        crow[j + 1] -= acc[2 * p + h][2 * q + 1];
+                }
+            }
+        }
+}
+
+// ---------------------------------------------------------------- solve
+__global__ void gather_kernel(uint32_t n, const int32_t* __restrict__ perm, const double* __restrict__ b,
+                              double* __restrict__ out)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        out[i] = b[perm[i]];
+}
+
+__device__ __forceinline__ int32_t ld_acquire(const int32_t* p)
+{
+    int32_t v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release(int32_t* p, int32_t v)
+{
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Wavefront triangular solve over row blocks of kRB rows, one CTA per block.  LOWER:
+// unit-lower forward substitution, block b waits for blocks 0..b-1.  UPPER: backward
+// substitution with U's diagonal, block b waits for blocks nblk-1..b+1.  x holds the
+// right-hand side on entry and the solution on exit.  Each wait is bounded: on time-out
+// the CTA sets *err, publishes its flag so that no later block waits on it, and returns.
+template <bool LOWER>
+__global__ void __launch_bounds__(kSolveThreads) trsv_wavefront_kernel(uint32_t n, const double* __restrict__ M,
+                                                                       uint32_t lda, double* __restrict__ x,
+                                                                       int32_t* __restrict__ flags,
+                                                                       int32_t* __restrict__ err)
+{
+    __shared__ double s_acc[kRB];
+    __shared__ double s_x[kRB];
+    __shared__ double s_d[kRB][kRB + 1];
+    __shared__ int s_abort;
+    const uint32_t nblk = (n + kRB - 1) / kRB;
+    const uint32_t b = LOWER ? blockIdx.x : nblk - 1 - blockIdx.x;
+    const uint32_t r0 = b * kRB;
+    const uint32_t rows = min((uint32_t)kRB, n - r0);
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0)
+        s_abort = 0;
+    if (threadIdx.x < kRB)
+        s_acc[threadIdx.x] = 0.0;
+    // the diagonal block does not depend on any other block: stage it before waiting
+    for (uint32_t e = threadIdx.x; e < kRB * kRB; e += blockDim.x) {
+        const uint32_t r = e / kRB, c = e % kRB;
+        s_d[r][c] = (r < rows && c < rows) ? M[(size_t)(r0 + r) * lda + r0 + c] : 0.0;
+    }
+    __syncthreads();
+    const uint32_t n_dep = LOWER ? b : nblk - 1 - b;
+    for (uint32_t step = 0; step < n_dep; ++step) {
+        const uint32_t c = LOWER ? step : nblk - 1 - step;
+        if (threadIdx.x == 0) {
+            long long spins = 0;
+            while (ld_acquire(flags + c) == 0) {
+                if (++spins > kSpinLimit) {
+                    atomicExch(err, 1);
+                    s_abort = 1;
+                    break;
+                }
+                __nanosleep(100);
+            }
+        }
+        __syncthreads();
+        if (s_abort) {
+            if (threadIdx.x == 0)
+                st_release(flags + b, 1);
+            return;
+        }
+        const uint32_t c0 = c * kRB;
+        const uint32_t ccols = min((uint32_t)kRB, n - c0);
+        for (uint32_t r = warp; r < rows; r += kSolveThreads / 32) {
+            const double* mrow = M + (size_t)(r0 + r) * lda + c0;
+            double s = 0.0;
+            for (uint32_t k = lane; k < ccols; k += 32)
+                s += mrow[k] * __ldcg(x + c0 + k);
+            for (int o = 16; o > 0; o >>= 1)
+                s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0)
+                s_acc[r] += s;
+        }
+        __syncthreads();
+    }
+    if (warp == 0) {
+        for (uint32_t k = lane; k < rows; k += 32)
+            s_x[k] = __ldcg(x + r0 + k) - s_acc[k];
+        __syncwarp();
+        if (LOWER) {
+            for (uint32_t r = 1; r < rows; ++r) {
+                double s = 0.0;
+                for (uint32_t k = lane; k < r; k += 32)
+                    s += s_d[r][k] * s_x[k];
+                for (int o = 16; o > 0; o >>= 1)
+                    s += __shfl_xor_sync(0xffffffffu, s, o);
+                if (lane == 0)
+                    s_x[r] -= s;
+                __syncwarp();
+            }
+        } else {
+            for (int r = (int)rows - 1; r >= 0; --r) {
+                double s = 0.0;
+                for (uint32_t k = r + 1 + lane; k < rows; k += 32)
+                    s += s_d[r][k] * s_x[k];
+                for (int o = 16; o > 0; o >>= 1)
+                    s += __shfl_xor_sync(0xffffffffu, s, o);
+                if (lane == 0)
+                    s_x[r] = (s_x[r] - s) / s_d[r][r];
+                __syncwarp();
+            }
+        }
+        for (uint32_t k = lane; k < rows; k += 32)
+            x[r0 + k] = s_x[k];
+        __threadfence();
+        __syncwarp();
+        if (lane == 0)
+            st_release(flags + b, 1);
+    }
+}
+
+int coresident_blocks(const void* fn, int threads)
+{
+    int dev = 0, sms = 0, per = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+        return 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, 0) != cudaSuccess)
+        return 0;
+    return sms * per;
+}
+
+}  // namespace
+
+extern "C" size_t pvl_lu_workspace(uint32_t n) { return lu_ws_bytes(n); }
+
+extern "C" int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv, int32_t* info, void* ws,
+                             size_t ws_bytes, void* stream)
+{
+    if (n == 0)
+        return PVL_OK;
+    if (!A || !ipiv || !info || !ws)
+        return pvl_fail(PVL_ERR_ARG, "pvl_lu_factor: null pointer argument");
+    if (lda < n)
+        return pvl_fail(PVL_ERR_ARG, "pvl_lu_factor: lda %u < n %u", lda, n);
+    if (ws_bytes < lu_ws_bytes(n))
+        return pvl_fail(PVL_ERR_ALLOC, "pvl_lu_factor: workspace %zu < %zu", ws_bytes, lu_ws_bytes(n));
+    cudaStream_t st = (cudaStream_t)stream;
+    LuWs w = carve(ws, n);
+    const size_t gemm_smem = (size_t)(kGemmTile * kAStride + NB * kGemmTile) * sizeof(double);
+    const size_t trsm_smem = (size_t)(NB * (NB + 1) + NB * (kTrsmCols + 1)) * sizeof(double);
+    static bool attr_done = false;
+    if (!attr_done) {
+        PVL_CUDA_CHECK(cudaFuncSetAttribute(gemm_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)gemm_smem));
+        PVL_CUDA_CHECK(cudaFuncSetAttribute(trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)trsm_smem));
+        attr_done = true;
+    }
+    int32_t* perm = ipiv + n;
+    PVL_CUDA_CHECK(cudaMemsetAsync(info, 0, sizeof(int32_t), st));
+    init_perm_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, perm);
+    PVL_LAUNCH_CHECK();
+    const uint32_t n_panels = (n + NB - 1) / NB;
+    for (uint32_t p = 0; p < n_panels; ++p) {
+        const uint32_t k0 = p * NB;
+        const uint32_t nb = std::min<uint32_t>(NB, n - k0);
+        const uint32_t below = n - k0 - nb;
+        const uint32_t ctas = std::max<uint32_t>(1, (below + kSlabRows - 1) / kSlabRows);
+        panel_spec_kernel<<<ctas, 2 * kSlabRows, 0, st>>>(n, k0, nb, A, lda, w.backup, w.top_out, w.colmax);
+        PVL_LAUNCH_CHECK();
+        panel_pivot_kernel<<<1, 1024, 0, st>>>(n, k0, nb, A, lda, w.backup, w.top_out, w.colmax, ctas, w.ok, p, ipiv,
+                                               perm, info);
+        PVL_LAUNCH_CHECK();
+        if (n > nb) {
+            trsm_kernel<<<blocks_for(n - nb, kTrsmCols), kTrsmCols, trsm_smem, st>>>(n, k0, nb, A, lda, w.ok, p, ipiv);
+            PVL_LAUNCH_CHECK();
+        }
+        if (below > 0) {
+            dim3 g(blocks_for(below, kGemmTile), blocks_for(below, kGemmTile));
+            gemm_update_kernel<<<g, kGemmThreads, gemm_smem, st>>>(n, k0, nb, A, lda);
+            PVL_LAUNCH_CHECK();
+        }
+    }
+    return PVL_OK;
+}
+
+extern "C" size_t pvl_lu_solve_workspace(uint32_t n) { return lu_ws_bytes(n); }
+
+extern "C" int pvl_lu_solve(uint32_t n, const double* LU, uint32_t lda, const int32_t* ipiv, double* b,
+                            int32_t* err, void* ws, size_t ws_bytes, void* stream)
+{
+    if (n == 0)
+        return PVL_OK;
+    if (!LU || !ipiv || !b || !ws || !err)
+        return pvl_fail(PVL_ERR_ARG, "pvl_lu_solve: null pointer argument");
+    if (ws_bytes < lu_ws_bytes(n))
+        return pvl_fail(PVL_ERR_ALLOC, "pvl_lu_solve: workspace too small");
+    const uint32_t nblk = (n + kRB - 1) / kRB;
+    if ((int)nblk > coresident_blocks((const void*)trsv_wavefront_kernel<true>, kSolveThreads) ||
+        (int)nblk > coresident_blocks((const void*)trsv_wavefront_kernel<false>, kSolveThreads))
+        return pvl_fail(PVL_ERR_ARG, "pvl_lu_solve: n = %u needs %u co-resident blocks", n, nblk);
+    cudaStream_t st = (cudaStream_t)stream;
+    LuWs w = carve(ws, n);
+    const int32_t* perm = ipiv + n;
+    PVL_CUDA_CHECK(cudaMemsetAsync(err, 0, sizeof(int32_t), st));
+    gather_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, perm, b, w.tmp);
+    PVL_LAUNCH_CHECK();
+    for (int pass = 0; pass < 2; ++pass) {
+        PVL_CUDA_CHECK(cudaMemsetAsync(w.flags, 0, sizeof(int32_t) * (nblk + 1), st));
+        double* xt = w.tmp;
+        int32_t* fl = w.flags;
+        void* args[] = {(void*)&n, (void*)&LU, (void*)&lda, (void*)&xt, (void*)&fl, (void*)&err};
+        const void* fn = pass == 0 ? (const void*)trsv_wavefront_kernel<true> : (const void*)trsv_wavefront_kernel<false>;
+        PVL_CUDA_CHECK(cudaLaunchCooperativeKernel(fn, dim3(nblk), dim3(kSolveThreads), args, 0, st));
+        pvl_count_launch();
+    }
+    PVL_CUDA_CHECK(cudaMemcpyAsync(b, w.tmp, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    return PVL_OK;
+}

@@ -1,0 +1,82 @@
+// Shared device helpers for the pyvl_b200 CUDA kernels (sm_100a).
+//
+// Geometry ids follow the reference's geo_id_t (src/core/common.h:46-56): low 31 bits
+// index, bit 31 = reversed orientation, INVALID_ID = 0x7FFFFFFF.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "pvl_status.h"
+
+#define PVL_IDX(g) ((g) & 0x7FFFFFFFu)
+#define PVL_REV(g) ((g) >> 31)
+#define PVL_INVALID 0x7FFFFFFFu
+
+namespace pvl {
+
+// One vortex segment prepared for pair evaluation: start point r1, end point r2, unit
+// direction d = (r2 - r1)/len, length and the segment circulation gamma.  A segment
+// shorter than the cut-off radius is stored with len < 0 and contributes nothing
+// (src/core/flow_solver.c:107-112).
+template <typename T>
+struct __align__(16) Segment {
+    T r1x, r1y, r1z;
+    T r2x, r2y, r2z;
+    T dx, dy, dz;
+    T len;
+    T gamma;
+    T pad;
+};
+
+template <typename T> struct Vec3 { T x, y, z; };
+
+// Induction of one straight segment at point p, scaled by `scale`, added to `acc`.
+//
+// Follows the reference kernel (compute_line_induction, src/core/flow_solver.c:113-135):
+//   dr_k = p - r_k, t_k = d.dr_k, h^2 = ((|dr1|^2 - t1^2) + (|dr2|^2 - t2^2)) / 2,
+//   zero if h^2 < tol^2, else u = (dr1 x d) * (atan2(t2, h) - atan2(t1, h)) / h.
+// The angle difference is evaluated with one atan2 of the rotated pair: for h > 0,
+//   atan2(t2, h) - atan2(t1, h) = atan2(h (t2 - t1), h^2 + t1 t2)
+// and t2 - t1 = -len exactly, so the difference is atan2(-h len, h^2 + t1 t2).  This
+// is the same function of the inputs (the difference lies in (-pi, pi)), evaluated
+// without the cancellation of the two-atan2 form in the far field.
+template <typename T>
+__device__ __forceinline__ void segment_induction(const Segment<T>& s, T px, T py, T pz, T tol2, T scale,
+                                                  Vec3<T>& acc)
+{
+    const T ax = px - s.r1x, ay = py - s.r1y, az = pz - s.r1z;
+    const T bx = px - s.r2x, by = py - s.r2y, bz = pz - s.r2z;
+    const T t1 = s.dx * ax + s.dy * ay + s.dz * az;
+    const T t2 = s.dx * bx + s.dy * by + s.dz * bz;
+    const T n1 = (ax * ax + ay * ay + az * az) - t1 * t1;
+    const T n2 = (bx * bx + by * by + bz * bz) - t2 * t2;
+    const T hsq = (n1 + n2) / T(2);
+    if (hsq < tol2 || s.len < T(0))
+        return;
+    const T h = sqrt(hsq);
+    const T ang = atan2(-h * s.len, hsq + t1 * t2);
+    const T mag = scale * ang / h;
+    // (dr1 x d) * mag
+    acc.x += (ay * s.dz - az * s.dy) * mag;
+    acc.y += (az * s.dx - ax * s.dz) * mag;
+    acc.z += (ax * s.dy - ay * s.dx) * mag;
+}
+
+}  // namespace pvl
+
+#define PVL_CUDA_CHECK(expr)                                                                   \
+    do {                                                                                       \
+        cudaError_t _e = (expr);                                                               \
+        if (_e != cudaSuccess)                                                                 \
+            return pvl_fail(PVL_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #expr,           \
+                            cudaGetErrorString(_e));                                           \
+    } while (0)
+
+// Every kernel launch site is followed by PVL_LAUNCH_CHECK(), which also counts the launch.
+void pvl_count_launch();
+#define PVL_LAUNCH_CHECK()                   \
+    do {                                     \
+        pvl_count_launch();                  \
+        PVL_CUDA_CHECK(cudaGetLastError());  \
+    } while (0)

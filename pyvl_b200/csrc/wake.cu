@@ -1,0 +1,210 @@
+// Free-wake state kernels and the closed-body constraint helpers.
+//
+// Wake node layout is the reference's wake_positions (n_shed, 2, line_rows + 1, 3)
+// (python/pyvl/wake_models.py:66-68); wake circulations are (n_shed, line_rows)
+// (wake_models.py:74-75); node (s, side, row) = s*2*(R+1) + side*(R+1) + row.
+#include <cstdint>
+
+#include "pvl_common.cuh"
+
+namespace {
+
+inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+// One thread per system row: apply the shed lines' implicit columns in line order,
+// the same order (and so the same rounding) as wake_models.py:209-216.
+__global__ void fold_implicit_kernel(uint32_t n_cp, uint32_t n_shed, const double* __restrict__ implicit,
+                                     const uint32_t* __restrict__ adj, double* __restrict__ A, uint32_t lda)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_cp)
+        return;
+    double* row = A + (size_t)i * lda;
+    const double* imp = implicit + (size_t)i * n_shed;
+    for (uint32_t s = 0; s < n_shed; ++s) {
+        const double c = imp[s];
+        const uint32_t s1 = adj[2 * s + 1], s0 = adj[2 * s];
+        if (s1 != PVL_INVALID)
+            row[s1] -= c;
+        if (s0 != PVL_INVALID)
+            row[s0] += c;
+    }
+}
+
+// new[s, side, row]: row 0 = body node; row i+1 = old[i] + v[i] dt (i < complete); rows
+// beyond complete collapse onto row `complete` (wake_models.py:113-137).
+__global__ void advect_kernel(uint32_t n_shed, uint32_t R, uint32_t complete, const double* __restrict__ old_pos,
+                              const double* __restrict__ vel, double dt, const double* __restrict__ body,
+                              const uint32_t* __restrict__ bnodes, double* __restrict__ new_pos)
+{
+    const uint32_t npr = R + 1;
+    const uint64_t n = (uint64_t)n_shed * 2 * npr;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n)
+        return;
+    const uint32_t row = (uint32_t)(t % npr);
+    const uint64_t col = t / npr;  // s*2 + side
+    const uint32_t s = (uint32_t)(col / 2), side = (uint32_t)(col % 2);
+    // the source row for this output row
+    const uint32_t src = row <= complete ? row : complete;
+    double x, y, z;
+    if (src == 0) {
+        const uint32_t b = bnodes[2 * s + side];
+        x = body[3 * (size_t)b];
+        y = body[3 * (size_t)b + 1];
+        z = body[3 * (size_t)b + 2];
+    } else {
+        const uint32_t i = src - 1;  // new[i+1] = old[i] + v[i] dt
+        const double* o = old_pos + 3 * (col * npr + i);
+        const double* v = vel + 3 * (col * complete + i);
+        x = o[0] + v[0] * dt;
+        y = o[1] + v[1] * dt;
+        z = o[2] + v[2] * dt;
+    }
+    double* out = new_pos + 3 * t;
+    out[0] = x;
+    out[1] = y;
+    out[2] = z;
+}
+
+// wake_models.py:139-151
+__global__ void shed_kernel(uint32_t n_shed, uint32_t R, const double* __restrict__ old_circ,
+                            const uint32_t* __restrict__ adj, const double* __restrict__ gamma,
+                            double* __restrict__ new_circ)
+{
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (uint64_t)n_shed * R)
+        return;
+    const uint32_t s = (uint32_t)(t / R), r = (uint32_t)(t % R);
+    if (r > 0) {
+        new_circ[t] = old_circ[(size_t)s * R + r - 1];
+        return;
+    }
+    double c = 0.0;
+    const uint32_t a1 = adj[2 * s + 1], a0 = adj[2 * s];
+    if (a1 != PVL_INVALID)
+        c += gamma[a1];
+    if (a0 != PVL_INVALID)
+        c -= gamma[a0];
+    new_circ[t] = c;
+}
+
+// One CTA per group: mean by a block reduction, then subtract (solver.py:229-233).
+__global__ void group_mean_kernel(const uint32_t* __restrict__ goff, double* __restrict__ x)
+{
+    __shared__ double red[256];
+    const uint32_t g = blockIdx.x;
+    const uint32_t b = goff[g], e = goff[g + 1];
+    double s = 0.0;
+    for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x)
+        s += x[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (unsigned w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    const double mean = e > b ? red[0] / double(e - b) : 0.0;
+    for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x)
+        x[i] -= mean;
+}
+
+__global__ void border_kernel(uint32_t n, uint32_t m, const uint32_t* __restrict__ goff, double* __restrict__ A,
+                              uint32_t lda, double* __restrict__ rhs)
+{
+    // thread t < n + m fills border column entries of row t and border row entries of column t
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t N = n + m;
+    if (t >= N)
+        return;
+    for (uint32_t g = 0; g < m; ++g) {
+        const bool in = t < n && t >= goff[g] && t < goff[g + 1];
+        A[(size_t)t * lda + n + g] = in ? 1.0 : 0.0;  // column n+g
+        A[(size_t)(n + g) * lda + t] = in ? 1.0 : 0.0;  // row n+g
+    }
+    if (t >= n)
+        rhs[t] = 0.0;
+}
+
+int require(const void* p, const char* what)
+{
+    return p ? PVL_OK : pvl_fail(PVL_ERR_ARG, "%s is NULL", what);
+}
+
+}  // namespace
+
+#define PVL_REQUIRE(p)                   \
+    do {                                 \
+        if (int _r = require((p), #p))   \
+            return _r;                   \
+    } while (0)
+
+extern "C" int pvl_wake_fold_implicit(uint32_t n_cp, uint32_t n_shed, const double* implicit, const uint32_t* adjacent,
+                                      double* A, uint32_t lda, void* stream)
+{
+    if (n_cp == 0 || n_shed == 0)
+        return PVL_OK;
+    PVL_REQUIRE(implicit); PVL_REQUIRE(adjacent); PVL_REQUIRE(A);
+    fold_implicit_kernel<<<blocks_for(n_cp, 128), 128, 0, (cudaStream_t)stream>>>(n_cp, n_shed, implicit, adjacent, A,
+                                                                                   lda);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_wake_advect(uint32_t n_shed, uint32_t line_rows, uint32_t complete_rows, const double* old_pos,
+                               const double* node_vel, double dt, const double* body_positions,
+                               const uint32_t* bordering_nodes, double* new_pos, void* stream)
+{
+    if (n_shed == 0)
+        return PVL_OK;
+    if (complete_rows > line_rows)
+        return pvl_fail(PVL_ERR_ARG, "pvl_wake_advect: complete_rows %u > line_rows %u", complete_rows, line_rows);
+    PVL_REQUIRE(old_pos); PVL_REQUIRE(body_positions); PVL_REQUIRE(bordering_nodes); PVL_REQUIRE(new_pos);
+    if (complete_rows > 0)
+        PVL_REQUIRE(node_vel);
+    if (old_pos == new_pos)
+        return pvl_fail(PVL_ERR_ARG, "pvl_wake_advect: old_pos and new_pos must not alias");
+    const uint64_t n = (uint64_t)n_shed * 2 * (line_rows + 1);
+    advect_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(
+        n_shed, line_rows, complete_rows, old_pos, node_vel, dt, body_positions, bordering_nodes, new_pos);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_wake_shed(uint32_t n_shed, uint32_t line_rows, const double* old_circ, const uint32_t* adjacent,
+                             const double* gamma, double* new_circ, void* stream)
+{
+    if (n_shed == 0 || line_rows == 0)
+        return PVL_OK;
+    PVL_REQUIRE(old_circ); PVL_REQUIRE(adjacent); PVL_REQUIRE(gamma); PVL_REQUIRE(new_circ);
+    if (old_circ == new_circ)
+        return pvl_fail(PVL_ERR_ARG, "pvl_wake_shed: old_circ and new_circ must not alias");
+    shed_kernel<<<blocks_for((uint64_t)n_shed * line_rows, 256), 256, 0, (cudaStream_t)stream>>>(
+        n_shed, line_rows, old_circ, adjacent, gamma, new_circ);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_group_mean_remove(uint32_t n_groups, const uint32_t* group_offsets, double* x, void* stream)
+{
+    if (n_groups == 0)
+        return PVL_OK;
+    PVL_REQUIRE(group_offsets); PVL_REQUIRE(x);
+    group_mean_kernel<<<n_groups, 256, 0, (cudaStream_t)stream>>>(group_offsets, x);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_border_groups(uint32_t n, uint32_t m, const uint32_t* group_offsets, double* A, uint32_t lda,
+                                 double* rhs, void* stream)
+{
+    if (m == 0)
+        return PVL_OK;
+    PVL_REQUIRE(group_offsets); PVL_REQUIRE(A); PVL_REQUIRE(rhs);
+    if (lda < n + m)
+        return pvl_fail(PVL_ERR_ARG, "pvl_border_groups: lda %u < n + m = %u", lda, n + m);
+    border_kernel<<<blocks_for(n + m, 256), 256, 0, (cudaStream_t)stream>>>(n, m, group_offsets, A, lda, rhs);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}

@@ -357,6 +357,25 @@ def batch_wings(n_cases: int = 256, seed: int = 3, steps: int = 50,
     return out
 
 
+def synthetic_full_wake(te_positions, line_rows: int, freestream, dt: float, seed: int = 0):
+    """A seeded, fully developed wake state with every row present.
+
+    te_positions is (S, 2, 3): the two trailing-edge nodes of each shedding line.  Row r
+    sits r * dt * U_inf downstream of the trailing edge with a smooth seeded vertical wave;
+    circulations are smooth seeded values of the size a lifting wing sheds.  Returns
+    positions (S, 2, R+1, 3) and circulations (S, R)."""
+    rng = np.random.default_rng(seed)
+    te = np.asarray(te_positions, np.float64)
+    S, R = te.shape[0], int(line_rows)
+    u = np.asarray(freestream, np.float64)
+    r = np.arange(R + 1, dtype=np.float64)
+    ph = rng.uniform(0, 2 * np.pi)
+    pos = te[:, :, None, :] + r[None, None, :, None] * dt * u[None, None, None, :]
+    pos[..., 2] += 0.05 * np.sin(0.07 * r + ph)[None, None, :]
+    circ = 0.02 * np.sin(0.05 * np.arange(R)[None, :] + np.linspace(0, np.pi, S)[:, None] + ph)
+    return pos, circ
+
+
 def by_name(name: str) -> Case:
     """Workloads by their short names: flat_wing, swept_pitching, icosphere, flapping."""
     table = {

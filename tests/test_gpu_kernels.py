@@ -1,0 +1,166 @@
+"""CUDA kernels vs the reference (golden vectors) and the CPU oracle.  Needs a B200.
+
+Tolerances: the plain path must match the reference's FP64 kernels to <= 1e-12 relative
+Frobenius error; cut-off zeros must be exact zeros.
+"""
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+import scipy.linalg as la
+
+pytestmark = pytest.mark.gpu
+
+GOLD = Path(__file__).resolve().parent / "golden"
+TOL = 1e-6
+PARITY = 1e-12
+
+
+def rel(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    den = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (den if den > 0 else 1.0)
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+
+    assert torch.cuda.is_available(), "GPU tests need CUDA"
+    return torch
+
+
+def _names():
+    d = np.load(GOLD / "kernels.npz")
+    return sorted({k.split("/")[0] for k in d.files})
+
+
+@pytest.mark.parametrize("name", _names())
+def test_kernels_match_reference(torch_cuda, name):
+    from pyvl_b200.cvl import Mesh
+
+    d = np.load(GOLD / "kernels.npz")
+    g = lambda k: d[f"{name}/{k}"]  # noqa: E731
+    elems = np.split(g("elements_flat"), np.cumsum(g("elements_counts"))[:-1])
+    pos, cps, nrm = g("positions"), g("cps"), g("normals")
+    m = Mesh(pos.shape[0], elems)
+    li = m.line_induction_matrix(TOL, pos, cps)
+    assert rel(li, g("line_ind")) <= PARITY
+    # the cut-off zeroes whole pairs (flow_solver.c:107-130): same pairs as the reference.
+    # Single components may differ in zero-ness: FMA contraction of (dr1 x d) rounds
+    # differently from the reference's separate multiply and subtract.
+    assert np.array_equal(np.all(li == 0, axis=-1), np.all(g("line_ind") == 0, axis=-1))
+    assert rel(m.induction_matrix(TOL, pos, cps), g("ind_vec")) <= PARITY
+    assert rel(m.induction_matrix3(TOL, pos, cps, nrm), g("ind_nrm")) <= PARITY
+    assert rel(m.surface_normal(pos), g("surface_normal")) <= 1e-15
+    assert rel(m.surface_average_vec3(pos), g("surface_center")) <= 1e-15
+    f = Mesh.line_forces(m, m.compute_dual(), g("circ"), pos, g("velocity"))
+    assert rel(f, g("line_forces")) <= 1e-15
+
+
+def test_overlap_self_entries_are_exact_zeros(torch_cuda):
+    """test/pytests/test_mesh.py:105-111 on the GPU."""
+    from pyvl_b200.cvl import Mesh
+
+    msh = Mesh(4, [[0, 1, 2, 3]])
+    positions = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0]], np.float64)
+    mat = msh.line_induction_matrix(1e-6, positions, positions)
+    for i in range(4):
+        assert all(mat[i, i, :] == (0, 0, 0))
+
+
+@pytest.mark.parametrize("name", ["swept_pitching", "flapping"])
+def test_full_size_body_matrix_checksums(torch_cuda, name):
+    """Full-size (1024 and 4096 ring) body matrices vs the reference's checksums."""
+    from pyvl_b200 import workloads
+    from pyvl_b200.cvl import Mesh
+
+    gold = np.load(GOLD / "checksums.npz")
+    case = workloads.by_name(name)
+    t = float(gold[f"{name}/t"])
+    m = Mesh(case.n_points, case.elements)
+    pos = case.positions_at(t)
+    cps = m.surface_average_vec3(pos)
+    nrm = m.surface_normal(pos)
+    A = m.induction_matrix3(TOL, pos, cps, nrm)
+    assert rel(A @ gold[f"{name}/v"], gold[f"{name}/Av"]) <= PARITY
+    assert rel(A.T @ gold[f"{name}/w"], gold[f"{name}/ATw"]) <= PARITY
+    assert rel(A[gold[f"{name}/ii"], gold[f"{name}/jj"]], gold[f"{name}/Aij"]) <= PARITY
+    assert rel(np.diag(A), gold[f"{name}/diag"]) <= PARITY
+    assert abs(np.linalg.norm(A) - gold[f"{name}/fro"]) <= PARITY * gold[f"{name}/fro"]
+
+
+def test_induced_velocity_matches_oracle_contraction(torch_cuda):
+    """Fused sum_j K_ij Gamma_j vs the reference's materialised matrix + vecdot (oracle)."""
+    from oracle.kernels import OracleMesh
+    from pyvl_b200 import workloads
+    from pyvl_b200.cvl import Mesh
+
+    case = workloads.swept_pitching(ns=16, nc=8)
+    rng = np.random.default_rng(3)
+    pos = case.positions_at(0.4)
+    pts = rng.normal(size=(777, 3)) * 3
+    pts[:10] = pos[:10]  # points on nodes: cut-off
+    gam = rng.normal(size=case.n_surfaces)
+    om = OracleMesh(case.n_points, case.elements)
+    want = np.vecdot(om.induction_matrix(TOL, pos, pts), gam[None, :, None], axis=1)
+    m = Mesh(case.n_points, case.elements)
+    got = m.induced_velocity(TOL, pos, pts, gam)
+    assert rel(got, want) <= PARITY
+
+
+def _lu_roundtrip(torch, A, b):
+    from pyvl_b200 import _lib
+    from pyvl_b200.device import Workspace, ptr, stream_ptr
+
+    n = A.shape[0]
+    dA = torch.tensor(A, device="cuda")
+    ipiv = torch.zeros(2 * n, dtype=torch.int32, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    ws, nb = Workspace.get(_lib.query("pvl_lu_workspace", n))
+    _lib.call("pvl_lu_factor", n, ptr(dA), n, ptr(ipiv), ptr(info), ws, nb, stream_ptr())
+    db = torch.tensor(b, device="cuda")
+    _lib.call("pvl_lu_solve", n, ptr(dA), n, ptr(ipiv), ptr(db), ptr(err), ws, nb, stream_ptr())
+    torch.cuda.synchronize()
+    return dA.cpu().numpy(), ipiv.cpu().numpy(), int(info.item()), int(err.item()), db.cpu().numpy()
+
+
+@pytest.mark.parametrize("n,kind", [(64, "dominant"), (200, "dominant"), (1000, "dominant"), (333, "general"),
+                                    (130, "general"), (777, "singular_last")])
+def test_lu_matches_lapack(torch_cuda, n, kind):
+    rng = np.random.default_rng(n)
+    A = rng.normal(size=(n, n))
+    if kind == "dominant":
+        A = A * 1e-3 - 2 * np.pi * np.eye(n)
+    if kind == "singular_last":
+        A[:, -1] = 0.0
+    b = rng.normal(size=n)
+    LU, ipiv, info, err, x = _lu_roundtrip(torch_cuda, A, b)
+    assert err == 0
+    lu_ref, piv_ref = la.lu_factor(A)
+    assert np.array_equal(ipiv[:n], piv_ref)
+    assert rel(LU, lu_ref) <= 1e-13
+    if kind == "singular_last":
+        assert info == n
+        return
+    assert info == 0
+    x_ref = la.lu_solve((lu_ref, piv_ref), b)
+    assert rel(x, x_ref) <= 1e-12
+
+
+def test_lu_bordered_sphere(torch_cuda):
+    """Closed sphere: the bordered (zero-mean) system vs the numpy/LAPACK oracle."""
+    from oracle.solver import bordered_solve
+
+    gold = np.load(GOLD / "sphere.npz")
+    A, rhs = gold["A"], gold["rhs"]
+    n = A.shape[0]
+    K = np.zeros((n + 1, n + 1))
+    K[:n, :n] = A
+    K[:n, n] = K[n, :n] = 1.0
+    LU, ipiv, info, err, x = _lu_roundtrip(torch_cuda, K, np.concatenate([rhs, [0.0]]))
+    assert info == 0 and err == 0
+    want = bordered_solve(A, rhs, [np.arange(n)])
+    assert rel(x[:n], want) <= 1e-12
