@@ -216,8 +216,10 @@ size_t pvl_lu_solve_workspace(uint32_t n);
 int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv, int32_t* info, void* ws,
                   size_t ws_bytes, void* stream);
 
-/* Solve A x = b in place in b (device, n) with the factors and ipiv of pvl_lu_factor.  err
- * (device int32) receives 0, or 1 if a wait between row blocks timed out.
+/* Solve A x = b in place in b (device, n) with the factors and ipiv of pvl_lu_factor.  ws
+ * must be the workspace the factorisation ran with, unchanged since: it holds the inverted
+ * 64 x 64 diagonal blocks of L and U.  err (device int32) receives 0, or 1 if a wait between
+ * row blocks timed out.
  * Replaces scipy.linalg.lu_solve (python/pyvl/solver.py:227). */
 int pvl_lu_solve(uint32_t n, const double* LU, uint32_t lda, const int32_t* ipiv, double* b,
                  int32_t* err, void* ws, size_t ws_bytes, void* stream);

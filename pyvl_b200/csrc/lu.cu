@@ -46,20 +46,19 @@ inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1)
 struct LuWs {
     double* backup;         // (n, NB) copy of the current panel before speculation
     double* top_out;        // (NB, NB) speculative top block
-    unsigned long long* colmax;  // (n_slab_ctas + 1, NB) |x| maxima as ordered bit patterns
+    int32_t* reject;        // per panel: the speculation failed
     int32_t* ok;            // per panel: speculative factors accepted
     int32_t* flags;         // wavefront flags (solve)
     double* tmp;            // (n) solve vector
+    double* inv;            // (n_blocks, 2, kRB, kRB): inverses of the diagonal blocks of L and U
 };
-
-uint32_t slab_ctas(uint32_t n) { return (n + kSlabRows - 1) / kSlabRows + 1; }
 
 size_t lu_ws_bytes(uint32_t n)
 {
     return align256((size_t)n * NB * sizeof(double)) + align256((size_t)NB * NB * sizeof(double)) +
-           align256((size_t)slab_ctas(n) * NB * sizeof(unsigned long long)) +
+           align256(((size_t)n / NB + 2) * sizeof(int32_t)) +
            align256(((size_t)n / NB + 2) * sizeof(int32_t)) + align256(((size_t)n / kRB + 2) * sizeof(int32_t)) +
-           align256((size_t)n * sizeof(double));
+           align256((size_t)n * sizeof(double)) + align256(((size_t)n + kRB - 1) / kRB * 2 * kRB * kRB * sizeof(double));
 }
 
 LuWs carve(void* ws, uint32_t n)
@@ -70,20 +69,16 @@ LuWs carve(void* ws, uint32_t n)
     p += align256((size_t)n * NB * sizeof(double));
     w.top_out = reinterpret_cast<double*>(p);
     p += align256((size_t)NB * NB * sizeof(double));
-    w.colmax = reinterpret_cast<unsigned long long*>(p);
-    p += align256((size_t)slab_ctas(n) * NB * sizeof(unsigned long long));
+    w.reject = reinterpret_cast<int32_t*>(p);
+    p += align256(((size_t)n / NB + 2) * sizeof(int32_t));
     w.ok = reinterpret_cast<int32_t*>(p);
     p += align256(((size_t)n / NB + 2) * sizeof(int32_t));
     w.flags = reinterpret_cast<int32_t*>(p);
     p += align256(((size_t)n / kRB + 2) * sizeof(int32_t));
     w.tmp = reinterpret_cast<double*>(p);
+    p += align256((size_t)n * sizeof(double));
+    w.inv = reinterpret_cast<double*>(p);
     return w;
-}
-
-// |x| as an integer whose order matches the order of non-negative doubles.
-__device__ __forceinline__ unsigned long long abs_bits(double x)
-{
-    return (unsigned long long)__double_as_longlong(fabs(x));
 }
 
 __global__ void init_perm_kernel(uint32_t n, int32_t* __restrict__ perm)
@@ -98,22 +93,22 @@ __global__ void init_perm_kernel(uint32_t n, int32_t* __restrict__ perm)
 // the top block (every CTA factors the same top block, so no CTA waits for another), threads
 // 64..127 hold this CTA's rows below it.  Each thread keeps its row in registers (columns
 // beyond nb are zero; missing top rows are unit rows) and eliminates column j with the row
-// that thread j publishes in shared memory -- the recurrence of getf2 without interchanges.
-// Per column, the largest |entry| on or below the diagonal row before elimination is reduced
-// per warp into shared memory.  Slab rows are backed up and overwritten in place; the
-// factored top block goes to `top_out` (committed by panel_pivot_kernel) so that no CTA can
-// read a half-written top block.
+// that thread j publishes in shared memory, scaling by the reciprocal of the pivot as getf2
+// does -- the recurrence of getf2 without interchanges.  Partial pivoting would keep the
+// diagonal in column j iff no entry below it is larger in magnitude at that moment; every
+// thread checks this for its own row, and any violation (or a zero/NaN pivot) marks the panel.
+// Slab rows are backed up and overwritten in place; the factored top block goes to `top_out`
+// (committed by panel_pivot_kernel) so that no CTA can read a half-written top block.
 __global__ void __launch_bounds__(2 * kSlabRows) panel_spec_kernel(uint32_t n, uint32_t k0, uint32_t nb,
                                                                    double* __restrict__ A, uint32_t lda,
                                                                    double* __restrict__ backup,
                                                                    double* __restrict__ top_out,
-                                                                   unsigned long long* __restrict__ colmax)
+                                                                   int32_t* __restrict__ reject)
 {
     __shared__ double U[NB][NB + 1];
-    __shared__ unsigned long long cm[4][NB];
+    __shared__ double s_rcp[NB];
     const uint32_t tid = threadIdx.x;
     const bool is_top = tid < NB;
-    const uint32_t lane = tid & 31, warp = tid >> 5;
     const uint32_t r_begin = k0 + nb + blockIdx.x * kSlabRows;
     // global row of this thread (top: k0 + tid, slab: r_begin + tid - 64)
     const uint32_t grow = is_top ? k0 + tid : r_begin + (tid - NB);
@@ -133,31 +128,30 @@ __global__ void __launch_bounds__(2 * kSlabRows) panel_spec_kernel(uint32_t n, u
         for (int c = 0; c < NB; ++c)
             if ((uint32_t)c < nb)
                 backup[(size_t)(grow - k0) * NB + c] = row[c];
+    bool bad = false;
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
         if (tid == (uint32_t)j) {
 #pragma unroll
             for (int c = j; c < NB; ++c)
                 U[j][c] = row[c];
+            s_rcp[j] = 1.0 / row[j];
+            bad |= !(fabs(row[j]) > 0.0);
         }
         __syncthreads();
         const bool act = is_top ? tid > (uint32_t)j : valid;
-        const double v = row[j];
-        unsigned long long m = act ? abs_bits(v) : 0ull;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
-            m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-        if (lane == 0)
-            cm[warp][j] = m;
         if (act) {
-            const double x = v / U[j][j];
+            const double v = row[j];
+            bad |= !(fabs(v) <= fabs(U[j][j]));
+            const double x = v * s_rcp[j];
             row[j] = x;
 #pragma unroll
             for (int c = j + 1; c < NB; ++c)
                 row[c] -= x * U[j][c];
         }
     }
-    __syncthreads();
+    if (__syncthreads_or(bad) && tid == 0)
+        atomicExch(reject, 1);
     if (is_top) {
         if (blockIdx.x == 0 && valid)
 #pragma unroll
@@ -170,40 +164,22 @@ __global__ void __launch_bounds__(2 * kSlabRows) panel_spec_kernel(uint32_t n, u
             if ((uint32_t)c < nb)
                 A[(size_t)grow * lda + k0 + c] = row[c];
     }
-    if (tid < NB)
-        colmax[(size_t)blockIdx.x * NB + tid] =
-            max(max(cm[0][tid], cm[1][tid]), max(cm[2][tid], cm[3][tid]));
 }
 
 // ---------------------------------------------------------------- 3. accept or pivot
 __global__ void __launch_bounds__(1024) panel_pivot_kernel(uint32_t n, uint32_t k0, uint32_t nb, double* __restrict__ A,
                                                            uint32_t lda, const double* __restrict__ backup,
                                                            const double* __restrict__ top_out,
-                                                           const unsigned long long* __restrict__ colmax,
-                                                           uint32_t n_cm, int32_t* __restrict__ ok,
-                                                           uint32_t panel, int32_t* __restrict__ ipiv,
-                                                           int32_t* __restrict__ perm, int32_t* __restrict__ info)
+                                                           const int32_t* __restrict__ reject,
+                                                           int32_t* __restrict__ ok, uint32_t panel,
+                                                           int32_t* __restrict__ ipiv, int32_t* __restrict__ perm,
+                                                           int32_t* __restrict__ info)
 {
-    __shared__ int bad;
     __shared__ double s_val[32];
     __shared__ uint32_t s_idx[32];
     __shared__ uint32_t s_piv;
     __shared__ double s_prow[NB];
-    if (threadIdx.x == 0)
-        bad = 0;
-    __syncthreads();
-    for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
-        unsigned long long m = 0;
-        for (uint32_t c = 0; c < n_cm; ++c)
-            m = max(m, colmax[(size_t)c * NB + j]);
-        const double d = top_out[(size_t)j * NB + j];
-        // m is the largest |entry| strictly below the diagonal; speculation holds iff it is
-        // not larger than |d| (a tie keeps the diagonal, as idamax does).  Zero or NaN
-        // pivots reject.
-        if (!(fabs(d) > 0.0) || abs_bits(d) < m)
-            atomicOr(&bad, 1);
-    }
-    __syncthreads();
+    const int bad = reject[panel];
     if (!bad) {
         if (threadIdx.x == 0)
             ok[panel] = 1;
@@ -284,9 +260,10 @@ __global__ void __launch_bounds__(1024) panel_pivot_kernel(uint32_t n, uint32_t 
             __syncthreads();
             continue;
         }
+        const double rcp = 1.0 / piv;
         for (uint32_t r = col + 1 + threadIdx.x; r < n; r += blockDim.x) {
             double* row = A + (size_t)r * lda + k0;
-            const double l = row[j] / piv;
+            const double l = row[j] * rcp;
             row[j] = l;
             for (uint32_t c = j + 1; c < nb; ++c)
                 row[c] -= l * s_prow[c];
@@ -451,6 +428,55 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_update_kernel(uint32_t n, u
         }
 }
 
+// ---------------------------------------------------------------- diagonal-block inverses
+// One CTA per kRB-row block b: threads 0..63 form column c of L_bb^-1 (unit lower, forward
+// substitution), threads 64..127 column c of U_bb^-1 (backward substitution), each column
+// held in registers.  A partial last block is padded with identity.  The wavefront solves
+// then apply each diagonal block as one parallel matrix-vector product.
+__global__ void __launch_bounds__(2 * kRB, 1) diag_inverse_kernel(uint32_t n, const double* __restrict__ M,
+                                                                  uint32_t lda, double* __restrict__ inv)
+{
+    __shared__ double D[kRB][kRB + 1];
+    const uint32_t b = blockIdx.x, r0 = b * kRB;
+    const uint32_t rows = min((uint32_t)kRB, n - r0);
+    for (uint32_t e = threadIdx.x; e < kRB * kRB; e += blockDim.x) {
+        const uint32_t r = e / kRB, c = e % kRB;
+        D[r][c] = (r < rows && c < rows) ? M[(size_t)(r0 + r) * lda + r0 + c] : (r == c ? 1.0 : 0.0);
+    }
+    __syncthreads();
+    const bool lower = threadIdx.x < kRB;
+    const int c = (int)(threadIdx.x & (kRB - 1));
+    double y[kRB];
+    if (lower) {
+#pragma unroll
+        for (int r = 0; r < kRB; ++r)
+            y[r] = r == c ? 1.0 : 0.0;
+#pragma unroll
+        for (int q = 0; q < kRB - 1; ++q) {
+            const double yq = y[q];
+#pragma unroll
+            for (int r = q + 1; r < kRB; ++r)
+                y[r] -= D[r][q] * yq;
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < kRB; ++r)
+            y[r] = r == c ? 1.0 : 0.0;
+#pragma unroll
+        for (int q = kRB - 1; q >= 0; --q) {
+            const double yq = y[q] / D[q][q];
+            y[q] = yq;
+#pragma unroll
+            for (int r = 0; r < q; ++r)
+                y[r] -= D[r][q] * yq;
+        }
+    }
+    double* out = inv + ((size_t)b * 2 + (lower ? 0 : 1)) * kRB * kRB;
+#pragma unroll
+    for (int r = 0; r < kRB; ++r)
+        out[(size_t)r * kRB + c] = y[r];
+}
+
 // ---------------------------------------------------------------- solve
 __global__ void gather_kernel(uint32_t n, const int32_t* __restrict__ perm, const double* __restrict__ b,
                               double* __restrict__ out)
@@ -479,13 +505,14 @@ __device__ __forceinline__ void st_release(int32_t* p, int32_t v)
 // the CTA sets *err, publishes its flag so that no later block waits on it, and returns.
 template <bool LOWER>
 __global__ void __launch_bounds__(kSolveThreads) trsv_wavefront_kernel(uint32_t n, const double* __restrict__ M,
-                                                                       uint32_t lda, double* __restrict__ x,
+                                                                       uint32_t lda,
+                                                                       const double* __restrict__ inv,
+                                                                       double* __restrict__ x,
                                                                        int32_t* __restrict__ flags,
                                                                        int32_t* __restrict__ err)
 {
     __shared__ double s_acc[kRB];
-    __shared__ double s_x[kRB];
-    __shared__ double s_d[kRB][kRB + 1];
+    __shared__ double s_r[kRB];
     __shared__ int s_abort;
     const uint32_t nblk = (n + kRB - 1) / kRB;
     const uint32_t b = LOWER ? blockIdx.x : nblk - 1 - blockIdx.x;
@@ -496,11 +523,6 @@ __global__ void __launch_bounds__(kSolveThreads) trsv_wavefront_kernel(uint32_t 
         s_abort = 0;
     if (threadIdx.x < kRB)
         s_acc[threadIdx.x] = 0.0;
-    // the diagonal block does not depend on any other block: stage it before waiting
-    for (uint32_t e = threadIdx.x; e < kRB * kRB; e += blockDim.x) {
-        const uint32_t r = e / kRB, c = e % kRB;
-        s_d[r][c] = (r < rows && c < rows) ? M[(size_t)(r0 + r) * lda + r0 + c] : 0.0;
-    }
     __syncthreads();
     const uint32_t n_dep = LOWER ? b : nblk - 1 - b;
     for (uint32_t step = 0; step < n_dep; ++step) {
@@ -513,7 +535,7 @@ __global__ void __launch_bounds__(kSolveThreads) trsv_wavefront_kernel(uint32_t 
                     s_abort = 1;
                     break;
                 }
-                __nanosleep(100);
+                __nanosleep(64);
             }
         }
         __syncthreads();
@@ -524,11 +546,11 @@ __global__ void __launch_bounds__(kSolveThreads) trsv_wavefront_kernel(uint32_t 
         }
         const uint32_t c0 = c * kRB;
         const uint32_t ccols = min((uint32_t)kRB, n - c0);
+        const double x0 = lane < ccols ? __ldcg(x + c0 + lane) : 0.0;
+        const double x1 = lane + 32 < ccols ? __ldcg(x + c0 + lane + 32) : 0.0;
         for (uint32_t r = warp; r < rows; r += kSolveThreads / 32) {
             const double* mrow = M + (size_t)(r0 + r) * lda + c0;
-            double s = 0.0;
-            for (uint32_t k = lane; k < ccols; k += 32)
-                s += mrow[k] * __ldcg(x + c0 + k);
+            double s = (lane < ccols ? mrow[lane] * x0 : 0.0) + (lane + 32 < ccols ? mrow[lane + 32] * x1 : 0.0);
             for (int o = 16; o > 0; o >>= 1)
                 s += __shfl_xor_sync(0xffffffffu, s, o);
             if (lane == 0)
@@ -536,40 +558,22 @@ __global__ void __launch_bounds__(kSolveThreads) trsv_wavefront_kernel(uint32_t 
         }
         __syncthreads();
     }
-    if (warp == 0) {
-        for (uint32_t k = lane; k < rows; k += 32)
-            s_x[k] = __ldcg(x + r0 + k) - s_acc[k];
-        __syncwarp();
-        if (LOWER) {
-            for (uint32_t r = 1; r < rows; ++r) {
-                double s = 0.0;
-                for (uint32_t k = lane; k < r; k += 32)
-                    s += s_d[r][k] * s_x[k];
-                for (int o = 16; o > 0; o >>= 1)
-                    s += __shfl_xor_sync(0xffffffffu, s, o);
-                if (lane == 0)
-                    s_x[r] -= s;
-                __syncwarp();
-            }
-        } else {
-            for (int r = (int)rows - 1; r >= 0; --r) {
-                double s = 0.0;
-                for (uint32_t k = r + 1 + lane; k < rows; k += 32)
-                    s += s_d[r][k] * s_x[k];
-                for (int o = 16; o > 0; o >>= 1)
-                    s += __shfl_xor_sync(0xffffffffu, s, o);
-                if (lane == 0)
-                    s_x[r] = (s_x[r] - s) / s_d[r][r];
-                __syncwarp();
-            }
-        }
-        for (uint32_t k = lane; k < rows; k += 32)
-            x[r0 + k] = s_x[k];
-        __threadfence();
-        __syncwarp();
+    // diagonal block: x_b = inv(D_bb) (r_b - acc), one parallel matrix-vector product
+    if (threadIdx.x < kRB)
+        s_r[threadIdx.x] = threadIdx.x < rows ? __ldcg(x + r0 + threadIdx.x) - s_acc[threadIdx.x] : 0.0;
+    __syncthreads();
+    const double* D = inv + ((size_t)b * 2 + (LOWER ? 0 : 1)) * kRB * kRB;
+    for (uint32_t r = warp; r < rows; r += kSolveThreads / 32) {
+        double s = D[(size_t)r * kRB + lane] * s_r[lane] + D[(size_t)r * kRB + lane + 32] * s_r[lane + 32];
+        for (int o = 16; o > 0; o >>= 1)
+            s += __shfl_xor_sync(0xffffffffu, s, o);
         if (lane == 0)
-            st_release(flags + b, 1);
+            x[r0 + r] = s;
     }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0)
+        st_release(flags + b, 1);
 }
 
 int coresident_blocks(const void* fn, int threads)
@@ -616,15 +620,16 @@ extern "C" int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv,
     init_perm_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, perm);
     PVL_LAUNCH_CHECK();
     const uint32_t n_panels = (n + NB - 1) / NB;
+    PVL_CUDA_CHECK(cudaMemsetAsync(w.reject, 0, sizeof(int32_t) * (n_panels + 1), st));
     for (uint32_t p = 0; p < n_panels; ++p) {
         const uint32_t k0 = p * NB;
         const uint32_t nb = std::min<uint32_t>(NB, n - k0);
         const uint32_t below = n - k0 - nb;
         const uint32_t ctas = std::max<uint32_t>(1, (below + kSlabRows - 1) / kSlabRows);
-        panel_spec_kernel<<<ctas, 2 * kSlabRows, 0, st>>>(n, k0, nb, A, lda, w.backup, w.top_out, w.colmax);
+        panel_spec_kernel<<<ctas, 2 * kSlabRows, 0, st>>>(n, k0, nb, A, lda, w.backup, w.top_out, w.reject + p);
         PVL_LAUNCH_CHECK();
-        panel_pivot_kernel<<<1, 1024, 0, st>>>(n, k0, nb, A, lda, w.backup, w.top_out, w.colmax, ctas, w.ok, p, ipiv,
-                                               perm, info);
+        panel_pivot_kernel<<<1, 1024, 0, st>>>(n, k0, nb, A, lda, w.backup, w.top_out, w.reject, w.ok, p, ipiv, perm,
+                                               info);
         PVL_LAUNCH_CHECK();
         if (n > nb) {
             trsm_kernel<<<blocks_for(n - nb, kTrsmCols), kTrsmCols, trsm_smem, st>>>(n, k0, nb, A, lda, w.ok, p, ipiv);
@@ -636,6 +641,8 @@ extern "C" int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv,
             PVL_LAUNCH_CHECK();
         }
     }
+    diag_inverse_kernel<<<(n + kRB - 1) / kRB, 2 * kRB, 0, st>>>(n, A, lda, w.inv);
+    PVL_LAUNCH_CHECK();
     return PVL_OK;
 }
 
@@ -664,7 +671,8 @@ extern "C" int pvl_lu_solve(uint32_t n, const double* LU, uint32_t lda, const in
         PVL_CUDA_CHECK(cudaMemsetAsync(w.flags, 0, sizeof(int32_t) * (nblk + 1), st));
         double* xt = w.tmp;
         int32_t* fl = w.flags;
-        void* args[] = {(void*)&n, (void*)&LU, (void*)&lda, (void*)&xt, (void*)&fl, (void*)&err};
+        const double* iv = w.inv;
+        void* args[] = {(void*)&n, (void*)&LU, (void*)&lda, (void*)&iv, (void*)&xt, (void*)&fl, (void*)&err};
         const void* fn = pass == 0 ? (const void*)trsv_wavefront_kernel<true> : (const void*)trsv_wavefront_kernel<false>;
         PVL_CUDA_CHECK(cudaLaunchCooperativeKernel(fn, dim3(nblk), dim3(kSolveThreads), args, 0, st));
         pvl_count_launch();

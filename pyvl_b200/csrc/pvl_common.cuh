@@ -54,9 +54,11 @@ __device__ __forceinline__ void segment_induction(const Segment<T>& s, T px, T p
     const T hsq = (n1 + n2) / T(2);
     if (hsq < tol2 || s.len < T(0))
         return;
-    const T h = sqrt(hsq);
+    // one reciprocal square root gives both h and 1/h (no separate sqrt and division)
+    const T rh = rsqrt(hsq);
+    const T h = hsq * rh;
     const T ang = atan2(-h * s.len, hsq + t1 * t2);
-    const T mag = scale * ang / h;
+    const T mag = scale * ang * rh;
     // (dr1 x d) * mag
     acc.x += (ay * s.dz - az * s.dy) * mag;
     acc.y += (az * s.dx - ax * s.dz) * mag;
