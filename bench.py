@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--path", choices=["plain"], default="plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-kernel", choices=["line_sum", "lu"], default=None,
+                    help="set up the workload, launch only that kernel family twice and exit (for ncu captures)")
     ap.add_argument("--fraction", type=int, default=16,
                     help="reference arm: wake correction and advection are timed on 1/F of their points")
     return ap.parse_args()
@@ -172,10 +174,48 @@ def cpu_baseline() -> dict | None:
 
 
 # ------------------------------------------------------------------ our arm
+def profile_kernel(args) -> None:
+    """Two launches of one kernel family on the benchmark state, nothing else (ncu target)."""
+    import torch
+
+    from pyvl_b200 import _lib
+    from pyvl_b200.device import ptr, stream_ptr
+    from pyvl_b200.engine import SolverEngine
+
+    case = workload()
+    mesh, spec, wpos, wcirc, t0 = wake_setup(case)
+    eng = SolverEngine(mesh, case.freestream, case.tol, spec)
+    eng.set_wake_state(wpos, wcirc, step_count=case.line_rows + 1, time=t0 - case.dt)
+    eng.load_inputs(case.positions_at(t0), case.velocities_at(t0))
+    if args.profile_kernel == "line_sum":
+        S, R, L = spec.shedding_lines.size, case.line_rows, mesh.n_lines
+        d = mesh.device_arrays()
+        nv = torch.empty((S, 2, R, 3), dtype=torch.float64, device="cuda")
+        wsb = _lib.query("pvl_wake_node_velocity_workspace", L, S, R, _lib.PVL_F64)
+        ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+        for _ in range(2):
+            _lib.call("pvl_wake_node_velocity", _lib.PVL_F64, mesh.n_points, L, ptr(d["lines"]), ptr(eng.pos),
+                      ptr(eng.body_line_gamma), S, R, R, ptr(eng.wake_positions), 1.0, 0.0, 0.0, case.tol, ptr(nv),
+                      ptr(ws), wsb, stream_ptr())
+    else:
+        eng.iteration = 1
+        eng.assemble()
+        A0 = eng.A.clone()
+        for _ in range(2):
+            eng.A.copy_(A0)
+            _lib.call("pvl_lu_factor", eng.N, ptr(eng.A), eng.N, ptr(eng.ipiv), ptr(eng.info), ptr(eng.ws),
+                      eng._ws_bytes, stream_ptr())
+    torch.cuda.synchronize()
+    eng.check_status()
+    print("profile-kernel done", args.profile_kernel)
+
+
 def main() -> None:
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_kernel:
+        return profile_kernel(args)
     import torch
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

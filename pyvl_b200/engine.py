@@ -52,6 +52,18 @@ def wake_ring_connectivity(line_rows: int, n_shed: int) -> np.ndarray:
     return rc.reshape(-1, 4).astype(np.uint32)
 
 
+def wake_row0_mesh(wake_mesh: Mesh, n_shed: int, line_rows: int) -> Mesh:
+    """The first-row rings (ring s * line_rows of each strip) over the wake mesh's lines and
+    points: their induction is the implicit part of the wake correction."""
+    off = wake_mesh.surface_offsets
+    sl = wake_mesh.surface_lines
+    rows0 = np.arange(n_shed) * line_rows
+    cnt = (off[rows0 + 1] - off[rows0]).astype(np.uint32)
+    off0 = np.concatenate([[0], np.cumsum(cnt)]).astype(np.uint32)
+    sl0 = np.concatenate([sl[off[r]: off[r + 1]] for r in rows0]).astype(np.uint32)
+    return Mesh._from_arrays(wake_mesh.n_points, wake_mesh.line_data.copy(), off0, sl0)
+
+
 @dataclass
 class WakeSpec:
     """What the wake model needs from the geometry (wake_models.py:54-81)."""
@@ -145,12 +157,8 @@ class SolverEngine:
             raise ValueError("bordering nodes out of range")
         wmesh = Mesh(2 * (R + 1) * S, wake_ring_connectivity(R, S))
         # first-row rings (r = 0) as their own CSR over the wake's lines
-        off = wmesh.surface_offsets
-        sl = wmesh.surface_lines
-        rows0 = np.arange(S) * R
-        cnt = (off[rows0 + 1] - off[rows0]).astype(np.uint32)
-        off0 = np.concatenate([[0], np.cumsum(cnt)]).astype(np.uint32)
-        sl0 = np.concatenate([sl[off[r]: off[r + 1]] for r in rows0]).astype(np.uint32)
+        row0 = wake_row0_mesh(wmesh, S, R)
+        off0, sl0 = row0.surface_offsets, row0.surface_lines
         f64 = dict(dtype=torch.float64, device=self.dev)
         self.wake = {
             "S": S, "R": R, "mesh": wmesh, "d": wmesh.device_arrays(),
@@ -212,7 +220,8 @@ class SolverEngine:
                 host.numpy()[...] = np.asarray(src, np.float64).reshape(host.shape)
                 dev.copy_(host, non_blocking=True)
 
-    def assemble(self) -> None:
+    def assemble_body_only(self) -> None:
+        """Control points, normals, RHS for a uniform stream and the body matrix."""
         s = stream_ptr()
         d, P = self.d_body, self.P
         msh = self.mesh
@@ -229,10 +238,19 @@ class SolverEngine:
         _lib.call("pvl_induction_normal", _lib.PVL_F64, msh.n_points, msh.n_lines, ptr(d["lines"]), ptr(self.pos), P,
                   ptr(d["offsets"]), ptr(d["surface_lines"]), P, ptr(self.cps), ptr(self.nrm), self.tol, ptr(self.A),
                   self.N, ws, nb, s)
+
+    def border(self) -> None:
+        """Zero-mean rows/columns of the closed bodies (bordered system)."""
+        if self.m:
+            _lib.call("pvl_border_groups", self.P, self.m, ptr(self.goff), ptr(self.A), self.N, ptr(self.rhs),
+                      stream_ptr())
+
+    def assemble(self) -> None:
+        """The corrected system of this iteration (solver.py:194-220)."""
+        self.assemble_body_only()
         if self.wake is not None and self.iteration > 0:
             self._wake_corrections()
-        if self.m:
-            _lib.call("pvl_border_groups", P, self.m, ptr(self.goff), ptr(self.A), self.N, ptr(self.rhs), s)
+        self.border()
 
     def _wake_corrections(self) -> None:
         """Implicit first row into A, explicit rows into the RHS (wake_models.py:199-223)."""

@@ -275,6 +275,47 @@ def make_checksums(pyvl):
     np.savez_compressed(HERE / "checksums.npz", **data)
 
 
+def make_frames(pyvl):
+    """ReferenceFrame transforms (src/referenceframeobject.c) and the Python frame subclasses."""
+    rng = np.random.default_rng(23)
+    RF = pyvl.ReferenceFrame
+    f0 = RF(rng.normal(size=3), rng.normal(size=3) * 2)
+    f1 = RF(rng.normal(size=3), rng.normal(size=3) * 2, f0)
+    f2 = RF(rng.normal(size=3), (-7.0, 0.3, 11.0), f1)
+    x = rng.normal(size=(5, 4, 3))
+    data = {"x": x}
+    for name, f in (("f0", f0), ("f1", f1), ("f2", f2)):
+        data[f"{name}/angles"] = f.angles
+        data[f"{name}/offset"] = f.offset
+        data[f"{name}/rot"] = f.rotation_matrix
+        data[f"{name}/rot_inv"] = f.rotation_matrix_inverse
+        for fn in ("from_parent_with_offset", "from_parent_without_offset", "to_parent_with_offset",
+                   "to_parent_without_offset", "from_global_with_offset", "from_global_without_offset",
+                   "to_global_with_offset", "to_global_without_offset"):
+            data[f"{name}/{fn}"] = getattr(f, fn)(x)
+        data[f"{name}/rot_x"] = f.rotate_x(2.1).angles
+        data[f"{name}/rot_y"] = f.rotate_y(-1.1).angles
+        data[f"{name}/rot_z"] = f.rotate_z(7.5).angles
+    data["angles_from_rotation"] = RF.angles_from_rotation(f2.rotation_matrix)
+    tr = pyvl.TranslatingReferenceFrame((1, 2, 3), (0.1, 0.2, 0.3), (0.5, -1, 2), f0, 0.5)
+    trt = tr.at_time(2.25)
+    data["translating/offset"] = trt.offset
+    data["translating/angles"] = trt.angles
+    v = np.zeros((7, 3))
+    p = rng.normal(size=(7, 3))
+    trt.add_velocity(p, v)
+    data["translating/p"] = p
+    data["translating/velocity"] = v
+    rr = pyvl.RotorReferenceFrame((0, 1, 0), (0.3, 0.0, 0.2), None, (0.1, 0.2, 2.0), 0.0)
+    rrt = rr.at_time(1.7)
+    data["rotor/offset"] = rrt.offset
+    data["rotor/angles"] = rrt.angles
+    v = np.zeros((7, 3))
+    rrt.add_velocity(p, v)
+    data["rotor/velocity"] = v
+    np.savez_compressed(HERE / "frames.npz", **data)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -286,6 +327,7 @@ def main():
     make_sphere(pyvl)
     make_wedge(pyvl)
     make_checksums(pyvl)
+    make_frames(pyvl)
     for p in sorted(HERE.glob("*.npz")):
         print(p.name, p.stat().st_size)
 
