@@ -155,6 +155,24 @@ int pvl_line_velocity(int precision, uint32_t n_points, uint32_t n_lines, const 
                       const double* pts, const double* normals, double tol, double alpha,
                       double beta, double* out, void* ws, size_t ws_bytes, void* stream);
 
+/* Size of the static device array behind pvl_line_velocity_noalloc (32 MiB). */
+#define PVL_NOALLOC_SCRATCH_BYTES (32u << 20)
+
+/* pvl_line_velocity without a workspace, for callers that cannot allocate device memory
+ * (hosts that own all device memory through their own pool, or loops where an allocation
+ * and the synchronisation of a cudaFree are not acceptable).  No counterpart in the
+ * reference.  Same arguments and result as pvl_line_velocity minus (ws, ws_bytes): the
+ * scratch is a file-scope device array of PVL_NOALLOC_SCRATCH_BYTES that every GPU loading
+ * the library keeps until exit.  Calls needing more scratch than that are rejected with
+ * PVL_ERR_ARG.  All calls share the array, so calls whose kernels overlap on the GPU race;
+ * calls ordered on one stream are safe.  The first call on a device looks up the array's
+ * address (cudaGetSymbolAddress); make it before any stream capture.  Allocates nothing. */
+int pvl_line_velocity_noalloc(int precision, uint32_t n_points, uint32_t n_lines,
+                              const uint32_t* lines, const double* positions,
+                              const double* line_gamma, uint32_t n_pts, const double* pts,
+                              const double* normals, double tol, double alpha, double beta,
+                              double* out, void* stream);
+
 /* Line circulations gamma_line[k] = sum over the rings holding line k of +-gamma_ring
  * (sign from the orientation bit).  With ring_period > 0, rings whose index is a multiple
  * of ring_period are skipped (the implicit first wake row).  Uses pvl_line_ring_map. */

@@ -49,6 +49,7 @@ SIGNATURES = {
     "pvl_line_velocity_workspace": (_Z, [_U, _U, _I]),
     "pvl_line_velocity": (_I, [_I, _U, _U, _P, _P, _P, _U, _P, _P, _D, _D, _D, _P, _P, _Z, _P]),
     "pvl_line_circulation": (_I, [_U, _P, _P, _P, _U, _P, _P]),
+    "pvl_line_velocity_noalloc": (_I, [_I, _U, _U, _P, _P, _P, _U, _P, _P, _D, _D, _D, _P, _P]),
     "pvl_wake_node_velocity_workspace": (_Z, [_U, _U, _U, _I]),
     "pvl_wake_node_velocity": (_I, [_I, _U, _U, _P, _P, _P, _U, _U, _U, _P, _D, _D, _D, _D, _P, _P, _Z, _P]),
     "pvl_wake_fold_implicit": (_I, [_U, _U, _P, _P, _P, _U, _P]),
