@@ -254,6 +254,18 @@ int pvl_group_mean_remove(uint32_t n_groups, const uint32_t* group_offsets, doub
 int pvl_border_groups(uint32_t n, uint32_t m, const uint32_t* group_offsets, double* A,
                       uint32_t lda, double* rhs, void* stream);
 
+/* ------------------------------------------------------------------ tensor cores */
+
+/* C = alpha * A * B + beta * C on the 5th-generation tensor cores (tcgen05, accumulator in
+ * tensor memory): FP32 storage, TF32 multiplication, FP32 accumulation.  Row-major A (M x K),
+ * B (K x N), C (M x N); M and N multiples of 128, K a multiple of 32, leading dimensions
+ * multiples of 4 floats, 16-byte aligned bases.  err (device int32) is set to 1 if an
+ * internal wait timed out.  No reference counterpart: it builds the low-precision
+ * preconditioner that replaces the per-step FP64 factorisation in the mixed path. */
+int pvl_gemm_tf32(uint32_t M, uint32_t N, uint32_t K, float alpha, const float* A, uint32_t lda,
+                  const float* B, uint32_t ldb, float beta, float* C, uint32_t ldc, int32_t* err,
+                  void* stream);
+
 /* ------------------------------------------------------------------ forces */
 
 /* Kutta-Joukowski line forces F_k = (r_end - r_begin) x (0.5 c_k (v_p1 + v_p2)),

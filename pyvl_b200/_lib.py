@@ -62,6 +62,7 @@ SIGNATURES = {
     "pvl_group_mean_remove": (_I, [_U, _P, _P, _P]),
     "pvl_border_groups": (_I, [_U, _U, _P, _P, _U, _P, _P]),
     "pvl_line_forces": (_I, [_U, _P, _P, _P, _P, _P, _P, _P]),
+    "pvl_gemm_tf32": (_I, [_U, _U, _U, ctypes.c_float, _P, _U, _P, _U, ctypes.c_float, _P, _U, _P, _P]),
     "pvl_launch_count": (ctypes.c_ulonglong, []),
     "pvl_fma_probe": (_D, [_I, _U, _U, _P, _P]),
 }
