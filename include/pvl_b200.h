@@ -202,6 +202,16 @@ int pvl_wake_node_velocity(int precision, uint32_t n_points, uint32_t n_lines, c
                            double ux, double uy, double uz, double tol, double* node_vel, void* ws,
                            size_t ws_bytes, void* stream);
 
+/* The rows [row_begin, row_end) of pvl_wake_node_velocity only (same node_vel layout, other
+ * rows untouched), so that near and far rows can run in different precisions.  The
+ * workspace it needs is pvl_line_velocity_workspace(n_lines, 2 n_shed (row_end - row_begin),
+ * precision).  No reference counterpart (the reference evaluates every row in FP64). */
+int pvl_wake_node_velocity_rows(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
+                                const double* positions, const double* line_gamma, uint32_t n_shed,
+                                uint32_t line_rows, uint32_t complete_rows, uint32_t row_begin,
+                                uint32_t row_end, const double* wake_pos, double ux, double uy, double uz,
+                                double tol, double* node_vel, void* ws, size_t ws_bytes, void* stream);
+
 /* Advance wake node rows (explicit Euler) from `old_pos` into `new_pos` (both
  * (n_shed, 2, line_rows + 1, 3)): new[:, :, i+1] = old[:, :, i] + node_vel[:, :, i] * dt for
  * i < complete_rows; row 0 pinned to the bordering body nodes; rows beyond complete_rows
@@ -258,13 +268,64 @@ int pvl_border_groups(uint32_t n, uint32_t m, const uint32_t* group_offsets, dou
 
 /* C = alpha * A * B + beta * C on the 5th-generation tensor cores (tcgen05, accumulator in
  * tensor memory): FP32 storage, TF32 multiplication, FP32 accumulation.  Row-major A (M x K),
- * B (K x N), C (M x N); M and N multiples of 128, K a multiple of 32, leading dimensions
- * multiples of 4 floats, 16-byte aligned bases.  err (device int32) is set to 1 if an
+ * B (K x N), C (M x N); any M and N, K a multiple of 32, leading dimensions multiples of
+ * 4 floats, 16-byte aligned bases.  err (device int32) is set to 1 if an
  * internal wait timed out.  No reference counterpart: it builds the low-precision
  * preconditioner that replaces the per-step FP64 factorisation in the mixed path. */
 int pvl_gemm_tf32(uint32_t M, uint32_t N, uint32_t K, float alpha, const float* A, uint32_t lda,
                   const float* B, uint32_t ldb, float beta, float* C, uint32_t ldc, int32_t* err,
                   void* stream);
+
+/* ------------------------------------------------------------------ mixed-precision solve */
+
+/* y = alpha * A x + beta * y with an FP64 (pvl_gemv_f64) or FP32 (pvl_gemv_f32mat) row-major
+ * matrix; vectors and accumulation FP64.  The FP64 form computes the residuals of the
+ * mixed-precision solve against the FP64 system; the FP32 form applies the approximate
+ * inverse.  No reference counterpart (the reference factorises every step, solver.py:223). */
+int pvl_gemv_f64(uint32_t rows, uint32_t cols, double alpha, const double* A, uint32_t lda,
+                 const double* x, double beta, double* y, void* stream);
+int pvl_gemv_f32mat(uint32_t rows, uint32_t cols, double alpha, const float* M, uint32_t ldm,
+                    const double* x, double beta, double* y, void* stream);
+
+/* One classical Gram-Schmidt pass against the k rows of V (row stride ldv):
+ * c = V w; w -= V^T c; h[0..k) += c.  h needs 2k doubles ([k, 2k) is scratch). */
+int pvl_basis_project(uint32_t n, uint32_t k, const double* V, uint32_t ldv, double* w, double* h,
+                      void* stream);
+
+/* nrm[0] = ||w||_2 and, when v != NULL, v = w / ||w||. */
+int pvl_normalize(uint32_t n, const double* w, double* v, double* nrm, void* stream);
+
+/* x += sum_{i<k} c[i] Z_i (rows of Z, stride ldz; c on the device). */
+int pvl_combine(uint32_t n, uint32_t k, const double* Z, uint32_t ldz, const double* c, double* x,
+                void* stream);
+
+/* b (npad x npad, row stride ldb, FP32) = a (n x n, FP64) padded with the identity: the input
+ * of the FP32 factorisation (whose inverse needs a multiple of 64 rows). */
+int pvl_pad_convert_f32(uint32_t n, const double* a, uint32_t lda, float* b, uint32_t ldb, uint32_t npad,
+                        void* stream);
+
+/* FP32 LU with partial pivoting of the n x n row-major A (in place), the low-precision
+ * factorisation of the mixed path: the FP64 factorisation's panel/pivot/TRSM steps in FP32
+ * and the trailing update on the tensor cores (pvl_gemm_tf32).  ipiv as pvl_lu_factor
+ * (2n int32: LAPACK interchanges, then the row permutation).  lda a multiple of 4 and A
+ * 16-byte aligned; ws of pvl_lu32_workspace(n) bytes, which keeps the inverted diagonal
+ * blocks for pvl_lu32_inverse.  *err = 1 if a tensor-core wait timed out.  Replaces
+ * scipy.linalg.lu_factor (solver.py:223) inside the preconditioner only. */
+size_t pvl_lu32_workspace(uint32_t n);
+int pvl_lu32_factor(uint32_t n, float* A, uint32_t lda, int32_t* ipiv, int32_t* info, int32_t* err,
+                    void* ws, size_t ws_bytes, void* stream);
+
+/* X = U^-1 L^-1 from pvl_lu32_factor's factors (same ws, not modified in between): blocked
+ * triangular inversion, diagonal blocks in FP32 on CUDA cores, rank-64 updates on the
+ * tensor cores.  Y (n x ldy) is scratch.  n a multiple of 64; leading dimensions multiples of
+ * 4, arrays 16-byte aligned.  A^-1 b = X (P b) with (P b)[i] = b[perm[i]]. */
+int pvl_lu32_inverse(uint32_t n, const float* LU, uint32_t lda, float* X, uint32_t ldx, float* Y,
+                     uint32_t ldy, int32_t* err, void* ws, size_t ws_bytes, void* stream);
+
+/* z = X v[perm] (X FP32, v and z FP64, FP64 accumulation): the preconditioner of the mixed
+ * solve applied to a Krylov vector.  v and z must not alias. */
+int pvl_precond_apply(uint32_t n, const float* X, uint32_t ldx, const int32_t* perm, const double* v,
+                      double* z, void* stream);
 
 /* ------------------------------------------------------------------ forces */
 

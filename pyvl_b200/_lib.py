@@ -52,6 +52,8 @@ SIGNATURES = {
     "pvl_line_velocity_noalloc": (_I, [_I, _U, _U, _P, _P, _P, _U, _P, _P, _D, _D, _D, _P, _P]),
     "pvl_wake_node_velocity_workspace": (_Z, [_U, _U, _U, _I]),
     "pvl_wake_node_velocity": (_I, [_I, _U, _U, _P, _P, _P, _U, _U, _U, _P, _D, _D, _D, _D, _P, _P, _Z, _P]),
+    "pvl_wake_node_velocity_rows": (_I, [_I, _U, _U, _P, _P, _P, _U, _U, _U, _U, _U, _P, _D, _D, _D, _D, _P, _P, _Z,
+                                         _P]),
     "pvl_wake_fold_implicit": (_I, [_U, _U, _P, _P, _P, _U, _P]),
     "pvl_wake_advect": (_I, [_U, _U, _U, _P, _P, _D, _P, _P, _P, _P]),
     "pvl_wake_shed": (_I, [_U, _U, _P, _P, _P, _P, _P]),
@@ -63,6 +65,16 @@ SIGNATURES = {
     "pvl_border_groups": (_I, [_U, _U, _P, _P, _U, _P, _P]),
     "pvl_line_forces": (_I, [_U, _P, _P, _P, _P, _P, _P, _P]),
     "pvl_gemm_tf32": (_I, [_U, _U, _U, ctypes.c_float, _P, _U, _P, _U, ctypes.c_float, _P, _U, _P, _P]),
+    "pvl_gemv_f64": (_I, [_U, _U, _D, _P, _U, _P, _D, _P, _P]),
+    "pvl_gemv_f32mat": (_I, [_U, _U, _D, _P, _U, _P, _D, _P, _P]),
+    "pvl_basis_project": (_I, [_U, _U, _P, _U, _P, _P, _P]),
+    "pvl_normalize": (_I, [_U, _P, _P, _P, _P]),
+    "pvl_combine": (_I, [_U, _U, _P, _U, _P, _P, _P]),
+    "pvl_pad_convert_f32": (_I, [_U, _P, _U, _P, _U, _U, _P]),
+    "pvl_lu32_workspace": (_Z, [_U]),
+    "pvl_lu32_factor": (_I, [_U, _P, _U, _P, _P, _P, _P, _Z, _P]),
+    "pvl_lu32_inverse": (_I, [_U, _P, _U, _P, _U, _P, _U, _P, _P, _Z, _P]),
+    "pvl_precond_apply": (_I, [_U, _P, _U, _P, _P, _P, _P]),
     "pvl_launch_count": (ctypes.c_ulonglong, []),
     "pvl_fma_probe": (_D, [_I, _U, _U, _P, _P]),
 }

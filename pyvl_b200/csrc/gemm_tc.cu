@@ -2,8 +2,10 @@
 // and FP32 accumulation (tcgen05.mma kind::tf32, accumulator in tensor memory).
 //
 // Used by the low-precision preconditioner (the approximate inverse of the system matrix,
-// refreshed every few steps).  Row-major A (M x K), B (K x N), C (M x N); M, N multiples of
-// 128, K a multiple of 32, leading dimensions multiples of 4 floats, 16-byte aligned bases.
+// refreshed every few steps, and the trailing update of the FP32 LU).  Row-major A (M x K),
+// B (K x N), C (M x N); any M and N (rows and columns past the edge of a tile are staged as
+// zeros and not stored), K a multiple of 32, leading dimensions multiples of 4 floats,
+// 16-byte aligned bases.
 //
 // One CTA = one 128 x 128 output tile, 128 threads.  The K loop runs over 32-wide tiles in two
 // shared-memory stages of 32 KB (A tile and B^T tile, both stored K-major in the canonical
@@ -165,7 +167,9 @@ __global__ void __launch_bounds__(kThreads) gemm_tf32_kernel(uint32_t M, uint32_
         for (int g = 0; g < (kTile * kKT / 4) / kThreads; ++g) {
             const uint32_t idx = tid + g * kThreads;
             const uint32_t r = idx >> 3, c = idx & 7u;
-            const float4 v = *reinterpret_cast<const float4*>(A + (size_t)(m0 + r) * lda + k0 + 4 * c);
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (m0 + r < M)
+                v = *reinterpret_cast<const float4*>(A + (size_t)(m0 + r) * lda + k0 + 4 * c);
             *reinterpret_cast<float4*>(sa + sw128(r, c)) = v;
         }
         // B^T tile: row n holds B[k0 .. k0+31][n0 + n]; four consecutive k per 16-byte chunk
@@ -173,12 +177,14 @@ __global__ void __launch_bounds__(kThreads) gemm_tf32_kernel(uint32_t M, uint32_
         for (int g = 0; g < (kTile * kKT / 4) / kThreads; ++g) {
             const uint32_t idx = tid + g * kThreads;
             const uint32_t n = idx & (kTile - 1), c = idx >> 7;
-            const float* src = B + (size_t)(k0 + 4 * c) * ldb + n0 + n;
-            float4 v;
-            v.x = src[0];
-            v.y = src[(size_t)ldb];
-            v.z = src[2 * (size_t)ldb];
-            v.w = src[3 * (size_t)ldb];
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (n0 + n < N) {
+                const float* src = B + (size_t)(k0 + 4 * c) * ldb + n0 + n;
+                v.x = src[0];
+                v.y = src[(size_t)ldb];
+                v.z = src[2 * (size_t)ldb];
+                v.w = src[3 * (size_t)ldb];
+            }
             *reinterpret_cast<float4*>(sb + sw128(n, c)) = v;
         }
         // generic-proxy stores -> visible to the tensor core's async proxy
@@ -207,22 +213,36 @@ __global__ void __launch_bounds__(kThreads) gemm_tf32_kernel(uint32_t M, uint32_
         if (tid == 0)
             atomicExch(err, 1);
     } else if (n_kt > 0) {
-        // epilogue: warp w owns TMEM lanes (rows) 32w .. 32w+31
+        // epilogue: warp w owns TMEM lanes (rows) 32w .. 32w+31 (every warp reads TMEM: the
+        // load is warp-collective; rows and columns past the edge are not stored)
         const uint32_t row = m0 + 32 * warp + lane;
-        float* crow = C + (size_t)row * ldc + n0;
+        const bool row_ok = row < M;
+        float* crow = C + (size_t)(row_ok ? row : 0) * ldc + n0;
 #pragma unroll 1
         for (uint32_t c0 = 0; c0 < kTile; c0 += 16) {
             float v[16];
+            __syncwarp();
             tmem_ld16(tmem + ((32u * warp) << 16) + c0, v);
+            if (!row_ok || n0 + c0 >= N)
+                continue;
+            if (n0 + c0 + 16 <= N) {
 #pragma unroll
-            for (int i = 0; i < 16; i += 4) {
-                float4* p = reinterpret_cast<float4*>(crow + c0 + i);
-                float4 o = beta == 0.0f ? make_float4(0.f, 0.f, 0.f, 0.f) : *p;
-                o.x = alpha * v[i] + beta * o.x;
-                o.y = alpha * v[i + 1] + beta * o.y;
-                o.z = alpha * v[i + 2] + beta * o.z;
-                o.w = alpha * v[i + 3] + beta * o.w;
-                *p = o;
+                for (int i = 0; i < 16; i += 4) {
+                    float4* p = reinterpret_cast<float4*>(crow + c0 + i);
+                    float4 o = beta == 0.0f ? make_float4(0.f, 0.f, 0.f, 0.f) : *p;
+                    o.x = alpha * v[i] + beta * o.x;
+                    o.y = alpha * v[i + 1] + beta * o.y;
+                    o.z = alpha * v[i + 2] + beta * o.z;
+                    o.w = alpha * v[i + 3] + beta * o.w;
+                    *p = o;
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < 16; ++i)
+                    if (n0 + c0 + i < N) {
+                        float* p = crow + c0 + i;
+                        *p = alpha * v[i] + (beta == 0.0f ? 0.0f : beta * *p);
+                    }
             }
         }
     }
@@ -243,9 +263,8 @@ extern "C" int pvl_gemm_tf32(uint32_t M, uint32_t N, uint32_t K, float alpha, co
         return PVL_OK;
     if (!A || !B || !C || !err)
         return pvl_fail(PVL_ERR_ARG, "pvl_gemm_tf32: null pointer argument");
-    if (M % kTile || N % kTile || K % kKT)
-        return pvl_fail(PVL_ERR_ARG, "pvl_gemm_tf32: M, N must be multiples of %d and K of %d (got %u, %u, %u)", kTile,
-                        kKT, M, N, K);
+    if (K % kKT)
+        return pvl_fail(PVL_ERR_ARG, "pvl_gemm_tf32: K must be a multiple of %d (got %u)", kKT, K);
     if (lda % 4 || ldb % 4 || ldc % 4 || lda < K || ldb < N || ldc < N)
         return pvl_fail(PVL_ERR_ARG, "pvl_gemm_tf32: leading dimensions must be >= the row length and multiples of 4");
     if (((uintptr_t)A | (uintptr_t)B | (uintptr_t)C) & 15u)
@@ -256,7 +275,7 @@ extern "C" int pvl_gemm_tf32(uint32_t M, uint32_t N, uint32_t K, float alpha, co
         PVL_CUDA_CHECK(cudaFuncSetAttribute(gemm_tf32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
-    dim3 grid(N / kTile, M / kTile);
+    dim3 grid((N + kTile - 1) / kTile, (M + kTile - 1) / kTile);
     if (grid.y > 65535)
         return pvl_fail(PVL_ERR_ARG, "pvl_gemm_tf32: M too large");
     gemm_tf32_kernel<<<grid, kThreads, smem, (cudaStream_t)stream>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc,

@@ -155,14 +155,15 @@ __global__ void __launch_bounds__(kRingThreads) line_matrix_kernel(uint32_t n_li
 }
 
 // N-body sweep: partial[(split*n_pts + p)*3 + c] = sum over this split's segments of gamma_k u_k(p).
-// Point p of the sweep is pts[(p / group) * stride + p % group]: group == stride == n_pts
-// is a plain array; group = complete rows, stride = rows + 1 walks the advecting wake rows.
+// Point p of the sweep is pts[(p / group) * stride + p % group + in_off]: group == stride ==
+// n_pts is a plain array; group = a range of wake rows, stride = rows + 1, in_off = first row
+// walks those rows of every wake strip side.
 template <typename T>
 __global__ void __launch_bounds__(kSumThreads) line_sum_kernel(const Segment<T>* __restrict__ seg, uint32_t n_lines,
                                                                uint32_t lines_per_split,
                                                                const double* __restrict__ pts, uint32_t n_pts,
-                                                               uint32_t group, uint32_t stride, T tol2,
-                                                               T* __restrict__ partial)
+                                                               uint32_t group, uint32_t stride, uint32_t in_off,
+                                                               T tol2, T* __restrict__ partial)
 {
     __shared__ Segment<T> s_seg[kSegTile];
     const uint32_t split = blockIdx.y;
@@ -174,7 +175,7 @@ __global__ void __launch_bounds__(kSumThreads) line_sum_kernel(const Segment<T>*
     for (int t = 0; t < kSumPPT; ++t) {
         const uint32_t p = blockIdx.x * (kSumThreads * kSumPPT) + t * kSumThreads + threadIdx.x;
         const bool ok = p < n_pts;
-        const size_t q = ok ? (size_t)(p / group) * stride + p % group : 0;
+        const size_t q = ok ? (size_t)(p / group) * stride + p % group + in_off : 0;
         px[t] = ok ? T(pts[3 * q]) : T(0);
         py[t] = ok ? T(pts[3 * q + 1]) : T(0);
         pz[t] = ok ? T(pts[3 * q + 2]) : T(0);
@@ -208,14 +209,18 @@ __global__ void __launch_bounds__(kSumThreads) line_sum_kernel(const Segment<T>*
 }
 
 // out = beta * out + alpha * v (+ (ux, uy, uz) for vector output), v = sum of the partials.
+// Point p is written at o = (p / group) * out_stride + p % group + out_off (normals are
+// indexed by p: normal output is always a plain array).
 template <typename T>
 __global__ void reduce_partials_kernel(uint32_t n_pts, uint32_t n_split, const T* __restrict__ partial,
                                        const double* __restrict__ normals, double alpha, double beta, double ux,
-                                       double uy, double uz, double* __restrict__ out)
+                                       double uy, double uz, uint32_t group, uint32_t out_stride, uint32_t out_off,
+                                       double* __restrict__ out)
 {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n_pts)
         return;
+    const size_t op = (size_t)(p / group) * out_stride + p % group + out_off;
     double vx = 0, vy = 0, vz = 0;
     for (uint32_t s = 0; s < n_split; ++s) {
         const T* q = partial + 3 * ((size_t)s * n_pts + p);
@@ -227,7 +232,7 @@ __global__ void reduce_partials_kernel(uint32_t n_pts, uint32_t n_split, const T
         const double v = vx * normals[3 * (size_t)p] + vy * normals[3 * (size_t)p + 1] + vz * normals[3 * (size_t)p + 2];
         out[p] = beta == 0.0 ? alpha * v : beta * out[p] + alpha * v;
     } else {
-        double* o = out + 3 * (size_t)p;
+        double* o = out + 3 * op;
         if (beta == 0.0) {
             o[0] = ux + alpha * vx;
             o[1] = uy + alpha * vy;
@@ -548,14 +553,16 @@ namespace {
 // Shared driver of the N-body sweep: segment table, split sweep, deterministic reduction.
 int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines, const double* positions,
                  const double* line_gamma, uint32_t n_pts, const double* pts, uint32_t group, uint32_t stride,
-                 const double* normals, double tol, double alpha, double beta, double ux, double uy, double uz,
-                 double* out, void* ws, size_t ws_bytes, cudaStream_t st, const char* who)
+                 uint32_t in_off, uint32_t out_stride, uint32_t out_off, const double* normals, double tol,
+                 double alpha, double beta, double ux, double uy, double uz, double* out, void* ws, size_t ws_bytes,
+                 cudaStream_t st, const char* who)
 {
     if (precision != PVL_F64 && precision != PVL_F32)
         return pvl_fail(PVL_ERR_ARG, "%s: unknown precision %d", who, precision);
     if (n_lines == 0) {
         reduce_partials_kernel<double><<<blocks_for(n_pts, 256), 256, 0, st>>>(n_pts, 0, nullptr, normals, alpha,
-                                                                               beta, ux, uy, uz, out);
+                                                                               beta, ux, uy, uz, group, out_stride,
+                                                                               out_off, out);
         PVL_LAUNCH_CHECK();
         return PVL_OK;
     }
@@ -574,21 +581,21 @@ int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint3
         auto* part = reinterpret_cast<double*>(base + pvl_segments_workspace(n_lines, PVL_F64));
         if (int r = prep_segments<double>(n_points, n_lines, lines, positions, line_gamma, tol, seg, st))
             return r;
-        line_sum_kernel<double><<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride,
+        line_sum_kernel<double><<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off,
                                                               tol * tol, part);
         PVL_LAUNCH_CHECK();
-        reduce_partials_kernel<double><<<blocks_for(n_pts, 256), 256, 0, st>>>(n_pts, n_split_used, part, normals,
-                                                                               alpha, beta, ux, uy, uz, out);
+        reduce_partials_kernel<double><<<blocks_for(n_pts, 256), 256, 0, st>>>(
+            n_pts, n_split_used, part, normals, alpha, beta, ux, uy, uz, group, out_stride, out_off, out);
     } else {
         auto* seg = reinterpret_cast<Segment<float>*>(base);
         auto* part = reinterpret_cast<float*>(base + pvl_segments_workspace(n_lines, PVL_F32));
         if (int r = prep_segments<float>(n_points, n_lines, lines, positions, line_gamma, tol, seg, st))
             return r;
-        line_sum_kernel<float><<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride,
+        line_sum_kernel<float><<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off,
                                                              float(tol * tol), part);
         PVL_LAUNCH_CHECK();
-        reduce_partials_kernel<float><<<blocks_for(n_pts, 256), 256, 0, st>>>(n_pts, n_split_used, part, normals,
-                                                                              alpha, beta, ux, uy, uz, out);
+        reduce_partials_kernel<float><<<blocks_for(n_pts, 256), 256, 0, st>>>(
+            n_pts, n_split_used, part, normals, alpha, beta, ux, uy, uz, group, out_stride, out_off, out);
     }
     PVL_LAUNCH_CHECK();
     return PVL_OK;
@@ -604,8 +611,8 @@ extern "C" int pvl_line_velocity(int precision, uint32_t n_points, uint32_t n_li
     if (n_pts == 0)
         return PVL_OK;
     PVL_REQUIRE(pts); PVL_REQUIRE(out);
-    return run_line_sum(precision, n_points, n_lines, lines, positions, line_gamma, n_pts, pts, n_pts, n_pts, normals,
-                        tol, alpha, beta, 0.0, 0.0, 0.0, out, ws, ws_bytes, (cudaStream_t)stream,
+    return run_line_sum(precision, n_points, n_lines, lines, positions, line_gamma, n_pts, pts, n_pts, n_pts, 0,
+                        n_pts, 0, normals, tol, alpha, beta, 0.0, 0.0, 0.0, out, ws, ws_bytes, (cudaStream_t)stream,
                         "pvl_line_velocity");
 }
 
@@ -615,24 +622,40 @@ extern "C" size_t pvl_wake_node_velocity_workspace(uint32_t n_lines, uint32_t n_
     return pvl_line_velocity_workspace(n_lines, 2 * n_shed * complete_rows, precision);
 }
 
+extern "C" int pvl_wake_node_velocity_rows(int precision, uint32_t n_points, uint32_t n_lines,
+                                           const uint32_t* lines, const double* positions, const double* line_gamma,
+                                           uint32_t n_shed, uint32_t line_rows, uint32_t complete_rows,
+                                           uint32_t row_begin, uint32_t row_end, const double* wake_pos, double ux,
+                                           double uy, double uz, double tol, double* node_vel, void* ws,
+                                           size_t ws_bytes, void* stream)
+{
+    if (complete_rows > line_rows)
+        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity: complete_rows %u > line_rows %u", complete_rows,
+                        line_rows);
+    if (row_begin > row_end || row_end > complete_rows)
+        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity_rows: rows [%u, %u) outside [0, %u)", row_begin, row_end,
+                        complete_rows);
+    if (n_shed == 0 || row_end == row_begin)
+        return PVL_OK;
+    PVL_REQUIRE(wake_pos); PVL_REQUIRE(node_vel);
+    const uint32_t group = row_end - row_begin;
+    const uint64_t n_pts = 2ull * n_shed * group;
+    if (n_pts > 0xFFFFFFFFull)
+        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity: too many nodes");
+    return run_line_sum(precision, n_points, n_lines, lines, positions, line_gamma, (uint32_t)n_pts, wake_pos, group,
+                        line_rows + 1, row_begin, complete_rows, row_begin, nullptr, tol, 1.0, 0.0, ux, uy, uz,
+                        node_vel, ws, ws_bytes, (cudaStream_t)stream, "pvl_wake_node_velocity");
+}
+
 extern "C" int pvl_wake_node_velocity(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
                                       const double* positions, const double* line_gamma, uint32_t n_shed,
                                       uint32_t line_rows, uint32_t complete_rows, const double* wake_pos, double ux,
                                       double uy, double uz, double tol, double* node_vel, void* ws, size_t ws_bytes,
                                       void* stream)
 {
-    if (n_shed == 0 || complete_rows == 0)
-        return PVL_OK;
-    if (complete_rows > line_rows)
-        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity: complete_rows %u > line_rows %u", complete_rows,
-                        line_rows);
-    PVL_REQUIRE(wake_pos); PVL_REQUIRE(node_vel);
-    const uint64_t n_pts = 2ull * n_shed * complete_rows;
-    if (n_pts > 0xFFFFFFFFull)
-        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity: too many nodes");
-    return run_line_sum(precision, n_points, n_lines, lines, positions, line_gamma, (uint32_t)n_pts, wake_pos,
-                        complete_rows, line_rows + 1, nullptr, tol, 1.0, 0.0, ux, uy, uz, node_vel, ws, ws_bytes,
-                        (cudaStream_t)stream, "pvl_wake_node_velocity");
+    return pvl_wake_node_velocity_rows(precision, n_points, n_lines, lines, positions, line_gamma, n_shed, line_rows,
+                                       complete_rows, 0, complete_rows, wake_pos, ux, uy, uz, tol, node_vel, ws,
+                                       ws_bytes, stream);
 }
 
 extern "C" int pvl_line_circulation(uint32_t n_lines, const uint32_t* map_offsets, const uint32_t* map_entries,

@@ -99,28 +99,29 @@ __global__ void init_perm_kernel(uint32_t n, int32_t* __restrict__ perm)
 // thread checks this for its own row, and any violation (or a zero/NaN pivot) marks the panel.
 // Slab rows are backed up and overwritten in place; the factored top block goes to `top_out`
 // (committed by panel_pivot_kernel) so that no CTA can read a half-written top block.
+template <typename T>
 __global__ void __launch_bounds__(2 * kSlabRows) panel_spec_kernel(uint32_t n, uint32_t k0, uint32_t nb,
-                                                                   double* __restrict__ A, uint32_t lda,
-                                                                   double* __restrict__ backup,
-                                                                   double* __restrict__ top_out,
+                                                                   T* __restrict__ A, uint32_t lda,
+                                                                   T* __restrict__ backup,
+                                                                   T* __restrict__ top_out,
                                                                    int32_t* __restrict__ reject)
 {
-    __shared__ double U[NB][NB + 1];
-    __shared__ double s_rcp[NB];
+    __shared__ T U[NB][NB + 1];
+    __shared__ T s_rcp[NB];
     const uint32_t tid = threadIdx.x;
     const bool is_top = tid < NB;
     const uint32_t r_begin = k0 + nb + blockIdx.x * kSlabRows;
     // global row of this thread (top: k0 + tid, slab: r_begin + tid - 64)
     const uint32_t grow = is_top ? k0 + tid : r_begin + (tid - NB);
     const bool valid = is_top ? tid < nb : grow < n;
-    double row[NB];
+    T row[NB];
 #pragma unroll
     for (int c = 0; c < NB; ++c) {
-        double v = 0.0;
+        T v = T(0);
         if (valid && (uint32_t)c < nb)
             v = A[(size_t)grow * lda + k0 + c];
         else if (is_top && !valid && (uint32_t)c == tid)
-            v = 1.0;  // unit row standing in for a missing top row
+            v = T(1);  // unit row standing in for a missing top row
         row[c] = v;
     }
     if (!is_top && valid)
@@ -135,15 +136,15 @@ __global__ void __launch_bounds__(2 * kSlabRows) panel_spec_kernel(uint32_t n, u
 #pragma unroll
             for (int c = j; c < NB; ++c)
                 U[j][c] = row[c];
-            s_rcp[j] = 1.0 / row[j];
-            bad |= !(fabs(row[j]) > 0.0);
+            s_rcp[j] = T(1) / row[j];
+            bad |= !(fabs(row[j]) > T(0));
         }
         __syncthreads();
         const bool act = is_top ? tid > (uint32_t)j : valid;
         if (act) {
-            const double v = row[j];
+            const T v = row[j];
             bad |= !(fabs(v) <= fabs(U[j][j]));
-            const double x = v * s_rcp[j];
+            const T x = v * s_rcp[j];
             row[j] = x;
 #pragma unroll
             for (int c = j + 1; c < NB; ++c)
@@ -167,18 +168,19 @@ __global__ void __launch_bounds__(2 * kSlabRows) panel_spec_kernel(uint32_t n, u
 }
 
 // ---------------------------------------------------------------- 3. accept or pivot
-__global__ void __launch_bounds__(1024) panel_pivot_kernel(uint32_t n, uint32_t k0, uint32_t nb, double* __restrict__ A,
-                                                           uint32_t lda, const double* __restrict__ backup,
-                                                           const double* __restrict__ top_out,
+template <typename T>
+__global__ void __launch_bounds__(1024) panel_pivot_kernel(uint32_t n, uint32_t k0, uint32_t nb, T* __restrict__ A,
+                                                           uint32_t lda, const T* __restrict__ backup,
+                                                           const T* __restrict__ top_out,
                                                            const int32_t* __restrict__ reject,
                                                            int32_t* __restrict__ ok, uint32_t panel,
                                                            int32_t* __restrict__ ipiv, int32_t* __restrict__ perm,
                                                            int32_t* __restrict__ info)
 {
-    __shared__ double s_val[32];
+    __shared__ T s_val[32];
     __shared__ uint32_t s_idx[32];
     __shared__ uint32_t s_piv;
-    __shared__ double s_prow[NB];
+    __shared__ T s_prow[NB];
     const int bad = reject[panel];
     if (!bad) {
         if (threadIdx.x == 0)
@@ -203,17 +205,17 @@ __global__ void __launch_bounds__(1024) panel_pivot_kernel(uint32_t n, uint32_t 
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (uint32_t j = 0; j < nb; ++j) {
         const uint32_t col = k0 + j;
-        double best = -1.0;
+        T best = T(-1);
         uint32_t bidx = 0xFFFFFFFFu;
         for (uint32_t r = col + threadIdx.x; r < n; r += blockDim.x) {
-            const double v = fabs(A[(size_t)r * lda + col]);
+            const T v = fabs(A[(size_t)r * lda + col]);
             if (v > best) {
                 best = v;
                 bidx = r;
             }
         }
         for (int o = 16; o > 0; o >>= 1) {
-            const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+            const T ov = __shfl_xor_sync(0xffffffffu, best, o);
             const uint32_t oi = __shfl_xor_sync(0xffffffffu, bidx, o);
             if (ov > best || (ov == best && oi < bidx)) {
                 best = ov;
@@ -226,7 +228,7 @@ __global__ void __launch_bounds__(1024) panel_pivot_kernel(uint32_t n, uint32_t 
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            double b = -1.0;
+            T b = T(-1);
             uint32_t bi = col;
             for (uint32_t w = 0; w < blockDim.x / 32; ++w)
                 if (s_val[w] > b || (s_val[w] == b && s_idx[w] < bi)) {
@@ -245,7 +247,7 @@ __global__ void __launch_bounds__(1024) panel_pivot_kernel(uint32_t n, uint32_t 
         const uint32_t p = s_piv;
         if (p != col)
             for (uint32_t c = threadIdx.x; c < nb; c += blockDim.x) {
-                const double a = A[(size_t)col * lda + k0 + c];
+                const T a = A[(size_t)col * lda + k0 + c];
                 A[(size_t)col * lda + k0 + c] = A[(size_t)p * lda + k0 + c];
                 A[(size_t)p * lda + k0 + c] = a;
             }
@@ -253,17 +255,17 @@ __global__ void __launch_bounds__(1024) panel_pivot_kernel(uint32_t n, uint32_t 
         for (uint32_t c = threadIdx.x; c < nb; c += blockDim.x)
             s_prow[c] = A[(size_t)col * lda + k0 + c];
         __syncthreads();
-        const double piv = s_prow[j];
-        if (piv == 0.0) {
+        const T piv = s_prow[j];
+        if (piv == T(0)) {
             if (threadIdx.x == 0)
                 atomicCAS(info, 0, (int32_t)(col + 1));
             __syncthreads();
             continue;
         }
-        const double rcp = 1.0 / piv;
+        const T rcp = T(1) / piv;
         for (uint32_t r = col + 1 + threadIdx.x; r < n; r += blockDim.x) {
-            double* row = A + (size_t)r * lda + k0;
-            const double l = row[j] * rcp;
+            T* row = A + (size_t)r * lda + k0;
+            const T l = row[j] * rcp;
             row[j] = l;
             for (uint32_t c = j + 1; c < nb; ++c)
                 row[c] -= l * s_prow[c];
@@ -279,14 +281,16 @@ __global__ void __launch_bounds__(1024) panel_pivot_kernel(uint32_t n, uint32_t 
 // registers during the substitution.
 constexpr int kTrsmCols = 128;
 
+template <typename T>
 __global__ void __launch_bounds__(kTrsmCols, 1) trsm_kernel(uint32_t n, uint32_t k0, uint32_t nb,
-                                                            double* __restrict__ A, uint32_t lda,
+                                                            T* __restrict__ A, uint32_t lda,
                                                             const int32_t* __restrict__ ok, uint32_t panel,
                                                             const int32_t* __restrict__ ipiv)
 {
-    extern __shared__ double tsm[];
-    double(*L)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(tsm);                   // [NB][NB + 1]
-    double(*X)[kTrsmCols + 1] = reinterpret_cast<double(*)[kTrsmCols + 1]>(tsm + NB * (NB + 1));  // [NB][129]
+    extern __shared__ double tsm_raw[];
+    T* tsm = reinterpret_cast<T*>(tsm_raw);
+    T(*L)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(tsm);                        // [NB][NB + 1]
+    T(*X)[kTrsmCols + 1] = reinterpret_cast<T(*)[kTrsmCols + 1]>(tsm + NB * (NB + 1));  // [NB][129]
     const bool swapped = !ok[panel];
     const uint32_t t = blockIdx.x * kTrsmCols + threadIdx.x;
     const uint32_t n_out = n - nb;
@@ -295,7 +299,7 @@ __global__ void __launch_bounds__(kTrsmCols, 1) trsm_kernel(uint32_t n, uint32_t
         for (uint32_t j = 0; j < nb; ++j) {
             const uint32_t r1 = k0 + j, r2 = (uint32_t)ipiv[k0 + j];
             if (r1 != r2) {
-                const double a = A[(size_t)r1 * lda + col];
+                const T a = A[(size_t)r1 * lda + col];
                 A[(size_t)r1 * lda + col] = A[(size_t)r2 * lda + col];
                 A[(size_t)r2 * lda + col] = a;
             }
@@ -307,22 +311,22 @@ __global__ void __launch_bounds__(kTrsmCols, 1) trsm_kernel(uint32_t n, uint32_t
     __syncthreads();  // swaps of this CTA's columns are visible before staging
     for (uint32_t e = threadIdx.x; e < NB * NB; e += kTrsmCols) {
         const uint32_t r = e / NB, c = e % NB;
-        L[r][c] = (r < nb && c < nb) ? A[(size_t)(k0 + r) * lda + k0 + c] : 0.0;
+        L[r][c] = (r < nb && c < nb) ? A[(size_t)(k0 + r) * lda + k0 + c] : T(0);
     }
     for (uint32_t e = threadIdx.x; e < NB * kTrsmCols; e += kTrsmCols) {
         const uint32_t r = e / kTrsmCols, c = e % kTrsmCols;
         const uint32_t tt = c_first + c;
         const uint32_t cc = tt < k0 ? tt : tt + nb;
-        X[r][c] = (r < nb && tt < n_out && cc >= k0 + nb) ? A[(size_t)(k0 + r) * lda + cc] : 0.0;
+        X[r][c] = (r < nb && tt < n_out && cc >= k0 + nb) ? A[(size_t)(k0 + r) * lda + cc] : T(0);
     }
     __syncthreads();
-    double x[NB];
+    T x[NB];
 #pragma unroll
     for (int r = 0; r < NB; ++r)
         x[r] = X[r][threadIdx.x];
 #pragma unroll
     for (int q = 0; q < NB - 1; ++q) {
-        const double xq = x[q];
+        const T xq = x[q];
 #pragma unroll
         for (int r = q + 1; r < NB; ++r)
             x[r] -= L[r][q] * xq;
@@ -433,27 +437,28 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_update_kernel(uint32_t n, u
 // substitution), threads 64..127 column c of U_bb^-1 (backward substitution), each column
 // held in registers.  A partial last block is padded with identity.  The wavefront solves
 // then apply each diagonal block as one parallel matrix-vector product.
-__global__ void __launch_bounds__(2 * kRB, 1) diag_inverse_kernel(uint32_t n, const double* __restrict__ M,
-                                                                  uint32_t lda, double* __restrict__ inv)
+template <typename T>
+__global__ void __launch_bounds__(2 * kRB, 1) diag_inverse_kernel(uint32_t n, const T* __restrict__ M,
+                                                                  uint32_t lda, T* __restrict__ inv)
 {
-    __shared__ double D[kRB][kRB + 1];
+    __shared__ T D[kRB][kRB + 1];
     const uint32_t b = blockIdx.x, r0 = b * kRB;
     const uint32_t rows = min((uint32_t)kRB, n - r0);
     for (uint32_t e = threadIdx.x; e < kRB * kRB; e += blockDim.x) {
         const uint32_t r = e / kRB, c = e % kRB;
-        D[r][c] = (r < rows && c < rows) ? M[(size_t)(r0 + r) * lda + r0 + c] : (r == c ? 1.0 : 0.0);
+        D[r][c] = (r < rows && c < rows) ? M[(size_t)(r0 + r) * lda + r0 + c] : (r == c ? T(1) : T(0));
     }
     __syncthreads();
     const bool lower = threadIdx.x < kRB;
     const int c = (int)(threadIdx.x & (kRB - 1));
-    double y[kRB];
+    T y[kRB];
     if (lower) {
 #pragma unroll
         for (int r = 0; r < kRB; ++r)
-            y[r] = r == c ? 1.0 : 0.0;
+            y[r] = r == c ? T(1) : T(0);
 #pragma unroll
         for (int q = 0; q < kRB - 1; ++q) {
-            const double yq = y[q];
+            const T yq = y[q];
 #pragma unroll
             for (int r = q + 1; r < kRB; ++r)
                 y[r] -= D[r][q] * yq;
@@ -461,17 +466,17 @@ __global__ void __launch_bounds__(2 * kRB, 1) diag_inverse_kernel(uint32_t n, co
     } else {
 #pragma unroll
         for (int r = 0; r < kRB; ++r)
-            y[r] = r == c ? 1.0 : 0.0;
+            y[r] = r == c ? T(1) : T(0);
 #pragma unroll
         for (int q = kRB - 1; q >= 0; --q) {
-            const double yq = y[q] / D[q][q];
+            const T yq = y[q] / D[q][q];
             y[q] = yq;
 #pragma unroll
             for (int r = 0; r < q; ++r)
                 y[r] -= D[r][q] * yq;
         }
     }
-    double* out = inv + ((size_t)b * 2 + (lower ? 0 : 1)) * kRB * kRB;
+    T* out = inv + ((size_t)b * 2 + (lower ? 0 : 1)) * kRB * kRB;
 #pragma unroll
     for (int r = 0; r < kRB; ++r)
         out[(size_t)r * kRB + c] = y[r];
@@ -611,7 +616,7 @@ extern "C" int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv,
     if (!attr_done) {
         PVL_CUDA_CHECK(cudaFuncSetAttribute(gemm_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)gemm_smem));
-        PVL_CUDA_CHECK(cudaFuncSetAttribute(trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        PVL_CUDA_CHECK(cudaFuncSetAttribute(trsm_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)trsm_smem));
         attr_done = true;
     }
@@ -626,13 +631,15 @@ extern "C" int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv,
         const uint32_t nb = std::min<uint32_t>(NB, n - k0);
         const uint32_t below = n - k0 - nb;
         const uint32_t ctas = std::max<uint32_t>(1, (below + kSlabRows - 1) / kSlabRows);
-        panel_spec_kernel<<<ctas, 2 * kSlabRows, 0, st>>>(n, k0, nb, A, lda, w.backup, w.top_out, w.reject + p);
+        panel_spec_kernel<double><<<ctas, 2 * kSlabRows, 0, st>>>(n, k0, nb, A, lda, w.backup, w.top_out,
+                                                                  w.reject + p);
         PVL_LAUNCH_CHECK();
-        panel_pivot_kernel<<<1, 1024, 0, st>>>(n, k0, nb, A, lda, w.backup, w.top_out, w.reject, w.ok, p, ipiv, perm,
-                                               info);
+        panel_pivot_kernel<double><<<1, 1024, 0, st>>>(n, k0, nb, A, lda, w.backup, w.top_out, w.reject, w.ok, p, ipiv,
+                                                       perm, info);
         PVL_LAUNCH_CHECK();
         if (n > nb) {
-            trsm_kernel<<<blocks_for(n - nb, kTrsmCols), kTrsmCols, trsm_smem, st>>>(n, k0, nb, A, lda, w.ok, p, ipiv);
+            trsm_kernel<double><<<blocks_for(n - nb, kTrsmCols), kTrsmCols, trsm_smem, st>>>(n, k0, nb, A, lda, w.ok, p,
+                                                                                           ipiv);
             PVL_LAUNCH_CHECK();
         }
         if (below > 0) {
@@ -641,7 +648,7 @@ extern "C" int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv,
             PVL_LAUNCH_CHECK();
         }
     }
-    diag_inverse_kernel<<<(n + kRB - 1) / kRB, 2 * kRB, 0, st>>>(n, A, lda, w.inv);
+    diag_inverse_kernel<double><<<(n + kRB - 1) / kRB, 2 * kRB, 0, st>>>(n, A, lda, w.inv);
     PVL_LAUNCH_CHECK();
     return PVL_OK;
 }
@@ -678,5 +685,201 @@ extern "C" int pvl_lu_solve(uint32_t n, const double* LU, uint32_t lda, const in
         pvl_count_launch();
     }
     PVL_CUDA_CHECK(cudaMemcpyAsync(b, w.tmp, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    return PVL_OK;
+}
+
+// ================================================================ FP32 LU (TF32 trailing update)
+// The low-precision factorisation behind the mixed path's preconditioner.  Same panel,
+// pivot and TRSM kernels as the FP64 factorisation (instantiated for float), with the
+// trailing update A22 -= L21 U12 on the tensor cores (pvl_gemm_tf32: TF32 products, FP32
+// accumulation).  The explicit inverse U^-1 L^-1 is then formed from the factors by blocked
+// triangular inversion: the 64 x 64 diagonal-block products on CUDA cores in FP32, every
+// rank-64 update on the tensor cores.  Applying the preconditioner is then one FP32
+// matrix-vector product per Krylov iteration instead of two latency-bound triangular solves.
+namespace {
+
+// out[r][j] = sum_k D[r][k] in[k][j] for the 64 rows of a block (FP32, CUDA cores: the
+// diagonal blocks of the inverse carry the O(1) entries whose TF32 rounding would dominate
+// the preconditioner's error).  One thread per column, D staged in shared memory.
+__global__ void __launch_bounds__(128) block_apply_kernel(uint32_t cols, const float* __restrict__ D,
+                                                          const float* __restrict__ in, uint32_t ldi,
+                                                          float* __restrict__ out, uint32_t ldo)
+{
+    __shared__ float sD[kRB][kRB];
+    for (uint32_t e = threadIdx.x; e < kRB * kRB; e += blockDim.x)
+        sD[e / kRB][e % kRB] = D[e];
+    __syncthreads();
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= cols)
+        return;
+    float x[kRB];
+#pragma unroll
+    for (int k = 0; k < kRB; ++k)
+        x[k] = in[(size_t)k * ldi + j];
+#pragma unroll 4
+    for (int r = 0; r < kRB; ++r) {
+        float s = 0.0f;
+#pragma unroll
+        for (int k = 0; k < kRB; ++k)
+            s = fmaf(sD[r][k], x[k], s);
+        out[(size_t)r * ldo + j] = s;
+    }
+}
+
+__global__ void set_identity_kernel(uint32_t n, float* __restrict__ X, uint32_t ldx)
+{
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)n * n)
+        return;
+    const uint32_t r = (uint32_t)(t / n), c = (uint32_t)(t % n);
+    X[(size_t)r * ldx + c] = r == c ? 1.0f : 0.0f;
+}
+
+// z = alpha * X v[perm] + beta * z: the preconditioner applied to an FP64 vector (FP32 matrix,
+// FP64 accumulation), one warp per row.
+__global__ void __launch_bounds__(256) precond_apply_kernel(uint32_t n, const float* __restrict__ X, uint32_t ldx,
+                                                            const int32_t* __restrict__ perm,
+                                                            const double* __restrict__ v, double* __restrict__ z)
+{
+    const uint32_t r = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (r >= n)
+        return;
+    const float* row = X + (size_t)r * ldx;
+    double s = 0.0;
+    for (uint32_t j = lane; j < n; j += 32) {
+        const uint32_t q = (uint32_t)perm[j];
+        if (q < n)  // a valid factorisation never maps outside [0, n)
+            s += (double)row[j] * v[q];
+    }
+    for (int o = 16; o > 0; o >>= 1)
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0)
+        z[r] = s;
+}
+
+}  // namespace
+
+extern "C" int pvl_gemm_tf32(uint32_t M, uint32_t N, uint32_t K, float alpha, const float* A, uint32_t lda,
+                             const float* B, uint32_t ldb, float beta, float* C, uint32_t ldc, int32_t* err,
+                             void* stream);
+
+extern "C" size_t pvl_lu32_workspace(uint32_t n) { return lu_ws_bytes(n); }
+
+extern "C" int pvl_lu32_factor(uint32_t n, float* A, uint32_t lda, int32_t* ipiv, int32_t* info, int32_t* err,
+                               void* ws, size_t ws_bytes, void* stream)
+{
+    if (n == 0)
+        return PVL_OK;
+    if (!A || !ipiv || !info || !err || !ws)
+        return pvl_fail(PVL_ERR_ARG, "pvl_lu32_factor: null pointer argument");
+    if (lda < n || lda % 4 || ((uintptr_t)A & 15u))
+        return pvl_fail(PVL_ERR_ARG, "pvl_lu32_factor: lda must be >= n and a multiple of 4, A 16-byte aligned");
+    if (ws_bytes < lu_ws_bytes(n))
+        return pvl_fail(PVL_ERR_ALLOC, "pvl_lu32_factor: workspace %zu < %zu", ws_bytes, lu_ws_bytes(n));
+    cudaStream_t st = (cudaStream_t)stream;
+    LuWs w = carve(ws, n);
+    float* backup = reinterpret_cast<float*>(w.backup);
+    float* top_out = reinterpret_cast<float*>(w.top_out);
+    float* inv = reinterpret_cast<float*>(w.inv);
+    const size_t trsm_smem = (size_t)(NB * (NB + 1) + NB * (kTrsmCols + 1)) * sizeof(float);
+    static bool attr_done = false;
+    if (!attr_done) {
+        PVL_CUDA_CHECK(cudaFuncSetAttribute(trsm_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)trsm_smem));
+        attr_done = true;
+    }
+    int32_t* perm = ipiv + n;
+    PVL_CUDA_CHECK(cudaMemsetAsync(info, 0, sizeof(int32_t), st));
+    PVL_CUDA_CHECK(cudaMemsetAsync(err, 0, sizeof(int32_t), st));
+    init_perm_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, perm);
+    PVL_LAUNCH_CHECK();
+    const uint32_t n_panels = (n + NB - 1) / NB;
+    PVL_CUDA_CHECK(cudaMemsetAsync(w.reject, 0, sizeof(int32_t) * (n_panels + 1), st));
+    for (uint32_t p = 0; p < n_panels; ++p) {
+        const uint32_t k0 = p * NB;
+        const uint32_t nb = std::min<uint32_t>(NB, n - k0);
+        const uint32_t below = n - k0 - nb;
+        const uint32_t ctas = std::max<uint32_t>(1, (below + kSlabRows - 1) / kSlabRows);
+        panel_spec_kernel<float><<<ctas, 2 * kSlabRows, 0, st>>>(n, k0, nb, A, lda, backup, top_out, w.reject + p);
+        PVL_LAUNCH_CHECK();
+        panel_pivot_kernel<float><<<1, 1024, 0, st>>>(n, k0, nb, A, lda, backup, top_out, w.reject, w.ok, p, ipiv,
+                                                      perm, info);
+        PVL_LAUNCH_CHECK();
+        if (n > nb) {
+            trsm_kernel<float><<<blocks_for(n - nb, kTrsmCols), kTrsmCols, trsm_smem, st>>>(n, k0, nb, A, lda, w.ok, p,
+                                                                                          ipiv);
+            PVL_LAUNCH_CHECK();
+        }
+        if (below > 0) {
+            // every panel with rows below it is a full NB = 64 wide, so K = 64 (a multiple of 32)
+            float* a22 = A + (size_t)(k0 + nb) * lda + k0 + nb;
+            if (int r = pvl_gemm_tf32(below, below, nb, -1.0f, A + (size_t)(k0 + nb) * lda + k0, lda,
+                                      A + (size_t)k0 * lda + k0 + nb, lda, 1.0f, a22, lda, err, stream))
+                return r;
+        }
+    }
+    diag_inverse_kernel<float><<<(n + kRB - 1) / kRB, 2 * kRB, 0, st>>>(n, A, lda, inv);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_lu32_inverse(uint32_t n, const float* LU, uint32_t lda, float* X, uint32_t ldx, float* Y,
+                                uint32_t ldy, int32_t* err, void* ws, size_t ws_bytes, void* stream)
+{
+    if (n == 0)
+        return PVL_OK;
+    if (!LU || !X || !Y || !err || !ws)
+        return pvl_fail(PVL_ERR_ARG, "pvl_lu32_inverse: null pointer argument");
+    if (n % kRB)
+        return pvl_fail(PVL_ERR_ARG, "pvl_lu32_inverse: n = %u must be a multiple of %d", n, kRB);
+    if (lda < n || ldx < n || ldy < n || lda % 4 || ldx % 4 || ldy % 4 ||
+        (((uintptr_t)LU | (uintptr_t)X | (uintptr_t)Y) & 15u))
+        return pvl_fail(PVL_ERR_ARG, "pvl_lu32_inverse: leading dimensions must be >= n and multiples of 4, "
+                                     "arrays 16-byte aligned");
+    if (ws_bytes < lu_ws_bytes(n))
+        return pvl_fail(PVL_ERR_ALLOC, "pvl_lu32_inverse: workspace too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    LuWs w = carve(ws, n);
+    const float* inv = reinterpret_cast<const float*>(w.inv);  // written by pvl_lu32_factor
+    const uint32_t nblk = n / kRB;
+    // forward: Y = L^-1, with X as the working right-hand side (starts as I)
+    set_identity_kernel<<<blocks_for((size_t)n * n, 256), 256, 0, st>>>(n, X, ldx);
+    PVL_LAUNCH_CHECK();
+    PVL_CUDA_CHECK(cudaMemset2DAsync(Y, (size_t)ldy * sizeof(float), 0, (size_t)n * sizeof(float), n, st));
+    for (uint32_t k = 0; k < nblk; ++k) {
+        const uint32_t r0 = k * kRB, cols = r0 + kRB;  // L^-1 is zero right of the diagonal block
+        block_apply_kernel<<<blocks_for(cols, 128), 128, 0, st>>>(cols, inv + (size_t)k * 2 * kRB * kRB,
+                                                                 X + (size_t)r0 * ldx, ldx, Y + (size_t)r0 * ldy, ldy);
+        PVL_LAUNCH_CHECK();
+        if (cols < n)
+            if (int r = pvl_gemm_tf32(n - cols, cols, kRB, -1.0f, LU + (size_t)cols * lda + r0, lda,
+                                      Y + (size_t)r0 * ldy, ldy, 1.0f, X + (size_t)cols * ldx, ldx, err, stream))
+                return r;
+    }
+    // backward: X = U^-1 Y, with Y as the working right-hand side
+    for (uint32_t kk = nblk; kk-- > 0;) {
+        const uint32_t r0 = kk * kRB;
+        block_apply_kernel<<<blocks_for(n, 128), 128, 0, st>>>(n, inv + ((size_t)kk * 2 + 1) * kRB * kRB,
+                                                              Y + (size_t)r0 * ldy, ldy, X + (size_t)r0 * ldx, ldx);
+        PVL_LAUNCH_CHECK();
+        if (r0 > 0)
+            if (int r = pvl_gemm_tf32(r0, n, kRB, -1.0f, LU + r0, lda, X + (size_t)r0 * ldx, ldx, 1.0f, Y, ldy, err,
+                                      stream))
+                return r;
+    }
+    return PVL_OK;
+}
+
+extern "C" int pvl_precond_apply(uint32_t n, const float* X, uint32_t ldx, const int32_t* perm, const double* v,
+                                 double* z, void* stream)
+{
+    if (n == 0)
+        return PVL_OK;
+    if (!X || !perm || !v || !z)
+        return pvl_fail(PVL_ERR_ARG, "pvl_precond_apply: null pointer argument");
+    if (v == z)
+        return pvl_fail(PVL_ERR_ARG, "pvl_precond_apply: v and z must not alias");
+    precond_apply_kernel<<<blocks_for(n, 8), 256, 0, (cudaStream_t)stream>>>(n, X, ldx, perm, v, z);
+    PVL_LAUNCH_CHECK();
     return PVL_OK;
 }

@@ -335,3 +335,279 @@ class SolverEngine:
             raise _lib.PvlError(_lib.PVL_ERR_TIMEOUT, "a wavefront wait in the triangular solve timed out")
         if info:
             raise _lib.PvlError(_lib.PVL_ERR_SINGULAR, f"exactly singular system: U[{info - 1},{info - 1}] == 0")
+
+
+class MixedSolverEngine(SolverEngine):
+    """The mixed-precision step: the FP64 system solved to FP64 accuracy with cheaper arithmetic.
+
+    * Body matrix, implicit wake row and every residual stay FP64.
+    * The solve is right-preconditioned GMRES with FP64 vectors and FP64 residuals against the
+      FP64 matrix.  The preconditioner is the explicit inverse of an FP32 LU factorisation of
+      the system (trailing updates and the triangular inversion's rank-64 updates on the
+      tensor cores in TF32, pvl_lu32_factor / pvl_lu32_inverse), refreshed every ``refresh``
+      steps and applied as one FP32 matrix-vector product per iteration.  If GMRES has not
+      reached ``gmres_tol`` (relative residual) after ``max_iter`` iterations the step falls
+      back to the plain FP64 factorisation.
+    * The explicit wake term runs in FP64 for the wake rows below ``near_rows`` and in FP32
+      beyond (far rows induce little, so their FP32 rounding stays far below the tolerance).
+    * The advection sweep runs in FP64 for wake node rows below ``advect_near_rows`` and in
+      FP32 beyond; it moves the wake and does not enter this step's solve.
+    ``judge()`` re-assembles the step's system entirely in FP64 and solves it with the FP64
+    factorisation, which is how the mixed answer's error is measured.
+    """
+
+    def __init__(self, mesh: Mesh, freestream, tol: float, wake: WakeSpec | None = None, closed_groups=None,
+                 refresh: int = 25, near_rows: int = 8, advect_near_rows: int = 8, gmres_tol: float = 1e-12,
+                 max_iter: int = 20):
+        super().__init__(mesh, freestream, tol, wake, closed_groups)
+        self.refresh = int(refresh)
+        self.gmres_tol = float(gmres_tol)
+        self.max_iter = int(max_iter)
+        n = self.N
+        self.npad = ((n + 63) // 64) * 64
+        f32 = dict(dtype=torch.float32, device=self.dev)
+        f64 = dict(dtype=torch.float64, device=self.dev)
+        self.A32 = torch.zeros((self.npad, self.npad), **f32)
+        self.Xinv = torch.zeros((self.npad, self.npad), **f32)
+        self.Yscr = torch.zeros((self.npad, self.npad), **f32)
+        self.ipiv32 = torch.zeros(2 * self.npad, dtype=torch.int32, device=self.dev)
+        self.info32 = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        self.err32 = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        m = self.max_iter
+        self.V = torch.zeros((m + 1, n), **f64)
+        self.Z = torch.zeros((m, n), **f64)
+        self.wv = torch.zeros(n, **f64)
+        self.hbuf = torch.zeros(2 * (m + 2), **f64)
+        self.scal = torch.zeros(2, **f64)
+        self.y = torch.zeros(m, **f64)
+        self.x = torch.zeros(n, **f64)
+        self.b_saved = torch.zeros(n, **f64)
+        self.h_h = torch.zeros(2 * (m + 2), dtype=torch.float64, pin_memory=True)
+        self.have_precond = False
+        self.steps_since_refresh = 0
+        self.stats = {"gmres_iters": [], "fallbacks": 0, "refreshes": 0, "final_rel_residual": [], "judge": []}
+        need = _lib.query("pvl_lu32_workspace", self.npad)
+        if self.wake is not None:
+            need = max(need, self._init_row_major_wake(near_rows, advect_near_rows))
+        if need + 256 > self._ws_bytes:
+            self._ws_bytes = need + 256
+            self.ws = torch.empty(self._ws_bytes, dtype=torch.uint8, device=self.dev)
+
+    # ------------------------------------------------------------------ wake in row-major ring order
+    def _init_row_major_wake(self, near_rows: int, advect_near_rows: int) -> int:
+        w = self.wake
+        S, R = w["S"], w["R"]
+        rc = wake_ring_connectivity(R, S).reshape(S, R, 4).transpose(1, 0, 2).reshape(-1, 4)
+        rm = Mesh(2 * (R + 1) * S, rc)  # ring r*S + s: lines are numbered row band by row band
+        self.near_rows = max(1, min(int(near_rows), R))
+        self.advect_near_rows = max(0, min(int(advect_near_rows), R))
+        off, sl = rm.surface_offsets, rm.surface_lines
+        ids = sl[: int(off[self.near_rows * S])] & 0x7FFFFFFF
+        self.n_near_lines = int(ids.max()) + 1  # lines of rows < near_rows come first
+        w["rm"] = rm
+        w["rm_d"] = rm.device_arrays()
+        w["circ_rs"] = torch.zeros((R, S), dtype=torch.float64, device=self.dev)
+        w["rm_line_gamma"] = torch.zeros(max(rm.n_lines, 1), dtype=torch.float64, device=self.dev)
+        L, P = self.mesh.n_lines, self.P
+        need = [_lib.query("pvl_segments_workspace", rm.n_lines, _lib.PVL_F64),
+                _lib.query("pvl_line_velocity_workspace", self.n_near_lines, P, _lib.PVL_F64),
+                _lib.query("pvl_line_velocity_workspace", max(rm.n_lines - self.n_near_lines, 1), P, _lib.PVL_F32)]
+        for c in range(1, R + 1):  # every row split the advection can see as the wake grows
+            nr = min(self.advect_near_rows, c)
+            if nr:
+                need.append(_lib.query("pvl_line_velocity_workspace", L, 2 * S * nr, _lib.PVL_F64))
+            if c > nr:
+                need.append(_lib.query("pvl_line_velocity_workspace", L, 2 * S * (c - nr), _lib.PVL_F32))
+        return max(need)
+
+    def _wake_corrections(self) -> None:
+        s = stream_ptr()
+        w = self.wake
+        S, R = w["S"], w["R"]
+        rm, d = w["rm"], w["rm_d"]
+        wpos = self.wake_positions.reshape(-1, 3)
+        ws, nb = ptr(self.ws), self._ws_bytes
+        # implicit: the first S rings of the row-major mesh are row 0 of every strip, in strip order
+        _lib.call("pvl_induction_normal", _lib.PVL_F64, rm.n_points, rm.n_lines, ptr(d["lines"]), ptr(wpos), S,
+                  ptr(d["offsets"]), ptr(d["surface_lines"]), self.P, ptr(self.cps), ptr(self.nrm), self.tol,
+                  ptr(w["implicit"]), S, ws, nb, s)
+        _lib.call("pvl_wake_fold_implicit", self.P, S, ptr(w["implicit"]), ptr(w["adj"]), ptr(self.A), self.N, s)
+        if R <= 1:
+            return
+        crs = w["circ_rs"]
+        crs.copy_(self.wake_circulation.t())
+        crs[0].zero_()  # row 0 is implicit
+        lg = w["rm_line_gamma"]
+        _lib.call("pvl_line_circulation", rm.n_lines, ptr(d["map_offsets"]), ptr(d["map_entries"]), ptr(crs), 0,
+                  ptr(lg), s)
+        Ln = self.n_near_lines
+        lines = d["lines"]
+        _lib.call("pvl_line_velocity", _lib.PVL_F64, rm.n_points, Ln, ptr(lines), ptr(wpos), ptr(lg), self.P,
+                  ptr(self.cps), ptr(self.nrm), self.tol, 1.0, 1.0, ptr(self.rhs), ws, nb, s)
+        if rm.n_lines > Ln:
+            _lib.call("pvl_line_velocity", _lib.PVL_F32, rm.n_points, rm.n_lines - Ln, lines.data_ptr() + 8 * Ln,
+                      ptr(wpos), lg.data_ptr() + 8 * Ln, self.P, ptr(self.cps), ptr(self.nrm), self.tol, 1.0, 1.0,
+                      ptr(self.rhs), ws, nb, s)
+
+    # ------------------------------------------------------------------ preconditioner
+    def refresh_preconditioner(self) -> None:
+        """FP32 LU of the current system (tensor-core trailing updates) and its explicit inverse."""
+        s = stream_ptr()
+        n, npad = self.N, self.npad
+        _lib.call("pvl_pad_convert_f32", n, ptr(self.A), self.N, ptr(self.A32), npad, npad, s)
+        ws, nb = ptr(self.ws), self._ws_bytes
+        _lib.call("pvl_lu32_factor", npad, ptr(self.A32), npad, ptr(self.ipiv32), ptr(self.info32), ptr(self.err32),
+                  ws, nb, s)
+        _lib.call("pvl_lu32_inverse", npad, ptr(self.A32), npad, ptr(self.Xinv), npad, ptr(self.Yscr), npad,
+                  ptr(self.err32), ws, nb, s)
+        self.have_precond = True
+        self.steps_since_refresh = 0
+        self.stats["refreshes"] += 1
+
+    # ------------------------------------------------------------------ GMRES
+    def solve_mixed(self, x0: torch.Tensor | None = None) -> bool:
+        """Right-preconditioned GMRES on A x = b in FP64; True if the relative residual met gmres_tol."""
+        s = stream_ptr()
+        n = self.N
+        A, b = self.A, self.rhs
+        if (not self.have_precond) or self.steps_since_refresh >= self.refresh:
+            self.refresh_preconditioner()
+        self.steps_since_refresh += 1
+        x = self.x
+        if x0 is not None:
+            x.copy_(x0.reshape(-1)[:n])
+        else:
+            x[: self.P].copy_(self.gamma)  # the previous step's circulation
+        perm = self.ipiv32.data_ptr() + 4 * self.npad
+        hb, sc = self.hbuf, self.scal
+        # r0 = b - A x0 ; ||b|| and ||r0|| in one host read
+        self.wv.copy_(b)
+        _lib.call("pvl_gemv_f64", n, n, -1.0, ptr(A), self.N, ptr(x), 1.0, ptr(self.wv), s)
+        _lib.call("pvl_normalize", n, ptr(b), None, sc.data_ptr(), s)
+        _lib.call("pvl_normalize", n, ptr(self.wv), ptr(self.V[0]), sc.data_ptr() + 8, s)
+        bnorm, beta = (float(v) for v in sc.cpu())
+        target = self.gmres_tol * bnorm
+        iters = 0
+        if beta > target:
+            m = self.max_iter
+            H = np.zeros((m + 1, m))
+            cs, sn = np.zeros(m), np.zeros(m)
+            g = np.zeros(m + 1)
+            g[0] = beta
+            k = 0
+            hh = self.h_h
+            for j in range(m):
+                _lib.call("pvl_precond_apply", n, ptr(self.Xinv), self.npad, perm, ptr(self.V[j]), ptr(self.Z[j]), s)
+                _lib.call("pvl_gemv_f64", n, n, 1.0, ptr(A), self.N, ptr(self.Z[j]), 0.0, ptr(self.wv), s)
+                hb.zero_()
+                for _ in range(2):  # classical Gram-Schmidt, twice
+                    _lib.call("pvl_basis_project", n, j + 1, ptr(self.V), n, ptr(self.wv), ptr(hb), s)
+                _lib.call("pvl_normalize", n, ptr(self.wv), ptr(self.V[j + 1]), hb.data_ptr() + 8 * (j + 1), s)
+                hh[: j + 2].copy_(hb[: j + 2], non_blocking=True)
+                torch.cuda.current_stream().synchronize()
+                H[: j + 2, j] = hh[: j + 2].numpy()
+                hnext = H[j + 1, j]
+                for i in range(j):  # previous Givens rotations
+                    t = cs[i] * H[i, j] + sn[i] * H[i + 1, j]
+                    H[i + 1, j] = -sn[i] * H[i, j] + cs[i] * H[i + 1, j]
+                    H[i, j] = t
+                den = float(np.hypot(H[j, j], H[j + 1, j]))
+                cs[j], sn[j] = (1.0, 0.0) if den == 0.0 else (H[j, j] / den, H[j + 1, j] / den)
+                H[j, j] = cs[j] * H[j, j] + sn[j] * H[j + 1, j]
+                H[j + 1, j] = 0.0
+                g[j + 1] = -sn[j] * g[j]
+                g[j] = cs[j] * g[j]
+                k = j + 1
+                if abs(g[j + 1]) <= target or hnext == 0.0:  # converged, or the Krylov space is exhausted
+                    break
+            yk = np.zeros(k)
+            for i in range(k - 1, -1, -1):  # back substitution with the rotated Hessenberg
+                yk[i] = (g[i] - H[i, i + 1:k] @ yk[i + 1:]) / H[i, i] if H[i, i] != 0.0 else 0.0
+            self.y[:k].copy_(torch.from_numpy(yk))
+            _lib.call("pvl_combine", n, k, ptr(self.Z), n, ptr(self.y), ptr(x), s)
+            iters = k
+        # the true FP64 residual decides
+        self.wv.copy_(b)
+        _lib.call("pvl_gemv_f64", n, n, -1.0, ptr(A), self.N, ptr(x), 1.0, ptr(self.wv), s)
+        _lib.call("pvl_normalize", n, ptr(self.wv), None, sc.data_ptr(), s)
+        rel = float(sc[0].item()) / max(bnorm, 1e-300)
+        self.stats["gmres_iters"].append(iters)
+        self.stats["final_rel_residual"].append(rel)
+        return rel <= self.gmres_tol
+
+    def solve(self, x0: torch.Tensor | None = None) -> None:
+        self.b_saved.copy_(self.rhs)
+        if self.solve_mixed(x0):
+            self.gamma.copy_(self.x[: self.P])
+            if self.m:
+                _lib.call("pvl_group_mean_remove", self.m, ptr(self.goff), ptr(self.gamma), stream_ptr())
+            return
+        self.stats["fallbacks"] += 1
+        self.rhs.copy_(self.b_saved)
+        super().solve()
+
+    def step(self, time: float, positions, velocities, x0: torch.Tensor | None = None) -> torch.Tensor:
+        self.load_inputs(positions, velocities)
+        self.assemble()
+        self.solve(x0)
+        if self.wake is not None:
+            self.wake_update(time)
+        self.iteration += 1
+        return self.gamma
+
+    # ------------------------------------------------------------------ error against FP64
+    def judge(self) -> float:
+        """Relative error of the current circulation against the all-FP64 step.
+
+        Call after assemble/solve and before the wake update of a step (``step_judged`` does
+        this): the system is re-assembled in FP64 (body, implicit and explicit wake terms) and
+        solved with the FP64 factorisation; the mixed circulation is kept."""
+        mixed = self.gamma.clone()
+        self.assemble_body_only()
+        if self.wake is not None and self.iteration > 0:
+            SolverEngine._wake_corrections(self)
+        self.border()
+        SolverEngine.solve(self)
+        ref = self.gamma.clone()
+        self.gamma.copy_(mixed)
+        err = float((torch.linalg.vector_norm(mixed - ref) / torch.linalg.vector_norm(ref)).item())
+        self.stats["judge"].append(err)
+        return err
+
+    def step_judged(self, time: float, positions, velocities, x0: torch.Tensor | None = None) -> float:
+        self.load_inputs(positions, velocities)
+        self.assemble()
+        self.solve(x0)
+        err = self.judge()
+        if self.wake is not None:
+            self.wake_update(time)
+        self.iteration += 1
+        return err
+
+    def wake_update(self, time: float) -> None:
+        """As the plain update, with the advection sweep split into FP64 near rows and FP32 far rows."""
+        s = stream_ptr()
+        w = self.wake
+        S, R = w["S"], w["R"]
+        dt = float(time) - w["time"]
+        w["time"] = float(time)
+        if w["step_count"] == 0:
+            self._advect(0, 0.0)
+            w["step_count"] = 1
+        complete = min(w["step_count"], R)
+        msh, d = self.mesh, self.d_body
+        _lib.call("pvl_line_circulation", msh.n_lines, ptr(d["map_offsets"]), ptr(d["map_entries"]), ptr(self.gamma), 0,
+                  ptr(self.body_line_gamma), s)
+        u = self.u_inf
+        nr = min(self.advect_near_rows, complete)
+        for prec, r0, r1 in ((_lib.PVL_F64, 0, nr), (_lib.PVL_F32, nr, complete)):
+            if r1 > r0:
+                _lib.call("pvl_wake_node_velocity_rows", prec, msh.n_points, msh.n_lines, ptr(d["lines"]),
+                          ptr(self.pos), ptr(self.body_line_gamma), S, R, complete, r0, r1, ptr(self.wake_positions),
+                          float(u[0]), float(u[1]), float(u[2]), self.tol, ptr(w["node_vel"]), ptr(self.ws),
+                          self._ws_bytes, s)
+        self._advect(complete, dt)
+        c = w["ccur"]
+        _lib.call("pvl_wake_shed", S, R, ptr(w["circ"][c]), ptr(w["adj"]), ptr(self.gamma), ptr(w["circ"][1 - c]), s)
+        w["ccur"] = 1 - c
+        w["step_count"] += 1

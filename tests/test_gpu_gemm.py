@@ -29,12 +29,43 @@ def test_gemm_tf32_matches_torch(M, N, K, alpha, beta):
     assert rel <= 3e-3, rel
 
 
+@pytest.mark.parametrize("M,N,K", [(100, 200, 64), (64, 4096 - 64, 64), (1, 7, 32), (300, 129, 96)])
+def test_gemm_tf32_ragged_submatrix(M, N, K):
+    """Edges that are not multiples of the 128 x 128 tile, operands and C inside larger
+    buffers: the block is updated, nothing outside it is touched."""
+    import torch
+
+    from pyvl_b200 import _lib
+    from pyvl_b200.device import ptr, stream_ptr
+
+    g = torch.Generator(device="cuda").manual_seed(7 * M + N)
+    n4 = (N + 3) // 4 * 4  # leading dimensions: multiples of 4 floats, blocks 16-byte aligned
+    lda, ldb, ldc = K + 8, n4 + 12, n4 + 20
+    A = torch.randn(M + 3, lda, device="cuda", generator=g)
+    B = torch.randn(K + 2, ldb, device="cuda", generator=g)
+    C = torch.randn(M + 5, ldc, device="cuda", generator=g)
+    C0 = C.clone()
+    a, b = A[1:1 + M, 4:4 + K], B[2:2 + K, 4:4 + N]
+    c = C[2:2 + M, 8:8 + N]
+    want = -(a.double() @ b.double()) + c.double()
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    _lib.call("pvl_gemm_tf32", M, N, K, -1.0, a.data_ptr(), lda, b.data_ptr(), ldb, 1.0, c.data_ptr(), ldc, ptr(err),
+              stream_ptr())
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    rel = (torch.linalg.norm(c.double() - want) / torch.linalg.norm(want)).item()
+    assert rel <= 3e-3, rel
+    mask = torch.ones_like(C, dtype=torch.bool)
+    mask[2:2 + M, 8:8 + N] = False
+    assert torch.equal(C[mask], C0[mask])
+
+
 def test_gemm_tf32_rejects_bad_shapes():
     import torch
 
     from pyvl_b200 import _lib
 
     x = torch.zeros(16, device="cuda")
-    with pytest.raises(ValueError):
-        _lib.call("pvl_gemm_tf32", 100, 128, 32, 1.0, x.data_ptr(), 32, x.data_ptr(), 128, 0.0, x.data_ptr(), 128,
+    with pytest.raises(ValueError):  # K not a multiple of 32: rejected before any launch
+        _lib.call("pvl_gemm_tf32", 128, 128, 20, 1.0, x.data_ptr(), 32, x.data_ptr(), 128, 0.0, x.data_ptr(), 128,
                   x.data_ptr(), None)

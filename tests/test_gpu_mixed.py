@@ -1,0 +1,218 @@
+"""The mixed-precision path on the GPU.
+
+* FP32 LU with tensor-core trailing updates and its explicit inverse: X A ~ I to FP32/TF32
+  accuracy, on a vortex-ring system and on a random matrix that needs row interchanges.
+* Row-range wake node velocity: FP64 pieces reassemble the full sweep; FP32 far rows stay
+  within FP32 rounding.
+* MixedSolverEngine: every step judged against the all-FP64 step (FP64 assembly of the same
+  state + FP64 LU): circulation within 1e-10 relative, no FP64 fallbacks, few GMRES iterations.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+MIXED_TOL = 1e-10
+
+
+def _lu32_inverse(A64):
+    import torch
+
+    from pyvl_b200 import _lib
+    from pyvl_b200.device import ptr, stream_ptr
+
+    n = A64.shape[0]
+    npad = (n + 63) // 64 * 64
+    A32 = torch.zeros((npad, npad), dtype=torch.float32, device="cuda")
+    X = torch.zeros_like(A32)
+    Y = torch.zeros_like(A32)
+    ipiv = torch.zeros(2 * npad, dtype=torch.int32, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    nb = _lib.query("pvl_lu32_workspace", npad)
+    ws = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    s = stream_ptr()
+    _lib.call("pvl_pad_convert_f32", n, ptr(A64), n, ptr(A32), npad, npad, s)
+    _lib.call("pvl_lu32_factor", npad, ptr(A32), npad, ptr(ipiv), ptr(info), ptr(err), ptr(ws), nb, s)
+    _lib.call("pvl_lu32_inverse", npad, ptr(A32), npad, ptr(X), npad, ptr(Y), npad, ptr(err), ptr(ws), nb, s)
+    torch.cuda.synchronize()
+    assert int(info.item()) == 0 and int(err.item()) == 0
+    perm = ipiv[npad:].long()
+    return X, perm, npad
+
+
+def _apply(X, perm, n, v):
+    import torch
+
+    from pyvl_b200 import _lib
+    from pyvl_b200.device import ptr, stream_ptr
+
+    z = torch.zeros(n, dtype=torch.float64, device="cuda")
+    _lib.call("pvl_precond_apply", n, ptr(X), X.shape[1], perm.to(torch.int32).data_ptr(), ptr(v), ptr(z),
+              stream_ptr())
+    torch.cuda.synchronize()
+    return z
+
+
+def test_lu32_inverse_of_ring_system():
+    import torch
+
+    from pyvl_b200.cvl import Mesh
+    from pyvl_b200.workloads import flapping
+
+    case = flapping(ns=32, nc=8, line_rows=4)
+    mesh = Mesh(case.n_points, case.elements)
+    pos = case.positions_at(0.37)
+    cps = mesh.surface_average_vec3(pos)
+    nrm = mesh.surface_normal(pos)
+    A = torch.as_tensor(mesh.induction_matrix3(case.tol, pos, cps, nrm), device="cuda")
+    X, perm, npad = _lu32_inverse(A)
+    n = A.shape[0]
+    g = torch.Generator(device="cuda").manual_seed(3)
+    b = torch.randn(n, dtype=torch.float64, device="cuda", generator=g)
+    x = _apply(X, perm, n, b)
+    ref = torch.linalg.solve(A, b)
+    rel = (torch.linalg.vector_norm(x - ref) / torch.linalg.vector_norm(ref)).item()
+    assert rel < 1e-5, rel  # FP32 factors, small off-diagonal entries through TF32
+
+
+def test_lu32_inverse_with_pivoting():
+    """Rows of a well-conditioned matrix shuffled: partial pivoting must undo the shuffle."""
+    import torch
+
+    n = 200  # not a multiple of 64: exercises the identity padding
+    g = torch.Generator(device="cuda").manual_seed(11)
+    base = 2.0 * torch.eye(n, dtype=torch.float64, device="cuda")
+    base += 0.3 * torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g) / n ** 0.5
+    shuffle = torch.randperm(n, generator=torch.Generator().manual_seed(4)).cuda()
+    A = base[shuffle].contiguous()
+    X, perm, npad = _lu32_inverse(A)
+    assert not torch.equal(perm[:n].cpu(), torch.arange(n)), "the shuffled rows need interchanges"
+    assert int(perm[:n].max()) < n and torch.equal(perm[n:].cpu(), torch.arange(n, npad))
+    b = torch.randn(n, dtype=torch.float64, device="cuda", generator=g)
+    x = _apply(X, perm, n, b)
+    ref = torch.linalg.solve(A, b)
+    rel = (torch.linalg.vector_norm(x - ref) / torch.linalg.vector_norm(ref)).item()
+    assert rel < 1e-3, rel  # TF32 products in the updates: ~2^-11 relative on the off-diagonal part
+
+
+def test_wake_node_velocity_rows_split():
+    import torch
+
+    from pyvl_b200 import _lib
+    from pyvl_b200.cvl import Mesh
+    from pyvl_b200.device import ptr, stream_ptr
+    from pyvl_b200.engine import synthetic_full_wake, wake_spec_from_te
+    from pyvl_b200.workloads import flapping
+
+    case = flapping(ns=32, nc=8, line_rows=24)
+    mesh = Mesh(case.n_points, case.elements)
+    t = 0.5
+    pos_h = case.positions_at(t)
+    spec = wake_spec_from_te(mesh, case.te_node_pairs, case.line_rows, t - case.dt)
+    wpos, _ = synthetic_full_wake(pos_h, spec, case.freestream, case.dt, seed=2)
+    S, R = len(spec.shedding_lines), case.line_rows
+    complete = R - 3
+    d = mesh.device_arrays()
+    pos = torch.as_tensor(pos_h, device="cuda")
+    wp = torch.as_tensor(np.ascontiguousarray(wpos), device="cuda")
+    g = torch.Generator(device="cuda").manual_seed(5)
+    lg = torch.randn(mesh.n_lines, dtype=torch.float64, device="cuda", generator=g)
+    u = case.freestream
+    nb = max(_lib.query("pvl_line_velocity_workspace", mesh.n_lines, 2 * S * c, p) for c in range(1, complete + 1)
+             for p in (_lib.PVL_F64, _lib.PVL_F32))
+    ws = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    s = stream_ptr()
+
+    def run(prec, r0, r1, out):
+        _lib.call("pvl_wake_node_velocity_rows", prec, mesh.n_points, mesh.n_lines, ptr(d["lines"]), ptr(pos), ptr(lg),
+                  S, R, complete, r0, r1, ptr(wp), float(u[0]), float(u[1]), float(u[2]), case.tol, ptr(out), ptr(ws),
+                  nb, s)
+
+    full = torch.zeros((S, 2, complete, 3), dtype=torch.float64, device="cuda")
+    _lib.call("pvl_wake_node_velocity", _lib.PVL_F64, mesh.n_points, mesh.n_lines, ptr(d["lines"]), ptr(pos), ptr(lg),
+              S, R, complete, ptr(wp), float(u[0]), float(u[1]), float(u[2]), case.tol, ptr(full), ptr(ws), nb, s)
+    parts = torch.full_like(full, float("nan"))
+    run(_lib.PVL_F64, 0, 5, parts)
+    run(_lib.PVL_F64, 5, complete, parts)
+    mixed = torch.full_like(full, float("nan"))
+    run(_lib.PVL_F64, 0, 5, mixed)
+    run(_lib.PVL_F32, 5, complete, mixed)
+    torch.cuda.synchronize()
+    assert not torch.isnan(parts).any() and not torch.isnan(mixed).any()
+    assert torch.allclose(parts, full, rtol=1e-13, atol=1e-13)
+    assert torch.equal(mixed[:, :, :5], parts[:, :, :5])
+    ind_full = full - torch.as_tensor(u, device="cuda")  # the induced part only
+    ind_mixed = mixed - torch.as_tensor(u, device="cuda")
+    rel = (torch.linalg.vector_norm(ind_mixed - ind_full) / torch.linalg.vector_norm(ind_full)).item()
+    assert rel < 1e-5, rel
+
+
+def _mixed_engine(case, **kw):
+    from pyvl_b200.cvl import Mesh
+    from pyvl_b200.engine import MixedSolverEngine, wake_spec_from_te
+
+    mesh = Mesh(case.n_points, case.elements)
+    wake = None
+    if case.line_rows > 0 and len(case.te_node_pairs):
+        wake = wake_spec_from_te(mesh, case.te_node_pairs, case.line_rows, case.t0)
+    groups = [(0, case.n_surfaces)] if case.closed else None
+    return MixedSolverEngine(mesh, case.freestream, case.tol, wake, groups, **kw)
+
+
+@pytest.mark.parametrize("factory,kw,steps", [
+    ("swept_pitching", dict(line_rows=30), 30),
+    ("flapping", dict(ns=64, nc=16, line_rows=40), 40),
+])
+def test_mixed_steps_judged_against_fp64(factory, kw, steps):
+    from pyvl_b200 import workloads
+
+    case = getattr(workloads, factory)(**kw)
+    eng = _mixed_engine(case, refresh=10, near_rows=4, advect_near_rows=4)
+    errs = []
+    for it in range(steps):
+        t = it * case.dt
+        errs.append(eng.step_judged(t, case.positions_at(t), case.velocities_at(t)))
+    eng.check_status()
+    st = eng.stats
+    assert max(errs) <= MIXED_TOL, max(errs)
+    assert st["fallbacks"] == 0
+    assert max(st["gmres_iters"]) <= 6, st["gmres_iters"]
+    assert st["refreshes"] == (steps + 9) // 10
+
+
+def test_mixed_closed_sphere_judged():
+    from pyvl_b200.workloads import icosphere
+
+    case = icosphere(subdiv=3)
+    eng = _mixed_engine(case, gmres_tol=1e-13)
+    for it in range(3):
+        t = it * case.dt
+        err = eng.step_judged(t, case.positions_at(t), case.velocities_at(t))
+        assert err <= MIXED_TOL, err
+    assert eng.stats["fallbacks"] == 0
+
+
+def test_mixed_trajectory_tracks_plain():
+    """Whole trajectories: the FP32 far-field terms perturb the wake slightly; the
+    circulation histories of the mixed and the plain engine stay close."""
+    from pyvl_b200.cvl import Mesh
+    from pyvl_b200.engine import SolverEngine, wake_spec_from_te
+    from pyvl_b200.workloads import flapping
+
+    case = flapping(ns=64, nc=16, line_rows=40)
+    mesh = Mesh(case.n_points, case.elements)
+    plain = SolverEngine(mesh, case.freestream, case.tol,
+                         wake_spec_from_te(mesh, case.te_node_pairs, case.line_rows, case.t0))
+    mixed = _mixed_engine(case, refresh=25, near_rows=4, advect_near_rows=4)
+    worst = 0.0
+    for it in range(60):
+        t = it * case.dt
+        p, v = case.positions_at(t), case.velocities_at(t)
+        plain.step(t, p, v)
+        mixed.step(t, p, v)
+        a, b = mixed.gamma_host(), plain.gamma_host()
+        worst = max(worst, float(np.linalg.norm(a - b) / np.linalg.norm(b)))
+    print(f"max trajectory difference over 60 steps: {worst:.3e}")
+    assert worst <= 1e-8, worst
