@@ -202,15 +202,20 @@ int pvl_wake_node_velocity(int precision, uint32_t n_points, uint32_t n_lines, c
                            double ux, double uy, double uz, double tol, double* node_vel, void* ws,
                            size_t ws_bytes, void* stream);
 
-/* The rows [row_begin, row_end) of pvl_wake_node_velocity only (same node_vel layout, other
- * rows untouched), so that near and far rows can run in different precisions.  The
- * workspace it needs is pvl_line_velocity_workspace(n_lines, 2 n_shed (row_end - row_begin),
- * precision).  No reference counterpart (the reference evaluates every row in FP64). */
-int pvl_wake_node_velocity_rows(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
+/* pvl_wake_node_velocity restricted to rows [row_begin, row_end) of n_cols node columns:
+ * column c is wake node column cols[c] (strip side s * 2 + side, < 2 n_shed; cols == NULL
+ * means all 2 n_shed columns in order).  Output node_vel[(c * complete_rows + i) * 3 + k] for
+ * the listed rows; other rows untouched.  Lets co-located node columns (adjacent strips share
+ * their trailing-edge node, and identical positions advect identically) be evaluated once,
+ * and near and far rows run in different precisions.  Workspace:
+ * pvl_line_velocity_workspace(n_lines, n_cols (row_end - row_begin), precision).  No
+ * reference counterpart (the reference evaluates every node of every row). */
+int pvl_wake_node_velocity_cols(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
                                 const double* positions, const double* line_gamma, uint32_t n_shed,
                                 uint32_t line_rows, uint32_t complete_rows, uint32_t row_begin,
-                                uint32_t row_end, const double* wake_pos, double ux, double uy, double uz,
-                                double tol, double* node_vel, void* ws, size_t ws_bytes, void* stream);
+                                uint32_t row_end, uint32_t n_cols, const uint32_t* cols, const double* wake_pos,
+                                double ux, double uy, double uz, double tol, double* node_vel, void* ws,
+                                size_t ws_bytes, void* stream);
 
 /* Advance wake node rows (explicit Euler) from `old_pos` into `new_pos` (both
  * (n_shed, 2, line_rows + 1, 3)): new[:, :, i+1] = old[:, :, i] + node_vel[:, :, i] * dt for
@@ -221,6 +226,14 @@ int pvl_wake_advect(uint32_t n_shed, uint32_t line_rows, uint32_t complete_rows,
                     const double* old_pos, const double* node_vel, double dt,
                     const double* body_positions, const uint32_t* bordering_nodes,
                     double* new_pos, void* stream);
+
+/* pvl_wake_advect with node column s * 2 + side reading its velocity row from slot
+ * col_slot[s * 2 + side] of node_vel ((n_slots, complete_rows, 3)), as written by
+ * pvl_wake_node_velocity_cols for a de-duplicated column list. */
+int pvl_wake_advect_cols(uint32_t n_shed, uint32_t line_rows, uint32_t complete_rows,
+                         const double* old_pos, const double* node_vel, const uint32_t* col_slot,
+                         uint32_t n_slots, double dt, const double* body_positions,
+                         const uint32_t* bordering_nodes, double* new_pos, void* stream);
 
 /* Shift wake circulations one row back and shed the new first row
  *   circ[:, 0] = gamma[adj[:,1]] - gamma[adj[:,0]]   (INVALID_ID sides skipped)

@@ -52,10 +52,11 @@ SIGNATURES = {
     "pvl_line_velocity_noalloc": (_I, [_I, _U, _U, _P, _P, _P, _U, _P, _P, _D, _D, _D, _P, _P]),
     "pvl_wake_node_velocity_workspace": (_Z, [_U, _U, _U, _I]),
     "pvl_wake_node_velocity": (_I, [_I, _U, _U, _P, _P, _P, _U, _U, _U, _P, _D, _D, _D, _D, _P, _P, _Z, _P]),
-    "pvl_wake_node_velocity_rows": (_I, [_I, _U, _U, _P, _P, _P, _U, _U, _U, _U, _U, _P, _D, _D, _D, _D, _P, _P, _Z,
-                                         _P]),
+    "pvl_wake_node_velocity_cols": (_I, [_I, _U, _U, _P, _P, _P, _U, _U, _U, _U, _U, _U, _P, _P, _D, _D, _D, _D, _P,
+                                         _P, _Z, _P]),
     "pvl_wake_fold_implicit": (_I, [_U, _U, _P, _P, _P, _U, _P]),
     "pvl_wake_advect": (_I, [_U, _U, _U, _P, _P, _D, _P, _P, _P, _P]),
+    "pvl_wake_advect_cols": (_I, [_U, _U, _U, _P, _P, _P, _U, _D, _P, _P, _P, _P]),
     "pvl_wake_shed": (_I, [_U, _U, _P, _P, _P, _P, _P]),
     "pvl_lu_workspace": (_Z, [_U]),
     "pvl_lu_solve_workspace": (_Z, [_U]),

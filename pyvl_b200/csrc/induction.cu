@@ -155,14 +155,16 @@ __global__ void __launch_bounds__(kRingThreads) line_matrix_kernel(uint32_t n_li
 }
 
 // N-body sweep: partial[(split*n_pts + p)*3 + c] = sum over this split's segments of gamma_k u_k(p).
-// Point p of the sweep is pts[(p / group) * stride + p % group + in_off]: group == stride ==
-// n_pts is a plain array; group = a range of wake rows, stride = rows + 1, in_off = first row
-// walks those rows of every wake strip side.
+// Point p of the sweep is pts[col(p / group) * stride + p % group + in_off] with col(c) =
+// cols ? cols[c] : c: group == stride == n_pts is a plain array; group = a range of wake
+// rows, stride = rows + 1, in_off = first row walks those rows of the listed wake node
+// columns (strip side s * 2 + side).
 template <typename T>
 __global__ void __launch_bounds__(kSumThreads) line_sum_kernel(const Segment<T>* __restrict__ seg, uint32_t n_lines,
                                                                uint32_t lines_per_split,
                                                                const double* __restrict__ pts, uint32_t n_pts,
                                                                uint32_t group, uint32_t stride, uint32_t in_off,
+                                                               const uint32_t* __restrict__ cols, uint32_t col_limit,
                                                                T tol2, T* __restrict__ partial)
 {
     __shared__ Segment<T> s_seg[kSegTile];
@@ -174,8 +176,13 @@ __global__ void __launch_bounds__(kSumThreads) line_sum_kernel(const Segment<T>*
 #pragma unroll
     for (int t = 0; t < kSumPPT; ++t) {
         const uint32_t p = blockIdx.x * (kSumThreads * kSumPPT) + t * kSumThreads + threadIdx.x;
-        const bool ok = p < n_pts;
-        const size_t q = ok ? (size_t)(p / group) * stride + p % group + in_off : 0;
+        bool ok = p < n_pts;
+        uint32_t col = ok ? (cols ? cols[p / group] : p / group) : 0;
+        if (col >= col_limit) {  // a listed column outside the point array: skip the point
+            ok = false;
+            col = 0;
+        }
+        const size_t q = ok ? (size_t)col * stride + p % group + in_off : 0;
         px[t] = ok ? T(pts[3 * q]) : T(0);
         py[t] = ok ? T(pts[3 * q + 1]) : T(0);
         pz[t] = ok ? T(pts[3 * q + 2]) : T(0);
@@ -553,7 +560,8 @@ namespace {
 // Shared driver of the N-body sweep: segment table, split sweep, deterministic reduction.
 int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines, const double* positions,
                  const double* line_gamma, uint32_t n_pts, const double* pts, uint32_t group, uint32_t stride,
-                 uint32_t in_off, uint32_t out_stride, uint32_t out_off, const double* normals, double tol,
+                 uint32_t in_off, const uint32_t* cols, uint32_t col_limit, uint32_t out_stride, uint32_t out_off,
+                 const double* normals, double tol,
                  double alpha, double beta, double ux, double uy, double uz, double* out, void* ws, size_t ws_bytes,
                  cudaStream_t st, const char* who)
 {
@@ -582,7 +590,7 @@ int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint3
         if (int r = prep_segments<double>(n_points, n_lines, lines, positions, line_gamma, tol, seg, st))
             return r;
         line_sum_kernel<double><<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off,
-                                                              tol * tol, part);
+                                                              cols, col_limit, tol * tol, part);
         PVL_LAUNCH_CHECK();
         reduce_partials_kernel<double><<<blocks_for(n_pts, 256), 256, 0, st>>>(
             n_pts, n_split_used, part, normals, alpha, beta, ux, uy, uz, group, out_stride, out_off, out);
@@ -592,7 +600,7 @@ int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint3
         if (int r = prep_segments<float>(n_points, n_lines, lines, positions, line_gamma, tol, seg, st))
             return r;
         line_sum_kernel<float><<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off,
-                                                             float(tol * tol), part);
+                                                             cols, col_limit, float(tol * tol), part);
         PVL_LAUNCH_CHECK();
         reduce_partials_kernel<float><<<blocks_for(n_pts, 256), 256, 0, st>>>(
             n_pts, n_split_used, part, normals, alpha, beta, ux, uy, uz, group, out_stride, out_off, out);
@@ -612,7 +620,7 @@ extern "C" int pvl_line_velocity(int precision, uint32_t n_points, uint32_t n_li
         return PVL_OK;
     PVL_REQUIRE(pts); PVL_REQUIRE(out);
     return run_line_sum(precision, n_points, n_lines, lines, positions, line_gamma, n_pts, pts, n_pts, n_pts, 0,
-                        n_pts, 0, normals, tol, alpha, beta, 0.0, 0.0, 0.0, out, ws, ws_bytes, (cudaStream_t)stream,
+                        nullptr, 0xFFFFFFFFu, n_pts, 0, normals, tol, alpha, beta, 0.0, 0.0, 0.0, out, ws, ws_bytes, (cudaStream_t)stream,
                         "pvl_line_velocity");
 }
 
@@ -622,28 +630,31 @@ extern "C" size_t pvl_wake_node_velocity_workspace(uint32_t n_lines, uint32_t n_
     return pvl_line_velocity_workspace(n_lines, 2 * n_shed * complete_rows, precision);
 }
 
-extern "C" int pvl_wake_node_velocity_rows(int precision, uint32_t n_points, uint32_t n_lines,
+extern "C" int pvl_wake_node_velocity_cols(int precision, uint32_t n_points, uint32_t n_lines,
                                            const uint32_t* lines, const double* positions, const double* line_gamma,
                                            uint32_t n_shed, uint32_t line_rows, uint32_t complete_rows,
-                                           uint32_t row_begin, uint32_t row_end, const double* wake_pos, double ux,
-                                           double uy, double uz, double tol, double* node_vel, void* ws,
-                                           size_t ws_bytes, void* stream)
+                                           uint32_t row_begin, uint32_t row_end, uint32_t n_cols,
+                                           const uint32_t* cols, const double* wake_pos, double ux, double uy,
+                                           double uz, double tol, double* node_vel, void* ws, size_t ws_bytes,
+                                           void* stream)
 {
     if (complete_rows > line_rows)
         return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity: complete_rows %u > line_rows %u", complete_rows,
                         line_rows);
     if (row_begin > row_end || row_end > complete_rows)
-        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity_rows: rows [%u, %u) outside [0, %u)", row_begin, row_end,
+        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity_cols: rows [%u, %u) outside [0, %u)", row_begin, row_end,
                         complete_rows);
-    if (n_shed == 0 || row_end == row_begin)
+    if (!cols && n_cols != 2 * n_shed)
+        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity_cols: without a column list n_cols must be 2 n_shed");
+    if (n_cols == 0 || row_end == row_begin)
         return PVL_OK;
     PVL_REQUIRE(wake_pos); PVL_REQUIRE(node_vel);
     const uint32_t group = row_end - row_begin;
-    const uint64_t n_pts = 2ull * n_shed * group;
+    const uint64_t n_pts = (uint64_t)n_cols * group;
     if (n_pts > 0xFFFFFFFFull)
         return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity: too many nodes");
     return run_line_sum(precision, n_points, n_lines, lines, positions, line_gamma, (uint32_t)n_pts, wake_pos, group,
-                        line_rows + 1, row_begin, complete_rows, row_begin, nullptr, tol, 1.0, 0.0, ux, uy, uz,
+                        line_rows + 1, row_begin, cols, 2 * n_shed, complete_rows, row_begin, nullptr, tol, 1.0, 0.0, ux, uy, uz,
                         node_vel, ws, ws_bytes, (cudaStream_t)stream, "pvl_wake_node_velocity");
 }
 
@@ -653,9 +664,9 @@ extern "C" int pvl_wake_node_velocity(int precision, uint32_t n_points, uint32_t
                                       double uy, double uz, double tol, double* node_vel, void* ws, size_t ws_bytes,
                                       void* stream)
 {
-    return pvl_wake_node_velocity_rows(precision, n_points, n_lines, lines, positions, line_gamma, n_shed, line_rows,
-                                       complete_rows, 0, complete_rows, wake_pos, ux, uy, uz, tol, node_vel, ws,
-                                       ws_bytes, stream);
+    return pvl_wake_node_velocity_cols(precision, n_points, n_lines, lines, positions, line_gamma, n_shed, line_rows,
+                                       complete_rows, 0, complete_rows, 2 * n_shed, nullptr, wake_pos, ux, uy, uz,
+                                       tol, node_vel, ws, ws_bytes, stream);
 }
 
 extern "C" int pvl_line_circulation(uint32_t n_lines, const uint32_t* map_offsets, const uint32_t* map_entries,

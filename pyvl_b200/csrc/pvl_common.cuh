@@ -31,6 +31,43 @@ struct __align__(16) Segment {
 
 template <typename T> struct Vec3 { T x, y, z; };
 
+// Far-field evaluation of ang / h (see segment_induction).  For x = h^2 + t1 t2 > 0 the angle
+// is atan(z) with z = -h len / x, and the Taylor series of the arctangent,
+//   atan(z) = z (1 - w/3 + w^2/5 - w^3/7 + ...),  w = z^2,
+// gives ang / h = -(len / x) S(w) with w = h^2 len^2 / x^2 -- no square root and no atan2.
+// The series is used only for w <= kW, where the first omitted term bounds the relative
+// truncation error: double, 8 terms, w <= 0.01: 0.01^8 / 17 < 1e-17; float, 6 terms,
+// w <= 0.04: 0.04^6 / 13 < 4e-10.  Closer pairs (larger w, or x <= 0) take the atan2 form.
+template <typename T> struct FarSeries;
+template <> struct FarSeries<double> {
+    static constexpr double kW = 0.01;
+    static __device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
+    static __device__ __forceinline__ double sum(double w)
+    {
+        double s = -1.0 / 15.0;
+        s = fma(s, w, 1.0 / 13.0);
+        s = fma(s, w, -1.0 / 11.0);
+        s = fma(s, w, 1.0 / 9.0);
+        s = fma(s, w, -1.0 / 7.0);
+        s = fma(s, w, 1.0 / 5.0);
+        s = fma(s, w, -1.0 / 3.0);
+        return fma(s, w, 1.0);
+    }
+};
+template <> struct FarSeries<float> {
+    static constexpr float kW = 0.04f;
+    static __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+    static __device__ __forceinline__ float sum(float w)
+    {
+        float s = -1.0f / 11.0f;
+        s = fmaf(s, w, 1.0f / 9.0f);
+        s = fmaf(s, w, -1.0f / 7.0f);
+        s = fmaf(s, w, 1.0f / 5.0f);
+        s = fmaf(s, w, -1.0f / 3.0f);
+        return fmaf(s, w, 1.0f);
+    }
+};
+
 // Induction of one straight segment at point p, scaled by `scale`, added to `acc`.
 //
 // Follows the reference kernel (compute_line_induction, src/core/flow_solver.c:113-135):
@@ -40,7 +77,8 @@ template <typename T> struct Vec3 { T x, y, z; };
 //   atan2(t2, h) - atan2(t1, h) = atan2(h (t2 - t1), h^2 + t1 t2)
 // and t2 - t1 = -len exactly, so the difference is atan2(-h len, h^2 + t1 t2).  This
 // is the same function of the inputs (the difference lies in (-pi, pi)), evaluated
-// without the cancellation of the two-atan2 form in the far field.
+// without the cancellation of the two-atan2 form in the far field.  Far pairs evaluate
+// ang / h by the arctangent series of FarSeries.
 template <typename T>
 __device__ __forceinline__ void segment_induction(const Segment<T>& s, T px, T py, T pz, T tol2, T scale,
                                                   Vec3<T>& acc)
@@ -54,11 +92,19 @@ __device__ __forceinline__ void segment_induction(const Segment<T>& s, T px, T p
     const T hsq = (n1 + n2) / T(2);
     if (hsq < tol2 || s.len < T(0))
         return;
-    // one reciprocal square root gives both h and 1/h (no separate sqrt and division)
-    const T rh = rsqrt(hsq);
-    const T h = hsq * rh;
-    const T ang = atan2(-h * s.len, hsq + t1 * t2);
-    const T mag = scale * ang * rh;
+    const T x = hsq + t1 * t2;
+    const T hl2 = hsq * (s.len * s.len);
+    T mag;
+    if (x > T(0) && hl2 <= FarSeries<T>::kW * (x * x)) {
+        const T r = FarSeries<T>::rcp(x);
+        mag = -scale * s.len * r * FarSeries<T>::sum(hl2 * (r * r));
+    } else {
+        // one reciprocal square root gives both h and 1/h (no separate sqrt and division)
+        const T rh = rsqrt(hsq);
+        const T h = hsq * rh;
+        const T ang = atan2(-h * s.len, x);
+        mag = scale * ang * rh;
+    }
     // (dr1 x d) * mag
     acc.x += (ay * s.dz - az * s.dy) * mag;
     acc.y += (az * s.dx - ax * s.dz) * mag;

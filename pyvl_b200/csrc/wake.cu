@@ -34,7 +34,9 @@ __global__ void fold_implicit_kernel(uint32_t n_cp, uint32_t n_shed, const doubl
 // new[s, side, row]: row 0 = body node; row i+1 = old[i] + v[i] dt (i < complete); rows
 // beyond complete collapse onto row `complete` (wake_models.py:113-137).
 __global__ void advect_kernel(uint32_t n_shed, uint32_t R, uint32_t complete, const double* __restrict__ old_pos,
-                              const double* __restrict__ vel, double dt, const double* __restrict__ body,
+                              const double* __restrict__ vel, const uint32_t* __restrict__ col_slot,
+                              uint32_t n_slots, double dt,
+                              const double* __restrict__ body,
                               const uint32_t* __restrict__ bnodes, double* __restrict__ new_pos)
 {
     const uint32_t npr = R + 1;
@@ -56,10 +58,17 @@ __global__ void advect_kernel(uint32_t n_shed, uint32_t R, uint32_t complete, co
     } else {
         const uint32_t i = src - 1;  // new[i+1] = old[i] + v[i] dt
         const double* o = old_pos + 3 * (col * npr + i);
-        const double* v = vel + 3 * (col * complete + i);
-        x = o[0] + v[0] * dt;
-        y = o[1] + v[1] * dt;
-        z = o[2] + v[2] * dt;
+        const uint64_t slot = col_slot ? col_slot[col] : col;  // node columns may share one velocity row
+        if (slot < n_slots) {
+            const double* v = vel + 3 * (slot * complete + i);
+            x = o[0] + v[0] * dt;
+            y = o[1] + v[1] * dt;
+            z = o[2] + v[2] * dt;
+        } else {  // a slot outside node_vel (broken column map): the node is not moved
+            x = o[0];
+            y = o[1];
+            z = o[2];
+        }
     }
     double* out = new_pos + 3 * t;
     out[0] = x;
@@ -152,9 +161,11 @@ extern "C" int pvl_wake_fold_implicit(uint32_t n_cp, uint32_t n_shed, const doub
     return PVL_OK;
 }
 
-extern "C" int pvl_wake_advect(uint32_t n_shed, uint32_t line_rows, uint32_t complete_rows, const double* old_pos,
-                               const double* node_vel, double dt, const double* body_positions,
-                               const uint32_t* bordering_nodes, double* new_pos, void* stream)
+extern "C" int pvl_wake_advect_cols(uint32_t n_shed, uint32_t line_rows, uint32_t complete_rows,
+                                    const double* old_pos, const double* node_vel, const uint32_t* col_slot,
+                                    uint32_t n_slots, double dt,
+                                    const double* body_positions, const uint32_t* bordering_nodes, double* new_pos,
+                                    void* stream)
 {
     if (n_shed == 0)
         return PVL_OK;
@@ -167,9 +178,18 @@ extern "C" int pvl_wake_advect(uint32_t n_shed, uint32_t line_rows, uint32_t com
         return pvl_fail(PVL_ERR_ARG, "pvl_wake_advect: old_pos and new_pos must not alias");
     const uint64_t n = (uint64_t)n_shed * 2 * (line_rows + 1);
     advect_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(
-        n_shed, line_rows, complete_rows, old_pos, node_vel, dt, body_positions, bordering_nodes, new_pos);
+        n_shed, line_rows, complete_rows, old_pos, node_vel, col_slot, col_slot ? n_slots : 2 * n_shed, dt,
+        body_positions, bordering_nodes, new_pos);
     PVL_LAUNCH_CHECK();
     return PVL_OK;
+}
+
+extern "C" int pvl_wake_advect(uint32_t n_shed, uint32_t line_rows, uint32_t complete_rows, const double* old_pos,
+                               const double* node_vel, double dt, const double* body_positions,
+                               const uint32_t* bordering_nodes, double* new_pos, void* stream)
+{
+    return pvl_wake_advect_cols(n_shed, line_rows, complete_rows, old_pos, node_vel, nullptr, 2 * n_shed, dt,
+                                body_positions, bordering_nodes, new_pos, stream);
 }
 
 extern "C" int pvl_wake_shed(uint32_t n_shed, uint32_t line_rows, const double* old_circ, const uint32_t* adjacent,

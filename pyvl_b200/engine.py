@@ -35,11 +35,18 @@ from .cvl import INVALID_ID, Mesh
 from .device import ptr, require_cuda, stream_ptr, to_device, to_device_u32
 
 
-def wake_ring_connectivity(line_rows: int, n_shed: int) -> np.ndarray:
+def wake_ring_connectivity(line_rows: int, n_shed: int, bordering_nodes=None) -> np.ndarray:
     """Rings of the wake strips: strip s, row r -> nodes (s,0,r), (s,1,r), (s,1,r+1), (s,0,r+1).
 
     Same node numbering and ring order as the reference's wake mesh
     (python/pyvl/wake_models.py:35-52), so wake ring s*line_rows + r holds circulation[s, r].
+    With ``bordering_nodes`` ((n_shed, 2) body node ids), node columns that start at the same
+    body node -- the shared trailing-edge node of adjacent strips -- are referenced through
+    one representative column (``wake_node_columns``).  Those columns hold bitwise identical
+    positions at every step (same start, same advection), so the two coincident streamwise
+    segments of neighbouring strips become one line carrying the difference of the two
+    strips' circulations: the same induced velocity in exact arithmetic with a third fewer
+    wake lines.
     """
     npr = line_rows + 1
     r = np.arange(line_rows, dtype=np.uint64)
@@ -49,7 +56,33 @@ def wake_ring_connectivity(line_rows: int, n_shed: int) -> np.ndarray:
     rc[:, :, 1] = r + npr + base
     rc[:, :, 2] = r + npr + 1 + base
     rc[:, :, 3] = r + 1 + base
-    return rc.reshape(-1, 4).astype(np.uint32)
+    rc = rc.reshape(-1, 4)
+    if bordering_nodes is not None:
+        rep, _, _ = wake_node_columns(bordering_nodes)
+        col, row = rc // npr, rc % npr
+        rc = rep.astype(np.uint64)[col] * npr + row
+    return rc.astype(np.uint32)
+
+
+def wake_node_columns(bordering_nodes):
+    """Node columns (strip side s*2 + side) of the wake that start at the same body node.
+
+    Returns (rep, cols, slot): rep[c] the first column with column c's body node, cols the
+    distinct representatives in ascending order and slot[c] the position of rep[c] in cols.
+    """
+    bn = np.asarray(bordering_nodes, np.int64).reshape(-1)
+    first = {}
+    rep = np.empty(bn.size, np.int64)
+    for c, node in enumerate(bn):
+        rep[c] = first.setdefault(int(node), c)
+    cols = np.unique(rep)
+    slot = np.searchsorted(cols, rep)
+    return rep, cols.astype(np.uint32), slot.astype(np.uint32)
+
+
+def _node_velocity_workspace(n_lines: int, n_cols: int, rows: int, precision: int) -> int:
+    """Largest sweep workspace over every row count 1..rows the growing wake passes through."""
+    return max(_lib.query("pvl_line_velocity_workspace", n_lines, n_cols * c, precision) for c in range(1, rows + 1))
 
 
 def wake_row0_mesh(wake_mesh: Mesh, n_shed: int, line_rows: int) -> Mesh:
@@ -155,7 +188,8 @@ class SolverEngine:
             raise ValueError("adjacent surfaces out of range")
         if bn.min() < 0 or bn.max() >= self.mesh.n_points:
             raise ValueError("bordering nodes out of range")
-        wmesh = Mesh(2 * (R + 1) * S, wake_ring_connectivity(R, S))
+        wmesh = Mesh(2 * (R + 1) * S, wake_ring_connectivity(R, S, bn))
+        _, cols, slot = wake_node_columns(bn)
         # first-row rings (r = 0) as their own CSR over the wake's lines
         row0 = wake_row0_mesh(wmesh, S, R)
         off0, sl0 = row0.surface_offsets, row0.surface_lines
@@ -170,7 +204,10 @@ class SolverEngine:
             "cur": 0,    # current buffer of "pos"
             "ccur": 0,   # current buffer of "circ"
             "implicit": torch.zeros((self.P, S), **f64),
-            "node_vel": torch.zeros((S, 2, R, 3), **f64),
+            "cols": to_device_u32(cols, self.dev),
+            "slot": to_device_u32(slot, self.dev),
+            "n_cols": int(cols.size),
+            "node_vel": torch.zeros((int(cols.size), R, 3), **f64),
             "line_gamma": torch.zeros(max(wmesh.n_lines, 1), **f64),
             "time": float(w.time),
             "step_count": 0,
@@ -189,7 +226,7 @@ class SolverEngine:
             need += [
                 _lib.query("pvl_segments_workspace", Lw, _lib.PVL_F64),
                 _lib.query("pvl_line_velocity_workspace", Lw, self.P, _lib.PVL_F64),
-                _lib.query("pvl_wake_node_velocity_workspace", L, w["S"], w["R"], _lib.PVL_F64),
+                _node_velocity_workspace(L, w["n_cols"], w["R"], _lib.PVL_F64),
             ]
         return max(need) + 256
 
@@ -296,9 +333,10 @@ class SolverEngine:
         _lib.call("pvl_line_circulation", msh.n_lines, ptr(d["map_offsets"]), ptr(d["map_entries"]), ptr(self.gamma), 0,
                   ptr(self.body_line_gamma), s)
         u = self.u_inf
-        _lib.call("pvl_wake_node_velocity", _lib.PVL_F64, msh.n_points, msh.n_lines, ptr(d["lines"]), ptr(self.pos),
-                  ptr(self.body_line_gamma), S, R, complete, ptr(self.wake_positions), float(u[0]), float(u[1]),
-                  float(u[2]), self.tol, ptr(w["node_vel"]), ptr(self.ws), self._ws_bytes, s)
+        _lib.call("pvl_wake_node_velocity_cols", _lib.PVL_F64, msh.n_points, msh.n_lines, ptr(d["lines"]),
+                  ptr(self.pos), ptr(self.body_line_gamma), S, R, complete, 0, complete, w["n_cols"], ptr(w["cols"]),
+                  ptr(self.wake_positions), float(u[0]), float(u[1]), float(u[2]), self.tol, ptr(w["node_vel"]),
+                  ptr(self.ws), self._ws_bytes, s)
         self._advect(complete, dt)
         c = w["ccur"]
         _lib.call("pvl_wake_shed", S, R, ptr(w["circ"][c]), ptr(w["adj"]), ptr(self.gamma), ptr(w["circ"][1 - c]), s)
@@ -309,8 +347,8 @@ class SolverEngine:
         s = stream_ptr()
         w = self.wake
         cur = w["cur"]
-        _lib.call("pvl_wake_advect", w["S"], w["R"], complete, ptr(w["pos"][cur]), ptr(w["node_vel"]), dt,
-                  ptr(self.pos), ptr(w["bn"]), ptr(w["pos"][1 - cur]), s)
+        _lib.call("pvl_wake_advect_cols", w["S"], w["R"], complete, ptr(w["pos"][cur]), ptr(w["node_vel"]),
+                  ptr(w["slot"]), w["n_cols"], dt, ptr(self.pos), ptr(w["bn"]), ptr(w["pos"][1 - cur]), s)
         w["cur"] = 1 - cur
 
     def step(self, time: float, positions, velocities) -> torch.Tensor:
@@ -349,7 +387,9 @@ class MixedSolverEngine(SolverEngine):
       reached ``gmres_tol`` (relative residual) after ``max_iter`` iterations the step falls
       back to the plain FP64 factorisation.
     * The explicit wake term runs in FP64 for the wake rows below ``near_rows`` and in FP32
-      beyond (far rows induce little, so their FP32 rounding stays far below the tolerance).
+      beyond.  The default keeps every row FP64: the far wake still carries a large share of
+      the normal wash (co-located segments of neighbouring strips and the long trailing
+      lines), and FP32 rounding of those terms alone moves the circulation by ~1e-8.
     * The advection sweep runs in FP64 for wake node rows below ``advect_near_rows`` and in
       FP32 beyond; it moves the wake and does not enter this step's solve.
     ``judge()`` re-assembles the step's system entirely in FP64 and solves it with the FP64
@@ -357,7 +397,8 @@ class MixedSolverEngine(SolverEngine):
     """
 
     def __init__(self, mesh: Mesh, freestream, tol: float, wake: WakeSpec | None = None, closed_groups=None,
-                 refresh: int = 25, near_rows: int = 8, advect_near_rows: int = 8, gmres_tol: float = 1e-12,
+                 refresh: int = 25, near_rows: int | None = None, advect_near_rows: int = 8,
+                 gmres_tol: float = 1e-12,
                  max_iter: int = 20):
         super().__init__(mesh, freestream, tol, wake, closed_groups)
         self.refresh = int(refresh)
@@ -394,12 +435,13 @@ class MixedSolverEngine(SolverEngine):
             self.ws = torch.empty(self._ws_bytes, dtype=torch.uint8, device=self.dev)
 
     # ------------------------------------------------------------------ wake in row-major ring order
-    def _init_row_major_wake(self, near_rows: int, advect_near_rows: int) -> int:
+    def _init_row_major_wake(self, near_rows: int | None, advect_near_rows: int) -> int:
         w = self.wake
         S, R = w["S"], w["R"]
-        rc = wake_ring_connectivity(R, S).reshape(S, R, 4).transpose(1, 0, 2).reshape(-1, 4)
+        bn = self.wake["bn"].cpu().numpy().astype(np.int64)
+        rc = wake_ring_connectivity(R, S, bn).reshape(S, R, 4).transpose(1, 0, 2).reshape(-1, 4)
         rm = Mesh(2 * (R + 1) * S, rc)  # ring r*S + s: lines are numbered row band by row band
-        self.near_rows = max(1, min(int(near_rows), R))
+        self.near_rows = R if near_rows is None else max(1, min(int(near_rows), R))
         self.advect_near_rows = max(0, min(int(advect_near_rows), R))
         off, sl = rm.surface_offsets, rm.surface_lines
         ids = sl[: int(off[self.near_rows * S])] & 0x7FFFFFFF
@@ -412,12 +454,13 @@ class MixedSolverEngine(SolverEngine):
         need = [_lib.query("pvl_segments_workspace", rm.n_lines, _lib.PVL_F64),
                 _lib.query("pvl_line_velocity_workspace", self.n_near_lines, P, _lib.PVL_F64),
                 _lib.query("pvl_line_velocity_workspace", max(rm.n_lines - self.n_near_lines, 1), P, _lib.PVL_F32)]
+        nc = w["n_cols"]
         for c in range(1, R + 1):  # every row split the advection can see as the wake grows
             nr = min(self.advect_near_rows, c)
             if nr:
-                need.append(_lib.query("pvl_line_velocity_workspace", L, 2 * S * nr, _lib.PVL_F64))
+                need.append(_lib.query("pvl_line_velocity_workspace", L, nc * nr, _lib.PVL_F64))
             if c > nr:
-                need.append(_lib.query("pvl_line_velocity_workspace", L, 2 * S * (c - nr), _lib.PVL_F32))
+                need.append(_lib.query("pvl_line_velocity_workspace", L, nc * (c - nr), _lib.PVL_F32))
         return max(need)
 
     def _wake_corrections(self) -> None:
@@ -602,10 +645,10 @@ class MixedSolverEngine(SolverEngine):
         nr = min(self.advect_near_rows, complete)
         for prec, r0, r1 in ((_lib.PVL_F64, 0, nr), (_lib.PVL_F32, nr, complete)):
             if r1 > r0:
-                _lib.call("pvl_wake_node_velocity_rows", prec, msh.n_points, msh.n_lines, ptr(d["lines"]),
-                          ptr(self.pos), ptr(self.body_line_gamma), S, R, complete, r0, r1, ptr(self.wake_positions),
-                          float(u[0]), float(u[1]), float(u[2]), self.tol, ptr(w["node_vel"]), ptr(self.ws),
-                          self._ws_bytes, s)
+                _lib.call("pvl_wake_node_velocity_cols", prec, msh.n_points, msh.n_lines, ptr(d["lines"]),
+                          ptr(self.pos), ptr(self.body_line_gamma), S, R, complete, r0, r1, w["n_cols"],
+                          ptr(w["cols"]), ptr(self.wake_positions), float(u[0]), float(u[1]), float(u[2]), self.tol,
+                          ptr(w["node_vel"]), ptr(self.ws), self._ws_bytes, s)
         self._advect(complete, dt)
         c = w["ccur"]
         _lib.call("pvl_wake_shed", S, R, ptr(w["circ"][c]), ptr(w["adj"]), ptr(self.gamma), ptr(w["circ"][1 - c]), s)

@@ -106,3 +106,24 @@ def test_line_ring_map_is_transpose():
         for g in m.surface_lines[m.surface_offsets[s]:m.surface_offsets[s + 1]]:
             ref.append((s, int(g) & 0x7FFFFFFF, int(g) >> 31))
     assert sorted(seen) == sorted(ref)
+
+
+def test_wake_node_columns_merge_shared_trailing_edge_nodes():
+    """Adjacent strips share a trailing-edge node: their node columns get one representative,
+    and the merged wake mesh keeps one streamwise line per shared column."""
+    import numpy as np
+
+    from pyvl_b200.cvl import Mesh
+    from pyvl_b200.engine import wake_node_columns, wake_ring_connectivity
+
+    bn = np.array([[0, 1], [1, 2], [2, 3], [7, 6]])  # strips 0-2 chained, strip 3 separate and reversed
+    rep, cols, slot = wake_node_columns(bn)
+    assert rep.tolist() == [0, 1, 1, 3, 3, 5, 6, 7]
+    assert cols.tolist() == [0, 1, 3, 5, 6, 7]
+    assert (cols[slot] == rep).all()
+    R, S = 5, 4
+    plain = Mesh(2 * (R + 1) * S, wake_ring_connectivity(R, S))
+    merged = Mesh(2 * (R + 1) * S, wake_ring_connectivity(R, S, bn))
+    # per strip: R + 1 spanwise and 2 R streamwise lines; two shared columns save 2 R lines
+    assert plain.n_lines == S * (3 * R + 1)
+    assert merged.n_lines == plain.n_lines - 2 * R

@@ -97,7 +97,7 @@ def test_lu32_inverse_with_pivoting():
     assert rel < 1e-3, rel  # TF32 products in the updates: ~2^-11 relative on the off-diagonal part
 
 
-def test_wake_node_velocity_rows_split():
+def test_wake_node_velocity_column_and_row_split():
     import torch
 
     from pyvl_b200 import _lib
@@ -125,10 +125,10 @@ def test_wake_node_velocity_rows_split():
     ws = torch.empty(nb, dtype=torch.uint8, device="cuda")
     s = stream_ptr()
 
-    def run(prec, r0, r1, out):
-        _lib.call("pvl_wake_node_velocity_rows", prec, mesh.n_points, mesh.n_lines, ptr(d["lines"]), ptr(pos), ptr(lg),
-                  S, R, complete, r0, r1, ptr(wp), float(u[0]), float(u[1]), float(u[2]), case.tol, ptr(out), ptr(ws),
-                  nb, s)
+    def run(prec, r0, r1, out, n_cols=2 * S, cols=None):
+        _lib.call("pvl_wake_node_velocity_cols", prec, mesh.n_points, mesh.n_lines, ptr(d["lines"]), ptr(pos),
+                  ptr(lg), S, R, complete, r0, r1, n_cols, ptr(cols) if cols is not None else None, ptr(wp),
+                  float(u[0]), float(u[1]), float(u[2]), case.tol, ptr(out), ptr(ws), nb, s)
 
     full = torch.zeros((S, 2, complete, 3), dtype=torch.float64, device="cuda")
     _lib.call("pvl_wake_node_velocity", _lib.PVL_F64, mesh.n_points, mesh.n_lines, ptr(d["lines"]), ptr(pos), ptr(lg),
@@ -147,6 +147,17 @@ def test_wake_node_velocity_rows_split():
     ind_mixed = mixed - torch.as_tensor(u, device="cuda")
     rel = (torch.linalg.vector_norm(ind_mixed - ind_full) / torch.linalg.vector_norm(ind_full)).item()
     assert rel < 1e-5, rel
+    # de-duplicated columns: each representative column gets the full sweep's velocities
+    from pyvl_b200.engine import wake_node_columns
+
+    _, cols, slot = wake_node_columns(spec.bordering_nodes)
+    assert cols.size < 2 * S
+    dcols = torch.as_tensor(cols.astype(np.int32), device="cuda")
+    dedup = torch.full((cols.size, complete, 3), float("nan"), dtype=torch.float64, device="cuda")
+    run(_lib.PVL_F64, 0, complete, dedup, int(cols.size), dcols)
+    torch.cuda.synchronize()
+    want = full.reshape(2 * S, complete, 3)[torch.as_tensor(cols.astype(np.int64), device="cuda")]
+    assert torch.allclose(dedup, want, rtol=1e-13, atol=1e-13)
 
 
 def _mixed_engine(case, **kw):
@@ -169,7 +180,7 @@ def test_mixed_steps_judged_against_fp64(factory, kw, steps):
     from pyvl_b200 import workloads
 
     case = getattr(workloads, factory)(**kw)
-    eng = _mixed_engine(case, refresh=10, near_rows=4, advect_near_rows=4)
+    eng = _mixed_engine(case, refresh=10, advect_near_rows=4)
     errs = []
     for it in range(steps):
         t = it * case.dt
@@ -205,7 +216,7 @@ def test_mixed_trajectory_tracks_plain():
     mesh = Mesh(case.n_points, case.elements)
     plain = SolverEngine(mesh, case.freestream, case.tol,
                          wake_spec_from_te(mesh, case.te_node_pairs, case.line_rows, case.t0))
-    mixed = _mixed_engine(case, refresh=25, near_rows=4, advect_near_rows=4)
+    mixed = _mixed_engine(case, refresh=25, advect_near_rows=4)
     worst = 0.0
     for it in range(60):
         t = it * case.dt
