@@ -328,17 +328,52 @@ size_t pvl_lu32_workspace(uint32_t n);
 int pvl_lu32_factor(uint32_t n, float* A, uint32_t lda, int32_t* ipiv, int32_t* info, int32_t* err,
                     void* ws, size_t ws_bytes, void* stream);
 
-/* X = U^-1 L^-1 from pvl_lu32_factor's factors (same ws, not modified in between): blocked
- * triangular inversion, diagonal blocks in FP32 on CUDA cores, rank-64 updates on the
- * tensor cores.  Y (n x ldy) is scratch.  n a multiple of 64; leading dimensions multiples of
- * 4, arrays 16-byte aligned.  A^-1 b = X (P b) with (P b)[i] = b[perm[i]]. */
-int pvl_lu32_inverse(uint32_t n, const float* LU, uint32_t lda, float* X, uint32_t ldx, float* Y,
-                     uint32_t ldy, int32_t* err, void* ws, size_t ws_bytes, void* stream);
+/* X = U^-1 L^-1 P from pvl_lu32_factor's factors (same ws, not modified in between):
+ * blocked triangular inversion, diagonal blocks in FP32 on CUDA cores, rank-64 updates on the
+ * tensor cores; with perm (the second half of ipiv) the row permutation is folded into X's
+ * columns so that A^-1 b ~ X b (perm NULL: X = U^-1 L^-1).  Y (n x ldy) is scratch.  n a
+ * multiple of 64; leading dimensions multiples of 4, arrays 16-byte aligned.  The mixed solve
+ * applies X with pvl_gemv_f32mat. */
+int pvl_lu32_inverse(uint32_t n, const float* LU, uint32_t lda, const int32_t* perm, float* X, uint32_t ldx,
+                     float* Y, uint32_t ldy, int32_t* err, void* ws, size_t ws_bytes, void* stream);
 
-/* z = X v[perm] (X FP32, v and z FP64, FP64 accumulation): the preconditioner of the mixed
- * solve applied to a Krylov vector.  v and z must not alias. */
-int pvl_precond_apply(uint32_t n, const float* X, uint32_t ldx, const int32_t* perm, const double* v,
-                      double* z, void* stream);
+/* ------------------------------------------------------------------ learned warm start */
+/* The per-panel MLP that seeds the mixed solve: 12 inputs -> 128 -> 128 -> 1 (ReLU), BF16
+ * weights and activations, FP32 accumulation.  params_bf16 / params are the flat parameter
+ * vector (pvl_mlp_param_count() values: W1 128x12, b1, W2 128x128, b2, w3, b3) as BF16 and
+ * as FP32.  No reference counterpart (the reference solves every step from scratch,
+ * python/pyvl/solver.py:223-227). */
+uint32_t pvl_mlp_param_count(void);
+uint32_t pvl_mlp_input_count(void);
+
+/* Inputs of each panel from the device state of a step: g0/g1 the circulations of the last
+ * two steps, rem0/rem1 what those steps' solutions added to their own Jacobi corrections,
+ * resid = b - A g0 for the new system (A, lda; rhs = b) and rnorm[0] = ||resid||, rhs_prev
+ * the last step's RHS, normals and control-point velocities ((n, 3) each).  Increments are
+ * divided by s = ||resid|| / sqrt(n).  X (n, 12) = (input - mean) * inv_std;
+ * base = g0 + resid / diag(A) (one Jacobi correction). */
+int pvl_mlp_features(uint32_t n, const double* g0, const double* g1, const double* rem0, const double* rem1,
+                     const double* resid, const double* rnorm, const double* A, uint32_t lda, const double* rhs, const double* rhs_prev,
+                     const double* normals, const double* cp_vel, const float* mean, const float* inv_std,
+                     float* X, double* base, void* stream);
+
+/* out[i] = base[i] + scale * mul[0] * mlp(X[i]) (base and mul may be NULL; mul on the device). */
+int pvl_mlp_forward(uint32_t n, const float* X, const void* params_bf16, double scale, const double* mul,
+                    const double* base, double* out, void* stream);
+
+/* grad = d/dparams mean_i (mlp(X[i]) - T[i])^2 and *loss (device floats; loss may be NULL),
+ * over n samples with up to n_ctas persistent CTAs; ws of pvl_mlp_train_workspace(n_ctas)
+ * bytes.  The partial gradients of the CTAs are summed in a fixed order. */
+size_t pvl_mlp_train_workspace(uint32_t n_ctas);
+int pvl_mlp_gradient(uint32_t n, const float* X, const float* T, const void* params_bf16, uint32_t n_ctas,
+                     float* grad, float* loss, void* ws, size_t ws_bytes, void* stream);
+
+/* One Adam step (step >= 1) on the FP32 parameters with moments m, v; refreshes the BF16 copy. */
+int pvl_mlp_adam(float* params, void* params_bf16, const float* grad, float* m, float* v, uint32_t step,
+                 float lr, float beta1, float beta2, float eps, void* stream);
+
+/* params_bf16 = BF16(params). */
+int pvl_mlp_to_bf16(const float* params, void* params_bf16, void* stream);
 
 /* ------------------------------------------------------------------ forces */
 

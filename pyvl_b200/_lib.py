@@ -74,8 +74,16 @@ SIGNATURES = {
     "pvl_pad_convert_f32": (_I, [_U, _P, _U, _P, _U, _U, _P]),
     "pvl_lu32_workspace": (_Z, [_U]),
     "pvl_lu32_factor": (_I, [_U, _P, _U, _P, _P, _P, _P, _Z, _P]),
-    "pvl_lu32_inverse": (_I, [_U, _P, _U, _P, _U, _P, _U, _P, _P, _Z, _P]),
-    "pvl_precond_apply": (_I, [_U, _P, _U, _P, _P, _P, _P]),
+    "pvl_lu32_inverse": (_I, [_U, _P, _U, _P, _P, _U, _P, _U, _P, _P, _Z, _P]),
+    "pvl_mlp_param_count": (_U, []),
+    "pvl_mlp_input_count": (_U, []),
+    "pvl_mlp_features": (_I, [_U, _P, _P, _P, _P, _P, _P, _P, _U, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "pvl_mlp_forward": (_I, [_U, _P, _P, _D, _P, _P, _P, _P]),
+    "pvl_mlp_train_workspace": (_Z, [_U]),
+    "pvl_mlp_gradient": (_I, [_U, _P, _P, _P, _U, _P, _P, _P, _Z, _P]),
+    "pvl_mlp_adam": (_I, [_P, _P, _P, _P, _P, _U, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                          _P]),
+    "pvl_mlp_to_bf16": (_I, [_P, _P, _P]),
     "pvl_launch_count": (ctypes.c_ulonglong, []),
     "pvl_fma_probe": (_D, [_I, _U, _U, _P, _P]),
 }

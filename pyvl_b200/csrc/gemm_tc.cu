@@ -13,8 +13,8 @@
 // 16-byte chunk c at chunk c ^ (r%8)).  All threads stage a tile (A straight from its rows,
 // B transposed on the way); thread 0 issues four K=8 MMAs per tile and commits them to the
 // stage's mbarrier, which the threads wait on before overwriting that stage.  After the last
-// tile the four warps read their 32 TMEM lanes (rows) back with tcgen05.ld and combine them
-// with C.  Every wait is bounded; a time-out sets *err and the CTA still waits (bounded) for
+// tile the four warps read their 32 TMEM lanes (rows) back with tcgen05.ld into a shared FP32
+// tile, and then combine it with C in coalesced rows.  Every wait is bounded; a time-out sets *err and the CTA still waits (bounded) for
 // its own MMAs and frees its tensor memory before returning.
 #include <cstdint>
 
@@ -213,36 +213,45 @@ __global__ void __launch_bounds__(kThreads) gemm_tf32_kernel(uint32_t M, uint32_
         if (tid == 0)
             atomicExch(err, 1);
     } else if (n_kt > 0) {
-        // epilogue: warp w owns TMEM lanes (rows) 32w .. 32w+31 (every warp reads TMEM: the
-        // load is warp-collective; rows and columns past the edge are not stored)
-        const uint32_t row = m0 + 32 * warp + lane;
-        const bool row_ok = row < M;
-        float* crow = C + (size_t)(row_ok ? row : 0) * ldc + n0;
+        // epilogue, two phases through the (now idle) stage buffers:
+        // 1. warp w reads its 32 TMEM lanes (rows 32w .. 32w+31) and stores them row-wise into a
+        //    128 x 128 FP32 tile, 16-byte chunks XOR-swizzled by (row & 7) (conflict-free);
+        // 2. each warp walks rows w, w+4, ..., lane l owning columns 4l .. 4l+3, so that C is read
+        //    and written in 512-byte coalesced rows.
+        float* tile = reinterpret_cast<float*>(smem);
+        const uint32_t trow = 32 * warp + lane;
 #pragma unroll 1
         for (uint32_t c0 = 0; c0 < kTile; c0 += 16) {
             float v[16];
             __syncwarp();
             tmem_ld16(tmem + ((32u * warp) << 16) + c0, v);
-            if (!row_ok || n0 + c0 >= N)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t chunk = (c0 >> 2) + q;
+                *reinterpret_cast<float4*>(tile + trow * kTile + ((chunk ^ (trow & 7u)) << 2)) =
+                    make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            }
+        }
+        __syncthreads();
+        const uint32_t col = n0 + 4 * lane;
+#pragma unroll 1
+        for (uint32_t r = warp; r < kTile; r += kThreads / 32) {
+            const uint32_t grow = m0 + r;
+            if (grow >= M || col >= N)
                 continue;
-            if (n0 + c0 + 16 <= N) {
-#pragma unroll
-                for (int i = 0; i < 16; i += 4) {
-                    float4* p = reinterpret_cast<float4*>(crow + c0 + i);
-                    float4 o = beta == 0.0f ? make_float4(0.f, 0.f, 0.f, 0.f) : *p;
-                    o.x = alpha * v[i] + beta * o.x;
-                    o.y = alpha * v[i + 1] + beta * o.y;
-                    o.z = alpha * v[i + 2] + beta * o.z;
-                    o.w = alpha * v[i + 3] + beta * o.w;
-                    *p = o;
-                }
+            const float4 a = *reinterpret_cast<const float4*>(tile + r * kTile + ((lane ^ (r & 7u)) << 2));
+            float* crow = C + (size_t)grow * ldc + col;
+            if (col + 4 <= N) {
+                float4 o = beta == 0.0f ? make_float4(0.f, 0.f, 0.f, 0.f) : *reinterpret_cast<const float4*>(crow);
+                o.x = alpha * a.x + beta * o.x;
+                o.y = alpha * a.y + beta * o.y;
+                o.z = alpha * a.z + beta * o.z;
+                o.w = alpha * a.w + beta * o.w;
+                *reinterpret_cast<float4*>(crow) = o;
             } else {
-#pragma unroll
-                for (int i = 0; i < 16; ++i)
-                    if (n0 + c0 + i < N) {
-                        float* p = crow + c0 + i;
-                        *p = alpha * v[i] + (beta == 0.0f ? 0.0f : beta * *p);
-                    }
+                const float av[4] = {a.x, a.y, a.z, a.w};
+                for (uint32_t i = 0; i < 4 && col + i < N; ++i)
+                    crow[i] = alpha * av[i] + (beta == 0.0f ? 0.0f : beta * crow[i]);
             }
         }
     }

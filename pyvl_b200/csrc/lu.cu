@@ -735,26 +735,17 @@ __global__ void set_identity_kernel(uint32_t n, float* __restrict__ X, uint32_t 
     X[(size_t)r * ldx + c] = r == c ? 1.0f : 0.0f;
 }
 
-// z = alpha * X v[perm] + beta * z: the preconditioner applied to an FP64 vector (FP32 matrix,
-// FP64 accumulation), one warp per row.
-__global__ void __launch_bounds__(256) precond_apply_kernel(uint32_t n, const float* __restrict__ X, uint32_t ldx,
-                                                            const int32_t* __restrict__ perm,
-                                                            const double* __restrict__ v, double* __restrict__ z)
+// out[r][perm[c]] = X[r][c]: the inverse's columns permuted, so that A^-1 b = out b.
+__global__ void permute_columns_kernel(uint32_t n, const float* __restrict__ X, uint32_t ldx,
+                                       const int32_t* __restrict__ perm, float* __restrict__ out, uint32_t ldo)
 {
-    const uint32_t r = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-    if (r >= n)
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)n * n)
         return;
-    const float* row = X + (size_t)r * ldx;
-    double s = 0.0;
-    for (uint32_t j = lane; j < n; j += 32) {
-        const uint32_t q = (uint32_t)perm[j];
-        if (q < n)  // a valid factorisation never maps outside [0, n)
-            s += (double)row[j] * v[q];
-    }
-    for (int o = 16; o > 0; o >>= 1)
-        s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0)
-        z[r] = s;
+    const uint32_t r = (uint32_t)(t / n), c = (uint32_t)(t % n);
+    const uint32_t q = (uint32_t)perm[c];
+    if (q < n)  // a valid factorisation never maps outside [0, n)
+        out[(size_t)r * ldo + q] = X[(size_t)r * ldx + c];
 }
 
 }  // namespace
@@ -823,8 +814,9 @@ extern "C" int pvl_lu32_factor(uint32_t n, float* A, uint32_t lda, int32_t* ipiv
     return PVL_OK;
 }
 
-extern "C" int pvl_lu32_inverse(uint32_t n, const float* LU, uint32_t lda, float* X, uint32_t ldx, float* Y,
-                                uint32_t ldy, int32_t* err, void* ws, size_t ws_bytes, void* stream)
+extern "C" int pvl_lu32_inverse(uint32_t n, const float* LU, uint32_t lda, const int32_t* perm, float* X,
+                                uint32_t ldx, float* Y, uint32_t ldy, int32_t* err, void* ws, size_t ws_bytes,
+                                void* stream)
 {
     if (n == 0)
         return PVL_OK;
@@ -867,19 +859,12 @@ extern "C" int pvl_lu32_inverse(uint32_t n, const float* LU, uint32_t lda, float
                                       stream))
                 return r;
     }
-    return PVL_OK;
-}
-
-extern "C" int pvl_precond_apply(uint32_t n, const float* X, uint32_t ldx, const int32_t* perm, const double* v,
-                                 double* z, void* stream)
-{
-    if (n == 0)
-        return PVL_OK;
-    if (!X || !perm || !v || !z)
-        return pvl_fail(PVL_ERR_ARG, "pvl_precond_apply: null pointer argument");
-    if (v == z)
-        return pvl_fail(PVL_ERR_ARG, "pvl_precond_apply: v and z must not alias");
-    precond_apply_kernel<<<blocks_for(n, 8), 256, 0, (cudaStream_t)stream>>>(n, X, ldx, perm, v, z);
-    PVL_LAUNCH_CHECK();
+    if (perm) {
+        // A^-1 = U^-1 L^-1 P with (P b)[i] = b[perm[i]]: fold P into the columns
+        permute_columns_kernel<<<blocks_for((size_t)n * n, 256), 256, 0, st>>>(n, X, ldx, perm, Y, ldy);
+        PVL_LAUNCH_CHECK();
+        PVL_CUDA_CHECK(cudaMemcpy2DAsync(X, (size_t)ldx * sizeof(float), Y, (size_t)ldy * sizeof(float),
+                                         (size_t)n * sizeof(float), n, cudaMemcpyDeviceToDevice, st));
+    }
     return PVL_OK;
 }

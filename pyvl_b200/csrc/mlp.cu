@@ -1,0 +1,461 @@
+// The learned warm start of the mixed solve: a per-panel MLP, 12 -> 128 -> 128 -> 1, with
+// BF16 weights and BF16 activations and FP32 accumulation.  No reference counterpart: the
+// reference solves every step from scratch (python/pyvl/solver.py:223-227).
+//
+// Kernels:
+//   features_kernel -- the 12 normalised inputs of each panel and the base of the prediction
+//                      (previous circulation + one Jacobi correction of the new system);
+//   forward_kernel  -- inference: one CTA of 128 threads per tile of 32 panels, thread j owns
+//                      hidden unit j; W2 staged transposed in shared memory (conflict-free);
+//   train_kernel    -- forward + backward of the mean squared error over a batch, persistent
+//                      CTAs, each accumulating its gradient in shared memory (FP32) and
+//                      writing one partial gradient row; reduce_kernel sums the rows in a
+//                      fixed order (deterministic);
+//   adam_kernel     -- Adam (Kingma & Ba, 2015) on the FP32 master copy, refreshing the BF16
+//                      working copy.
+// Parameter vector (FP32 master and BF16 copy alike): W1 (128 x 12), b1 (128), W2 (128 x 128),
+// b2 (128), w3 (128), b3 (1).
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "pvl_common.cuh"
+
+namespace {
+
+constexpr int kIn = 12;
+constexpr int kH = 128;
+constexpr int kTile = 32;  // panels per tile
+constexpr int kThreads = kH;
+constexpr int oW1 = 0, oB1 = oW1 + kH * kIn, oW2 = oB1 + kH, oB2 = oW2 + kH * kH, oW3 = oB2 + kH, oB3 = oW3 + kH;
+constexpr int kParams = oB3 + 1;
+constexpr int kDW2Stride = kH + 1;  // padded rows of the W2 gradient (conflict-free row-per-thread updates)
+
+inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+__device__ __forceinline__ float bf(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+__device__ __forceinline__ float ldb(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+
+struct FwdSmem {
+    __nv_bfloat16 w2t[kH][kH];  // w2t[k][j] = W2[j][k]
+    float x[kTile][kIn];
+    float h1[kTile][kH];
+    float red[kThreads / 32][kTile];
+};
+
+// Layers 1 and 2 for one tile; returns h2[s] (BF16-rounded) for this thread's unit j in h2.
+__device__ __forceinline__ void tile_forward(const FwdSmem& sm, float (&h1s)[kTile][kH], const float (&w1)[kIn],
+                                             float b1, float b2, int ns, float (&h2)[kTile])
+{
+    const int j = threadIdx.x;
+    for (int s = 0; s < kTile; ++s) {
+        float a = b1;
+#pragma unroll
+        for (int i = 0; i < kIn; ++i)
+            a = fmaf(w1[i], sm.x[s][i], a);
+        h1s[s][j] = s < ns ? bf(fmaxf(a, 0.0f)) : 0.0f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < kTile; ++s)
+        h2[s] = b2;
+    for (int k = 0; k < kH; k += 4) {
+        float w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            w[q] = __bfloat162float(sm.w2t[k + q][j]);
+#pragma unroll
+        for (int s = 0; s < kTile; ++s) {
+            const float4 h = *reinterpret_cast<const float4*>(&h1s[s][k]);
+            h2[s] = fmaf(w[0], h.x, fmaf(w[1], h.y, fmaf(w[2], h.z, fmaf(w[3], h.w, h2[s]))));
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < kTile; ++s)
+        h2[s] = bf(fmaxf(h2[s], 0.0f));
+}
+
+// y[s] = b3 + sum_j w3[j] h2[s][j] for the tile (all threads take part; result in red[0][s]).
+__device__ __forceinline__ void tile_output(FwdSmem& sm, float w3, const float (&h2)[kTile])
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int s = 0; s < kTile; ++s) {
+        float v = w3 * h2[s];
+        for (int o = 16; o > 0; o >>= 1)
+            v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0)
+            sm.red[warp][s] = v;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void load_x_tile(FwdSmem& sm, const float* __restrict__ X, uint64_t s0, int ns)
+{
+    for (int e = threadIdx.x; e < kTile * kIn; e += kThreads) {
+        const int s = e / kIn, i = e % kIn;
+        sm.x[s][i] = s < ns ? bf(X[(s0 + s) * kIn + i]) : 0.0f;
+    }
+}
+
+__device__ __forceinline__ void load_w2t(FwdSmem& sm, const __nv_bfloat16* __restrict__ P)
+{
+    for (int e = threadIdx.x; e < kH * kH; e += kThreads) {
+        const int j = e / kH, k = e % kH;
+        sm.w2t[k][j] = P[oW2 + e];
+    }
+}
+
+// out[p] = base[p] + scale * mul[0] * y(p)   (base and mul may be NULL)
+__global__ void __launch_bounds__(kThreads) forward_kernel(uint32_t n, const float* __restrict__ X,
+                                                           const __nv_bfloat16* __restrict__ P, double scale,
+                                                           const double* __restrict__ mul,
+                                                           const double* __restrict__ base, double* __restrict__ out)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    FwdSmem& sm = *reinterpret_cast<FwdSmem*>(smem_raw);
+    const int j = threadIdx.x;
+    load_w2t(sm, P);
+    float w1[kIn];
+#pragma unroll
+    for (int i = 0; i < kIn; ++i)
+        w1[i] = ldb(P + oW1 + j * kIn + i);
+    const float b1 = ldb(P + oB1 + j), b2 = ldb(P + oB2 + j), w3 = ldb(P + oW3 + j), b3 = ldb(P + oB3);
+    const double sc = mul ? scale * mul[0] : scale;
+    for (uint64_t s0 = (uint64_t)blockIdx.x * kTile; s0 < n; s0 += (uint64_t)gridDim.x * kTile) {
+        const int ns = (int)(n - s0 < (uint64_t)kTile ? n - s0 : (uint64_t)kTile);
+        __syncthreads();
+        load_x_tile(sm, X, s0, ns);
+        __syncthreads();
+        float h2[kTile];
+        tile_forward(sm, sm.h1, w1, b1, b2, ns, h2);
+        tile_output(sm, w3, h2);
+        if (j < ns) {
+            float y = b3;
+            for (int w = 0; w < kThreads / 32; ++w)
+                y += sm.red[w][j];
+            out[s0 + j] = (base ? base[s0 + j] : 0.0) + sc * (double)y;
+        }
+    }
+}
+
+struct TrainSmem {
+    FwdSmem f;
+    __nv_bfloat16 w2[kH][kH];  // row-major W2 for the input gradient
+    float dh2[kTile][kH];
+    float dy[kTile];
+    float dW2[kH][kDW2Stride];
+    float loss[kThreads / 32];
+};
+
+// Forward + backward of mean((y - t)^2) over samples [0, n) (normalised by n_total, so that
+// batches can be split over launches), CTAs striding over 32-sample tiles.  Each CTA writes
+// its partial gradient to part[blockIdx.x * kParams + p] and its partial loss to
+// part_loss[blockIdx.x].
+__global__ void __launch_bounds__(kThreads, 1) train_kernel(uint32_t n, double n_total, const float* __restrict__ X,
+                                                            const float* __restrict__ T,
+                                                            const __nv_bfloat16* __restrict__ P,
+                                                            float* __restrict__ part, float* __restrict__ part_loss)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TrainSmem& sm = *reinterpret_cast<TrainSmem*>(smem_raw);
+    const int j = threadIdx.x, lane = j & 31, warp = j >> 5;
+    load_w2t(sm.f, P);
+    for (int e = j; e < kH * kH; e += kThreads)
+        sm.w2[e / kH][e % kH] = P[oW2 + e];
+    for (int e = j; e < kH * kDW2Stride; e += kThreads)
+        (&sm.dW2[0][0])[e] = 0.0f;
+    float w1[kIn], dW1[kIn];
+#pragma unroll
+    for (int i = 0; i < kIn; ++i) {
+        w1[i] = ldb(P + oW1 + j * kIn + i);
+        dW1[i] = 0.0f;
+    }
+    const float b1 = ldb(P + oB1 + j), b2 = ldb(P + oB2 + j), w3 = ldb(P + oW3 + j), b3 = ldb(P + oB3);
+    float db1 = 0.0f, db2 = 0.0f, dw3 = 0.0f, db3 = 0.0f, loss = 0.0f;
+    const float inv_n = (float)(2.0 / n_total);
+    for (uint64_t s0 = (uint64_t)blockIdx.x * kTile; s0 < n; s0 += (uint64_t)gridDim.x * kTile) {
+        const int ns = (int)(n - s0 < (uint64_t)kTile ? n - s0 : (uint64_t)kTile);
+        __syncthreads();
+        load_x_tile(sm.f, X, s0, ns);
+        __syncthreads();
+        float h2[kTile];
+        tile_forward(sm.f, sm.f.h1, w1, b1, b2, ns, h2);
+        tile_output(sm.f, w3, h2);
+        if (j < kTile) {
+            float d = 0.0f;
+            if (j < ns) {
+                float y = b3;
+                for (int w = 0; w < kThreads / 32; ++w)
+                    y += sm.f.red[w][j];
+                const float r = y - T[s0 + j];
+                loss += r * r;
+                d = r * inv_n;
+            }
+            sm.dy[j] = d;
+        }
+        __syncthreads();
+        // output layer and the gradient at h2 (unit j; kept in registers and shared)
+        float dh2[kTile];
+#pragma unroll
+        for (int s = 0; s < kTile; ++s) {
+            const float d = sm.dy[s];
+            if (j == 0)
+                db3 += d;
+            dw3 = fmaf(d, h2[s], dw3);
+            const float g = h2[s] > 0.0f ? d * w3 : 0.0f;
+            dh2[s] = g;
+            sm.dh2[s][j] = g;
+            db2 += g;
+        }
+        __syncthreads();
+        // dW2[j][k] += sum_s dh2[s][j] h1[s][k]      (thread j owns row j)
+        for (int k = 0; k < kH; ++k) {
+            float g = 0.0f;
+#pragma unroll
+            for (int s = 0; s < kTile; ++s)
+                g = fmaf(dh2[s], sm.f.h1[s][k], g);
+            sm.dW2[j][k] += g;
+        }
+        // dh1[s][k] = [h1 > 0] sum_j dh2[s][j] W2[j][k]  (thread k = j), then dW1, db1
+        float dh1[kTile];
+#pragma unroll
+        for (int s = 0; s < kTile; ++s)
+            dh1[s] = 0.0f;
+        for (int q = 0; q < kH; ++q) {
+            const float w = __bfloat162float(sm.w2[q][j]);
+#pragma unroll
+            for (int s = 0; s < kTile; ++s)
+                dh1[s] = fmaf(sm.dh2[s][q], w, dh1[s]);
+        }
+#pragma unroll
+        for (int s = 0; s < kTile; ++s) {
+            const float g = sm.f.h1[s][j] > 0.0f ? dh1[s] : 0.0f;
+            db1 += g;
+#pragma unroll
+            for (int i = 0; i < kIn; ++i)
+                dW1[i] = fmaf(g, sm.f.x[s][i], dW1[i]);
+        }
+    }
+    __syncthreads();
+    float* g = part + (size_t)blockIdx.x * kParams;
+#pragma unroll
+    for (int i = 0; i < kIn; ++i)
+        g[oW1 + j * kIn + i] = dW1[i];
+    g[oB1 + j] = db1;
+    for (int k = 0; k < kH; ++k)
+        g[oW2 + j * kH + k] = sm.dW2[j][k];
+    g[oB2 + j] = db2;
+    g[oW3 + j] = dw3;
+    if (j == 0)
+        g[oB3] = db3;
+    for (int o = 16; o > 0; o >>= 1)
+        loss += __shfl_xor_sync(0xffffffffu, loss, o);
+    if (lane == 0)
+        sm.loss[warp] = loss;
+    __syncthreads();
+    if (j == 0) {
+        float t = 0.0f;
+        for (int w = 0; w < kThreads / 32; ++w)
+            t += sm.loss[w];
+        part_loss[blockIdx.x] = t;
+    }
+}
+
+// grad[p] = sum over CTAs of part[c * kParams + p], in CTA order; loss likewise (thread 0).
+__global__ void reduce_kernel(uint32_t n_parts, const float* __restrict__ part, const float* __restrict__ part_loss,
+                              double n_total, float* __restrict__ grad, float* __restrict__ loss)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < kParams) {
+        float s = 0.0f;
+        for (uint32_t c = 0; c < n_parts; ++c)
+            s += part[(size_t)c * kParams + p];
+        grad[p] = s;
+    }
+    if (p == 0 && loss) {
+        double s = 0.0;
+        for (uint32_t c = 0; c < n_parts; ++c)
+            s += part_loss[c];
+        *loss = (float)(s / n_total);
+    }
+}
+
+__global__ void adam_kernel(float* __restrict__ w, __nv_bfloat16* __restrict__ wb, const float* __restrict__ g,
+                            float* __restrict__ m, float* __restrict__ v, float lr, float b1, float b2, float eps,
+                            float c1, float c2)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= kParams)
+        return;
+    const float gp = g[p];
+    const float mp = b1 * m[p] + (1.0f - b1) * gp;
+    const float vp = b2 * v[p] + (1.0f - b2) * gp * gp;
+    m[p] = mp;
+    v[p] = vp;
+    const float wn = w[p] - lr * (mp / c1) / (sqrtf(vp / c2) + eps);
+    w[p] = wn;
+    wb[p] = __float2bfloat16_rn(wn);
+}
+
+__global__ void to_bf16_kernel(uint32_t n, const float* __restrict__ w, __nv_bfloat16* __restrict__ wb)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n)
+        wb[p] = __float2bfloat16_rn(w[p]);
+}
+
+// Inputs of panel i (before normalisation):
+//   0 g0            1 g0 - g1        2 rem0           3 r_i / A_ii (r = b - A g0: one Jacobi step)
+//   4 b_i           5 b_i - bprev_i  6 A_ii + 2 pi    7..9 normal
+//   10 normal . control-point velocity               11 rem1
+// where rem0 / rem1 are what the last two steps' solutions added to their own Jacobi
+// corrections (gamma - base), the quantity the network predicts for this step.  The
+// increments (1, 2, 3, 5, 11) are divided by the step scale s = ||r|| / sqrt(n), so that the
+// network sees the shape of this step's change, not its size (s = 1 when r = 0).
+// X[i][f] = (v_f - mean_f) * inv_std_f; base[i] = g0_i + r_i / A_ii.
+__global__ void features_kernel(uint32_t n, const double* __restrict__ g0, const double* __restrict__ g1,
+                                const double* __restrict__ rem0, const double* __restrict__ rem1,
+                                const double* __restrict__ resid, const double* __restrict__ rnorm,
+                                const double* __restrict__ A, uint32_t lda,
+                                const double* __restrict__ rhs, const double* __restrict__ rhs_prev,
+                                const double* __restrict__ nrm, const double* __restrict__ cpv,
+                                const float* __restrict__ mean, const float* __restrict__ inv_std,
+                                float* __restrict__ X, double* __restrict__ base)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const double aii = A[(size_t)i * lda + i];
+    const double jac = aii != 0.0 ? resid[i] / aii : 0.0;
+    const double nx = nrm[3 * (size_t)i], ny = nrm[3 * (size_t)i + 1], nz = nrm[3 * (size_t)i + 2];
+    const double rn = rnorm[0] / sqrt((double)n);
+    const double inv_s = rn > 0.0 ? 1.0 / rn : 1.0;
+    double f[kIn];
+    f[0] = g0[i];
+    f[1] = (g0[i] - g1[i]) * inv_s;
+    f[2] = rem0[i] * inv_s;
+    f[3] = jac * inv_s;
+    f[4] = rhs[i];
+    f[5] = (rhs[i] - rhs_prev[i]) * inv_s;
+    f[6] = aii + 6.283185307179586;
+    f[7] = nx;
+    f[8] = ny;
+    f[9] = nz;
+    f[10] = nx * cpv[3 * (size_t)i] + ny * cpv[3 * (size_t)i + 1] + nz * cpv[3 * (size_t)i + 2];
+    f[11] = rem1[i] * inv_s;
+#pragma unroll
+    for (int k = 0; k < kIn; ++k)
+        X[(size_t)i * kIn + k] = (float)((f[k] - (double)mean[k]) * (double)inv_std[k]);
+    base[i] = g0[i] + jac;
+}
+
+bool g_attr_done = false;
+
+int set_attrs()
+{
+    if (g_attr_done)
+        return PVL_OK;
+    PVL_CUDA_CHECK(cudaFuncSetAttribute(forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sizeof(FwdSmem)));
+    PVL_CUDA_CHECK(cudaFuncSetAttribute(train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sizeof(TrainSmem)));
+    g_attr_done = true;
+    return PVL_OK;
+}
+
+}  // namespace
+
+extern "C" uint32_t pvl_mlp_param_count(void) { return kParams; }
+
+extern "C" uint32_t pvl_mlp_input_count(void) { return kIn; }
+
+extern "C" size_t pvl_mlp_train_workspace(uint32_t n_ctas)
+{
+    return ((size_t)n_ctas * kParams + n_ctas + kParams + 64) * sizeof(float);
+}
+
+extern "C" int pvl_mlp_features(uint32_t n, const double* g0, const double* g1, const double* rem0,
+                                const double* rem1, const double* resid, const double* rnorm, const double* A,
+                                uint32_t lda,
+                                const double* rhs, const double* rhs_prev, const double* normals, const double* cp_vel,
+                                const float* mean, const float* inv_std, float* X, double* base, void* stream)
+{
+    if (n == 0)
+        return PVL_OK;
+    if (!g0 || !g1 || !rem0 || !rem1 || !resid || !rnorm || !A || !rhs || !rhs_prev || !normals || !cp_vel || !mean ||
+        !inv_std || !X || !base)
+        return pvl_fail(PVL_ERR_ARG, "pvl_mlp_features: null pointer argument");
+    if (lda < n)
+        return pvl_fail(PVL_ERR_ARG, "pvl_mlp_features: lda < n");
+    features_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(n, g0, g1, rem0, rem1, resid, rnorm, A, lda, rhs,
+                                                                         rhs_prev, normals, cp_vel, mean, inv_std, X,
+                                                                         base);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_mlp_forward(uint32_t n, const float* X, const void* params_bf16, double scale, const double* mul,
+                               const double* base, double* out, void* stream)
+{
+    if (n == 0)
+        return PVL_OK;
+    if (!X || !params_bf16 || !out)
+        return pvl_fail(PVL_ERR_ARG, "pvl_mlp_forward: null pointer argument");
+    if (int r = set_attrs())
+        return r;
+    const unsigned grid = (unsigned)std::min<uint64_t>(blocks_for(n, kTile), 148ull * 4);
+    forward_kernel<<<grid, kThreads, sizeof(FwdSmem), (cudaStream_t)stream>>>(
+        n, X, static_cast<const __nv_bfloat16*>(params_bf16), scale, mul, base, out);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_mlp_gradient(uint32_t n, const float* X, const float* T, const void* params_bf16, uint32_t n_ctas,
+                                float* grad, float* loss, void* ws, size_t ws_bytes, void* stream)
+{
+    if (!X || !T || !params_bf16 || !grad || !ws)
+        return pvl_fail(PVL_ERR_ARG, "pvl_mlp_gradient: null pointer argument");
+    if (n == 0 || n_ctas == 0)
+        return pvl_fail(PVL_ERR_ARG, "pvl_mlp_gradient: empty batch or no CTAs");
+    if (ws_bytes < pvl_mlp_train_workspace(n_ctas))
+        return pvl_fail(PVL_ERR_ALLOC, "pvl_mlp_gradient: workspace too small");
+    if (int r = set_attrs())
+        return r;
+    cudaStream_t st = (cudaStream_t)stream;
+    float* part = static_cast<float*>(ws);
+    float* part_loss = part + (size_t)n_ctas * kParams;
+    const unsigned grid = (unsigned)std::min<uint64_t>(n_ctas, blocks_for(n, kTile));
+    train_kernel<<<grid, kThreads, sizeof(TrainSmem), st>>>(n, (double)n, X, T,
+                                                            static_cast<const __nv_bfloat16*>(params_bf16), part,
+                                                            part_loss);
+    PVL_LAUNCH_CHECK();
+    reduce_kernel<<<blocks_for(kParams, 256), 256, 0, st>>>(grid, part, part_loss, (double)n, grad, loss);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_mlp_adam(float* params, void* params_bf16, const float* grad, float* m, float* v, uint32_t step,
+                            float lr, float beta1, float beta2, float eps, void* stream)
+{
+    if (!params || !params_bf16 || !grad || !m || !v)
+        return pvl_fail(PVL_ERR_ARG, "pvl_mlp_adam: null pointer argument");
+    if (step == 0)
+        return pvl_fail(PVL_ERR_ARG, "pvl_mlp_adam: steps count from 1");
+    const float c1 = 1.0f - powf(beta1, (float)step), c2 = 1.0f - powf(beta2, (float)step);
+    adam_kernel<<<blocks_for(kParams, 256), 256, 0, (cudaStream_t)stream>>>(
+        params, static_cast<__nv_bfloat16*>(params_bf16), grad, m, v, lr, beta1, beta2, eps, c1, c2);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_mlp_to_bf16(const float* params, void* params_bf16, void* stream)
+{
+    if (!params || !params_bf16)
+        return pvl_fail(PVL_ERR_ARG, "pvl_mlp_to_bf16: null pointer argument");
+    to_bf16_kernel<<<blocks_for(kParams, 256), 256, 0, (cudaStream_t)stream>>>(
+        kParams, params, static_cast<__nv_bfloat16*>(params_bf16));
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}

@@ -73,26 +73,24 @@ template <> struct FarSeries<float> {
 // Follows the reference kernel (compute_line_induction, src/core/flow_solver.c:113-135):
 //   dr_k = p - r_k, t_k = d.dr_k, h^2 = ((|dr1|^2 - t1^2) + (|dr2|^2 - t2^2)) / 2,
 //   zero if h^2 < tol^2, else u = (dr1 x d) * (atan2(t2, h) - atan2(t1, h)) / h.
-// The angle difference is evaluated with one atan2 of the rotated pair: for h > 0,
-//   atan2(t2, h) - atan2(t1, h) = atan2(h (t2 - t1), h^2 + t1 t2)
-// and t2 - t1 = -len exactly, so the difference is atan2(-h len, h^2 + t1 t2).  This
-// is the same function of the inputs (the difference lies in (-pi, pi)), evaluated
-// without the cancellation of the two-atan2 form in the far field.  Far pairs evaluate
-// ang / h by the arctangent series of FarSeries.
+// Three exact identities of that formula are used:
+//   * dr2 = dr1 - len d, so t2 = t1 - len, and both perpendicular distances equal
+//     |dr1 x d|: h^2 = |c|^2 with c = dr1 x d, the vector the result points along anyway
+//     (no cancellation of |dr|^2 - t^2 for points near the segment's line);
+//   * for h > 0, atan2(t2, h) - atan2(t1, h) = atan2(h (t2 - t1), h^2 + t1 t2)
+//     = atan2(-h len, h^2 + t1 t2), one atan2 without the far-field cancellation of two;
+//   * far pairs evaluate ang / h by the arctangent series of FarSeries (no sqrt, no atan2).
 template <typename T>
 __device__ __forceinline__ void segment_induction(const Segment<T>& s, T px, T py, T pz, T tol2, T scale,
                                                   Vec3<T>& acc)
 {
     const T ax = px - s.r1x, ay = py - s.r1y, az = pz - s.r1z;
-    const T bx = px - s.r2x, by = py - s.r2y, bz = pz - s.r2z;
     const T t1 = s.dx * ax + s.dy * ay + s.dz * az;
-    const T t2 = s.dx * bx + s.dy * by + s.dz * bz;
-    const T n1 = (ax * ax + ay * ay + az * az) - t1 * t1;
-    const T n2 = (bx * bx + by * by + bz * bz) - t2 * t2;
-    const T hsq = (n1 + n2) / T(2);
+    const T cx = ay * s.dz - az * s.dy, cy = az * s.dx - ax * s.dz, cz = ax * s.dy - ay * s.dx;
+    const T hsq = cx * cx + cy * cy + cz * cz;
     if (hsq < tol2 || s.len < T(0))
         return;
-    const T x = hsq + t1 * t2;
+    const T x = hsq + t1 * (t1 - s.len);
     const T hl2 = hsq * (s.len * s.len);
     T mag;
     if (x > T(0) && hl2 <= FarSeries<T>::kW * (x * x)) {
@@ -105,10 +103,9 @@ __device__ __forceinline__ void segment_induction(const Segment<T>& s, T px, T p
         const T ang = atan2(-h * s.len, x);
         mag = scale * ang * rh;
     }
-    // (dr1 x d) * mag
-    acc.x += (ay * s.dz - az * s.dy) * mag;
-    acc.y += (az * s.dx - ax * s.dz) * mag;
-    acc.z += (ax * s.dy - ay * s.dx) * mag;
+    acc.x += cx * mag;
+    acc.y += cy * mag;
+    acc.z += cz * mag;
 }
 
 }  // namespace pvl

@@ -418,15 +418,18 @@ class MixedSolverEngine(SolverEngine):
         self.V = torch.zeros((m + 1, n), **f64)
         self.Z = torch.zeros((m, n), **f64)
         self.wv = torch.zeros(n, **f64)
-        self.hbuf = torch.zeros(2 * (m + 2), **f64)
+        self.Hd = torch.zeros((m, 2 * (m + 2)), **f64)  # column j: h[0..j+1] and basis_project scratch
+        self.h_H = torch.zeros((m, 2 * (m + 2)), dtype=torch.float64, pin_memory=True)
         self.scal = torch.zeros(2, **f64)
+        self.h_sc = torch.zeros(2, dtype=torch.float64, pin_memory=True)
+        self.spec_iters = 2
         self.y = torch.zeros(m, **f64)
         self.x = torch.zeros(n, **f64)
         self.b_saved = torch.zeros(n, **f64)
-        self.h_h = torch.zeros(2 * (m + 2), dtype=torch.float64, pin_memory=True)
         self.have_precond = False
         self.steps_since_refresh = 0
-        self.stats = {"gmres_iters": [], "fallbacks": 0, "refreshes": 0, "final_rel_residual": [], "judge": []}
+        self.stats = {"gmres_iters": [], "fallbacks": 0, "refreshes": 0, "initial_rel_residual": [],
+                      "final_rel_residual": [], "judge": []}
         need = _lib.query("pvl_lu32_workspace", self.npad)
         if self.wake is not None:
             need = max(need, self._init_row_major_wake(near_rows, advect_near_rows))
@@ -501,15 +504,34 @@ class MixedSolverEngine(SolverEngine):
         ws, nb = ptr(self.ws), self._ws_bytes
         _lib.call("pvl_lu32_factor", npad, ptr(self.A32), npad, ptr(self.ipiv32), ptr(self.info32), ptr(self.err32),
                   ws, nb, s)
-        _lib.call("pvl_lu32_inverse", npad, ptr(self.A32), npad, ptr(self.Xinv), npad, ptr(self.Yscr), npad,
+        perm = self.ipiv32.data_ptr() + 4 * npad
+        _lib.call("pvl_lu32_inverse", npad, ptr(self.A32), npad, perm, ptr(self.Xinv), npad, ptr(self.Yscr), npad,
                   ptr(self.err32), ws, nb, s)
         self.have_precond = True
         self.steps_since_refresh = 0
         self.stats["refreshes"] += 1
 
     # ------------------------------------------------------------------ GMRES
+    def _arnoldi(self, j: int) -> None:
+        """Column j of the right-preconditioned Arnoldi process, entirely on the device:
+        Z_j = M V_j, w = A Z_j, two classical Gram-Schmidt passes into Hd[j][0..j],
+        Hd[j][j+1] = ||w||, V_{j+1} = w / ||w||."""
+        s = stream_ptr()
+        n = self.N
+        hj = self.Hd[j]
+        _lib.call("pvl_gemv_f32mat", n, n, 1.0, ptr(self.Xinv), self.npad, ptr(self.V[j]), 0.0, ptr(self.Z[j]), s)
+        _lib.call("pvl_gemv_f64", n, n, 1.0, ptr(self.A), self.N, ptr(self.Z[j]), 0.0, ptr(self.wv), s)
+        for _ in range(2):
+            _lib.call("pvl_basis_project", n, j + 1, ptr(self.V), n, ptr(self.wv), ptr(hj), s)
+        _lib.call("pvl_normalize", n, ptr(self.wv), ptr(self.V[j + 1]), hj.data_ptr() + 8 * (j + 1), s)
+
     def solve_mixed(self, x0: torch.Tensor | None = None) -> bool:
-        """Right-preconditioned GMRES on A x = b in FP64; True if the relative residual met gmres_tol."""
+        """Right-preconditioned GMRES on A x = b in FP64; True if the relative residual met gmres_tol.
+
+        The Arnoldi columns run on the device without host round trips; the host reads the
+        small Hessenberg matrix after ``spec_iters`` columns (the last solve's iteration count),
+        then one column at a time, applies the Givens rotations and forms the update.  The true
+        FP64 residual b - A x decides convergence."""
         s = stream_ptr()
         n = self.N
         A, b = self.A, self.rhs
@@ -521,34 +543,38 @@ class MixedSolverEngine(SolverEngine):
             x.copy_(x0.reshape(-1)[:n])
         else:
             x[: self.P].copy_(self.gamma)  # the previous step's circulation
-        perm = self.ipiv32.data_ptr() + 4 * self.npad
-        hb, sc = self.hbuf, self.scal
-        # r0 = b - A x0 ; ||b|| and ||r0|| in one host read
+        sc = self.scal
         self.wv.copy_(b)
         _lib.call("pvl_gemv_f64", n, n, -1.0, ptr(A), self.N, ptr(x), 1.0, ptr(self.wv), s)
         _lib.call("pvl_normalize", n, ptr(b), None, sc.data_ptr(), s)
         _lib.call("pvl_normalize", n, ptr(self.wv), ptr(self.V[0]), sc.data_ptr() + 8, s)
-        bnorm, beta = (float(v) for v in sc.cpu())
-        target = self.gmres_tol * bnorm
-        iters = 0
-        if beta > target:
-            m = self.max_iter
-            H = np.zeros((m + 1, m))
-            cs, sn = np.zeros(m), np.zeros(m)
-            g = np.zeros(m + 1)
-            g[0] = beta
-            k = 0
-            hh = self.h_h
-            for j in range(m):
-                _lib.call("pvl_precond_apply", n, ptr(self.Xinv), self.npad, perm, ptr(self.V[j]), ptr(self.Z[j]), s)
-                _lib.call("pvl_gemv_f64", n, n, 1.0, ptr(A), self.N, ptr(self.Z[j]), 0.0, ptr(self.wv), s)
-                hb.zero_()
-                for _ in range(2):  # classical Gram-Schmidt, twice
-                    _lib.call("pvl_basis_project", n, j + 1, ptr(self.V), n, ptr(self.wv), ptr(hb), s)
-                _lib.call("pvl_normalize", n, ptr(self.wv), ptr(self.V[j + 1]), hb.data_ptr() + 8 * (j + 1), s)
-                hh[: j + 2].copy_(hb[: j + 2], non_blocking=True)
-                torch.cuda.current_stream().synchronize()
-                H[: j + 2, j] = hh[: j + 2].numpy()
+        self.Hd.zero_()
+        m = self.max_iter
+        H = np.zeros((m + 1, m))
+        cs, sn = np.zeros(m), np.zeros(m)
+        g = np.zeros(m + 1)
+        k, done, first = 0, False, True
+        bnorm = beta = target = 0.0
+        while k < m and not done:
+            nxt = min(m, k + (self.spec_iters if first else 1))
+            for j in range(k, nxt):
+                self._arnoldi(j)
+            self.h_H[: nxt].copy_(self.Hd[: nxt], non_blocking=True)
+            if first:
+                self.h_sc.copy_(sc, non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+            if first:
+                bnorm, beta = float(self.h_sc[0]), float(self.h_sc[1])
+                self.stats["initial_rel_residual"].append(beta / max(bnorm, 1e-300))
+                target = self.gmres_tol * bnorm
+                g[0] = beta
+                first = False
+                if beta <= target:
+                    k, done = 0, True
+                    break
+            hh = self.h_H.numpy()
+            for j in range(k, nxt):
+                H[: j + 2, j] = hh[j, : j + 2]
                 hnext = H[j + 1, j]
                 for i in range(j):  # previous Givens rotations
                     t = cs[i] * H[i, j] + sn[i] * H[i + 1, j]
@@ -562,19 +588,21 @@ class MixedSolverEngine(SolverEngine):
                 g[j] = cs[j] * g[j]
                 k = j + 1
                 if abs(g[j + 1]) <= target or hnext == 0.0:  # converged, or the Krylov space is exhausted
+                    done = True
                     break
+        if k:
             yk = np.zeros(k)
             for i in range(k - 1, -1, -1):  # back substitution with the rotated Hessenberg
                 yk[i] = (g[i] - H[i, i + 1:k] @ yk[i + 1:]) / H[i, i] if H[i, i] != 0.0 else 0.0
             self.y[:k].copy_(torch.from_numpy(yk))
             _lib.call("pvl_combine", n, k, ptr(self.Z), n, ptr(self.y), ptr(x), s)
-            iters = k
+            self.spec_iters = max(1, k)
         # the true FP64 residual decides
         self.wv.copy_(b)
         _lib.call("pvl_gemv_f64", n, n, -1.0, ptr(A), self.N, ptr(x), 1.0, ptr(self.wv), s)
         _lib.call("pvl_normalize", n, ptr(self.wv), None, sc.data_ptr(), s)
         rel = float(sc[0].item()) / max(bnorm, 1e-300)
-        self.stats["gmres_iters"].append(iters)
+        self.stats["gmres_iters"].append(k)
         self.stats["final_rel_residual"].append(rel)
         return rel <= self.gmres_tol
 

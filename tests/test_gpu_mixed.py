@@ -35,7 +35,8 @@ def _lu32_inverse(A64):
     s = stream_ptr()
     _lib.call("pvl_pad_convert_f32", n, ptr(A64), n, ptr(A32), npad, npad, s)
     _lib.call("pvl_lu32_factor", npad, ptr(A32), npad, ptr(ipiv), ptr(info), ptr(err), ptr(ws), nb, s)
-    _lib.call("pvl_lu32_inverse", npad, ptr(A32), npad, ptr(X), npad, ptr(Y), npad, ptr(err), ptr(ws), nb, s)
+    _lib.call("pvl_lu32_inverse", npad, ptr(A32), npad, ipiv.data_ptr() + 4 * npad, ptr(X), npad, ptr(Y), npad,
+              ptr(err), ptr(ws), nb, s)
     torch.cuda.synchronize()
     assert int(info.item()) == 0 and int(err.item()) == 0
     perm = ipiv[npad:].long()
@@ -43,14 +44,14 @@ def _lu32_inverse(A64):
 
 
 def _apply(X, perm, n, v):
+    """z = X v with the permutation already folded into X's columns."""
     import torch
 
     from pyvl_b200 import _lib
     from pyvl_b200.device import ptr, stream_ptr
 
     z = torch.zeros(n, dtype=torch.float64, device="cuda")
-    _lib.call("pvl_precond_apply", n, ptr(X), X.shape[1], perm.to(torch.int32).data_ptr(), ptr(v), ptr(z),
-              stream_ptr())
+    _lib.call("pvl_gemv_f32mat", n, n, 1.0, ptr(X), X.shape[1], ptr(v), 0.0, ptr(z), stream_ptr())
     torch.cuda.synchronize()
     return z
 
