@@ -375,6 +375,72 @@ int pvl_mlp_adam(float* params, void* params_bf16, const float* grad, float* m, 
 /* params_bf16 = BF16(params). */
 int pvl_mlp_to_bf16(const float* params, void* params_bf16, void* stream);
 
+/* ------------------------------------------------------------------ batched cases */
+/* Many independent cases of uneven size stepped with one launch per kernel over the whole
+ * batch (persistent CTAs taking work items from an atomic counter).  The batch is one
+ * concatenated mesh plus device job tables that keep each case's pairs inside the case; the
+ * table records are the structs of csrc/batch.cu, whose sizes the *_bytes() queries return
+ * (the host packs them with the same field order: see pyvl_b200/batch.py).  No reference
+ * counterpart: the reference steps one geometry per solver loop (solver.py:145-265). */
+size_t pvl_batch_ring_job_bytes(void);
+size_t pvl_batch_sweep_job_bytes(void);
+size_t pvl_batch_wake_case_bytes(void);
+size_t pvl_batch_solve_case_bytes(void);
+size_t pvl_batch_gmres_state_bytes(void);
+uint32_t pvl_batch_gmres_max_iter(void);
+
+/* Segment table (pvl_segments_workspace bytes) of a line set: r1, r2, unit direction,
+ * length (negative below tol), line circulation (1 when line_gamma is NULL). */
+int pvl_prep_segments(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
+                      const double* positions, const double* line_gamma, double tol, void* segments,
+                      void* stream);
+
+/* Ring-matrix blocks of every job: out[job.out_begin + i*ld + j] = n_i . sum_{k in ring j} +-u_k(cp_i)
+ * (FP64).  cpb = control points per CTA (4, 8 or 16; the autotuner's choice); n_ctas 0 = fill
+ * the GPU.  counter: one device uint32 (reset by the call). */
+int pvl_batch_ring_matrix(int cpb, const void* jobs, const uint32_t* job_item, uint32_t n_jobs, uint32_t n_items,
+                          uint32_t* counter, const uint32_t* offsets, const uint32_t* surface_lines,
+                          uint32_t n_lines, const void* segments, const double* cps, const double* normals,
+                          double tol, double* out, uint32_t n_ctas, void* stream);
+
+/* Segment sweeps of every job into per-job partials (FP64); tile = (threads, points per
+ * thread) in {(128,1),(128,2),(128,4),(256,1),(256,2)}; rows: device uint32 (the step's row
+ * count for jobs whose point count grows with the wake). */
+int pvl_batch_sweep(int threads, int ppt, const void* jobs, const uint32_t* job_item, uint32_t n_jobs,
+                    uint32_t n_items, uint32_t* counter, const uint32_t* rows, const void* segments,
+                    const double* pts, const uint32_t* pidx, double tol, double* partials, uint32_t n_ctas,
+                    void* stream);
+
+/* Reduce the sweeps' partials: mode 0 jobs add n . v to out (the RHS), mode 1 jobs write
+ * U_case + v (node velocities; uinf is (n_cases, 3)).  pt_item: first thread of each job. */
+int pvl_batch_sweep_reduce(const void* jobs, const uint32_t* pt_item, uint32_t n_jobs, uint32_t n_total,
+                           const uint32_t* rows, const double* partials, const double* normals,
+                           const double* uinf, double* out, void* stream);
+
+/* Per-case wake bookkeeping of pvl_wake_fold_implicit / pvl_wake_advect_cols / pvl_wake_shed
+ * over every case (row_case, node_case, circ_case: the case of each row / node / circulation). */
+int pvl_batch_fold_implicit(const void* cases, const uint32_t* row_case, uint32_t n_rows,
+                            const double* implicit, const uint32_t* adjacent, double* A, void* stream);
+int pvl_batch_wake_advect(const void* cases, const uint32_t* node_case, uint32_t n_nodes, uint32_t R,
+                          const uint32_t* rows, const double* old_pos, const double* node_vel,
+                          const uint32_t* col_slot, const double* body, const uint32_t* bordering_nodes,
+                          double* new_pos, void* stream);
+int pvl_batch_wake_shed(const void* cases, const uint32_t* circ_case, uint32_t n_circ, uint32_t R,
+                        const double* old_circ, const uint32_t* adjacent, const double* gamma,
+                        double* new_circ, void* stream);
+
+/* *value += 1 on the device (the step counter of a captured step). */
+int pvl_batch_increment(uint32_t* value, void* stream);
+
+/* Jacobi right-preconditioned GMRES of every case with FP64 residuals, entirely on the device
+ * (no host synchronisation: capturable in a CUDA graph).  x holds the start and receives the
+ * solution; max_iter (<= 16) iterations are launched, converged cases skip their work.
+ * fail_flags[c] = 1 where ||b - A x||_c > 10 tol ||b||_c; fail_count accumulates their number. */
+size_t pvl_batch_gmres_workspace(uint32_t n_rows, uint32_t n_cases, uint32_t max_iter);
+int pvl_batch_gmres(const void* cases, const uint32_t* row_case, uint32_t n_rows, uint32_t n_cases,
+                    const double* A, const double* b, double* x, uint32_t max_iter, double tol,
+                    uint8_t* fail_flags, uint32_t* fail_count, void* ws, size_t ws_bytes, void* stream);
+
 /* ------------------------------------------------------------------ forces */
 
 /* Kutta-Joukowski line forces F_k = (r_end - r_begin) x (0.5 c_k (v_p1 + v_p2)),

@@ -75,6 +75,22 @@ SIGNATURES = {
     "pvl_lu32_workspace": (_Z, [_U]),
     "pvl_lu32_factor": (_I, [_U, _P, _U, _P, _P, _P, _P, _Z, _P]),
     "pvl_lu32_inverse": (_I, [_U, _P, _U, _P, _P, _U, _P, _U, _P, _P, _Z, _P]),
+    "pvl_batch_ring_job_bytes": (_Z, []),
+    "pvl_batch_sweep_job_bytes": (_Z, []),
+    "pvl_batch_wake_case_bytes": (_Z, []),
+    "pvl_batch_solve_case_bytes": (_Z, []),
+    "pvl_batch_gmres_state_bytes": (_Z, []),
+    "pvl_batch_gmres_max_iter": (_U, []),
+    "pvl_prep_segments": (_I, [_I, _U, _U, _P, _P, _P, _D, _P, _P]),
+    "pvl_batch_ring_matrix": (_I, [_I, _P, _P, _U, _U, _P, _P, _P, _U, _P, _P, _P, _D, _P, _U, _P]),
+    "pvl_batch_sweep": (_I, [_I, _I, _P, _P, _U, _U, _P, _P, _P, _P, _P, _D, _P, _U, _P]),
+    "pvl_batch_sweep_reduce": (_I, [_P, _P, _U, _U, _P, _P, _P, _P, _P, _P]),
+    "pvl_batch_fold_implicit": (_I, [_P, _P, _U, _P, _P, _P, _P]),
+    "pvl_batch_wake_advect": (_I, [_P, _P, _U, _U, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "pvl_batch_wake_shed": (_I, [_P, _P, _U, _U, _P, _P, _P, _P, _P]),
+    "pvl_batch_increment": (_I, [_P, _P]),
+    "pvl_batch_gmres_workspace": (_Z, [_U, _U, _U]),
+    "pvl_batch_gmres": (_I, [_P, _P, _U, _U, _P, _P, _P, _U, _D, _P, _P, _P, _Z, _P]),
     "pvl_mlp_param_count": (_U, []),
     "pvl_mlp_input_count": (_U, []),
     "pvl_mlp_features": (_I, [_U, _P, _P, _P, _P, _P, _P, _P, _U, _P, _P, _P, _P, _P, _P, _P, _P, _P]),

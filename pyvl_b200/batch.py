@@ -1,0 +1,435 @@
+"""Batched stepping of many independent wings (or bodies) of uneven size.
+
+``BatchEngine(cases)`` steps every case of a list of workload ``Case`` objects together, one
+launch per kernel over the whole batch (csrc/batch.cu), with the same per-case arithmetic as
+``SolverEngine``: control points, normals and RHS, the body matrix, the implicit first wake row
+folded into it, the explicit wake rows in the RHS, the solve, the wake advection by freestream
+plus body induction, and the shedding of the trailing-edge circulation (python/pyvl/solver.py:175-263,
+python/pyvl/wake_models.py:83-223 per case).  The solve is the device-resident Jacobi-preconditioned
+GMRES with FP64 residuals (tolerance ``solve_tol``, relative residual), so a whole step runs without
+host synchronisation and, from the second step on, is captured once as a CUDA graph and replayed.
+``tune()`` is the autotuner: it times every tile shape of the persistent sweep and ring kernels on
+this batch and keeps the fastest.
+
+The reference steps one geometry per solver loop and has no batched form; a per-case loop of
+``SolverEngine`` is the comparison (bench.py --workload batch).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+from .cvl import Mesh
+from .device import ptr, require_cuda, stream_ptr, to_device_u32
+from .engine import wake_node_columns, wake_ring_connectivity, wake_row0_mesh, wake_spec_from_te
+
+RING_JOB = np.dtype([("cp_begin", "<u4"), ("n_cp", "<u4"), ("ring_begin", "<u4"), ("n_rings", "<u4"),
+                     ("out_begin", "<u8"), ("ld", "<u4"), ("item_begin", "<u4")])
+SWEEP_JOB = np.dtype([(k, "<u4") for k in ("seg_begin", "seg_count", "pt_begin", "pt_max", "pt_per_row",
+                                          "out_begin", "n_split", "per", "part_begin", "item_begin", "mode",
+                                          "case_id")])
+WAKE_CASE = np.dtype({"names": ["P", "S", "n_cols", "ring_begin", "mat_begin", "imp_begin", "shed_begin",
+                                "pos_begin", "circ_begin", "vel_begin", "dt"],
+                      "formats": ["<u4", "<u4", "<u4", "<u4", "<u8", "<u4", "<u4", "<u4", "<u4", "<u4", "<f8"],
+                      "offsets": [0, 4, 8, 12, 16, 24, 28, 32, 36, 40, 48], "itemsize": 56})
+SOLVE_CASE = np.dtype([("row_begin", "<u4"), ("n", "<u4"), ("mat_begin", "<u8")])
+
+SWEEP_TILES = [(128, 1), (128, 2), (128, 4), (256, 1), (256, 2)]
+RING_TILES = [4, 8, 16]
+
+
+def _check_layouts() -> None:
+    for name, dt in (("ring_job", RING_JOB), ("sweep_job", SWEEP_JOB), ("wake_case", WAKE_CASE),
+                     ("solve_case", SOLVE_CASE)):
+        n = int(_lib.query(f"pvl_batch_{name}_bytes"))
+        if n != dt.itemsize:
+            raise RuntimeError(f"batch record {name}: library has {n} bytes, host layout {dt.itemsize}")
+
+
+def _dev_records(arr: np.ndarray, dev) -> torch.Tensor:
+    return torch.as_tensor(np.frombuffer(arr.tobytes(), np.uint8).copy(), device=dev)
+
+
+def _splits(n_segments: int, n_points: int, pts_per_cta: int, target_ctas: int = 148 * 8) -> tuple[int, int]:
+    """Segment ranges of one sweep job: enough work items for the GPU, >= 2 tiles per range."""
+    blocks = max(1, -(-n_points // pts_per_cta))
+    s = max(1, -(-target_ctas // blocks))
+    s = min(s, max(1, -(-n_segments // 256)))
+    per = -(-n_segments // s)
+    return -(-n_segments // per), per
+
+
+class BatchEngine:
+    """Every case of ``cases`` stepped together on the device (see the module docstring)."""
+
+    def __init__(self, cases, solve_tol: float = 1e-12, max_iter: int = 8, tile: dict | None = None,
+                 host_only: bool = False):
+        self.host_only = host_only  # build the tables on the host only (layout checks without a GPU)
+        self.dev = torch.device("cpu") if host_only else require_cuda()
+        _check_layouts()
+        self.cases = list(cases)
+        B = self.B = len(self.cases)
+        if B == 0:
+            raise ValueError("empty batch")
+        R = {int(c.line_rows) for c in self.cases}
+        if len(R) != 1:
+            raise ValueError("every case of a batch needs the same number of wake rows")
+        self.R = R = R.pop()
+        tols = {float(c.tol) for c in self.cases}
+        if len(tols) != 1:
+            raise ValueError("every case of a batch needs the same vortex tolerance")
+        self.tol = tols.pop()
+        self.solve_tol = float(solve_tol)
+        self.max_iter = int(max_iter)
+        self.tile = dict(tile or {"sweep": (128, 2), "ring": 8})
+        dev = self.dev
+        f64 = dict(dtype=torch.float64, device=dev)
+
+        # ---------------- topology, per case and concatenated
+        meshes, wmeshes, row0s, specs = [], [], [], []
+        P, S, NC, NP, L, WL = [], [], [], [], [], []
+        cols_all, slot_all, bn_all, adj_all = [], [], [], []
+        for c in self.cases:
+            m = Mesh(c.n_points, c.elements)
+            spec = wake_spec_from_te(m, c.te_node_pairs, R, c.t0)
+            s_ = int(spec.shedding_lines.size)
+            bn = np.asarray(spec.bordering_nodes, np.int64).reshape(s_, 2)
+            wm = Mesh(2 * (R + 1) * s_, wake_ring_connectivity(R, s_, bn))
+            _, cols, slot = wake_node_columns(bn)
+            meshes.append(m)
+            wmeshes.append(wm)
+            row0s.append(wake_row0_mesh(wm, s_, R))
+            specs.append(spec)
+            P.append(m.n_surfaces)
+            S.append(s_)
+            NC.append(int(cols.size))
+            NP.append(m.n_points)
+            L.append(m.n_lines)
+            WL.append(wm.n_lines)
+            cols_all.append(cols)
+            slot_all.append(slot)
+            bn_all.append(bn)
+            adj_all.append(np.asarray(spec.adjacent_surfaces, np.int64).reshape(s_, 2))
+        self.P, self.S, self.NC = np.array(P), np.array(S), np.array(NC)
+        ring_off = np.concatenate([[0], np.cumsum(P)]).astype(np.int64)
+        pt_off = np.concatenate([[0], np.cumsum(NP)]).astype(np.int64)
+        line_off = np.concatenate([[0], np.cumsum(L)]).astype(np.int64)
+        wline_off = np.concatenate([[0], np.cumsum(WL)]).astype(np.int64)
+        shed_off = np.concatenate([[0], np.cumsum(S)]).astype(np.int64)
+        wpt_off = 2 * (R + 1) * shed_off
+        mat_off = np.concatenate([[0], np.cumsum(np.asarray(P, np.int64) ** 2)]).astype(np.int64)
+        imp_off = np.concatenate([[0], np.cumsum(np.asarray(P, np.int64) * np.asarray(S))]).astype(np.int64)
+        vel_off = np.concatenate([[0], np.cumsum(np.asarray(NC, np.int64) * R)]).astype(np.int64)
+        self.ring_off, self.pt_off, self.mat_off = ring_off, pt_off, mat_off
+        self.n_rings, self.n_points = int(ring_off[-1]), int(pt_off[-1])
+        self.body = Mesh.merge_meshes(*meshes)
+        self.wake_mesh = Mesh.merge_meshes(*wmeshes)
+        # row-0 rings reference the wake lines: rebase them onto the merged wake mesh's lines
+        sl0 = []
+        for k, r0 in enumerate(row0s):
+            g = r0.surface_lines.astype(np.uint64)
+            sl0.append(((g & np.uint64(0x7FFFFFFF)) + np.uint64(wline_off[k])) | (g & np.uint64(0x80000000)))
+        off0 = np.concatenate([[0], np.cumsum([r.n_surfaces and int(r.surface_offsets[-1]) for r in row0s])])
+        self.row0_offsets = np.concatenate(
+            [[0]] + [r.surface_offsets[1:].astype(np.int64) + off0[k] for k, r in enumerate(row0s)]).astype(np.uint32)
+        self.row0_lines = np.concatenate(sl0).astype(np.uint32)
+        self.d_body = None if host_only else self.body.device_arrays()
+        self.d_wake = None if host_only else self.wake_mesh.device_arrays()
+        self.d_row0 = {"offsets": to_device_u32(self.row0_offsets, dev), "lines": to_device_u32(self.row0_lines, dev)}
+        n_wake_pts = int(wpt_off[-1])
+        self.n_wake_pts = n_wake_pts
+
+        # ---------------- per-case tables
+        uinf = np.stack([np.asarray(c.freestream, np.float64) for c in self.cases])
+        self.uinf = torch.as_tensor(uinf, device=dev)
+        self.flow = torch.as_tensor(np.repeat(uinf, P, axis=0), device=dev)
+        wc = np.zeros(B, WAKE_CASE)
+        wc["P"], wc["S"], wc["n_cols"] = P, S, NC
+        wc["ring_begin"], wc["mat_begin"], wc["imp_begin"] = ring_off[:-1], mat_off[:-1], imp_off[:-1]
+        wc["shed_begin"], wc["pos_begin"], wc["circ_begin"] = shed_off[:-1], wpt_off[:-1], R * shed_off[:-1]
+        wc["vel_begin"] = vel_off[:-1]
+        wc["dt"] = [float(c.dt) for c in self.cases]
+        self.wake_cases = _dev_records(wc, dev)
+        sc = np.zeros(B, SOLVE_CASE)
+        sc["row_begin"], sc["n"], sc["mat_begin"] = ring_off[:-1], P, mat_off[:-1]
+        self.solve_cases = _dev_records(sc, dev)
+        self.row_case = to_device_u32(np.repeat(np.arange(B), P).astype(np.uint32), dev)
+        self.node_case = to_device_u32(np.repeat(np.arange(B), 2 * (R + 1) * np.asarray(S)).astype(np.uint32), dev)
+        self.circ_case = to_device_u32(np.repeat(np.arange(B), R * np.asarray(S)).astype(np.uint32), dev)
+        self.bn = to_device_u32(np.concatenate([b + pt_off[k] for k, b in enumerate(bn_all)]).astype(np.uint32), dev)
+        adj = np.concatenate(adj_all)
+        self.adj = to_device_u32(np.where(adj == 0x7FFFFFFF, 0x7FFFFFFF, adj).astype(np.uint32), dev)
+        self.col_slot = to_device_u32(np.concatenate(slot_all).astype(np.uint32), dev)
+
+        # ring jobs: body blocks and implicit (first wake row) blocks, one job per case
+        self._ring_job_args = {
+            "body": (P, ring_off[:-1], mat_off[:-1], P),
+            "implicit": (S, shed_off[:-1], imp_off[:-1], S),
+        }
+        self.ring_tables: dict = {}
+
+        # sweep jobs: explicit wake term (points = control points, segments = the case's wake
+        # lines) and advection (points = the case's distinct wake node columns, row by row)
+        pidx = []
+        for k in range(B):
+            base = wpt_off[k]
+            cols = cols_all[k].astype(np.int64)
+            rows = np.arange(R, dtype=np.int64)[:, None]
+            pidx.append((base + cols[None, :] * (R + 1) + rows).reshape(-1))  # row-major: (row, column)
+        self.pidx = to_device_u32(np.concatenate(pidx).astype(np.uint32), dev)
+        self._sweep_specs = {
+            "wake": dict(seg_begin=wline_off[:-1], seg_count=WL, pt_begin=ring_off[:-1], pt_max=P,
+                         pt_per_row=[0] * B, out_begin=ring_off[:-1], mode=0),
+            "advect": dict(seg_begin=line_off[:-1], seg_count=L, pt_begin=R * np.concatenate([[0], np.cumsum(NC)[:-1]]),
+                           pt_max=np.asarray(NC) * R, pt_per_row=NC, out_begin=vel_off[:-1], mode=1),
+        }
+        self.sweep_tables: dict = {}
+
+        # ---------------- state
+        NR, NL, NWL = self.n_rings, self.body.n_lines, self.wake_mesh.n_lines
+        self.pos = torch.zeros((self.n_points, 3), **f64)
+        self.vel = torch.zeros((self.n_points, 3), **f64)
+        self.cps = torch.zeros((NR, 3), **f64)
+        self.cpv = torch.zeros((NR, 3), **f64)
+        self.nrm = torch.zeros((NR, 3), **f64)
+        self.rhs = torch.zeros(NR, **f64)
+        self.gamma = torch.zeros(NR, **f64)
+        self.A = torch.zeros(int(mat_off[-1]), **f64)
+        self.implicit = torch.zeros(int(imp_off[-1]), **f64)
+        self.seg_body = torch.empty(int(_lib.query("pvl_segments_workspace", max(NL, 1), _lib.PVL_F64)),
+                                    dtype=torch.uint8, device=dev)
+        self.seg_wake = torch.empty(int(_lib.query("pvl_segments_workspace", max(NWL, 1), _lib.PVL_F64)),
+                                    dtype=torch.uint8, device=dev)
+        self.body_line_gamma = torch.zeros(max(NL, 1), **f64)
+        self.wake_line_gamma = torch.zeros(max(NWL, 1), **f64)
+        # fixed buffers (a step writes the new wake into the scratch copies and copies it back), so
+        # that one captured graph serves every step
+        self.wpos = torch.zeros((n_wake_pts, 3), **f64)
+        self.wpos_new = torch.zeros((n_wake_pts, 3), **f64)
+        self.wcirc = torch.zeros(R * int(shed_off[-1]), **f64)
+        self.wcirc_new = torch.zeros(R * int(shed_off[-1]), **f64)
+        self.node_vel = torch.zeros((int(vel_off[-1]), 3), **f64)
+        self.rows = torch.zeros(1, dtype=torch.int32, device=dev)  # device step counter of the wake
+        self.counter = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.fail_flags = torch.zeros(B, dtype=torch.uint8, device=dev)
+        self.fail_count = torch.zeros(1, dtype=torch.int32, device=dev)
+        nb = int(_lib.query("pvl_batch_gmres_workspace", NR, B, self.max_iter))
+        self.gws = torch.empty(nb, dtype=torch.uint8, device=dev)
+        self.partials = None
+        self._build_tables()
+        self.iteration = 0
+        self.graph = None
+        self.h_gamma = torch.empty(NR, dtype=torch.float64, pin_memory=not host_only)
+
+    # ------------------------------------------------------------------ tables for the current tiles
+    def _build_tables(self) -> None:
+        B, dev = self.B, self.dev
+        cpb = int(self.tile["ring"])
+        for name, (ncols, rbeg, obeg, ld) in self._ring_job_args.items():
+            jobs = np.zeros(B, RING_JOB)
+            jobs["cp_begin"], jobs["n_cp"] = self.ring_off[:-1], self.P
+            jobs["ring_begin"], jobs["n_rings"] = rbeg, ncols
+            jobs["out_begin"], jobs["ld"] = obeg, ld
+            items = -(-np.asarray(self.P) // cpb) * (-(-np.asarray(ncols) // 128))
+            jobs["item_begin"] = np.concatenate([[0], np.cumsum(items)[:-1]])
+            self.ring_tables[name] = (_dev_records(jobs, dev), to_device_u32(jobs["item_begin"].astype(np.uint32), dev),
+                                      int(items.sum()))
+        threads, ppt = self.tile["sweep"]
+        kpts = threads * ppt
+        part_total = 0
+        for name, sp in self._sweep_specs.items():
+            jobs = np.zeros(B, SWEEP_JOB)
+            for k in ("seg_begin", "seg_count", "pt_begin", "pt_max", "pt_per_row", "out_begin"):
+                jobs[k] = sp[k]
+            jobs["mode"] = sp["mode"]
+            jobs["case_id"] = np.arange(B)
+            items = np.zeros(B, np.int64)
+            for c in range(B):
+                ns, per = _splits(int(jobs["seg_count"][c]), int(jobs["pt_max"][c]), kpts)
+                jobs["n_split"][c], jobs["per"][c] = ns, per
+                jobs["part_begin"][c] = part_total
+                part_total += ns * int(jobs["pt_max"][c])
+                items[c] = -(-int(jobs["pt_max"][c]) // kpts) * ns
+            jobs["item_begin"] = np.concatenate([[0], np.cumsum(items)[:-1]])
+            pt_item = np.concatenate([[0], np.cumsum(jobs["pt_max"].astype(np.int64))[:-1]]).astype(np.uint32)
+            self.sweep_tables[name] = (_dev_records(jobs, dev), to_device_u32(jobs["item_begin"].astype(np.uint32), dev),
+                                       int(items.sum()), to_device_u32(pt_item, dev),
+                                       int(jobs["pt_max"].astype(np.int64).sum()))
+        if self.partials is None or self.partials.numel() < 3 * part_total:
+            self.partials = torch.zeros(3 * max(part_total, 1), dtype=torch.float64, device=dev)
+
+    # ------------------------------------------------------------------ pieces of a step
+    def _ring(self, which: str, segs, off, sl, n_lines: int, out) -> None:
+        jobs, items, n_items = self.ring_tables[which]
+        _lib.call("pvl_batch_ring_matrix", int(self.tile["ring"]), ptr(jobs), ptr(items), self.B, n_items,
+                  ptr(self.counter), ptr(off), ptr(sl), n_lines, ptr(segs), ptr(self.cps), ptr(self.nrm), self.tol,
+                  ptr(out), 0, stream_ptr())
+
+    def _sweep(self, which: str, segs, pts, pidx, out) -> None:
+        jobs, items, n_items, pt_item, n_total = self.sweep_tables[which]
+        s = stream_ptr()
+        threads, ppt = self.tile["sweep"]
+        _lib.call("pvl_batch_sweep", threads, ppt, ptr(jobs), ptr(items), self.B, n_items, ptr(self.counter),
+                  ptr(self.rows), ptr(segs), ptr(pts), ptr(pidx) if pidx is not None else None, self.tol,
+                  ptr(self.partials), 0, s)
+        _lib.call("pvl_batch_sweep_reduce", ptr(jobs), ptr(pt_item), self.B, n_total, ptr(self.rows),
+                  ptr(self.partials), ptr(self.nrm), ptr(self.uinf), ptr(out), s)
+
+    def _assemble(self, with_wake: bool) -> None:
+        s = stream_ptr()
+        d, NR = self.d_body, self.n_rings
+        _lib.call("pvl_surface_average", NR, ptr(d["offsets"]), ptr(d["surface_lines"]), ptr(d["lines"]),
+                  ptr(self.pos), ptr(self.cps), s)
+        _lib.call("pvl_surface_average", NR, ptr(d["offsets"]), ptr(d["surface_lines"]), ptr(d["lines"]),
+                  ptr(self.vel), ptr(self.cpv), s)
+        _lib.call("pvl_surface_normal", NR, ptr(d["offsets"]), ptr(d["surface_lines"]), ptr(d["lines"]),
+                  ptr(self.pos), ptr(self.nrm), s)
+        _lib.call("pvl_rhs", NR, ptr(self.nrm), ptr(self.flow), 0.0, 0.0, 0.0, ptr(self.cpv), ptr(self.rhs), s)
+        _lib.call("pvl_prep_segments", _lib.PVL_F64, self.n_points, self.body.n_lines, ptr(d["lines"]), ptr(self.pos),
+                  None, self.tol, ptr(self.seg_body), s)
+        self._ring("body", self.seg_body, d["offsets"], d["surface_lines"], self.body.n_lines, self.A)
+        if not with_wake:
+            return
+        w, wpos = self.d_wake, self.wpos
+        _lib.call("pvl_line_circulation", self.wake_mesh.n_lines, ptr(w["map_offsets"]), ptr(w["map_entries"]),
+                  ptr(self.wcirc), self.R, ptr(self.wake_line_gamma), s)
+        _lib.call("pvl_prep_segments", _lib.PVL_F64, self.n_wake_pts, self.wake_mesh.n_lines, ptr(w["lines"]),
+                  ptr(wpos), ptr(self.wake_line_gamma), self.tol, ptr(self.seg_wake), s)
+        self._ring("implicit", self.seg_wake, self.d_row0["offsets"], self.d_row0["lines"], self.wake_mesh.n_lines,
+                   self.implicit)
+        _lib.call("pvl_batch_fold_implicit", ptr(self.wake_cases), ptr(self.row_case), self.n_rings,
+                  ptr(self.implicit), ptr(self.adj), ptr(self.A), s)
+        self._sweep("wake", self.seg_wake, self.cps, None, self.rhs)
+
+    def _solve(self) -> None:
+        _lib.call("pvl_batch_gmres", ptr(self.solve_cases), ptr(self.row_case), self.n_rings, self.B, ptr(self.A),
+                  ptr(self.rhs), ptr(self.gamma), self.max_iter, self.solve_tol, ptr(self.fail_flags),
+                  ptr(self.fail_count), ptr(self.gws), self.gws.numel(), stream_ptr())
+
+    def _advect(self) -> None:
+        s = stream_ptr()
+        _lib.call("pvl_batch_wake_advect", ptr(self.wake_cases), ptr(self.node_case), self.n_wake_pts, self.R,
+                  ptr(self.rows), ptr(self.wpos), ptr(self.node_vel), ptr(self.col_slot), ptr(self.pos),
+                  ptr(self.bn), ptr(self.wpos_new), s)
+        self.wpos.copy_(self.wpos_new)
+
+    def _wake_update(self) -> None:
+        s = stream_ptr()
+        d = self.d_body
+        _lib.call("pvl_line_circulation", self.body.n_lines, ptr(d["map_offsets"]), ptr(d["map_entries"]),
+                  ptr(self.gamma), 0, ptr(self.body_line_gamma), s)
+        _lib.call("pvl_prep_segments", _lib.PVL_F64, self.n_points, self.body.n_lines, ptr(d["lines"]), ptr(self.pos),
+                  ptr(self.body_line_gamma), self.tol, ptr(self.seg_body), s)
+        self._sweep("advect", self.seg_body, self.wpos, self.pidx, self.node_vel)
+        self._advect()
+        _lib.call("pvl_batch_wake_shed", ptr(self.wake_cases), ptr(self.circ_case), self.wcirc.numel(), self.R,
+                  ptr(self.wcirc), ptr(self.adj), ptr(self.gamma), ptr(self.wcirc_new), s)
+        self.wcirc.copy_(self.wcirc_new)
+        _lib.call("pvl_batch_increment", ptr(self.rows), s)
+
+    # ------------------------------------------------------------------ public stepping
+    def load_positions(self, positions: list) -> None:
+        """Body node positions of every case (list of (n_points_c, 3) arrays)."""
+        self.pos.copy_(torch.as_tensor(np.concatenate([np.asarray(p, np.float64) for p in positions]),
+                                       device=self.dev))
+
+    def start(self, time: float = 0.0) -> None:
+        """Positions at ``time`` and the wake pinned to the trailing edges (first wake update)."""
+        self.load_positions([c.positions_at(time) for c in self.cases])
+        self.vel.copy_(torch.as_tensor(np.concatenate([c.velocities_at(time) for c in self.cases]), device=self.dev))
+        self.rows.zero_()
+        self._advect()  # rows = 0: every row collapses onto the trailing edge
+        self.rows.fill_(1)
+        self.iteration = 0
+
+    def _step_body(self, with_wake: bool) -> None:
+        self._assemble(with_wake)
+        self._solve()
+        self._wake_update()
+
+    def step(self) -> None:
+        """One solver iteration of every case (static bodies: positions stay as loaded)."""
+        if self.iteration == 0:
+            self._step_body(with_wake=False)
+        elif self.graph is not None:
+            self.graph.replay()
+        else:
+            self._step_body(with_wake=True)
+        self.iteration += 1
+
+    def capture(self) -> None:
+        """Capture one steady step (iteration >= 1) as a CUDA graph; later steps replay it.
+        Capturing records the step without running it."""
+        if self.iteration == 0:
+            raise RuntimeError("capture after the first step")
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        n0 = _lib.lib().pvl_launch_count()
+        with torch.cuda.graph(g):
+            self._step_body(with_wake=True)
+        self.graph = g
+        self.graph_kernels = int(_lib.lib().pvl_launch_count() - n0)  # kernels each replay runs
+
+    def failures(self) -> int:
+        """Cases whose GMRES missed 10x its tolerance since the last call (host read)."""
+        n = int(self.fail_count.item())
+        self.fail_count.zero_()
+        return n
+
+    # ------------------------------------------------------------------ autotuner
+    def tune(self, reps: int = 3) -> dict:
+        """Time every tile shape of the two persistent kernels on this batch (with a full wake
+        row count) and keep the fastest; returns the timings in ms."""
+        saved_rows = self.rows.clone()
+        self.rows.fill_(self.R)
+        timings: dict = {"sweep": {}, "ring": {}}
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        best = dict(self.tile)
+        for tile in SWEEP_TILES:
+            self.tile["sweep"] = tile
+            self._build_tables()
+            t = 0.0
+            for r in range(reps + 1):
+                torch.cuda.synchronize()
+                ev0.record()
+                self._sweep("advect", self.seg_body, self.wpos, self.pidx, self.node_vel)
+                self._sweep("wake", self.seg_wake, self.cps, None, self.rhs)
+                ev1.record()
+                torch.cuda.synchronize()
+                if r:
+                    t += ev0.elapsed_time(ev1) / reps
+            timings["sweep"][f"{tile[0]}x{tile[1]}"] = t
+        best["sweep"] = min(SWEEP_TILES, key=lambda tl: timings["sweep"][f"{tl[0]}x{tl[1]}"])
+        self.tile["sweep"] = best["sweep"]
+        d = self.d_body
+        for cpb in RING_TILES:
+            self.tile["ring"] = cpb
+            self._build_tables()
+            t = 0.0
+            for r in range(reps + 1):
+                torch.cuda.synchronize()
+                ev0.record()
+                self._ring("body", self.seg_body, d["offsets"], d["surface_lines"], self.body.n_lines, self.A)
+                ev1.record()
+                torch.cuda.synchronize()
+                if r:
+                    t += ev0.elapsed_time(ev1) / reps
+            timings["ring"][str(cpb)] = t
+        best["ring"] = min(RING_TILES, key=lambda c: timings["ring"][str(c)])
+        self.tile = best
+        self._build_tables()
+        self.rows.copy_(saved_rows)
+        self.graph = None  # tables changed: recapture
+        return {"chosen": {"sweep": list(best["sweep"]), "ring": best["ring"]}, "ms": timings}
+
+    # ------------------------------------------------------------------ results
+    def gamma_of(self, k: int) -> np.ndarray:
+        a, b = int(self.ring_off[k]), int(self.ring_off[k + 1])
+        return self.gamma[a:b].cpu().numpy()
+
+    def wake_positions_of(self, k: int) -> np.ndarray:
+        S = int(self.S[k])
+        a = 2 * (self.R + 1) * int(np.sum(self.S[:k]))
+        return self.wpos[a:a + 2 * (self.R + 1) * S].cpu().numpy().reshape(S, 2, self.R + 1, 3)

@@ -431,6 +431,23 @@ extern "C" size_t pvl_segments_workspace(uint32_t n_lines, int precision)
     return align256((size_t)n_lines * (precision == PVL_F32 ? sizeof(Segment<float>) : sizeof(Segment<double>)));
 }
 
+extern "C" int pvl_prep_segments(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
+                                 const double* positions, const double* line_gamma, double tol, void* segments,
+                                 void* stream)
+{
+    if (n_lines == 0)
+        return PVL_OK;
+    PVL_REQUIRE(lines); PVL_REQUIRE(positions); PVL_REQUIRE(segments);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (precision == PVL_F64)
+        return prep_segments<double>(n_points, n_lines, lines, positions, line_gamma, tol,
+                                     static_cast<Segment<double>*>(segments), st);
+    if (precision == PVL_F32)
+        return prep_segments<float>(n_points, n_lines, lines, positions, line_gamma, tol,
+                                    static_cast<Segment<float>*>(segments), st);
+    return pvl_fail(PVL_ERR_ARG, "pvl_prep_segments: unknown precision %d", precision);
+}
+
 extern "C" int pvl_surface_normal(uint32_t n_surfaces, const uint32_t* off, const uint32_t* sl, const uint32_t* lines,
                                   const double* positions, double* out, void* stream)
 {
