@@ -59,7 +59,8 @@ def parse():
     ap.add_argument("--workload", choices=["flapping", "batch"], default="flapping",
                     help="flapping: the single deforming wing (headline); batch: 256 ragged wings x 50 steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile-kernel", choices=["line_sum", "wake_term", "lu", "lu32"], default=None,
+    ap.add_argument("--profile-kernel", choices=["line_sum", "wake_term", "lu", "lu32", "mixed_step", "batch_step"],
+                    default=None,
                     help="set up the workload, launch only that kernel family twice and exit (for ncu captures)")
     ap.add_argument("--fraction", type=int, default=16,
                     help="reference arm: wake correction and advection are timed on 1/F of their points")
@@ -184,8 +185,21 @@ def cpu_baseline() -> dict | None:
 
 # ------------------------------------------------------------------ our arm
 def profile_kernel(args) -> None:
-    """Two launches of one kernel family on the benchmark state, nothing else (ncu target)."""
+    """Two launches of one kernel family on the benchmark state, nothing else (ncu target);
+    mixed_step / batch_step: a few whole steps (launch lists)."""
     import torch
+
+    if args.profile_kernel == "batch_step":
+        from pyvl_b200.batch import BatchEngine
+        from pyvl_b200.workloads import batch_wings
+
+        beng = BatchEngine(batch_wings(n_cases=256, seed=3, steps=50), solve_tol=1e-12, max_iter=8)
+        beng.start(0.0)
+        for _ in range(4):
+            beng.step()
+        torch.cuda.synchronize()
+        print("profile-kernel done batch_step failures", beng.failures())
+        return
 
     from pyvl_b200 import _lib
     from pyvl_b200.device import ptr, stream_ptr
@@ -221,6 +235,10 @@ def profile_kernel(args) -> None:
             eng.A.copy_(A0)
             _lib.call("pvl_lu_factor", eng.N, ptr(eng.A), eng.N, ptr(eng.ipiv), ptr(eng.info), ptr(eng.ws),
                       eng._ws_bytes, stream_ptr())
+    elif args.profile_kernel == "mixed_step":  # 3 + 2 whole mixed steps (no warm start)
+        for k in range(5):
+            t = t0 + k * case.dt
+            eng.step(t, case.positions_at(t), case.velocities_at(t))
     else:  # the mixed path's preconditioner refresh (FP32 LU + inverse on the tensor cores)
         eng.assemble()
         for _ in range(2):
@@ -265,27 +283,34 @@ def run_batch(args) -> None:
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     steps = 50
-    cases = batch_wings(n_cases=256, seed=3, steps=steps)
-    eng = BatchEngine(cases, solve_tol=1e-12, max_iter=8)
-    eng.start(0.0)
-    eng.step()
-    eng.step()
-    tuning = eng.tune(reps=2)
-    eng.capture()
     first = 2
-    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record()
-    for _ in range(first, steps):
+    timed = steps - first
+    cases = batch_wings(n_cases=256, seed=3, steps=steps)
+
+    def run(reuse: bool):
+        eng = BatchEngine(cases, solve_tol=1e-12, max_iter=8, reuse_static_bodies=reuse)
+        eng.start(0.0)
         eng.step()
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
+        eng.step()
+        tuning = eng.tune(reps=2)
+        eng.capture()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(first, steps):
+            eng.step()
+        e1.record()
+        torch.cuda.synchronize()
+        return eng, tuning, e0.elapsed_time(e1)
+
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    eng, tuning, ms = run(False)
     clocks = sampler.stop()
     fails = eng.failures()
-    timed = steps - first
     case_steps = len(cases) * timed
+    eng_static, _, ms_static = run(True)
+    fails += eng_static.failures()
+    del eng_static
     # per-case loop on every 8th case, same step range
     sample = cases[::8]
     t_loop = 0.0
@@ -325,6 +350,9 @@ def run_batch(args) -> None:
         "per_case_loop": {"value": loop_rate, "unit": "case-steps/s", "engine": "SolverEngine (FP64 LU) per case",
                           "sample": f"every 8th case ({len(sample)} cases), same steps"},
         "speedup_vs_per_case_loop": rate / loop_rate,
+        "static_body_reuse": {"value": case_steps / (ms_static * 1e-3), "unit": "case-steps/s",
+                              "note": "the same batch with each motionless body's matrix built once and copied per "
+                                      "step (reuse_static_bodies=True); the per-case loop has no such reuse"},
         "accuracy": {"gamma_rel_err_vs_per_case_fp64_max": max(errs), "cases_checked": len(errs)},
         "gmres_failures": fails,
         "autotune": tuning,

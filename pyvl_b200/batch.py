@@ -65,7 +65,7 @@ class BatchEngine:
     """Every case of ``cases`` stepped together on the device (see the module docstring)."""
 
     def __init__(self, cases, solve_tol: float = 1e-12, max_iter: int = 8, tile: dict | None = None,
-                 host_only: bool = False):
+                 host_only: bool = False, reuse_static_bodies: bool = False):
         self.host_only = host_only  # build the tables on the host only (layout checks without a GPU)
         self.dev = torch.device("cpu") if host_only else require_cuda()
         _check_layouts()
@@ -83,6 +83,11 @@ class BatchEngine:
         self.tol = tols.pop()
         self.solve_tol = float(solve_tol)
         self.max_iter = int(max_iter)
+        # rigid, motionless bodies: their matrix is the same every step, so it can be built once
+        from .workloads import Static
+
+        self.static = bool(reuse_static_bodies) and all(isinstance(c.kinematics, Static) for c in self.cases)
+        self.A_body = None
         self.tile = dict(tile or {"sweep": (128, 2), "ring": 8})
         dev = self.dev
         f64 = dict(dtype=torch.float64, device=dev)
@@ -287,9 +292,14 @@ class BatchEngine:
         _lib.call("pvl_surface_normal", NR, ptr(d["offsets"]), ptr(d["surface_lines"]), ptr(d["lines"]),
                   ptr(self.pos), ptr(self.nrm), s)
         _lib.call("pvl_rhs", NR, ptr(self.nrm), ptr(self.flow), 0.0, 0.0, 0.0, ptr(self.cpv), ptr(self.rhs), s)
-        _lib.call("pvl_prep_segments", _lib.PVL_F64, self.n_points, self.body.n_lines, ptr(d["lines"]), ptr(self.pos),
-                  None, self.tol, ptr(self.seg_body), s)
-        self._ring("body", self.seg_body, d["offsets"], d["surface_lines"], self.body.n_lines, self.A)
+        if self.static and self.A_body is not None:
+            self.A.copy_(self.A_body)
+        else:
+            _lib.call("pvl_prep_segments", _lib.PVL_F64, self.n_points, self.body.n_lines, ptr(d["lines"]),
+                      ptr(self.pos), None, self.tol, ptr(self.seg_body), s)
+            self._ring("body", self.seg_body, d["offsets"], d["surface_lines"], self.body.n_lines, self.A)
+            if self.static:
+                self.A_body = self.A.clone()
         if not with_wake:
             return
         w, wpos = self.d_wake, self.wpos
@@ -338,6 +348,7 @@ class BatchEngine:
     def start(self, time: float = 0.0) -> None:
         """Positions at ``time`` and the wake pinned to the trailing edges (first wake update)."""
         self.load_positions([c.positions_at(time) for c in self.cases])
+        self.A_body = None
         self.vel.copy_(torch.as_tensor(np.concatenate([c.velocities_at(time) for c in self.cases]), device=self.dev))
         self.rows.zero_()
         self._advect()  # rows = 0: every row collapses onto the trailing edge

@@ -107,20 +107,13 @@ __global__ void __launch_bounds__(128) batched_ring_kernel(const RingJob* __rest
         const uint32_t j = ct * 128 + threadIdx.x;
         if (j < J.n_rings) {
             const uint32_t r = J.ring_begin + j;
-            const uint32_t k0 = off[r], k1 = off[r + 1];
+            pvl::RingSegments<double> rs;
+            rs.load(sl, off[r], off[r + 1], n_lines, seg);
 #pragma unroll 1
             for (int q = 0; q < CPB; ++q) {
                 if (i0 + q >= J.n_cp)
                     break;
-                Vec3<double> acc{0.0, 0.0, 0.0};
-                for (uint32_t k = k0; k < k1; ++k) {
-                    const uint32_t g = sl[k];
-                    const uint32_t l = PVL_IDX(g);
-                    if (l >= n_lines)
-                        continue;
-                    pvl::segment_induction(seg[l], s_p[q][0], s_p[q][1], s_p[q][2], tol2, PVL_REV(g) ? -1.0 : 1.0,
-                                           acc);
-                }
+                const Vec3<double> acc = rs.sum(sl, n_lines, seg, s_p[q][0], s_p[q][1], s_p[q][2], tol2);
                 out[J.out_begin + (size_t)(i0 + q) * J.ld + j] =
                     acc.x * s_n[q][0] + acc.y * s_n[q][1] + acc.z * s_n[q][2];
             }

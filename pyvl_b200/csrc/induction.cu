@@ -68,23 +68,6 @@ __global__ void prep_segments_kernel(uint32_t n_points, uint32_t n_lines, const 
     seg[i] = s;
 }
 
-template <typename T>
-__device__ __forceinline__ Vec3<T> ring_sum(const uint32_t* __restrict__ sl, uint32_t k0, uint32_t k1,
-                                            uint32_t n_lines, const Segment<T>* __restrict__ seg, T px, T py,
-                                            T pz, T tol2)
-{
-    Vec3<T> acc{T(0), T(0), T(0)};
-    for (uint32_t k = k0; k < k1; ++k) {
-        const uint32_t g = sl[k];
-        const uint32_t l = PVL_IDX(g);
-        if (l >= n_lines)
-            continue;
-        // reversed lines are subtracted (src/core/flow_solver.c:192-199)
-        pvl::segment_induction(seg[l], px, py, pz, tol2, PVL_REV(g) ? T(-1) : T(1), acc);
-    }
-    return acc;
-}
-
 // out[i*ld + j] = n_i . sum_{k in ring j} +-u_k(cp_i)        (MODE 0, OutT = T or float)
 // out[(i*n_surfaces + j)*3 + c] = sum_{k in ring j} +-u_k     (MODE 1, OutT = double)
 template <typename T, typename OutT, int MODE>
@@ -106,13 +89,14 @@ __global__ void __launch_bounds__(kRingThreads) ring_matrix_kernel(
     const uint32_t j = blockIdx.x * kRingThreads + threadIdx.x;
     if (j >= n_surfaces)
         return;
-    const uint32_t k0 = off[j], k1 = off[j + 1];
+    pvl::RingSegments<T> rs;
+    rs.load(sl, off[j], off[j + 1], n_lines, seg);
 #pragma unroll 1
     for (int c = 0; c < kRingCPB; ++c) {
         const uint32_t i = i0 + c;
         if (i >= n_cp)
             break;
-        const Vec3<T> v = ring_sum(sl, k0, k1, n_lines, seg, s_p[c][0], s_p[c][1], s_p[c][2], tol2);
+        const Vec3<T> v = rs.sum(sl, n_lines, seg, s_p[c][0], s_p[c][1], s_p[c][2], tol2);
         if (MODE == 0) {
             out[(size_t)i * ld + j] = OutT(v.x * s_n[c][0] + v.y * s_n[c][1] + v.z * s_n[c][2]);
         } else {

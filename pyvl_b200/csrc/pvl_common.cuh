@@ -109,6 +109,62 @@ __device__ __forceinline__ void segment_induction(const Segment<T>& s, T px, T p
     acc.z += cz * mag;
 }
 
+// The segments of one ring (its entries k0 .. k1 of the ring -> line CSR) held in registers,
+// so that a thread evaluating the ring at many control points loads them once.  Rings of up
+// to kMax lines are cached (quads and triangles); larger rings fall back to loading per point.
+template <typename T>
+struct RingSegments {
+    static constexpr int kMax = 4;
+    Segment<T> s[kMax];
+    T sign[kMax];
+    uint32_t k0, k1;
+    bool cached;
+
+    __device__ __forceinline__ void load(const uint32_t* __restrict__ sl, uint32_t k0_, uint32_t k1_,
+                                         uint32_t n_lines, const Segment<T>* __restrict__ seg)
+    {
+        k0 = k0_;
+        k1 = k1_;
+        cached = k1 - k0 <= (uint32_t)kMax;
+#pragma unroll
+        for (int q = 0; q < kMax; ++q) {
+            const uint32_t k = k0 + q;
+            bool ok = cached && k < k1;
+            uint32_t g = ok ? sl[k] : 0u;
+            const uint32_t l = PVL_IDX(g);
+            ok = ok && l < n_lines;
+            if (ok) {
+                s[q] = seg[l];
+            } else {
+                s[q].r1x = s[q].r1y = s[q].r1z = s[q].dx = s[q].dy = s[q].dz = T(0);
+                s[q].len = T(-1);  // contributes nothing
+            }
+            sign[q] = PVL_REV(g) ? T(-1) : T(1);
+        }
+    }
+
+    // sum over the ring's lines of +-u_k(p), in CSR order (the reference's order)
+    __device__ __forceinline__ Vec3<T> sum(const uint32_t* __restrict__ sl, uint32_t n_lines,
+                                           const Segment<T>* __restrict__ seg, T px, T py, T pz, T tol2) const
+    {
+        Vec3<T> acc{T(0), T(0), T(0)};
+        if (cached) {
+#pragma unroll
+            for (int q = 0; q < kMax; ++q)
+                segment_induction(s[q], px, py, pz, tol2, sign[q], acc);
+        } else {
+            for (uint32_t k = k0; k < k1; ++k) {
+                const uint32_t g = sl[k];
+                const uint32_t l = PVL_IDX(g);
+                if (l >= n_lines)
+                    continue;
+                segment_induction(seg[l], px, py, pz, tol2, PVL_REV(g) ? T(-1) : T(1), acc);
+            }
+        }
+        return acc;
+    }
+};
+
 }  // namespace pvl
 
 #define PVL_CUDA_CHECK(expr)                                                                   \

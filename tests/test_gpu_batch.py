@@ -59,15 +59,19 @@ def test_batch_graph_replay_is_bitwise_identical_and_tuning_keeps_results():
     cases = batch_wings(n_cases=5, seed=9, steps=steps, p_min=100, p_max=700)
     a = BatchEngine(cases, solve_tol=1e-13, max_iter=10)
     b = BatchEngine(cases, solve_tol=1e-13, max_iter=10)
-    a.start(0.0)
-    b.start(0.0)
+    c = BatchEngine(cases, solve_tol=1e-13, max_iter=10, reuse_static_bodies=True)
+    for e in (a, b, c):
+        e.start(0.0)
     for it in range(steps):
         a.step()
         b.step()
+        c.step()
         if it == 0:
             b.capture()
+            c.capture()
     for k in range(len(cases)):
         assert np.array_equal(a.gamma_of(k), b.gamma_of(k))
+        assert np.array_equal(a.gamma_of(k), c.gamma_of(k))  # the reused matrix is the same matrix
     rep = a.tune(reps=1)
     assert rep["chosen"]["ring"] in (4, 8, 16)
-    assert a.failures() == 0 and b.failures() == 0
+    assert a.failures() == 0 and b.failures() == 0 and c.failures() == 0
