@@ -89,9 +89,9 @@ void launch_gemv(uint32_t rows, uint32_t cols, double alpha, const MT* M, uint32
         gemv_kernel<MT, false><<<blocks_for(rows, 8), 256, 0, st>>>(rows, cols, alpha, M, ld, x, beta, y);
 }
 
-// h[i] += V_i . w for i < k (one CTA per basis vector).
+// c[i] = V_i . w for i < k (one CTA per basis vector).
 __global__ void __launch_bounds__(256) basis_dots_kernel(uint32_t n, const double* __restrict__ V, uint32_t ldv,
-                                                         const double* __restrict__ w, double* __restrict__ h)
+                                                         const double* __restrict__ w, double* __restrict__ c)
 {
     __shared__ double red[8];
     const uint32_t i = blockIdx.x;
@@ -108,28 +108,25 @@ __global__ void __launch_bounds__(256) basis_dots_kernel(uint32_t n, const doubl
         double t = 0.0;
         for (int q = 0; q < 8; ++q)
             t += red[q];
-        h[i] += t;
+        c[i] = t;
     }
 }
 
-// w -= sum_{i<k} c[i] V_i  (c on the device)
+// w += sign * sum_{i<k} c[i] V_i  (c on the device); with h != NULL, thread 0 also adds c to h.
 __global__ void basis_axpy_kernel(uint32_t n, uint32_t k, const double* __restrict__ V, uint32_t ldv,
-                                  const double* __restrict__ c, double sign, double* __restrict__ w)
+                                  const double* __restrict__ c, double sign, double* __restrict__ w,
+                                  double* __restrict__ h)
 {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h && j == 0)
+        for (uint32_t i = 0; i < k; ++i)
+            h[i] += c[i];
     if (j >= n)
         return;
     double s = 0.0;
     for (uint32_t i = 0; i < k; ++i)
         s += c[i] * V[(size_t)i * ldv + j];
     w[j] += sign * s;
-}
-
-__global__ void accumulate_kernel(uint32_t k, const double* __restrict__ c, double* __restrict__ h)
-{
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < k)
-        h[i] += c[i];
 }
 
 // nrm[0] = ||w||; v = w / nrm  (one CTA of 1024 threads)
@@ -211,12 +208,9 @@ extern "C" int pvl_basis_project(uint32_t n, uint32_t k, const double* V, uint32
     PVL_REQUIRE(V); PVL_REQUIRE(w); PVL_REQUIRE(h);
     cudaStream_t st = (cudaStream_t)stream;
     double* c = h + k;  // scratch: this pass's coefficients, right after the accumulated ones
-    PVL_CUDA_CHECK(cudaMemsetAsync(c, 0, sizeof(double) * k, st));
     basis_dots_kernel<<<k, 256, 0, st>>>(n, V, ldv, w, c);
     PVL_LAUNCH_CHECK();
-    basis_axpy_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, k, V, ldv, c, -1.0, w);
-    PVL_LAUNCH_CHECK();
-    accumulate_kernel<<<blocks_for(k, 32), 32, 0, st>>>(k, c, h);
+    basis_axpy_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, k, V, ldv, c, -1.0, w, h);
     PVL_LAUNCH_CHECK();
     return PVL_OK;
 }
@@ -237,7 +231,7 @@ extern "C" int pvl_combine(uint32_t n, uint32_t k, const double* Z, uint32_t ldz
     if (n == 0 || k == 0)
         return PVL_OK;
     PVL_REQUIRE(Z); PVL_REQUIRE(c); PVL_REQUIRE(x);
-    basis_axpy_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(n, k, Z, ldz, c, 1.0, x);
+    basis_axpy_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(n, k, Z, ldz, c, 1.0, x, nullptr);
     PVL_LAUNCH_CHECK();
     return PVL_OK;
 }

@@ -36,18 +36,24 @@ template <typename T> struct Vec3 { T x, y, z; };
 //   atan(z) = z (1 - w/3 + w^2/5 - w^3/7 + ...),  w = z^2,
 // gives ang / h = -(len / x) S(w) with w = h^2 len^2 / x^2 -- no square root and no atan2.
 // The series is used only for w <= kW, where the first omitted term bounds the relative
-// truncation error: double, 8 terms, w <= 0.01: 0.01^8 / 17 < 1e-17; float, 6 terms,
-// w <= 0.04: 0.04^6 / 13 < 4e-10.  Closer pairs (larger w, or x <= 0) take the atan2 form.
+// truncation error: double, 8 terms for w <= 0.01 (0.01^8 / 17 < 1e-17) and 5 terms for
+// w <= 1e-4 (1e-20 / 11 < 1e-21); float, 6 terms for w <= 0.04 (0.04^6 / 13 < 4e-10).
+// Closer pairs (larger w, or x <= 0) take the atan2 form.
 template <typename T> struct FarSeries;
 template <> struct FarSeries<double> {
     static constexpr double kW = 0.01;
     static __device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
     static __device__ __forceinline__ double sum(double w)
     {
-        double s = -1.0 / 15.0;
-        s = fma(s, w, 1.0 / 13.0);
-        s = fma(s, w, -1.0 / 11.0);
-        s = fma(s, w, 1.0 / 9.0);
+        double s;
+        if (w <= 1e-4) {  // most pairs of a wake sweep: the five-term series is exact to 1e-21
+            s = 1.0 / 9.0;
+        } else {
+            s = -1.0 / 15.0;
+            s = fma(s, w, 1.0 / 13.0);
+            s = fma(s, w, -1.0 / 11.0);
+            s = fma(s, w, 1.0 / 9.0);
+        }
         s = fma(s, w, -1.0 / 7.0);
         s = fma(s, w, 1.0 / 5.0);
         s = fma(s, w, -1.0 / 3.0);
@@ -92,11 +98,11 @@ __device__ __forceinline__ void segment_induction(const Segment<T>& s, T px, T p
     if (hsq < tol2 || s.len < T(0))
         return;
     const T x = hsq + t1 * (t1 - s.len);
-    const T hl2 = hsq * (s.len * s.len);
+    const T r = FarSeries<T>::rcp(x);  // wasted only on the rare near pairs
+    const T w = hsq * (s.len * s.len) * (r * r);
     T mag;
-    if (x > T(0) && hl2 <= FarSeries<T>::kW * (x * x)) {
-        const T r = FarSeries<T>::rcp(x);
-        mag = -scale * s.len * r * FarSeries<T>::sum(hl2 * (r * r));
+    if (x > T(0) && w <= FarSeries<T>::kW) {
+        mag = -scale * s.len * r * FarSeries<T>::sum(w);
     } else {
         // one reciprocal square root gives both h and 1/h (no separate sqrt and division)
         const T rh = rsqrt(hsq);

@@ -383,7 +383,9 @@ class MixedSolverEngine(SolverEngine):
       FP64 matrix.  The preconditioner is the explicit inverse of an FP32 LU factorisation of
       the system (trailing updates and the triangular inversion's rank-64 updates on the
       tensor cores in TF32, pvl_lu32_factor / pvl_lu32_inverse), refreshed every ``refresh``
-      steps and applied as one FP32 matrix-vector product per iteration.  If GMRES has not
+      steps (earlier when a solve needed ``refresh_on_iters`` iterations; built on a side
+      stream while the steps go on) and applied as one FP32 matrix-vector product per
+      iteration.  If GMRES has not
       reached ``gmres_tol`` (relative residual) after ``max_iter`` iterations the step falls
       back to the plain FP64 factorisation.
     * The explicit wake term runs in FP64 for the wake rows below ``near_rows`` and in FP32
@@ -398,8 +400,8 @@ class MixedSolverEngine(SolverEngine):
 
     def __init__(self, mesh: Mesh, freestream, tol: float, wake: WakeSpec | None = None, closed_groups=None,
                  refresh: int = 25, near_rows: int | None = None, advect_near_rows: int = 8,
-                 gmres_tol: float = 1e-12,
-                 max_iter: int = 20):
+                 gmres_tol: float = 1e-12, max_iter: int = 20, async_refresh: bool = True,
+                 refresh_on_iters: int = 5):
         super().__init__(mesh, freestream, tol, wake, closed_groups)
         self.refresh = int(refresh)
         self.gmres_tol = float(gmres_tol)
@@ -410,7 +412,14 @@ class MixedSolverEngine(SolverEngine):
         f64 = dict(dtype=torch.float64, device=self.dev)
         self.A32 = torch.zeros((self.npad, self.npad), **f32)
         self.Xinv = torch.zeros((self.npad, self.npad), **f32)
+        self.Xnew = torch.zeros((self.npad, self.npad), **f32)
         self.Yscr = torch.zeros((self.npad, self.npad), **f32)
+        self.rws = torch.empty(int(_lib.query("pvl_lu32_workspace", self.npad)) + 256, dtype=torch.uint8,
+                               device=self.dev)
+        self.async_refresh = bool(async_refresh)
+        self.refresh_on_iters = int(refresh_on_iters)  # a solve that needed this many iterations refreshes early
+        self.side = torch.cuda.Stream(device=self.dev)
+        self.refresh_done = None
         self.ipiv32 = torch.zeros(2 * self.npad, dtype=torch.int32, device=self.dev)
         self.info32 = torch.zeros(1, dtype=torch.int32, device=self.dev)
         self.err32 = torch.zeros(1, dtype=torch.int32, device=self.dev)
@@ -430,7 +439,7 @@ class MixedSolverEngine(SolverEngine):
         self.steps_since_refresh = 0
         self.stats = {"gmres_iters": [], "fallbacks": 0, "refreshes": 0, "initial_rel_residual": [],
                       "final_rel_residual": [], "judge": []}
-        need = _lib.query("pvl_lu32_workspace", self.npad)
+        need = 0
         if self.wake is not None:
             need = max(need, self._init_row_major_wake(near_rows, advect_near_rows))
         if need + 256 > self._ws_bytes:
@@ -496,20 +505,55 @@ class MixedSolverEngine(SolverEngine):
                       ptr(self.rhs), ws, nb, s)
 
     # ------------------------------------------------------------------ preconditioner
-    def refresh_preconditioner(self) -> None:
-        """FP32 LU of the current system (tensor-core trailing updates) and its explicit inverse."""
+    def refresh_preconditioner(self, wait: bool = True) -> None:
+        """FP32 LU of the current system (tensor-core trailing updates) and its explicit inverse.
+
+        With ``wait`` (the first refresh, or ``async_refresh=False``) the new inverse is built on
+        the current stream and used at once.  Otherwise the system is converted to FP32 on the
+        current stream and factorised and inverted on a side stream into a second buffer, with
+        its own workspace; the solves keep the previous inverse until the new one is complete
+        (``_adopt_refresh``), so the refresh overlaps the following steps' work."""
         s = stream_ptr()
         n, npad = self.N, self.npad
+        self._finish_refresh()  # never two refreshes in flight
         _lib.call("pvl_pad_convert_f32", n, ptr(self.A), self.N, ptr(self.A32), npad, npad, s)
-        ws, nb = ptr(self.ws), self._ws_bytes
-        _lib.call("pvl_lu32_factor", npad, ptr(self.A32), npad, ptr(self.ipiv32), ptr(self.info32), ptr(self.err32),
-                  ws, nb, s)
-        perm = self.ipiv32.data_ptr() + 4 * npad
-        _lib.call("pvl_lu32_inverse", npad, ptr(self.A32), npad, perm, ptr(self.Xinv), npad, ptr(self.Yscr), npad,
-                  ptr(self.err32), ws, nb, s)
+        target = self.Xinv if wait else self.Xnew
+
+        def build(stream):
+            ws, nb = ptr(self.rws), self.rws.numel()
+            _lib.call("pvl_lu32_factor", npad, ptr(self.A32), npad, ptr(self.ipiv32), ptr(self.info32),
+                      ptr(self.err32), ws, nb, stream)
+            perm = self.ipiv32.data_ptr() + 4 * npad
+            _lib.call("pvl_lu32_inverse", npad, ptr(self.A32), npad, perm, ptr(target), npad, ptr(self.Yscr), npad,
+                      ptr(self.err32), ws, nb, stream)
+
+        if wait:
+            build(s)
+        else:
+            converted = torch.cuda.Event()
+            converted.record()
+            with torch.cuda.stream(self.side):
+                self.side.wait_event(converted)
+                build(stream_ptr())
+                self.refresh_done = torch.cuda.Event()
+                self.refresh_done.record()
         self.have_precond = True
         self.steps_since_refresh = 0
         self.stats["refreshes"] += 1
+
+    def _adopt_refresh(self) -> None:
+        """Switch to the side stream's new inverse once it is complete (no host wait)."""
+        if self.refresh_done is not None and self.refresh_done.query():
+            torch.cuda.current_stream().wait_event(self.refresh_done)
+            self.Xinv, self.Xnew = self.Xnew, self.Xinv
+            self.refresh_done = None
+
+    def _finish_refresh(self) -> None:
+        """Adopt a refresh still in flight, making the current stream wait for it."""
+        if self.refresh_done is not None:
+            torch.cuda.current_stream().wait_event(self.refresh_done)
+            self.Xinv, self.Xnew = self.Xnew, self.Xinv
+            self.refresh_done = None
 
     # ------------------------------------------------------------------ GMRES
     def _arnoldi(self, j: int) -> None:
@@ -535,8 +579,13 @@ class MixedSolverEngine(SolverEngine):
         s = stream_ptr()
         n = self.N
         A, b = self.A, self.rhs
-        if (not self.have_precond) or self.steps_since_refresh >= self.refresh:
-            self.refresh_preconditioner()
+        self._adopt_refresh()
+        if not self.have_precond:
+            self.refresh_preconditioner(wait=True)
+        elif self.steps_since_refresh >= self.refresh or (
+                self.refresh_done is None and self.stats["gmres_iters"]
+                and self.stats["gmres_iters"][-1] >= self.refresh_on_iters and self.steps_since_refresh >= 2):
+            self.refresh_preconditioner(wait=not self.async_refresh)
         self.steps_since_refresh += 1
         x = self.x
         if x0 is not None:

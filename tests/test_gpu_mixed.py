@@ -191,7 +191,7 @@ def test_mixed_steps_judged_against_fp64(factory, kw, steps):
     assert max(errs) <= MIXED_TOL, max(errs)
     assert st["fallbacks"] == 0
     assert max(st["gmres_iters"]) <= 6, st["gmres_iters"]
-    assert st["refreshes"] == (steps + 9) // 10
+    assert (steps + 9) // 10 <= st["refreshes"] <= steps // 2  # every 10 steps, earlier after slow solves
 
 
 def test_mixed_closed_sphere_judged():
