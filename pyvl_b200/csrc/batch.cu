@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(THREADS) batched_sweep_kernel(const SweepJob* 
                 const Segment<double> s = s_seg[k];
 #pragma unroll
                 for (int t = 0; t < PPT; ++t)
-                    pvl::segment_induction(s, px[t], py[t], pz[t], tol2, s.gamma, acc[t]);
+                    pvl::segment_induction<double, true>(s, px[t], py[t], pz[t], tol2, s.gamma, acc[t]);
             }
             __syncthreads();
         }
@@ -584,7 +584,7 @@ int launch_ring(const void* jobs, const uint32_t* job_item, uint32_t n_jobs, uin
         n_ctas = persistent_ctas((const void*)batched_ring_kernel<CPB>, 128);
     batched_ring_kernel<CPB><<<n_ctas, 128, 0, st>>>(static_cast<const RingJob*>(jobs), job_item, n_jobs, n_items,
                                                       counter, off, sl, n_lines,
-                                                      static_cast<const Segment<double>*>(seg), cps, nrm, tol * tol,
+                                                      static_cast<const Segment<double>*>(seg), cps, nrm, pvl::cutoff2<double>(tol),
                                                       out);
     PVL_LAUNCH_CHECK();
     return PVL_OK;
@@ -599,7 +599,7 @@ int launch_sweep(const void* jobs, const uint32_t* job_item, uint32_t n_jobs, ui
         n_ctas = persistent_ctas((const void*)batched_sweep_kernel<THREADS, PPT>, THREADS);
     batched_sweep_kernel<THREADS, PPT><<<n_ctas, THREADS, 0, st>>>(
         static_cast<const SweepJob*>(jobs), job_item, n_jobs, n_items, counter, rows,
-        static_cast<const Segment<double>*>(seg), pts, pidx, tol * tol, part);
+        static_cast<const Segment<double>*>(seg), pts, pidx, pvl::cutoff2<double>(tol), part);
     PVL_LAUNCH_CHECK();
     return PVL_OK;
 }

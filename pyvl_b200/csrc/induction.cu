@@ -21,7 +21,8 @@ namespace {
 
 constexpr int kSegTile = 128;   // segments per shared-memory tile
 constexpr int kSumThreads = 128;
-constexpr int kSumPPT = 2;      // points per thread in the N-body sweep
+constexpr int kSumPPT = 2;      // nominal points per thread of the N-body sweep (sizes its range split)
+int g_sum_ppt = 1;              // points per thread the sweep runs with (measured best; pvl_set_sweep_points_per_thread)
 constexpr int kRingThreads = 128;
 constexpr int kRingCPB = 8;     // control points per CTA row-block in ring matrices
 
@@ -39,19 +40,24 @@ __global__ void prep_segments_kernel(uint32_t n_points, uint32_t n_lines, const 
     Segment<T> s;
     if (a >= n_points || b >= n_points) {
         s.r1x = s.r1y = s.r1z = s.r2x = s.r2y = s.r2z = s.dx = s.dy = s.dz = T(0);
-        s.len = T(-1);
-        s.gamma = T(0);
-        s.pad = T(0);
+        s.len = s.gamma = s.glen = T(0);
         seg[i] = s;
         return;
     }
     const double r1x = pos[3 * (size_t)a], r1y = pos[3 * (size_t)a + 1], r1z = pos[3 * (size_t)a + 2];
     const double r2x = pos[3 * (size_t)b], r2y = pos[3 * (size_t)b + 1], r2z = pos[3 * (size_t)b + 2];
     double dx = r2x - r1x, dy = r2y - r1y, dz = r2z - r1z;
-    const double len = sqrt(dx * dx + dy * dy + dz * dz);
-    dx /= len;
-    dy /= len;
-    dz /= len;
+    double len = sqrt(dx * dx + dy * dy + dz * dz);
+    if (len < tol) {
+        // src/core/flow_solver.c:107-112: a segment shorter than tol induces nothing (d = 0, len = 0:
+        // every point then has h^2 = 0, below the cut-off)
+        dx = dy = dz = 0.0;
+        len = 0.0;
+    } else {
+        dx /= len;
+        dy /= len;
+        dz /= len;
+    }
     s.r1x = T(r1x);
     s.r1y = T(r1y);
     s.r1z = T(r1z);
@@ -61,15 +67,13 @@ __global__ void prep_segments_kernel(uint32_t n_points, uint32_t n_lines, const 
     s.dx = T(dx);
     s.dy = T(dy);
     s.dz = T(dz);
-    // src/core/flow_solver.c:107-112: a segment shorter than tol induces nothing.
-    s.len = (len < tol) ? T(-1) : T(len);
-    s.gamma = line_gamma ? T(line_gamma[i]) : T(1);
-    s.pad = T(0);
+    s.len = T(len);
+    const double g = line_gamma ? line_gamma[i] : 1.0;
+    s.gamma = T(g);
+    s.glen = T(g * len);
     seg[i] = s;
 }
 
-// out[i*ld + j] = n_i . sum_{k in ring j} +-u_k(cp_i)        (MODE 0, OutT = T or float)
-// out[(i*n_surfaces + j)*3 + c] = sum_{k in ring j} +-u_k     (MODE 1, OutT = double)
 template <typename T, typename OutT, int MODE>
 __global__ void __launch_bounds__(kRingThreads) ring_matrix_kernel(
     uint32_t n_surfaces, const uint32_t* __restrict__ off, const uint32_t* __restrict__ sl, uint32_t n_lines,
@@ -143,7 +147,7 @@ __global__ void __launch_bounds__(kRingThreads) line_matrix_kernel(uint32_t n_li
 // cols ? cols[c] : c: group == stride == n_pts is a plain array; group = a range of wake
 // rows, stride = rows + 1, in_off = first row walks those rows of the listed wake node
 // columns (strip side s * 2 + side).
-template <typename T>
+template <typename T, int PPT>
 __global__ void __launch_bounds__(kSumThreads) line_sum_kernel(const Segment<T>* __restrict__ seg, uint32_t n_lines,
                                                                uint32_t lines_per_split,
                                                                const double* __restrict__ pts, uint32_t n_pts,
@@ -155,11 +159,11 @@ __global__ void __launch_bounds__(kSumThreads) line_sum_kernel(const Segment<T>*
     const uint32_t split = blockIdx.y;
     const uint32_t l_begin = split * lines_per_split;
     const uint32_t l_end = min(n_lines, l_begin + lines_per_split);
-    T px[kSumPPT], py[kSumPPT], pz[kSumPPT];
-    Vec3<T> acc[kSumPPT];
+    T px[PPT], py[PPT], pz[PPT];
+    Vec3<T> acc[PPT];
 #pragma unroll
-    for (int t = 0; t < kSumPPT; ++t) {
-        const uint32_t p = blockIdx.x * (kSumThreads * kSumPPT) + t * kSumThreads + threadIdx.x;
+    for (int t = 0; t < PPT; ++t) {
+        const uint32_t p = blockIdx.x * (kSumThreads * PPT) + t * kSumThreads + threadIdx.x;
         bool ok = p < n_pts;
         uint32_t col = ok ? (cols ? cols[p / group] : p / group) : 0;
         if (col >= col_limit) {  // a listed column outside the point array: skip the point
@@ -182,14 +186,14 @@ __global__ void __launch_bounds__(kSumThreads) line_sum_kernel(const Segment<T>*
         for (int k = 0; k < cnt; ++k) {
             const Segment<T> s = s_seg[k];
 #pragma unroll
-            for (int t = 0; t < kSumPPT; ++t)
-                pvl::segment_induction(s, px[t], py[t], pz[t], tol2, s.gamma, acc[t]);
+            for (int t = 0; t < PPT; ++t)
+                pvl::segment_induction<T, true>(s, px[t], py[t], pz[t], tol2, s.gamma, acc[t]);
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int t = 0; t < kSumPPT; ++t) {
-        const uint32_t p = blockIdx.x * (kSumThreads * kSumPPT) + t * kSumThreads + threadIdx.x;
+    for (int t = 0; t < PPT; ++t) {
+        const uint32_t p = blockIdx.x * (kSumThreads * PPT) + t * kSumThreads + threadIdx.x;
         if (p < n_pts) {
             T* o = partial + 3 * ((size_t)split * n_pts + p);
             o[0] = acc[t].x;
@@ -485,7 +489,7 @@ extern "C" int pvl_line_induction(uint32_t n_points, uint32_t n_lines, const uin
     dim3 grid(blocks_for(n_lines, kRingThreads), blocks_for(n_cp, kRingCPB));
     if (grid.y > 65535)
         return pvl_fail(PVL_ERR_ARG, "pvl_line_induction: too many points (%u)", n_cp);
-    line_matrix_kernel<<<grid, kRingThreads, 0, st>>>(n_lines, seg, n_cp, cps, tol * tol, out);
+    line_matrix_kernel<<<grid, kRingThreads, 0, st>>>(n_lines, seg, n_cp, cps, pvl::cutoff2<double>(tol), out);
     PVL_LAUNCH_CHECK();
     return PVL_OK;
 }
@@ -509,7 +513,7 @@ extern "C" int pvl_induction_matrix(uint32_t n_points, uint32_t n_lines, const u
     if (grid.y > 65535)
         return pvl_fail(PVL_ERR_ARG, "pvl_induction_matrix: too many points (%u)", n_cp);
     ring_matrix_kernel<double, double, 1><<<grid, kRingThreads, 0, st>>>(n_surfaces, off, sl, n_lines, seg, n_cp, cps,
-                                                                         nullptr, tol * tol, out, 0);
+                                                                         nullptr, pvl::cutoff2<double>(tol), out, 0);
     PVL_LAUNCH_CHECK();
     return PVL_OK;
 }
@@ -538,13 +542,13 @@ extern "C" int pvl_induction_normal(int precision, uint32_t n_points, uint32_t n
         if (int r = prep_segments<double>(n_points, n_lines, lines, positions, nullptr, tol, seg, st))
             return r;
         ring_matrix_kernel<double, double, 0><<<grid, kRingThreads, 0, st>>>(
-            n_surfaces, off, sl, n_lines, seg, n_cp, cps, normals, tol * tol, static_cast<double*>(out), ld);
+            n_surfaces, off, sl, n_lines, seg, n_cp, cps, normals, pvl::cutoff2<double>(tol), static_cast<double*>(out), ld);
     } else {
         auto* seg = static_cast<Segment<float>*>(ws);
         if (int r = prep_segments<float>(n_points, n_lines, lines, positions, nullptr, tol, seg, st))
             return r;
         ring_matrix_kernel<float, float, 0><<<grid, kRingThreads, 0, st>>>(
-            n_surfaces, off, sl, n_lines, seg, n_cp, cps, normals, float(tol * tol), static_cast<float*>(out), ld);
+            n_surfaces, off, sl, n_lines, seg, n_cp, cps, normals, pvl::cutoff2<float>(tol), static_cast<float*>(out), ld);
     }
     PVL_LAUNCH_CHECK();
     return PVL_OK;
@@ -583,15 +587,27 @@ int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint3
     const uint32_t n_split = sum_splits(n_lines, n_pts);
     const uint32_t per = (n_lines + n_split - 1) / n_split;
     const uint32_t n_split_used = (n_lines + per - 1) / per;
-    dim3 grid(blocks_for(n_pts, kSumThreads * kSumPPT), n_split_used);
+    const int ppt = g_sum_ppt;
+    dim3 grid(blocks_for(n_pts, kSumThreads * ppt), n_split_used);
     char* base = static_cast<char*>(ws);
+    auto sweep = [&](auto tag, const auto* seg, auto* part, auto tol2) -> void {
+        using T = decltype(tag);
+        if (ppt == 1)
+            line_sum_kernel<T, 1><<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off,
+                                                                 cols, col_limit, tol2, part);
+        else if (ppt == 4)
+            line_sum_kernel<T, 4><<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off,
+                                                                 cols, col_limit, tol2, part);
+        else
+            line_sum_kernel<T, 2><<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off,
+                                                                 cols, col_limit, tol2, part);
+    };
     if (precision == PVL_F64) {
         auto* seg = reinterpret_cast<Segment<double>*>(base);
         auto* part = reinterpret_cast<double*>(base + pvl_segments_workspace(n_lines, PVL_F64));
         if (int r = prep_segments<double>(n_points, n_lines, lines, positions, line_gamma, tol, seg, st))
             return r;
-        line_sum_kernel<double><<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off,
-                                                              cols, col_limit, tol * tol, part);
+        sweep(double(0), seg, part, pvl::cutoff2<double>(tol));
         PVL_LAUNCH_CHECK();
         reduce_partials_kernel<double><<<blocks_for(n_pts, 256), 256, 0, st>>>(
             n_pts, n_split_used, part, normals, alpha, beta, ux, uy, uz, group, out_stride, out_off, out);
@@ -600,8 +616,7 @@ int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint3
         auto* part = reinterpret_cast<float*>(base + pvl_segments_workspace(n_lines, PVL_F32));
         if (int r = prep_segments<float>(n_points, n_lines, lines, positions, line_gamma, tol, seg, st))
             return r;
-        line_sum_kernel<float><<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off,
-                                                             cols, col_limit, float(tol * tol), part);
+        sweep(float(0), seg, part, pvl::cutoff2<float>(tol));
         PVL_LAUNCH_CHECK();
         reduce_partials_kernel<float><<<blocks_for(n_pts, 256), 256, 0, st>>>(
             n_pts, n_split_used, part, normals, alpha, beta, ux, uy, uz, group, out_stride, out_off, out);
@@ -611,6 +626,15 @@ int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint3
 }
 
 }  // namespace
+
+extern "C" int pvl_set_sweep_points_per_thread(int ppt)
+{
+    if (ppt != 1 && ppt != 2 && ppt != 4)
+        return pvl_fail(PVL_ERR_ARG, "pvl_set_sweep_points_per_thread: 1, 2 or 4 (got %d)", ppt);
+    const int old = g_sum_ppt;
+    g_sum_ppt = ppt;
+    return old;
+}
 
 extern "C" int pvl_line_velocity(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
                                  const double* positions, const double* line_gamma, uint32_t n_pts, const double* pts,

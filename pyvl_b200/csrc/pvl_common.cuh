@@ -16,9 +16,10 @@
 namespace pvl {
 
 // One vortex segment prepared for pair evaluation: start point r1, end point r2, unit
-// direction d = (r2 - r1)/len, length and the segment circulation gamma.  A segment
-// shorter than the cut-off radius is stored with len < 0 and contributes nothing
-// (src/core/flow_solver.c:107-112).
+// direction d = (r2 - r1)/len, length, the segment circulation gamma and glen = gamma * len.
+// A segment shorter than the cut-off radius contributes nothing (src/core/flow_solver.c:107-112):
+// it is stored with d = 0 and len = 0, so every point sees h^2 = |dr1 x d|^2 = 0 below the
+// cut-off and skips it without a separate test.
 template <typename T>
 struct __align__(16) Segment {
     T r1x, r1y, r1z;
@@ -26,8 +27,18 @@ struct __align__(16) Segment {
     T dx, dy, dz;
     T len;
     T gamma;
-    T pad;
+    T glen;
 };
+
+// Squared cut-off radius as the kernels compare it: tol^2, but at least the smallest normal
+// number, so that a disabled segment (h^2 = 0 exactly) is skipped even for tol = 0.
+template <typename T>
+__host__ __device__ inline T cutoff2(double tol)
+{
+    const double t2 = tol * tol;
+    const double lo = sizeof(T) == sizeof(float) ? 1.1754943508222875e-38 : 2.2250738585072014e-308;
+    return T(t2 > lo ? t2 : lo);
+}
 
 template <typename T> struct Vec3 { T x, y, z; };
 
@@ -87,7 +98,9 @@ template <> struct FarSeries<float> {
 //   * for h > 0, atan2(t2, h) - atan2(t1, h) = atan2(h (t2 - t1), h^2 + t1 t2)
 //     = atan2(-h len, h^2 + t1 t2), one atan2 without the far-field cancellation of two;
 //   * far pairs evaluate ang / h by the arctangent series of FarSeries (no sqrt, no atan2).
-template <typename T>
+// GAMMA: the scale is the segment's own circulation (sweeps), so that gamma * len comes
+// precomputed from the table; otherwise `scale` (ring sums: +-1).
+template <typename T, bool GAMMA = false>
 __device__ __forceinline__ void segment_induction(const Segment<T>& s, T px, T py, T pz, T tol2, T scale,
                                                   Vec3<T>& acc)
 {
@@ -95,20 +108,20 @@ __device__ __forceinline__ void segment_induction(const Segment<T>& s, T px, T p
     const T t1 = s.dx * ax + s.dy * ay + s.dz * az;
     const T cx = ay * s.dz - az * s.dy, cy = az * s.dx - ax * s.dz, cz = ax * s.dy - ay * s.dx;
     const T hsq = cx * cx + cy * cy + cz * cz;
-    if (hsq < tol2 || s.len < T(0))
+    if (hsq < tol2)
         return;
     const T x = hsq + t1 * (t1 - s.len);
     const T r = FarSeries<T>::rcp(x);  // wasted only on the rare near pairs
     const T w = hsq * (s.len * s.len) * (r * r);
     T mag;
     if (x > T(0) && w <= FarSeries<T>::kW) {
-        mag = -scale * s.len * r * FarSeries<T>::sum(w);
+        mag = (GAMMA ? -s.glen : -scale * s.len) * r * FarSeries<T>::sum(w);
     } else {
         // one reciprocal square root gives both h and 1/h (no separate sqrt and division)
         const T rh = rsqrt(hsq);
         const T h = hsq * rh;
         const T ang = atan2(-h * s.len, x);
-        mag = scale * ang * rh;
+        mag = (GAMMA ? s.gamma : scale) * ang * rh;
     }
     acc.x += cx * mag;
     acc.y += cy * mag;
@@ -141,9 +154,9 @@ struct RingSegments {
             ok = ok && l < n_lines;
             if (ok) {
                 s[q] = seg[l];
-            } else {
+            } else {  // an empty slot: d = 0 gives h^2 = 0, below any cut-off
                 s[q].r1x = s[q].r1y = s[q].r1z = s[q].dx = s[q].dy = s[q].dz = T(0);
-                s[q].len = T(-1);  // contributes nothing
+                s[q].len = s[q].gamma = s[q].glen = T(0);
             }
             sign[q] = PVL_REV(g) ? T(-1) : T(1);
         }
