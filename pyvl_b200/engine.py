@@ -257,24 +257,27 @@ class SolverEngine:
                 host.numpy()[...] = np.asarray(src, np.float64).reshape(host.shape)
                 dev.copy_(host, non_blocking=True)
 
-    def assemble_body_only(self) -> None:
-        """Control points, normals, RHS for a uniform stream and the body matrix."""
+    def assemble_body_only(self, buf: dict | None = None) -> None:
+        """Control points, normals, RHS for a uniform stream and the body matrix (into ``buf``,
+        a set of pos/vel/cps/cpv/nrm/rhs/A/ws buffers, or the engine's own)."""
         s = stream_ptr()
         d, P = self.d_body, self.P
         msh = self.mesh
+        b = buf or {"pos": self.pos, "vel": self.vel, "cps": self.cps, "cpv": self.cpv, "nrm": self.nrm,
+                    "rhs": self.rhs, "A": self.A, "ws": self.ws}
         _lib.call("pvl_surface_average", P, ptr(d["offsets"]), ptr(d["surface_lines"]), ptr(d["lines"]),
-                  ptr(self.pos), ptr(self.cps), s)
+                  ptr(b["pos"]), ptr(b["cps"]), s)
         _lib.call("pvl_surface_average", P, ptr(d["offsets"]), ptr(d["surface_lines"]), ptr(d["lines"]),
-                  ptr(self.vel), ptr(self.cpv), s)
+                  ptr(b["vel"]), ptr(b["cpv"]), s)
         _lib.call("pvl_surface_normal", P, ptr(d["offsets"]), ptr(d["surface_lines"]), ptr(d["lines"]),
-                  ptr(self.pos), ptr(self.nrm), s)
+                  ptr(b["pos"]), ptr(b["nrm"]), s)
         u = self.u_inf
-        _lib.call("pvl_rhs", P, ptr(self.nrm), None, float(u[0]), float(u[1]), float(u[2]), ptr(self.cpv),
-                  ptr(self.rhs), s)
-        ws, nb = ptr(self.ws), self._ws_bytes
-        _lib.call("pvl_induction_normal", _lib.PVL_F64, msh.n_points, msh.n_lines, ptr(d["lines"]), ptr(self.pos), P,
-                  ptr(d["offsets"]), ptr(d["surface_lines"]), P, ptr(self.cps), ptr(self.nrm), self.tol, ptr(self.A),
-                  self.N, ws, nb, s)
+        _lib.call("pvl_rhs", P, ptr(b["nrm"]), None, float(u[0]), float(u[1]), float(u[2]), ptr(b["cpv"]),
+                  ptr(b["rhs"]), s)
+        ws = b["ws"]
+        _lib.call("pvl_induction_normal", _lib.PVL_F64, msh.n_points, msh.n_lines, ptr(d["lines"]), ptr(b["pos"]), P,
+                  ptr(d["offsets"]), ptr(d["surface_lines"]), P, ptr(b["cps"]), ptr(b["nrm"]), self.tol, ptr(b["A"]),
+                  self.N, ptr(ws), ws.numel(), s)
 
     def border(self) -> None:
         """Zero-mean rows/columns of the closed bodies (bordered system)."""
@@ -401,7 +404,7 @@ class MixedSolverEngine(SolverEngine):
     def __init__(self, mesh: Mesh, freestream, tol: float, wake: WakeSpec | None = None, closed_groups=None,
                  refresh: int = 25, near_rows: int | None = None, advect_near_rows: int = 8,
                  gmres_tol: float = 1e-12, max_iter: int = 20, async_refresh: bool = True,
-                 refresh_on_iters: int = 5):
+                 refresh_on_iters: int = 5, use_graphs: bool = True):
         super().__init__(mesh, freestream, tol, wake, closed_groups)
         self.refresh = int(refresh)
         self.gmres_tol = float(gmres_tol)
@@ -431,7 +434,10 @@ class MixedSolverEngine(SolverEngine):
         self.h_H = torch.zeros((m, 2 * (m + 2)), dtype=torch.float64, pin_memory=True)
         self.scal = torch.zeros(2, **f64)
         self.h_sc = torch.zeros(2, dtype=torch.float64, pin_memory=True)
+        self.h_y = torch.zeros(m, dtype=torch.float64, pin_memory=True)
         self.spec_iters = 2
+        self.use_graphs = bool(use_graphs)
+        self.graphs: dict = {}
         self.y = torch.zeros(m, **f64)
         self.x = torch.zeros(n, **f64)
         self.b_saved = torch.zeros(n, **f64)
@@ -542,17 +548,16 @@ class MixedSolverEngine(SolverEngine):
         self.stats["refreshes"] += 1
 
     def _adopt_refresh(self) -> None:
-        """Switch to the side stream's new inverse once it is complete (no host wait)."""
+        """Switch to the side stream's new inverse once it is complete (no host wait).  It is
+        copied into the inverse's fixed buffer, which the captured solve graphs read."""
         if self.refresh_done is not None and self.refresh_done.query():
-            torch.cuda.current_stream().wait_event(self.refresh_done)
-            self.Xinv, self.Xnew = self.Xnew, self.Xinv
-            self.refresh_done = None
+            self._finish_refresh()
 
     def _finish_refresh(self) -> None:
         """Adopt a refresh still in flight, making the current stream wait for it."""
         if self.refresh_done is not None:
             torch.cuda.current_stream().wait_event(self.refresh_done)
-            self.Xinv, self.Xnew = self.Xnew, self.Xinv
+            self.Xinv.copy_(self.Xnew)
             self.refresh_done = None
 
     # ------------------------------------------------------------------ GMRES
@@ -569,16 +574,46 @@ class MixedSolverEngine(SolverEngine):
             _lib.call("pvl_basis_project", n, j + 1, ptr(self.V), n, ptr(self.wv), ptr(hj), s)
         _lib.call("pvl_normalize", n, ptr(self.wv), ptr(self.V[j + 1]), hj.data_ptr() + 8 * (j + 1), s)
 
+    def _replay(self, key, fn) -> None:
+        """Run ``fn`` as a CUDA graph captured on first use under ``key`` (every buffer the
+        solve touches has a fixed address), or directly when graphs are off."""
+        if not self.use_graphs:
+            fn()
+            return
+        g = self.graphs.get(key)
+        if g is None:
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                fn()
+            self.graphs[key] = g
+        g.replay()
+
+    def _gmres_start(self) -> None:
+        s = stream_ptr()
+        n = self.N
+        self.wv.copy_(self.rhs)
+        _lib.call("pvl_gemv_f64", n, n, -1.0, ptr(self.A), self.N, ptr(self.x), 1.0, ptr(self.wv), s)
+        _lib.call("pvl_normalize", n, ptr(self.rhs), None, self.scal.data_ptr(), s)
+        _lib.call("pvl_normalize", n, ptr(self.wv), ptr(self.V[0]), self.scal.data_ptr() + 8, s)
+        self.Hd.zero_()
+
+    def _gmres_finish(self, k: int) -> None:
+        s = stream_ptr()
+        n = self.N
+        if k:
+            _lib.call("pvl_combine", n, k, ptr(self.Z), n, ptr(self.y), ptr(self.x), s)
+        self.wv.copy_(self.rhs)
+        _lib.call("pvl_gemv_f64", n, n, -1.0, ptr(self.A), self.N, ptr(self.x), 1.0, ptr(self.wv), s)
+        _lib.call("pvl_normalize", n, ptr(self.wv), None, self.scal.data_ptr(), s)
+
     def solve_mixed(self, x0: torch.Tensor | None = None) -> bool:
         """Right-preconditioned GMRES on A x = b in FP64; True if the relative residual met gmres_tol.
 
-        The Arnoldi columns run on the device without host round trips; the host reads the
-        small Hessenberg matrix after ``spec_iters`` columns (the last solve's iteration count),
-        then one column at a time, applies the Givens rotations and forms the update.  The true
-        FP64 residual b - A x decides convergence."""
-        s = stream_ptr()
+        The Arnoldi columns run on the device without host round trips (each a replayed CUDA
+        graph); the host reads the small Hessenberg matrix after as many columns as the
+        previous solve needed and then column by column, applies the Givens rotations and forms
+        the update.  The true FP64 residual b - A x decides convergence."""
         n = self.N
-        A, b = self.A, self.rhs
         self._adopt_refresh()
         if not self.have_precond:
             self.refresh_preconditioner(wait=True)
@@ -593,11 +628,7 @@ class MixedSolverEngine(SolverEngine):
         else:
             x[: self.P].copy_(self.gamma)  # the previous step's circulation
         sc = self.scal
-        self.wv.copy_(b)
-        _lib.call("pvl_gemv_f64", n, n, -1.0, ptr(A), self.N, ptr(x), 1.0, ptr(self.wv), s)
-        _lib.call("pvl_normalize", n, ptr(b), None, sc.data_ptr(), s)
-        _lib.call("pvl_normalize", n, ptr(self.wv), ptr(self.V[0]), sc.data_ptr() + 8, s)
-        self.Hd.zero_()
+        self._replay("start", self._gmres_start)
         m = self.max_iter
         H = np.zeros((m + 1, m))
         cs, sn = np.zeros(m), np.zeros(m)
@@ -607,7 +638,7 @@ class MixedSolverEngine(SolverEngine):
         while k < m and not done:
             nxt = min(m, k + (self.spec_iters if first else 1))
             for j in range(k, nxt):
-                self._arnoldi(j)
+                self._replay(("col", j), lambda j=j: self._arnoldi(j))
             self.h_H[: nxt].copy_(self.Hd[: nxt], non_blocking=True)
             if first:
                 self.h_sc.copy_(sc, non_blocking=True)
@@ -643,13 +674,11 @@ class MixedSolverEngine(SolverEngine):
             yk = np.zeros(k)
             for i in range(k - 1, -1, -1):  # back substitution with the rotated Hessenberg
                 yk[i] = (g[i] - H[i, i + 1:k] @ yk[i + 1:]) / H[i, i] if H[i, i] != 0.0 else 0.0
-            self.y[:k].copy_(torch.from_numpy(yk))
-            _lib.call("pvl_combine", n, k, ptr(self.Z), n, ptr(self.y), ptr(x), s)
+            self.h_y[:k] = torch.from_numpy(yk)
+            self.y[:k].copy_(self.h_y[:k], non_blocking=True)
             self.spec_iters = max(1, k)
         # the true FP64 residual decides
-        self.wv.copy_(b)
-        _lib.call("pvl_gemv_f64", n, n, -1.0, ptr(A), self.N, ptr(x), 1.0, ptr(self.wv), s)
-        _lib.call("pvl_normalize", n, ptr(self.wv), None, sc.data_ptr(), s)
+        self._replay(("finish", k), lambda: self._gmres_finish(k))
         rel = float(sc[0].item()) / max(bnorm, 1e-300)
         self.stats["gmres_iters"].append(k)
         self.stats["final_rel_residual"].append(rel)
@@ -666,9 +695,20 @@ class MixedSolverEngine(SolverEngine):
         self.rhs.copy_(self.b_saved)
         super().solve()
 
-    def step(self, time: float, positions, velocities, x0: torch.Tensor | None = None) -> torch.Tensor:
+    def assemble_rest(self) -> None:
+        """The wake corrections and the closed-body border, the body part already in place."""
+        if self.wake is not None and self.iteration > 0:
+            self._wake_corrections()
+        self.border()
+
+    def begin_step(self, positions, velocities) -> None:
+        """Inputs and body assembly of this step."""
         self.load_inputs(positions, velocities)
-        self.assemble()
+        self.assemble_body_only()
+
+    def step(self, time: float, positions, velocities, x0: torch.Tensor | None = None) -> torch.Tensor:
+        self.begin_step(positions, velocities)
+        self.assemble_rest()
         self.solve(x0)
         if self.wake is not None:
             self.wake_update(time)

@@ -228,3 +228,20 @@ def test_mixed_trajectory_tracks_plain():
         worst = max(worst, float(np.linalg.norm(a - b) / np.linalg.norm(b)))
     print(f"max trajectory difference over 60 steps: {worst:.3e}")
     assert worst <= 1e-8, worst
+
+
+def test_gmres_graph_replay_is_bitwise_identical():
+    """The GMRES pieces replayed as captured CUDA graphs give the same circulations, bit for
+    bit, as launching them directly."""
+    from pyvl_b200.workloads import flapping
+
+    case = flapping(ns=32, nc=8, line_rows=12)
+    a = _mixed_engine(case, refresh=5, use_graphs=False)
+    b = _mixed_engine(case, refresh=5, use_graphs=True)
+    for k in range(14):
+        t = k * case.dt
+        p, v = case.positions_at(t), case.velocities_at(t)
+        a.step(t, p, v)
+        b.step(t, p, v)
+        assert np.array_equal(a.gamma_host(), b.gamma_host()), k
+    assert len(b.graphs) > 2
