@@ -56,8 +56,9 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--path", choices=["mixed", "plain"], default="mixed")
     ap.add_argument("--train-steps", type=int, default=64, help="plain-engine steps the warm start is trained on")
-    ap.add_argument("--workload", choices=["flapping", "batch"], default="flapping",
-                    help="flapping: the single deforming wing (headline); batch: 256 ragged wings x 50 steps")
+    ap.add_argument("--workload", choices=["flapping", "batch", "swept", "sphere"], default="flapping",
+                    help="flapping: the deforming wing (headline); batch: 256 ragged wings x 50 steps; "
+                         "swept: pitching swept wing, 200 steps; sphere: closed 5120-ring sphere")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-kernel", choices=["line_sum", "wake_term", "lu", "lu32", "mixed_step", "batch_step"],
                     default=None,
@@ -269,6 +270,85 @@ def train_warm_start(mesh, case, t0: float, n_steps: int, seed: int = 0):
     return mlp, {"samples": int(X.shape[0]), "loss_first": losses[0], "loss_last": losses[-1]}
 
 
+def run_precision_case(args) -> None:
+    """Plain FP64 vs the mixed path on the pitching swept wing (1024 rings, 200 steps, wake
+    growing to 200 rows) or the closed sphere (5120 rings, bordered): time per step, the error
+    of every mixed step against the all-FP64 step of the same state, the divergence of whole
+    trajectories, and on the sphere the surface velocity."""
+    import torch
+
+    from pyvl_b200.cvl import Mesh
+    from pyvl_b200.engine import MixedSolverEngine, SolverEngine, wake_spec_from_te
+    from pyvl_b200 import workloads
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    case = workloads.swept_pitching() if args.workload == "swept" else workloads.icosphere()
+    mesh = Mesh(case.n_points, case.elements)
+    groups = [(0, case.n_surfaces)] if case.closed else None
+
+    def spec():
+        if case.line_rows <= 0 or not len(case.te_node_pairs):
+            return None
+        return wake_spec_from_te(mesh, case.te_node_pairs, case.line_rows, case.t0)
+
+    steps = case.nt if case.nt > 1 else max(args.steps, 5)
+    times = [k * case.dt for k in range(steps)]
+    runs = {}
+    for kind in ("plain", "mixed"):
+        eng = (SolverEngine(mesh, case.freestream, case.tol, spec(), groups) if kind == "plain" else
+               MixedSolverEngine(mesh, case.freestream, case.tol, spec(), groups,
+                                 gmres_tol=1e-13 if case.closed else 1e-12))
+        hist, ms = [], 0.0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for k, t in enumerate(times):
+            p, v = case.positions_at(t), case.velocities_at(t)
+            torch.cuda.synchronize()
+            e0.record()
+            eng.step(t, p, v)
+            e1.record()
+            torch.cuda.synchronize()
+            if k >= 2:
+                ms += e0.elapsed_time(e1)
+            hist.append(eng.gamma_host())
+        rec = {"ms_per_step": ms / max(1, steps - 2), "gamma": np.array(hist), "eng": eng}
+        runs[kind] = rec
+    mixed = runs["mixed"]["eng"]
+    # per-step error of the mixed path: a fresh mixed engine judged at every step of the same run
+    judge_eng = MixedSolverEngine(mesh, case.freestream, case.tol, spec(), groups,
+                                  gmres_tol=1e-13 if case.closed else 1e-12)
+    judged = [judge_eng.step_judged(t, case.positions_at(t), case.velocities_at(t)) for t in times]
+    gp, gm = runs["plain"]["gamma"], runs["mixed"]["gamma"]
+    traj = [float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(gm, gp)]
+    extra = {}
+    if case.closed:  # surface velocity at the control points: freestream + induced, both paths
+        t = times[-1]
+        pos = case.positions_at(t)
+        cps = mesh.surface_average_vec3(pos)
+        vel = {}
+        for kind in ("plain", "mixed"):
+            g = runs[kind]["gamma"][-1]
+            vel[kind] = np.asarray(mesh.induced_velocity(case.tol, pos, cps, g)) + case.freestream
+        extra["surface_velocity_rel_err"] = float(np.linalg.norm(vel["mixed"] - vel["plain"])
+                                                  / np.linalg.norm(vel["plain"]))
+    st = mixed.stats
+    print(json.dumps({
+        "metric": "UVLM steps/s, mixed vs plain FP64", "workload": args.workload,
+        "value": 1000.0 / runs["mixed"]["ms_per_step"], "unit": "steps/s", "n_gpus": 1, "steps": steps,
+        "higher_is_better": True, "dtype": "f64 residuals / f32+tf32 preconditioner", "data": "synthetic",
+        "config": {"workload": case.name, "rings": case.n_surfaces, "wake_rows": case.line_rows,
+                   "closed": bool(case.closed)},
+        "plain_fp64": {"steps_per_s": 1000.0 / runs["plain"]["ms_per_step"], "ms_per_step": runs["plain"]["ms_per_step"]},
+        "mixed": {"steps_per_s": 1000.0 / runs["mixed"]["ms_per_step"], "ms_per_step": runs["mixed"]["ms_per_step"],
+                  "gmres_iters_mean": float(np.mean(st["gmres_iters"])), "fallbacks": st["fallbacks"],
+                  "refreshes": st["refreshes"]},
+        "speedup_mixed_over_plain": runs["plain"]["ms_per_step"] / runs["mixed"]["ms_per_step"],
+        "accuracy": {"gamma_rel_err_per_step_max": max(judged), "trajectory_gamma_rel_diff_max": max(traj),
+                     "tolerance": 1e-10, **extra,
+                     "how": "every step judged against the all-FP64 step of the same state; trajectories of "
+                            "the two engines compared step by step"},
+    }), flush=True)
+
+
 def run_batch(args) -> None:
     """256 independent wings (ragged 128..2048 rings) x 50 free-wake steps: the batched engine
     (persistent launches, autotuned tiles, CUDA graph) against a per-case loop of the plain
@@ -370,6 +450,8 @@ def main() -> None:
         return profile_kernel(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload in ("swept", "sphere"):
+        return run_precision_case(args)
     import torch
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -174,6 +174,7 @@ class SolverEngine:
         self.h_pos = torch.empty((mesh.n_points, 3), dtype=torch.float64, pin_memory=True)
         self.h_vel = torch.empty((mesh.n_points, 3), dtype=torch.float64, pin_memory=True)
         self.h_gamma = torch.empty(self.P, dtype=torch.float64, pin_memory=True)
+        self._h2d_done = None  # event after the last copy out of h_pos / h_vel
 
     # ------------------------------------------------------------------ setup
     def _init_wake(self, w: WakeSpec) -> None:
@@ -249,13 +250,25 @@ class SolverEngine:
 
     # ------------------------------------------------------------------ the step
     def load_inputs(self, positions, velocities) -> None:
-        """Copy this step's body positions/velocities to the device (pinned, async)."""
+        """Copy this step's body positions/velocities to the device (pinned, async).
+
+        The pinned staging buffers are reused every step: before one is overwritten, the host
+        waits until the device has consumed the previous copy out of it (otherwise a host that
+        runs steps ahead of the device would hand a pending copy the next step's data)."""
+        if self._h2d_done is not None:
+            self._h2d_done.synchronize()
+            self._h2d_done = None
+        staged = False
         for host, dev, src in ((self.h_pos, self.pos, positions), (self.h_vel, self.vel, velocities)):
             if isinstance(src, torch.Tensor) and src.is_cuda:
                 dev.copy_(src.reshape(dev.shape))
             else:
                 host.numpy()[...] = np.asarray(src, np.float64).reshape(host.shape)
                 dev.copy_(host, non_blocking=True)
+                staged = True
+        if staged:
+            self._h2d_done = torch.cuda.Event()
+            self._h2d_done.record()
 
     def assemble_body_only(self, buf: dict | None = None) -> None:
         """Control points, normals, RHS for a uniform stream and the body matrix (into ``buf``,

@@ -96,3 +96,26 @@ def test_swept_pitching_long_wake_vs_oracle():
     # wake nodes are integrated over 40 explicit Euler steps: per-step rounding differences
     # (1e-16) accumulate along the trajectory, so the 40-step positions are held to 1e-11
     assert rel(eng.wake_positions.cpu().numpy(), orc.wake.wake_positions) <= 1e-11
+
+
+def test_host_inputs_without_per_step_sync():
+    """Steps fed from host arrays with no synchronisation between them (the host runs ahead of
+    the device) see each step's own inputs: the reused pinned staging buffers are not
+    overwritten before their copies ran."""
+    import torch
+
+    from pyvl_b200.workloads import flapping
+
+    import dataclasses
+
+    case = dataclasses.replace(flapping(ns=32, nc=8, line_rows=10), nt=12)
+    _, ref = run_engine(case)  # reads the circulations back every step
+    eng = make_engine(case)
+    hist = []
+    for it in range(12):
+        t = it * case.dt
+        eng.step(t, case.positions_at(t), case.velocities_at(t))
+        hist.append(eng.gamma.clone())
+    torch.cuda.synchronize()
+    got = torch.stack(hist).cpu().numpy()
+    assert np.array_equal(got, ref)
