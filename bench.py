@@ -60,7 +60,8 @@ def parse():
                     help="flapping: the deforming wing (headline); batch: 256 ragged wings x 50 steps; "
                          "swept: pitching swept wing, 200 steps; sphere: closed 5120-ring sphere")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile-kernel", choices=["line_sum", "wake_term", "lu", "lu32", "mixed_step", "batch_step"],
+    ap.add_argument("--profile-kernel", choices=["line_sum", "advect_f32", "wake_term", "lu", "lu32", "mixed_step",
+                                                 "batch_step"],
                     default=None,
                     help="set up the workload, launch only that kernel family twice and exit (for ncu captures)")
     ap.add_argument("--fraction", type=int, default=16,
@@ -214,12 +215,14 @@ def profile_kernel(args) -> None:
     eng.iteration = 1
     eng.assemble_body_only()
     w = eng.wake
-    if args.profile_kernel == "line_sum":  # advection sweep of the de-duplicated wake node columns, FP64
+    if args.profile_kernel in ("line_sum", "advect_f32"):  # advection sweep of the distinct wake node columns
         S, R, L = spec.shedding_lines.size, case.line_rows, mesh.n_lines
         d = eng.d_body
+        prec, r0 = (_lib.PVL_F64, 0) if args.profile_kernel == "line_sum" else (_lib.PVL_F32, 8)
+        eng.body_line_gamma.fill_(1e-2)
         for _ in range(2):
-            _lib.call("pvl_wake_node_velocity_cols", _lib.PVL_F64, mesh.n_points, L, ptr(d["lines"]), ptr(eng.pos),
-                      ptr(eng.body_line_gamma), S, R, R, 0, R, w["n_cols"], ptr(w["cols"]), ptr(eng.wake_positions),
+            _lib.call("pvl_wake_node_velocity_cols", prec, mesh.n_points, L, ptr(d["lines"]), ptr(eng.pos),
+                      ptr(eng.body_line_gamma), S, R, R, r0, R, w["n_cols"], ptr(w["cols"]), ptr(eng.wake_positions),
                       1.0, 0.0, 0.0, case.tol, ptr(w["node_vel"]), ptr(eng.ws), eng._ws_bytes, stream_ptr())
     elif args.profile_kernel == "wake_term":  # FP64 sweep of the explicit wake term
         rm, d = w["rm"], w["rm_d"]

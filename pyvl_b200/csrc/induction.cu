@@ -203,6 +203,110 @@ __global__ void __launch_bounds__(kSumThreads) line_sum_kernel(const Segment<T>*
     }
 }
 
+// The FP32 sweep with Blackwell's packed FP32x2 arithmetic (__ffma2_rn / __fadd2_rn /
+// __fmul2_rn): each thread evaluates every segment at two points held in the two lanes of
+// float2 registers, so one instruction serves two pairs (the FP32 sweep is bound by instruction
+// issue, not by the FMA pipe).  Both lanes take the far-field series of segment_induction; a
+// lane inside the cut-off contributes zero (selected, not computed), and a lane that needs the
+// near-field atan2 form takes a scalar side path.  Same function and layout as
+// line_sum_kernel<float>; points p and p + 128 of each 256-point block.
+__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
+
+__global__ void __launch_bounds__(kSumThreads) line_sum_f32x2_kernel(const Segment<float>* __restrict__ seg,
+                                                                     uint32_t n_lines, uint32_t lines_per_split,
+                                                                     const double* __restrict__ pts, uint32_t n_pts,
+                                                                     uint32_t group, uint32_t stride, uint32_t in_off,
+                                                                     const uint32_t* __restrict__ cols,
+                                                                     uint32_t col_limit, float tol2,
+                                                                     float* __restrict__ partial)
+{
+    __shared__ Segment<float> s_seg[kSegTile];
+    const uint32_t split = blockIdx.y;
+    const uint32_t l_begin = split * lines_per_split;
+    const uint32_t l_end = min(n_lines, l_begin + lines_per_split);
+    float pv[2][3];
+    uint32_t pid[2];
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+        const uint32_t p = blockIdx.x * (kSumThreads * 2) + t * kSumThreads + threadIdx.x;
+        pid[t] = p;
+        bool ok = p < n_pts;
+        uint32_t col = ok ? (cols ? cols[p / group] : p / group) : 0;
+        if (col >= col_limit) {
+            ok = false;
+            col = 0;
+        }
+        const size_t q = ok ? (size_t)col * stride + p % group + in_off : 0;
+        pv[t][0] = ok ? float(pts[3 * q]) : 0.0f;
+        pv[t][1] = ok ? float(pts[3 * q + 1]) : 0.0f;
+        pv[t][2] = ok ? float(pts[3 * q + 2]) : 0.0f;
+    }
+    const float2 px = make_float2(pv[0][0], pv[1][0]), py = make_float2(pv[0][1], pv[1][1]),
+                 pz = make_float2(pv[0][2], pv[1][2]);
+    float2 accx = bc2(0.0f), accy = bc2(0.0f), accz = bc2(0.0f);
+    constexpr float kW = pvl::FarSeries<float>::kW;
+    for (uint32_t l0 = l_begin; l0 < l_end; l0 += kSegTile) {
+        const uint32_t l = l0 + threadIdx.x;
+        if (threadIdx.x < kSegTile && l < l_end)
+            s_seg[threadIdx.x] = seg[l];
+        __syncthreads();
+        const int cnt = (int)min((uint32_t)kSegTile, l_end - l0);
+#pragma unroll 1
+        for (int k = 0; k < cnt; ++k) {
+            const Segment<float> s = s_seg[k];
+            const float2 ax = __fadd2_rn(px, bc2(-s.r1x)), ay = __fadd2_rn(py, bc2(-s.r1y)),
+                         az = __fadd2_rn(pz, bc2(-s.r1z));
+            float2 t1 = __fmul2_rn(bc2(s.dx), ax);
+            t1 = __ffma2_rn(bc2(s.dy), ay, t1);
+            t1 = __ffma2_rn(bc2(s.dz), az, t1);
+            const float2 cx = __ffma2_rn(az, bc2(-s.dy), __fmul2_rn(ay, bc2(s.dz)));
+            const float2 cy = __ffma2_rn(ax, bc2(-s.dz), __fmul2_rn(az, bc2(s.dx)));
+            const float2 cz = __ffma2_rn(ay, bc2(-s.dx), __fmul2_rn(ax, bc2(s.dy)));
+            float2 hsq = __fmul2_rn(cx, cx);
+            hsq = __ffma2_rn(cy, cy, hsq);
+            hsq = __ffma2_rn(cz, cz, hsq);
+            const float2 x = __ffma2_rn(t1, __fadd2_rn(t1, bc2(-s.len)), hsq);
+            const float2 r = make_float2(__fdividef(1.0f, x.x), __fdividef(1.0f, x.y));
+            const float2 w = __fmul2_rn(__fmul2_rn(hsq, bc2(s.len * s.len)), __fmul2_rn(r, r));
+            float2 S = bc2(-1.0f / 11.0f);
+            S = __ffma2_rn(S, w, bc2(1.0f / 9.0f));
+            S = __ffma2_rn(S, w, bc2(-1.0f / 7.0f));
+            S = __ffma2_rn(S, w, bc2(1.0f / 5.0f));
+            S = __ffma2_rn(S, w, bc2(-1.0f / 3.0f));
+            S = __ffma2_rn(S, w, bc2(1.0f));
+            float2 mag = __fmul2_rn(__fmul2_rn(bc2(-s.glen), r), S);
+            const bool cut0 = hsq.x < tol2, cut1 = hsq.y < tol2;
+            const bool far0 = x.x > 0.0f && w.x <= kW, far1 = x.y > 0.0f && w.y <= kW;
+            if (!(cut0 || far0) || !(cut1 || far1)) {  // rare: a lane in the near field
+                if (!(cut0 || far0)) {
+                    const float rh = rsqrtf(hsq.x);
+                    mag.x = s.gamma * atan2f(-(hsq.x * rh) * s.len, x.x) * rh;
+                }
+                if (!(cut1 || far1)) {
+                    const float rh = rsqrtf(hsq.y);
+                    mag.y = s.gamma * atan2f(-(hsq.y * rh) * s.len, x.y) * rh;
+                }
+            }
+            mag.x = cut0 ? 0.0f : mag.x;
+            mag.y = cut1 ? 0.0f : mag.y;
+            accx = __ffma2_rn(cx, mag, accx);
+            accy = __ffma2_rn(cy, mag, accy);
+            accz = __ffma2_rn(cz, mag, accz);
+        }
+        __syncthreads();
+    }
+    const float a[2][3] = {{accx.x, accy.x, accz.x}, {accx.y, accy.y, accz.y}};
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+        if (pid[t] < n_pts) {
+            float* o = partial + 3 * ((size_t)split * n_pts + pid[t]);
+            o[0] = a[t][0];
+            o[1] = a[t][1];
+            o[2] = a[t][2];
+        }
+    }
+}
+
 // out = beta * out + alpha * v (+ (ux, uy, uz) for vector output), v = sum of the partials.
 // Point p is written at o = (p / group) * out_stride + p % group + out_off (normals are
 // indexed by p: normal output is always a plain array).
@@ -589,6 +693,7 @@ int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint3
     const uint32_t n_split_used = (n_lines + per - 1) / per;
     const int ppt = g_sum_ppt;
     dim3 grid(blocks_for(n_pts, kSumThreads * ppt), n_split_used);
+    dim3 grid_x2(blocks_for(n_pts, kSumThreads * 2), n_split_used);
     char* base = static_cast<char*>(ws);
     auto sweep = [&](auto tag, const auto* seg, auto* part, auto tol2) -> void {
         using T = decltype(tag);
@@ -616,7 +721,8 @@ int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint3
         auto* part = reinterpret_cast<float*>(base + pvl_segments_workspace(n_lines, PVL_F32));
         if (int r = prep_segments<float>(n_points, n_lines, lines, positions, line_gamma, tol, seg, st))
             return r;
-        sweep(float(0), seg, part, pvl::cutoff2<float>(tol));
+        line_sum_f32x2_kernel<<<grid_x2, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off,
+                                                               cols, col_limit, pvl::cutoff2<float>(tol), part);
         PVL_LAUNCH_CHECK();
         reduce_partials_kernel<float><<<blocks_for(n_pts, 256), 256, 0, st>>>(
             n_pts, n_split_used, part, normals, alpha, beta, ux, uy, uz, group, out_stride, out_off, out);
