@@ -50,6 +50,18 @@ template <typename T> struct Vec3 { T x, y, z; };
 // truncation error: double, 8 terms for w <= 0.01 (0.01^8 / 17 < 1e-17) and 5 terms for
 // w <= 1e-4 (1e-20 / 11 < 1e-21); float, 6 terms for w <= 0.04 (0.04^6 / 13 < 4e-10).
 // Closer pairs (larger w, or x <= 0) take the atan2 form.
+// Comparisons of non-negative values (or +NaN) through their bit patterns: for IEEE numbers of
+// one sign, the order of the bit patterns is the order of the values, and the integer compare
+// runs on the ALU pipe instead of the FP64 pipe that bounds the FP64 sweeps.  le_nn(a, b):
+// a <= b; lt_nn(a, b): a < b; pos(x): x > +0 (a +NaN counts as positive, and then fails the
+// far-field test that follows).
+__device__ __forceinline__ bool lt_nn(double a, double b) { return __double_as_longlong(a) < __double_as_longlong(b); }
+__device__ __forceinline__ bool le_nn(double a, double b) { return __double_as_longlong(a) <= __double_as_longlong(b); }
+__device__ __forceinline__ bool pos(double x) { return __double_as_longlong(x) > 0; }
+__device__ __forceinline__ bool lt_nn(float a, float b) { return a < b; }
+__device__ __forceinline__ bool le_nn(float a, float b) { return a <= b; }
+__device__ __forceinline__ bool pos(float x) { return x > 0.0f; }
+
 template <typename T> struct FarSeries;
 template <> struct FarSeries<double> {
     static constexpr double kW = 0.01;
@@ -57,7 +69,7 @@ template <> struct FarSeries<double> {
     static __device__ __forceinline__ double sum(double w)
     {
         double s;
-        if (w <= 1e-4) {  // most pairs of a wake sweep: the five-term series is exact to 1e-21
+        if (le_nn(w, 1e-4)) {  // most pairs of a wake sweep: the five-term series is exact to 1e-21
             s = 1.0 / 9.0;
         } else {
             s = -1.0 / 15.0;
@@ -107,14 +119,14 @@ __device__ __forceinline__ void segment_induction(const Segment<T>& s, T px, T p
     const T ax = px - s.r1x, ay = py - s.r1y, az = pz - s.r1z;
     const T t1 = s.dx * ax + s.dy * ay + s.dz * az;
     const T cx = ay * s.dz - az * s.dy, cy = az * s.dx - ax * s.dz, cz = ax * s.dy - ay * s.dx;
-    const T hsq = cx * cx + cy * cy + cz * cz;
-    if (hsq < tol2)
+    const T hsq = cx * cx + cy * cy + cz * cz;  // >= +0
+    if (lt_nn(hsq, tol2))
         return;
     const T x = hsq + t1 * (t1 - s.len);
     const T r = FarSeries<T>::rcp(x);  // wasted only on the rare near pairs
-    const T w = hsq * (s.len * s.len) * (r * r);
+    const T w = hsq * (s.len * s.len) * (r * r);  // >= +0, or +NaN
     T mag;
-    if (x > T(0) && w <= FarSeries<T>::kW) {
+    if (pos(x) && le_nn(w, FarSeries<T>::kW)) {
         mag = (GAMMA ? -s.glen : -scale * s.len) * r * FarSeries<T>::sum(w);
     } else {
         // one reciprocal square root gives both h and 1/h (no separate sqrt and division)
