@@ -39,7 +39,7 @@ __global__ void prep_segments_kernel(uint32_t n_points, uint32_t n_lines, const 
     const uint32_t a = PVL_IDX(lines[2 * i]), b = PVL_IDX(lines[2 * i + 1]);
     Segment<T> s;
     if (a >= n_points || b >= n_points) {
-        s.r1x = s.r1y = s.r1z = s.r2x = s.r2y = s.r2z = s.dx = s.dy = s.dz = T(0);
+        s.r1x = s.r1y = s.r1z = s.len2 = s.pad0 = s.pad1 = s.dx = s.dy = s.dz = T(0);
         s.len = s.gamma = s.glen = T(0);
         seg[i] = s;
         return;
@@ -61,9 +61,9 @@ __global__ void prep_segments_kernel(uint32_t n_points, uint32_t n_lines, const 
     s.r1x = T(r1x);
     s.r1y = T(r1y);
     s.r1z = T(r1z);
-    s.r2x = T(r2x);
-    s.r2y = T(r2y);
-    s.r2z = T(r2z);
+    s.len2 = T(len * len);
+    s.pad0 = T(0);
+    s.pad1 = T(0);
     s.dx = T(dx);
     s.dy = T(dy);
     s.dz = T(dz);
@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(kSumThreads) line_sum_f32x2_kernel(const Segme
             hsq = __ffma2_rn(cz, cz, hsq);
             const float2 x = __ffma2_rn(t1, __fadd2_rn(t1, bc2(-s.len)), hsq);
             const float2 r = make_float2(__fdividef(1.0f, x.x), __fdividef(1.0f, x.y));
-            const float2 w = __fmul2_rn(__fmul2_rn(hsq, bc2(s.len * s.len)), __fmul2_rn(r, r));
+            const float2 w = __fmul2_rn(__fmul2_rn(hsq, bc2(s.len2)), __fmul2_rn(r, r));
             float2 S = bc2(-1.0f / 11.0f);
             S = __ffma2_rn(S, w, bc2(1.0f / 9.0f));
             S = __ffma2_rn(S, w, bc2(-1.0f / 7.0f));

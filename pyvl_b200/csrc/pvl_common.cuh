@@ -15,15 +15,16 @@
 
 namespace pvl {
 
-// One vortex segment prepared for pair evaluation: start point r1, end point r2, unit
-// direction d = (r2 - r1)/len, length, the segment circulation gamma and glen = gamma * len.
+// One vortex segment prepared for pair evaluation: start point r1, unit direction
+// d = (r2 - r1)/len, length and its square, the segment circulation gamma and glen = gamma * len
+// (the end point itself is never needed: dr2 = dr1 - len d).
 // A segment shorter than the cut-off radius contributes nothing (src/core/flow_solver.c:107-112):
 // it is stored with d = 0 and len = 0, so every point sees h^2 = |dr1 x d|^2 = 0 below the
 // cut-off and skips it without a separate test.
 template <typename T>
 struct __align__(16) Segment {
     T r1x, r1y, r1z;
-    T r2x, r2y, r2z;
+    T len2, pad0, pad1;
     T dx, dy, dz;
     T len;
     T gamma;
@@ -65,7 +66,20 @@ __device__ __forceinline__ bool pos(float x) { return x > 0.0f; }
 template <typename T> struct FarSeries;
 template <> struct FarSeries<double> {
     static constexpr double kW = 0.01;
-    static __device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
+    // 1/x by Newton-Raphson refinement, r <- r + r (1 - x r), of the hardware's approximate
+    // reciprocal (rcp.approx.ftz.f64, a seed good to ~2^-22): two steps reach full double
+    // precision (the relative error squares each step), within an ulp of the rounded quotient.
+    // Used only where x is a positive normal number; a zero, negative, huge or NaN x gives a
+    // value that the far-field test rejects, after which the atan2 form is taken.
+    static __device__ __forceinline__ double rcp(double x)
+    {
+        double r;
+        asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+        double e = fma(-x, r, 1.0);
+        r = fma(r, e, r);
+        e = fma(-x, r, 1.0);
+        return fma(r, e, r);
+    }
     static __device__ __forceinline__ double sum(double w)
     {
         double s;
@@ -124,7 +138,7 @@ __device__ __forceinline__ void segment_induction(const Segment<T>& s, T px, T p
         return;
     const T x = hsq + t1 * (t1 - s.len);
     const T r = FarSeries<T>::rcp(x);  // wasted only on the rare near pairs
-    const T w = hsq * (s.len * s.len) * (r * r);  // >= +0, or +NaN
+    const T w = hsq * s.len2 * (r * r);  // >= +0, or +NaN
     T mag;
     if (pos(x) && le_nn(w, FarSeries<T>::kW)) {
         mag = (GAMMA ? -s.glen : -scale * s.len) * r * FarSeries<T>::sum(w);
@@ -168,7 +182,8 @@ struct RingSegments {
                 s[q] = seg[l];
             } else {  // an empty slot: d = 0 gives h^2 = 0, below any cut-off
                 s[q].r1x = s[q].r1y = s[q].r1z = s[q].dx = s[q].dy = s[q].dz = T(0);
-                s[q].len = s[q].gamma = s[q].glen = T(0);
+                s[q].len = s[q].len2 = s[q].gamma = s[q].glen = T(0);
+                s[q].pad0 = s[q].pad1 = T(0);
             }
             sign[q] = PVL_REV(g) ? T(-1) : T(1);
         }
