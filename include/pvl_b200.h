@@ -318,6 +318,9 @@ int pvl_normalize(uint32_t n, const double* w, double* v, double* nrm, void* str
 int pvl_combine(uint32_t n, uint32_t k, const double* Z, uint32_t ldz, const double* c, double* x,
                 void* stream);
 
+/* y += alpha x (FP64). */
+int pvl_axpy_f64(uint32_t n, double alpha, const double* x, double* y, void* stream);
+
 /* b (npad x npad, row stride ldb, FP32) = a (n x n, FP64) padded with the identity: the input
  * of the FP32 factorisation (whose inverse needs a multiple of 64 rows). */
 int pvl_pad_convert_f32(uint32_t n, const double* a, uint32_t lda, float* b, uint32_t ldb, uint32_t npad,

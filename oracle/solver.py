@@ -49,8 +49,10 @@ class OracleWake:
         self.current_time = float(time)
         self.step_count = 0
 
-    def update(self, time, mesh: OracleMesh, positions, circulation, freestream):
-        """Advect, re-pin, collapse, shift and shed: wake_models.py:83-157."""
+    def update(self, time, mesh: OracleMesh, positions, circulation, freestream, self_induction: bool = False):
+        """Advect, re-pin, collapse, shift and shed: wake_models.py:83-157.  With self_induction
+        (an option the reference does not have) every node also moves with the velocity the
+        wake itself induces, evaluated on the wake as it was when the update began."""
         dt = time - self.current_time
         self.current_time = time
         bn = self.bordering_nodes.astype(np.int64)
@@ -59,12 +61,17 @@ class OracleWake:
             self.wake_positions[:, 1, 0, :] = positions[bn[:, 1], :]
             self.step_count = 1
         complete_rows = min(self.step_count, self.line_rows)
+        wake_vel = None
+        if self_induction:
+            wake_vel = self.get_velocity(self.wake_positions.reshape((-1, 3))).reshape(self.wake_positions.shape)
         for i in reversed(range(complete_rows)):
             old_pos = self.wake_positions[:, :, i, :]
             flat = np.array(old_pos.reshape((-1, 3)), np.float64)
             vel = np.broadcast_to(freestream, flat.shape).copy()
             ind = mesh.induction_matrix(self.vortex_tol, positions, flat)
             vel += np.vecdot(ind, circulation[None, :, None], axis=1)
+            if wake_vel is not None:
+                vel += wake_vel[:, :, i, :].reshape((-1, 3))
             self.wake_positions[:, :, i + 1, :] = old_pos + vel.reshape(old_pos.shape) * dt
         self.wake_positions[:, 0, 0, :] = positions[bn[:, 0], :]
         self.wake_positions[:, 1, 0, :] = positions[bn[:, 1], :]
@@ -150,8 +157,9 @@ def bordered_solve(A, b, groups):
 class OracleRun:
     """One run of the reference solver loop (solver.py:175-263) on a workload Case."""
 
-    def __init__(self, case, closed_mode: str = "reference"):
+    def __init__(self, case, closed_mode: str = "reference", wake_self_induction: bool = False):
         self.case = case
+        self.wake_self_induction = wake_self_induction
         self.mesh = OracleMesh(case.n_points, case.elements)
         self.closed_mode = closed_mode
         self.wake = None
@@ -190,7 +198,7 @@ class OracleRun:
         pos, cps, nrm, A, rhs = self.assemble(time)
         gamma = self.solve(A, rhs)
         if self.wake is not None:
-            self.wake.update(time, self.mesh, pos, gamma, self.case.freestream)
+            self.wake.update(time, self.mesh, pos, gamma, self.case.freestream, self.wake_self_induction)
         self.history.append(gamma)
         self.iteration += 1
         return gamma

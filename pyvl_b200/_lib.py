@@ -69,6 +69,7 @@ SIGNATURES = {
     "pvl_gemm_tf32": (_I, [_U, _U, _U, ctypes.c_float, _P, _U, _P, _U, ctypes.c_float, _P, _U, _P, _P]),
     "pvl_gemv_f64": (_I, [_U, _U, _D, _P, _U, _P, _D, _P, _P]),
     "pvl_gemv_f32mat": (_I, [_U, _U, _D, _P, _U, _P, _D, _P, _P]),
+    "pvl_axpy_f64": (_I, [_U, _D, _P, _P, _P]),
     "pvl_basis_project": (_I, [_U, _U, _P, _U, _P, _P, _P]),
     "pvl_normalize": (_I, [_U, _P, _P, _P, _P]),
     "pvl_combine": (_I, [_U, _U, _P, _U, _P, _P, _P]),

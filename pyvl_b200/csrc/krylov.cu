@@ -168,6 +168,13 @@ __global__ void pad_convert_kernel(uint32_t n, const double* __restrict__ a, uin
     b[(size_t)r * ldb + c] = (r < n && c < n) ? (float)a[(size_t)r * lda + c] : (r == c ? 1.0f : 0.0f);
 }
 
+__global__ void axpy_kernel(uint32_t n, double alpha, const double* __restrict__ x, double* __restrict__ y)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        y[i] += alpha * x[i];
+}
+
 int require(const void* p, const char* what) { return p ? PVL_OK : pvl_fail(PVL_ERR_ARG, "%s is NULL", what); }
 
 }  // namespace
@@ -246,6 +253,16 @@ extern "C" int pvl_pad_convert_f32(uint32_t n, const double* a, uint32_t lda, fl
         return pvl_fail(PVL_ERR_ARG, "pvl_pad_convert_f32: need n <= npad <= ldb and lda >= n");
     pad_convert_kernel<<<blocks_for((size_t)npad * npad, 256), 256, 0, (cudaStream_t)stream>>>(n, a, lda, b, ldb,
                                                                                              npad);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_axpy_f64(uint32_t n, double alpha, const double* x, double* y, void* stream)
+{
+    if (n == 0)
+        return PVL_OK;
+    PVL_REQUIRE(x); PVL_REQUIRE(y);
+    axpy_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(n, alpha, x, y);
     PVL_LAUNCH_CHECK();
     return PVL_OK;
 }

@@ -135,8 +135,10 @@ class SolverEngine:
     """Plain FP64 UVLM stepping with the wake resident on the device."""
 
     def __init__(self, mesh: Mesh, freestream, tol: float, wake: WakeSpec | None = None,
-                 closed_groups: list[tuple[int, int]] | None = None):
+                 closed_groups: list[tuple[int, int]] | None = None, wake_self_induction: bool = False):
         self.dev = require_cuda()
+        # off by default (the reference's wake moves with the freestream and the body only)
+        self.wake_self_induction = bool(wake_self_induction)
         self.mesh = mesh
         self.tol = float(tol)
         self.u_inf = np.asarray(freestream, np.float64).reshape(3)
@@ -210,6 +212,8 @@ class SolverEngine:
             "n_cols": int(cols.size),
             "node_vel": torch.zeros((int(cols.size), R, 3), **f64),
             "line_gamma": torch.zeros(max(wmesh.n_lines, 1), **f64),
+            "self_line_gamma": torch.zeros(max(wmesh.n_lines, 1), **f64),
+            "node_vel_self": torch.zeros((int(cols.size), R, 3), **f64),
             "time": float(w.time),
             "step_count": 0,
         }
@@ -229,6 +233,8 @@ class SolverEngine:
                 _lib.query("pvl_line_velocity_workspace", Lw, self.P, _lib.PVL_F64),
                 _node_velocity_workspace(L, w["n_cols"], w["R"], _lib.PVL_F64),
             ]
+            if self.wake_self_induction:
+                need.append(_node_velocity_workspace(Lw, w["n_cols"], w["R"], _lib.PVL_F64))
         return max(need) + 256
 
     # ------------------------------------------------------------------ state access
@@ -353,11 +359,29 @@ class SolverEngine:
                   ptr(self.pos), ptr(self.body_line_gamma), S, R, complete, 0, complete, w["n_cols"], ptr(w["cols"]),
                   ptr(self.wake_positions), float(u[0]), float(u[1]), float(u[2]), self.tol, ptr(w["node_vel"]),
                   ptr(self.ws), self._ws_bytes, s)
+        if self.wake_self_induction:
+            self._add_wake_self_velocity(complete)
         self._advect(complete, dt)
         c = w["ccur"]
         _lib.call("pvl_wake_shed", S, R, ptr(w["circ"][c]), ptr(w["adj"]), ptr(self.gamma), ptr(w["circ"][1 - c]), s)
         w["ccur"] = 1 - c
         w["step_count"] += 1
+
+    def _add_wake_self_velocity(self, complete: int) -> None:
+        """node_vel += the velocity the whole wake (every row, row 0 included) induces at the
+        advecting nodes, from the wake as it is before this update (FP64).  An option: the
+        reference's wake_models.py:113-137 moves the wake with the freestream and the body only."""
+        s = stream_ptr()
+        w = self.wake
+        S, R = w["S"], w["R"]
+        wm, wd = w["mesh"], w["d"]
+        _lib.call("pvl_line_circulation", wm.n_lines, ptr(wd["map_offsets"]), ptr(wd["map_entries"]),
+                  ptr(self.wake_circulation), 0, ptr(w["self_line_gamma"]), s)
+        _lib.call("pvl_wake_node_velocity_cols", _lib.PVL_F64, wm.n_points, wm.n_lines, ptr(wd["lines"]),
+                  ptr(self.wake_positions.reshape(-1, 3)), ptr(w["self_line_gamma"]), S, R, complete, 0, complete,
+                  w["n_cols"], ptr(w["cols"]), ptr(self.wake_positions), 0.0, 0.0, 0.0, self.tol,
+                  ptr(w["node_vel_self"]), ptr(self.ws), self._ws_bytes, s)
+        _lib.call("pvl_axpy_f64", w["n_cols"] * complete * 3, 1.0, ptr(w["node_vel_self"]), ptr(w["node_vel"]), s)
 
     def _advect(self, complete: int, dt: float) -> None:
         s = stream_ptr()
@@ -417,8 +441,8 @@ class MixedSolverEngine(SolverEngine):
     def __init__(self, mesh: Mesh, freestream, tol: float, wake: WakeSpec | None = None, closed_groups=None,
                  refresh: int = 25, near_rows: int | None = None, advect_near_rows: int = 8,
                  gmres_tol: float = 1e-12, max_iter: int = 20, async_refresh: bool = True,
-                 refresh_on_iters: int = 5, use_graphs: bool = True):
-        super().__init__(mesh, freestream, tol, wake, closed_groups)
+                 refresh_on_iters: int = 5, use_graphs: bool = True, wake_self_induction: bool = False):
+        super().__init__(mesh, freestream, tol, wake, closed_groups, wake_self_induction)
         self.refresh = int(refresh)
         self.gmres_tol = float(gmres_tol)
         self.max_iter = int(max_iter)
@@ -779,6 +803,8 @@ class MixedSolverEngine(SolverEngine):
                           ptr(self.pos), ptr(self.body_line_gamma), S, R, complete, r0, r1, w["n_cols"],
                           ptr(w["cols"]), ptr(self.wake_positions), float(u[0]), float(u[1]), float(u[2]), self.tol,
                           ptr(w["node_vel"]), ptr(self.ws), self._ws_bytes, s)
+        if self.wake_self_induction:
+            self._add_wake_self_velocity(complete)
         self._advect(complete, dt)
         c = w["ccur"]
         _lib.call("pvl_wake_shed", S, R, ptr(w["circ"][c]), ptr(w["adj"]), ptr(self.gamma), ptr(w["circ"][1 - c]), s)

@@ -160,3 +160,42 @@ def test_closed_sphere_run_solver():
         res = pv.run_solver(sim, settings, None, None)
     want = OracleRun(case, closed_mode="bordered").step()
     assert rel(res.circulations[0], want) <= PARITY
+
+
+def test_postprocess_fields_match_oracle():
+    """compute_velocities / compute_surface_dynamic_pressure (postprocess/velocity.py:11-89,
+    pressure.py:11-107) after run_solver, against the oracle's kernels on the same states."""
+    import pyvl_b200 as pv
+    from oracle.kernels import OracleMesh
+    from oracle.solver import OracleWake
+
+    case, sim, settings, wm = _flat_setup(pv)
+    with contextlib.redirect_stdout(io.StringIO()):
+        res = pv.run_solver(sim, settings, wm, None)
+    rng = np.random.default_rng(8)
+    pts = rng.normal(size=(40, 3)) * np.array([2.0, 4.0, 0.5]) + np.array([1.0, 0.0, 0.1])
+    vel = pv.postprocess.compute_velocities(res, pts)
+    pres = pv.postprocess.compute_surface_dynamic_pressure(res)
+    om = OracleMesh(case.n_points, case.elements)
+    times = settings.time_settings.output_times
+    for i, t in enumerate(times):
+        pos = res.geometry.positions_at_time(t)
+        g = res.circulations[i]
+        w = res.wake_models[i]
+        ow = None
+        if w is not None:
+            ow = OracleWake(w.bordering_nodes, w.shedding_lines, w.adjacent_surfaces, w.vortex_tol, t, w.line_rows)
+            ow.wake_positions[...] = w.wake_positions
+            ow.circulation[...] = w.circulation
+        want = np.vecdot(om.induction_matrix(case.tol, pos, pts), g[None, :, None], axis=1) + case.freestream
+        if ow is not None:
+            want = want + ow.get_velocity(pts)
+        assert rel(vel[i], want) <= PARITY, i
+        cps = om.surface_average_vec3(pos)
+        ind = np.vecdot(om.induction_matrix(case.tol, pos, cps), g[None, :, None], axis=1)
+        ind -= om.surface_average_vec3(res.geometry.velocity_at_time(t))
+        if ow is not None:
+            ind = ind + ow.get_velocity(cps)
+        rho = settings.flow_conditions.get_density(t, cps)
+        p = -rho * np.vecdot(ind, 0.5 * ind + np.broadcast_to(case.freestream, cps.shape), axis=-1)
+        assert rel(pres[i], p) <= PARITY, i

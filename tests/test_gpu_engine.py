@@ -119,3 +119,30 @@ def test_host_inputs_without_per_step_sync():
     torch.cuda.synchronize()
     got = torch.stack(hist).cpu().numpy()
     assert np.array_equal(got, ref)
+
+
+def test_wake_self_induction_option_matches_oracle():
+    """The optional wake self-induction (off by default; not in the reference) against the
+    oracle's restatement of the same option: circulations and wake positions."""
+    from oracle.kernels import OracleMesh
+    from oracle.solver import OracleRun, shedding_setup
+    from pyvl_b200.cvl import Mesh
+    from pyvl_b200.engine import SolverEngine, WakeSpec
+    from pyvl_b200.workloads import flat_wing
+
+    case = flat_wing(nt=8, line_rows=6)
+    mesh = Mesh(case.n_points, case.elements)
+    shed, nodes, adj = shedding_setup(OracleMesh(case.n_points, case.elements), case.te_node_pairs)
+    eng = SolverEngine(mesh, case.freestream, case.tol, WakeSpec(shed, nodes, adj, case.line_rows, case.t0),
+                       wake_self_induction=True)
+    off = make_engine(case)
+    orc = OracleRun(case, wake_self_induction=True)
+    for it in range(case.nt):
+        t = it * case.dt
+        eng.step(t, case.positions_at(t), case.velocities_at(t))
+        off.step(t, case.positions_at(t), case.velocities_at(t))
+        ref = orc.step()
+        assert rel(eng.gamma_host(), ref) <= PARITY, it
+    w = eng.wake_positions.cpu().numpy()
+    assert rel(w, orc.wake.wake_positions) <= 1e-11
+    assert rel(off.wake_positions.cpu().numpy(), orc.wake.wake_positions) > 1e-8  # the option does something
