@@ -14,6 +14,9 @@ import numpy as np
 import numpy.typing as npt
 
 
+_PKG = __name__.split(".")[0]  # this package's top-level name
+
+
 class HirearchicalMap(MutableMapping):
     """Mapping that holds values and nested HirearchicalMaps under unique keys."""
 
@@ -44,9 +47,14 @@ class HirearchicalMap(MutableMapping):
         self._map[key] = value
 
     def insert_type(self, key: str, t: type) -> None:
+        """Stored as "module.Name"; this package's classes are written under the reference's
+        module names (pyvl.*), so that the files are the reference's format."""
         if not isinstance(t, type):
             raise TypeError(f"The value was not a type but {type(t).__name__}")
-        self._insert(key, t.__module__ + "." + t.__name__)
+        mod = t.__module__
+        if mod == _PKG or mod.startswith(_PKG + "."):
+            mod = "pyvl" + mod[len(_PKG):]
+        self._insert(key, mod + "." + t.__name__)
 
     def insert_array(self, key: str, value: npt.ArrayLike) -> None:
         self._insert(key, np.array(value))
@@ -74,8 +82,12 @@ class HirearchicalMap(MutableMapping):
         self._insert(key, value)
 
     def get_type(self, key: str) -> type:
+        """The class named "module.Name"; the reference's pyvl.* names resolve to this
+        package's classes of the same module path and name."""
         name = str(self._map[key])
         mod, _, attr = name.rpartition(".")
+        if mod == "pyvl" or mod.startswith("pyvl."):
+            mod = _PKG + mod[len("pyvl"):]
         return getattr(importlib.import_module(mod), attr)
 
     def get_array(self, key: str) -> npt.NDArray:

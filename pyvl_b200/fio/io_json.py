@@ -1,43 +1,46 @@
-"""JSON form of a HirearchicalMap (python/pyvl/fio/io_json.py:15-49): arrays keep dtype and shape."""
+"""JSON form of a HirearchicalMap, in the reference's own file format
+(python/pyvl/fio/io_json.py:15-49): nested maps are JSON objects, arrays nested lists, scalars
+and strings as they are; reading turns every list back into a numpy array.  Files written by
+either package load in the other."""
 
 from __future__ import annotations
 
 import json
+from collections.abc import Sequence
 from pathlib import Path
+from typing import Any
 
 import numpy as np
 
 from .io_common import HirearchicalMap
 
 
-def _encode(hmap: HirearchicalMap) -> dict:
-    out = {}
-    for k in hmap:
-        v = hmap[k]
-        if isinstance(v, HirearchicalMap):
-            out[k] = {"__map__": _encode(v)}
-        elif isinstance(v, np.ndarray):
-            out[k] = {"__array__": v.tolist(), "dtype": str(v.dtype), "shape": list(v.shape)}
-        else:
-            out[k] = v
-    return out
+def _plain(value: Any) -> Any:
+    """JSON-ready form of one value (maps -> dicts, arrays -> lists, numpy scalars -> Python)."""
+    if isinstance(value, HirearchicalMap):
+        return {k: _plain(value[k]) for k in value}
+    if isinstance(value, np.ndarray):
+        return value.tolist()
+    if isinstance(value, np.generic):
+        return value.item()
+    return value
 
 
-def _decode(d: dict) -> HirearchicalMap:
+def _to_map(obj: dict) -> HirearchicalMap:
     hm = HirearchicalMap()
-    for k, v in d.items():
-        if isinstance(v, dict) and "__map__" in v:
-            hm[k] = _decode(v["__map__"])
-        elif isinstance(v, dict) and "__array__" in v:
-            hm[k] = np.array(v["__array__"], dtype=v["dtype"]).reshape(v["shape"])
+    for key, value in obj.items():
+        if isinstance(value, Sequence) and not isinstance(value, str):
+            hm[key] = np.array(value)
         else:
-            hm[k] = v
+            hm[key] = value
     return hm
 
 
 def serialize_json(hmap: HirearchicalMap, path: Path | str) -> None:
-    Path(path).write_text(json.dumps(_encode(hmap)))
+    """Save a HirearchicalMap into a JSON file."""
+    Path(path).write_text(json.dumps(_plain(hmap)))
 
 
 def deserialize_json(path: Path | str) -> HirearchicalMap:
-    return _decode(json.loads(Path(path).read_text()))
+    """Load a HirearchicalMap from a JSON file."""
+    return json.loads(Path(path).read_text(), object_hook=_to_map)

@@ -21,6 +21,10 @@ and records, for small seeded inputs:
 * wake_wedge.npz -- the wedge of test/pytests/test_wake_models.py:18-77 after 5 updates.
 * checksums.npz -- full-size body matrices (1024 and 4096 rings) reduced to
   A @ v, A^T @ w and sampled entries for seeded v, w.
+* checkpoint_flat.json / .npz -- the reference's own JSON solver-state snapshot (run_solver
+  with OutputSettings("JSON")) after a 3-step flat-wing run, with its circulation and wake.
+
+``--only NAME`` regenerates one fixture (e.g. ``--only checkpoint``).
 
 The fixtures are small (a few hundred KB in total) and committed.
 """
@@ -316,11 +320,41 @@ def make_frames(pyvl):
     np.savez_compressed(HERE / "frames.npz", **data)
 
 
+def make_checkpoint(pyvl):
+    """A solver-state snapshot written by the reference's own JSON output (run_solver with
+    OutputSettings("JSON"), solver.py:251-262) after the last step of a 3-step flat-wing run."""
+    import contextlib
+    import io
+    import shutil
+    import tempfile
+
+    case = workloads.flat_wing(nt=3, line_rows=3)
+    geo = pyvl.Geometry("wing", pyvl.ReferenceFrame(), ref_mesh(pyvl, case), case.positions)
+    sim = pyvl.SimulationGeometry(geo)
+    fc = pyvl.FlowConditionsUniform(*case.freestream)
+    settings = pyvl.SolverSettings(fc, pyvl.ModelSettings(TOL), pyvl.TimeSettings(case.nt, case.dt))
+    te = te_lines_for(sim.mesh, case.te_node_pairs)
+    nds, srf = sim.line_adjecency_information(te)
+    wm = pyvl.WakeModelLineExplicitUnsteady(nds, te, srf, TOL, case.t0, case.line_rows)
+    with tempfile.TemporaryDirectory() as tmp:
+        out = pyvl.OutputSettings("JSON", lambda i, t: f"{tmp}/state_{i}.json")
+        with contextlib.redirect_stdout(io.StringIO()):
+            res = pyvl.run_solver(sim, settings, wm, out)
+        shutil.copy(f"{tmp}/state_{case.nt - 1}.json", HERE / "checkpoint_flat.json")
+    np.savez_compressed(HERE / "checkpoint_flat.npz", circulation=res.circulations[-1],
+                        wake_positions=res.wake_models[-1].wake_positions,
+                        wake_circulation=res.wake_models[-1].circulation)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--only", default=None)
     args = ap.parse_args()
     pyvl = ref.load_pyvl(args.reference)
+    if args.only:
+        globals()[f"make_{args.only}"](pyvl)
+        return
     make_kernels(pyvl)
     make_flat_run(pyvl)
     make_kinematic_runs(pyvl)
@@ -328,6 +362,7 @@ def main():
     make_wedge(pyvl)
     make_checksums(pyvl)
     make_frames(pyvl)
+    make_checkpoint(pyvl)
     for p in sorted(HERE.glob("*.npz")):
         print(p.name, p.stat().st_size)
 
