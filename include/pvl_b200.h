@@ -141,6 +141,18 @@ int pvl_induction_normal(int precision, uint32_t n_points, uint32_t n_lines, con
                          void* out, uint32_t ld, void* ws, size_t ws_bytes, void* stream);
 
 /* Scratch for pvl_line_velocity. */
+/* pvl_induction_normal (FP64) with each line evaluated once per control point: rings in
+ * tiles of 128 consecutive rings; tile t's distinct lines are tile_lines[tile_offsets[t] ..
+ * tile_offsets[t+1]), sl_local[k] is the position of CSR entry k (surface_lines[k]) in its
+ * tile's list, max_tile_lines the largest list (Mesh.ring_tiles builds the three).  Same
+ * matrix as pvl_induction_normal to rounding (per-line dot products summed per ring).
+ * ws: pvl_segments_workspace(n_lines, PVL_F64) bytes. */
+int pvl_induction_normal_tiled(uint32_t n_points, uint32_t n_lines, const uint32_t* lines, const double* positions,
+                               uint32_t n_surfaces, const uint32_t* offsets, const uint32_t* surface_lines,
+                               const uint32_t* tile_offsets, const uint32_t* tile_lines, const uint32_t* sl_local,
+                               uint32_t max_tile_lines, uint32_t n_cp, const double* cps, const double* normals,
+                               double tol, double* out, uint32_t ld, void* ws, size_t ws_bytes, void* stream);
+
 /* Points per thread (1, 2 or 4; default 1) of the segment sweeps behind pvl_line_velocity,
  * pvl_wake_node_velocity(_cols) and the no-alloc entry, process-wide; returns the previous
  * value (or a negative status).  A tile-shape knob for autotuning; results do not depend on it.

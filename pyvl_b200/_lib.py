@@ -45,6 +45,8 @@ SIGNATURES = {
     "pvl_segments_workspace": (_Z, [_U, _I]),
     "pvl_line_induction": (_I, [_U, _U, _P, _P, _U, _P, _D, _P, _P, _Z, _P]),
     "pvl_induction_matrix": (_I, [_U, _U, _P, _P, _U, _P, _P, _U, _P, _D, _P, _P, _Z, _P]),
+    "pvl_induction_normal_tiled": (_I, [_U, _U, _P, _P, _U, _P, _P, _P, _P, _P, _U, _U, _P, _P, _D, _P, _U, _P, _Z,
+                                        _P]),
     "pvl_induction_normal": (_I, [_I, _U, _U, _P, _P, _U, _P, _P, _U, _P, _P, _D, _P, _U, _P, _Z, _P]),
     "pvl_set_sweep_points_per_thread": (_I, [_I]),
     "pvl_line_velocity_workspace": (_Z, [_U, _U, _I]),

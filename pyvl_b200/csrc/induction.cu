@@ -112,6 +112,71 @@ __global__ void __launch_bounds__(kRingThreads) ring_matrix_kernel(
     }
 }
 
+// Ring-matrix rows with each line evaluated once per control point: rings are taken in tiles
+// of kRingTile consecutive rings; a CTA evaluates n_i . u_l(cp_i) for the distinct lines of
+// its tile (tile_lines[tile_offsets[t] ..]) at its CPB control points into shared memory,
+// then each thread sums its ring's signed entries (sl_local: each CSR entry's position in its
+// tile's line list) in CSR order.  Adjacent rings share lines, so a structured wing needs
+// ~0.57 line evaluations per (point, ring line) instead of one.
+constexpr int kRingTile = 128;
+constexpr int kTileCPB = 16;
+
+__global__ void __launch_bounds__(kRingTile) ring_tile_kernel(uint32_t n_surfaces, const uint32_t* __restrict__ off,
+                                                              const uint32_t* __restrict__ sl,
+                                                              const uint32_t* __restrict__ sl_local,
+                                                              const uint32_t* __restrict__ tile_off,
+                                                              const uint32_t* __restrict__ tile_lines,
+                                                              uint32_t tile_stride, uint32_t n_lines,
+                                                              const Segment<double>* __restrict__ seg, uint32_t n_cp,
+                                                              const double* __restrict__ cps,
+                                                              const double* __restrict__ normals, double tol2,
+                                                              double* __restrict__ out, uint32_t ld)
+{
+    extern __shared__ double sV[];  // [kTileCPB][tile_stride]
+    __shared__ double s_p[kTileCPB][3], s_n[kTileCPB][3];
+    const uint32_t tile = blockIdx.x, i0 = blockIdx.y * kTileCPB;
+    if (threadIdx.x < kTileCPB * 3) {
+        const uint32_t c = threadIdx.x / 3, e = threadIdx.x % 3;
+        const bool ok = i0 + c < n_cp;
+        s_p[c][e] = ok ? cps[3 * (size_t)(i0 + c) + e] : 0.0;
+        s_n[c][e] = ok ? normals[3 * (size_t)(i0 + c) + e] : 0.0;
+    }
+    __syncthreads();
+    const uint32_t L0 = tile_off[tile], nl = tile_off[tile + 1] - L0;
+    for (uint32_t l = threadIdx.x; l < nl; l += kRingTile) {
+        const uint32_t g = tile_lines[L0 + l];
+        const bool ok = g < n_lines;
+        Segment<double> sg;
+        if (ok) {
+            sg = seg[g];
+        } else {
+            sg.r1x = sg.r1y = sg.r1z = sg.dx = sg.dy = sg.dz = 0.0;
+            sg.len = sg.len2 = sg.gamma = sg.glen = sg.pad0 = sg.pad1 = 0.0;
+        }
+#pragma unroll 4
+        for (int q = 0; q < kTileCPB; ++q) {
+            Vec3<double> acc{0.0, 0.0, 0.0};
+            pvl::segment_induction(sg, s_p[q][0], s_p[q][1], s_p[q][2], tol2, 1.0, acc);
+            sV[q * tile_stride + l] = acc.x * s_n[q][0] + acc.y * s_n[q][1] + acc.z * s_n[q][2];
+        }
+    }
+    __syncthreads();
+    const uint32_t j = tile * kRingTile + threadIdx.x;
+    if (j >= n_surfaces)
+        return;
+    const uint32_t k0 = off[j], k1 = off[j + 1];
+    for (int q = 0; q < kTileCPB; ++q) {
+        if (i0 + q >= n_cp)
+            break;
+        double v = 0.0;
+        for (uint32_t k = k0; k < k1; ++k) {
+            const double x = sV[q * tile_stride + sl_local[k]];
+            v += PVL_REV(sl[k]) ? -x : x;
+        }
+        out[(size_t)(i0 + q) * ld + j] = v;
+    }
+}
+
 // out[(i*n_lines + l)*3 + c] = u_l(cp_i)
 __global__ void __launch_bounds__(kRingThreads) line_matrix_kernel(uint32_t n_lines,
                                                                    const Segment<double>* __restrict__ seg,
@@ -654,6 +719,44 @@ extern "C" int pvl_induction_normal(int precision, uint32_t n_points, uint32_t n
         ring_matrix_kernel<float, float, 0><<<grid, kRingThreads, 0, st>>>(
             n_surfaces, off, sl, n_lines, seg, n_cp, cps, normals, pvl::cutoff2<float>(tol), static_cast<float*>(out), ld);
     }
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_induction_normal_tiled(uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
+                                          const double* positions, uint32_t n_surfaces, const uint32_t* offsets,
+                                          const uint32_t* surface_lines, const uint32_t* tile_offsets,
+                                          const uint32_t* tile_lines, const uint32_t* sl_local,
+                                          uint32_t max_tile_lines, uint32_t n_cp, const double* cps,
+                                          const double* normals, double tol, double* out, uint32_t ld, void* ws,
+                                          size_t ws_bytes, void* stream)
+{
+    if (n_cp == 0 || n_surfaces == 0)
+        return PVL_OK;
+    PVL_REQUIRE(lines); PVL_REQUIRE(positions); PVL_REQUIRE(offsets); PVL_REQUIRE(surface_lines);
+    PVL_REQUIRE(tile_offsets); PVL_REQUIRE(tile_lines); PVL_REQUIRE(sl_local); PVL_REQUIRE(cps);
+    PVL_REQUIRE(normals); PVL_REQUIRE(out); PVL_REQUIRE(ws);
+    if (ld < n_surfaces)
+        return pvl_fail(PVL_ERR_ARG, "pvl_induction_normal_tiled: ld < n_surfaces");
+    if (ws_bytes < pvl_segments_workspace(n_lines, PVL_F64))
+        return pvl_fail(PVL_ERR_ALLOC, "pvl_induction_normal_tiled: workspace too small");
+    const size_t smem = (size_t)kTileCPB * max_tile_lines * sizeof(double);
+    if (smem > 200 * 1024)
+        return pvl_fail(PVL_ERR_ARG, "pvl_induction_normal_tiled: %u lines in one ring tile exceed shared memory",
+                        max_tile_lines);
+    cudaStream_t st = (cudaStream_t)stream;
+    auto* seg = static_cast<Segment<double>*>(ws);
+    if (int r = prep_segments<double>(n_points, n_lines, lines, positions, nullptr, tol, seg, st))
+        return r;
+    static size_t attr = 0;
+    if (smem > attr) {
+        PVL_CUDA_CHECK(cudaFuncSetAttribute(ring_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr = smem;
+    }
+    dim3 grid((n_surfaces + kRingTile - 1) / kRingTile, (n_cp + kTileCPB - 1) / kTileCPB);
+    ring_tile_kernel<<<grid, kRingTile, smem, st>>>(n_surfaces, offsets, surface_lines, sl_local, tile_offsets,
+                                                    tile_lines, max_tile_lines, n_lines, seg, n_cp, cps, normals,
+                                                    pvl::cutoff2<double>(tol), out, ld);
     PVL_LAUNCH_CHECK();
     return PVL_OK;
 }

@@ -359,8 +359,36 @@ class Mesh:
                 "map_offsets": to_device_u32(offs, dev),
                 "map_entries": to_device_u32(ents if ents.size else np.zeros(1, np.uint32), dev),
             }
+            t_off, t_lines, sl_local, max_nl = self.ring_tiles()
+            d["tile_offsets"] = to_device_u32(t_off, dev)
+            d["tile_lines"] = to_device_u32(t_lines if t_lines.size else np.zeros(1, np.uint32), dev)
+            d["sl_local"] = to_device_u32(sl_local if sl_local.size else np.zeros(1, np.uint32), dev)
+            d["tile_max"] = max_nl
             self._dev[key] = d
         return d
+
+    RING_TILE = 128  # rings per tile of pvl_induction_normal_tiled
+
+    def ring_tiles(self):
+        """Per tile of RING_TILE consecutive rings: its distinct lines, and for every CSR entry
+        its position in its tile's list (inputs of pvl_induction_normal_tiled)."""
+        if getattr(self, "_ring_tiles", None) is None:
+            off = self._offsets.astype(np.int64)
+            ids = (self._surface_lines & np.uint32(0x7FFFFFFF)).astype(np.int64)
+            n_t = -(-self.n_surfaces // self.RING_TILE)
+            tile_off, tile_lines = [0], []
+            local = np.zeros(ids.size, np.uint32)
+            for t in range(n_t):
+                a = off[t * self.RING_TILE]
+                b = off[min((t + 1) * self.RING_TILE, self.n_surfaces)]
+                uniq, inv = np.unique(ids[a:b], return_inverse=True)
+                tile_lines.append(uniq)
+                local[a:b] = inv
+                tile_off.append(tile_off[-1] + uniq.size)
+            tl = np.concatenate(tile_lines) if tile_lines else np.zeros(1, np.int64)
+            max_nl = int(max((x.size for x in tile_lines), default=1))
+            self._ring_tiles = (np.array(tile_off, np.uint32), tl.astype(np.uint32), local, max_nl)
+        return self._ring_tiles
 
     def ring_map(self):
         """Line -> signed ring ids (transpose of the ring CSR)."""

@@ -294,9 +294,10 @@ class SolverEngine:
         _lib.call("pvl_rhs", P, ptr(b["nrm"]), None, float(u[0]), float(u[1]), float(u[2]), ptr(b["cpv"]),
                   ptr(b["rhs"]), s)
         ws = b["ws"]
-        _lib.call("pvl_induction_normal", _lib.PVL_F64, msh.n_points, msh.n_lines, ptr(d["lines"]), ptr(b["pos"]), P,
-                  ptr(d["offsets"]), ptr(d["surface_lines"]), P, ptr(b["cps"]), ptr(b["nrm"]), self.tol, ptr(b["A"]),
-                  self.N, ptr(ws), ws.numel(), s)
+        _lib.call("pvl_induction_normal_tiled", msh.n_points, msh.n_lines, ptr(d["lines"]), ptr(b["pos"]), P,
+                  ptr(d["offsets"]), ptr(d["surface_lines"]), ptr(d["tile_offsets"]), ptr(d["tile_lines"]),
+                  ptr(d["sl_local"]), d["tile_max"], P, ptr(b["cps"]), ptr(b["nrm"]), self.tol, ptr(b["A"]), self.N,
+                  ptr(ws), ws.numel(), s)
 
     def border(self) -> None:
         """Zero-mean rows/columns of the closed bodies (bordered system)."""

@@ -164,3 +164,34 @@ def test_lu_bordered_sphere(torch_cuda):
     assert info == 0 and err == 0
     want = bordered_solve(A, rhs, [np.arange(n)])
     assert rel(x[:n], want) <= 1e-12
+
+
+@pytest.mark.parametrize("factory", ["flapping_small", "sphere"])
+def test_tiled_ring_matrix_matches_ring_matrix(factory):
+    """pvl_induction_normal_tiled (each line once per control point per ring tile) gives the
+    matrix of pvl_induction_normal to rounding, on quads and on triangles."""
+    import torch
+
+    from pyvl_b200 import _lib
+    from pyvl_b200.cvl import Mesh
+    from pyvl_b200.device import Workspace, ptr, stream_ptr
+    from pyvl_b200.workloads import flapping, icosphere
+
+    case = flapping(ns=48, nc=12, line_rows=2) if factory == "flapping_small" else icosphere(subdiv=3)
+    mesh = Mesh(case.n_points, case.elements)
+    pos = torch.as_tensor(case.positions_at(0.3), device="cuda")
+    cps = torch.as_tensor(mesh.surface_average_vec3(case.positions_at(0.3)), device="cuda")
+    nrm = torch.as_tensor(mesh.surface_normal(case.positions_at(0.3)), device="cuda")
+    P = mesh.n_surfaces
+    d = mesh.device_arrays()
+    ws, nb = Workspace.get(_lib.query("pvl_segments_workspace", mesh.n_lines, _lib.PVL_F64))
+    a = torch.zeros((P, P), dtype=torch.float64, device="cuda")
+    b = torch.zeros_like(a)
+    s = stream_ptr()
+    _lib.call("pvl_induction_normal", _lib.PVL_F64, mesh.n_points, mesh.n_lines, ptr(d["lines"]), ptr(pos), P,
+              ptr(d["offsets"]), ptr(d["surface_lines"]), P, ptr(cps), ptr(nrm), case.tol, ptr(a), P, ws, nb, s)
+    _lib.call("pvl_induction_normal_tiled", mesh.n_points, mesh.n_lines, ptr(d["lines"]), ptr(pos), P,
+              ptr(d["offsets"]), ptr(d["surface_lines"]), ptr(d["tile_offsets"]), ptr(d["tile_lines"]),
+              ptr(d["sl_local"]), d["tile_max"], P, ptr(cps), ptr(nrm), case.tol, ptr(b), P, ws, nb, s)
+    torch.cuda.synchronize()
+    assert (torch.linalg.norm(a - b) / torch.linalg.norm(a)).item() <= 1e-14
