@@ -207,6 +207,12 @@ int pvl_line_circulation(uint32_t n_lines, const uint32_t* map_offsets,
 int pvl_wake_fold_implicit(uint32_t n_cp, uint32_t n_shed, const double* implicit,
                            const uint32_t* adjacent, double* A, uint32_t lda, void* stream);
 
+/* pvl_wake_fold_implicit in parallel over (row, shedding line), for adjacency tables in which
+ * every ring appears at most once over all shedding lines and sides (the caller checks; true
+ * for wings, where each trailing-edge ring has one shedding edge).  Same result. */
+int pvl_wake_fold_implicit_distinct(uint32_t n_cp, uint32_t n_shed, const double* implicit,
+                                    const uint32_t* adjacent, double* A, uint32_t lda, void* stream);
+
 /* Velocity of the wake nodes that advect this step: for every (s, side) and row
  * i < complete_rows, node_vel[(s*2 + side)*complete_rows + i] = U_inf + sum_k gamma_k u_k(node)
  * with the body segments (lines, positions, line_gamma).  wake_pos is (n_shed, 2,

@@ -31,6 +31,25 @@ __global__ void fold_implicit_kernel(uint32_t n_cp, uint32_t n_shed, const doubl
     }
 }
 
+// The same fold with one thread per (row, shedding line), for adjacency tables in which no ring
+// appears twice (then no two threads touch the same entry, and each entry receives exactly the
+// one update the sequential fold gives it).
+__global__ void fold_implicit_parallel_kernel(uint32_t n_cp, uint32_t n_shed, const double* __restrict__ implicit,
+                                              const uint32_t* __restrict__ adj, double* __restrict__ A, uint32_t lda)
+{
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (uint64_t)n_cp * n_shed)
+        return;
+    const uint32_t i = (uint32_t)(t / n_shed), s = (uint32_t)(t % n_shed);
+    const double c = implicit[t];
+    const uint32_t s1 = adj[2 * s + 1], s0 = adj[2 * s];
+    double* row = A + (size_t)i * lda;
+    if (s1 != PVL_INVALID)
+        row[s1] -= c;
+    if (s0 != PVL_INVALID)
+        row[s0] += c;
+}
+
 // new[s, side, row]: row 0 = body node; row i+1 = old[i] + v[i] dt (i < complete); rows
 // beyond complete collapse onto row `complete` (wake_models.py:113-137).
 __global__ void advect_kernel(uint32_t n_shed, uint32_t R, uint32_t complete, const double* __restrict__ old_pos,
@@ -157,6 +176,20 @@ extern "C" int pvl_wake_fold_implicit(uint32_t n_cp, uint32_t n_shed, const doub
     PVL_REQUIRE(implicit); PVL_REQUIRE(adjacent); PVL_REQUIRE(A);
     fold_implicit_kernel<<<blocks_for(n_cp, 128), 128, 0, (cudaStream_t)stream>>>(n_cp, n_shed, implicit, adjacent, A,
                                                                                    lda);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_wake_fold_implicit_distinct(uint32_t n_cp, uint32_t n_shed, const double* implicit,
+                                               const uint32_t* adjacent, double* A, uint32_t lda, void* stream)
+{
+    if (n_cp == 0 || n_shed == 0)
+        return PVL_OK;
+    PVL_REQUIRE(implicit); PVL_REQUIRE(adjacent); PVL_REQUIRE(A);
+    if (lda < n_cp)
+        return pvl_fail(PVL_ERR_ARG, "pvl_wake_fold_implicit_distinct: lda < n_cp");
+    fold_implicit_parallel_kernel<<<blocks_for((uint64_t)n_cp * n_shed, 256), 256, 0, (cudaStream_t)stream>>>(
+        n_cp, n_shed, implicit, adjacent, A, lda);
     PVL_LAUNCH_CHECK();
     return PVL_OK;
 }

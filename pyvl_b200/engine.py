@@ -193,6 +193,10 @@ class SolverEngine:
             raise ValueError("bordering nodes out of range")
         wmesh = Mesh(2 * (R + 1) * S, wake_ring_connectivity(R, S, bn))
         _, cols, slot = wake_node_columns(bn)
+        valid = adj[adj != INVALID_ID]
+        # each ring adjacent to at most one shedding line side: the fold may run in parallel
+        self._fold_fn = ("pvl_wake_fold_implicit_distinct" if np.unique(valid).size == valid.size
+                         else "pvl_wake_fold_implicit")
         # first-row rings (r = 0) as their own CSR over the wake's lines
         row0 = wake_row0_mesh(wmesh, S, R)
         off0, sl0 = row0.surface_offsets, row0.surface_lines
@@ -323,7 +327,7 @@ class SolverEngine:
         _lib.call("pvl_induction_normal", _lib.PVL_F64, wm.n_points, wm.n_lines, ptr(wd["lines"]), ptr(wpos), S,
                   ptr(w["off0"]), ptr(w["sl0"]), self.P, ptr(self.cps), ptr(self.nrm), self.tol, ptr(w["implicit"]),
                   S, ws, nb, s)
-        _lib.call("pvl_wake_fold_implicit", self.P, S, ptr(w["implicit"]), ptr(w["adj"]), ptr(self.A), self.N, s)
+        _lib.call(self._fold_fn, self.P, S, ptr(w["implicit"]), ptr(w["adj"]), ptr(self.A), self.N, s)
         if R > 1:
             _lib.call("pvl_line_circulation", wm.n_lines, ptr(wd["map_offsets"]), ptr(wd["map_entries"]),
                       ptr(self.wake_circulation), R, ptr(w["line_gamma"]), s)
@@ -527,10 +531,11 @@ class MixedSolverEngine(SolverEngine):
         wpos = self.wake_positions.reshape(-1, 3)
         ws, nb = ptr(self.ws), self._ws_bytes
         # implicit: the first S rings of the row-major mesh are row 0 of every strip, in strip order
-        _lib.call("pvl_induction_normal", _lib.PVL_F64, rm.n_points, rm.n_lines, ptr(d["lines"]), ptr(wpos), S,
-                  ptr(d["offsets"]), ptr(d["surface_lines"]), self.P, ptr(self.cps), ptr(self.nrm), self.tol,
+        _lib.call("pvl_induction_normal_tiled", rm.n_points, rm.n_lines, ptr(d["lines"]), ptr(wpos), S,
+                  ptr(d["offsets"]), ptr(d["surface_lines"]), ptr(d["tile_offsets"]), ptr(d["tile_lines"]),
+                  ptr(d["sl_local"]), d["tile_max"], self.P, ptr(self.cps), ptr(self.nrm), self.tol,
                   ptr(w["implicit"]), S, ws, nb, s)
-        _lib.call("pvl_wake_fold_implicit", self.P, S, ptr(w["implicit"]), ptr(w["adj"]), ptr(self.A), self.N, s)
+        _lib.call(self._fold_fn, self.P, S, ptr(w["implicit"]), ptr(w["adj"]), ptr(self.A), self.N, s)
         if R <= 1:
             return
         crs = w["circ_rs"]
