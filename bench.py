@@ -503,7 +503,7 @@ def main() -> None:
             eng = SolverEngine(mesh, case.freestream, case.tol, spec)
             warm = None
         else:
-            eng = MixedSolverEngine(mesh, case.freestream, case.tol, spec, refresh=25)
+            eng = MixedSolverEngine(mesh, case.freestream, case.tol, spec)
             warm = WarmStart(eng, mlp)
         eng.set_wake_state(wpos, wcirc, step_count=case.line_rows + 1, time=t0 - case.dt)
         eng.iteration = 1

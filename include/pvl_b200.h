@@ -288,6 +288,10 @@ int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv, int32_t* i
  * Replaces scipy.linalg.lu_solve (python/pyvl/solver.py:227). */
 int pvl_lu_solve(uint32_t n, const double* LU, uint32_t lda, const int32_t* ipiv, double* b,
                  int32_t* err, void* ws, size_t ws_bytes, void* stream);
+/* The same solve by blocked substitution, one launch per 64-row block step and no waits
+ * between CTAs (usable inside a conditional node of a CUDA graph); slower than the wavefront. */
+int pvl_lu_solve_blocked(uint32_t n, const double* LU, uint32_t lda, const int32_t* ipiv, double* b,
+                         void* ws, size_t ws_bytes, void* stream);
 
 /* Remove the mean of x over each group g: x[off[g]:off[g+1]] -= mean.  Replaces the
  * closed-body constraint of python/pyvl/solver.py:229-233. */
@@ -323,6 +327,47 @@ int pvl_gemv_f64(uint32_t rows, uint32_t cols, double alpha, const double* A, ui
                  const double* x, double beta, double* y, void* stream);
 int pvl_gemv_f32mat(uint32_t rows, uint32_t cols, double alpha, const float* M, uint32_t ldm,
                     const double* x, double beta, double* y, void* stream);
+/* The same with an FP32 vector x (the FP32 copy of a Krylov vector): the four products of each
+ * 16-byte vector are summed in FP32, the row in FP64. */
+int pvl_gemv_f32(uint32_t rows, uint32_t cols, double alpha, const float* M, uint32_t ldm, const float* x,
+                 double beta, double* y, void* stream);
+
+/* ------------------------------------------------------------------ device-driven GMRES graph */
+
+/* Outcome of one solve of the GMRES graph, written by the device. */
+typedef struct pvl_gmres_status {
+    uint32_t iterations;          /* Krylov columns used */
+    uint32_t converged;           /* 1: the true FP64 residual met tol; 0: the FP64 fallback ran */
+    double initial_rel_residual;  /* ||b - A x0|| / ||b|| */
+    double final_rel_residual;    /* ||b - A x|| / ||b|| before any fallback */
+} pvl_gmres_status;
+
+/* Bytes of the device control block (8-byte aligned) and the largest max_iter. */
+size_t pvl_gmres_ctl_bytes(void);
+uint32_t pvl_gmres_max_iter(void);
+
+/* Capture the whole mixed solve as one CUDA graph: r = b - A x (x holds the seed), right-
+ * preconditioned flexible GMRES with the FP32 approximate inverse Minv (ldm) inside a
+ * conditional WHILE node that the device ends (rotated residual <= tol ||b||, exhausted Krylov
+ * space, or max_iter columns), x += Z y, the true residual, the status record, and in a
+ * conditional IF node the FP64 fallback when that residual missed tol (pvl_lu_factor of A
+ * in place and pvl_lu_solve_blocked of b in place, x = b).  Then gamma = x[0..n_gamma) and,
+ * with n_groups, pvl_group_mean_remove.  Buffers (all device, fixed for the graph's life):
+ * V (max_iter + 1) x n, Z max_iter x n, w n doubles, v32 n floats (16-byte aligned), ctl of
+ * pvl_gmres_ctl_bytes(), ipiv 2n, info 1, ws >= pvl_lu_workspace(n).  *graph_out receives an
+ * opaque handle.  No reference counterpart (the reference factorises every step,
+ * python/pyvl/solver.py:223-227). */
+int pvl_gmres_graph_create(uint32_t n, double* A, uint32_t lda, const float* Minv, uint32_t ldm, double* b,
+                           double* x, double* V, double* Z, double* w, float* v32, void* ctl, uint32_t max_iter,
+                           double tol, int32_t* ipiv, int32_t* info, void* ws, size_t ws_bytes, double* gamma,
+                           uint32_t n_gamma, uint32_t n_groups, const uint32_t* group_offsets,
+                           pvl_gmres_status* status, uint64_t* graph_out);
+/* Enqueue one solve on stream; counts the graph's fixed kernels in pvl_launch_count(). */
+int pvl_gmres_graph_launch(uint64_t graph, void* stream);
+/* Add the kernels of `iterations` Krylov columns (and of the fallback) to pvl_launch_count()
+ * once the host has read a solve's status. */
+int pvl_gmres_graph_account(uint64_t graph, uint32_t iterations, uint32_t fell_back);
+int pvl_gmres_graph_destroy(uint64_t graph);
 
 /* One classical Gram-Schmidt pass against the k rows of V (row stride ldv):
  * c = V w; w -= V^T c; h[0..k) += c.  h needs 2k doubles ([k, 2k) is scratch). */

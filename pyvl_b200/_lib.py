@@ -72,6 +72,15 @@ SIGNATURES = {
     "pvl_gemm_tf32": (_I, [_U, _U, _U, ctypes.c_float, _P, _U, _P, _U, ctypes.c_float, _P, _U, _P, _P]),
     "pvl_gemv_f64": (_I, [_U, _U, _D, _P, _U, _P, _D, _P, _P]),
     "pvl_gemv_f32mat": (_I, [_U, _U, _D, _P, _U, _P, _D, _P, _P]),
+    "pvl_gemv_f32": (_I, [_U, _U, _D, _P, _U, _P, _D, _P, _P]),
+    "pvl_lu_solve_blocked": (_I, [_U, _P, _U, _P, _P, _P, _Z, _P]),
+    "pvl_gmres_ctl_bytes": (_Z, []),
+    "pvl_gmres_max_iter": (_U, []),
+    "pvl_gmres_graph_create": (_I, [_U, _P, _U, _P, _U, _P, _P, _P, _P, _P, _P, _P, _U, _D, _P, _P, _P, _Z, _P, _U,
+                                    _U, _P, _P, _P]),
+    "pvl_gmres_graph_launch": (_I, [ctypes.c_uint64, _P]),
+    "pvl_gmres_graph_account": (_I, [ctypes.c_uint64, _U, _U]),
+    "pvl_gmres_graph_destroy": (_I, [ctypes.c_uint64]),
     "pvl_axpy_f64": (_I, [_U, _D, _P, _P, _P]),
     "pvl_basis_project": (_I, [_U, _U, _P, _U, _P, _P, _P]),
     "pvl_normalize": (_I, [_U, _P, _P, _P, _P]),

@@ -4,90 +4,12 @@
 // iteration and keeps the small Hessenberg least-squares problem.
 #include <cstdint>
 
+#include "gemv.cuh"
 #include "pvl_common.cuh"
 
 namespace {
 
 inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
-
-// Vector of 16 bytes of the matrix type and the matching x values.
-template <typename MT> struct Vec16;
-template <> struct Vec16<double> {
-    static constexpr int kN = 2;
-    static __device__ __forceinline__ double dot(const double* __restrict__ m, const double* __restrict__ x)
-    {
-        const double2 a = __ldg(reinterpret_cast<const double2*>(m));
-        const double2 b = *reinterpret_cast<const double2*>(x);
-        return a.x * b.x + a.y * b.y;
-    }
-};
-template <> struct Vec16<float> {
-    static constexpr int kN = 4;
-    static __device__ __forceinline__ double dot(const float* __restrict__ m, const double* __restrict__ x)
-    {
-        const float4 a = __ldg(reinterpret_cast<const float4*>(m));
-        const double2 b0 = *reinterpret_cast<const double2*>(x);
-        const double2 b1 = *reinterpret_cast<const double2*>(x + 2);
-        return (double)a.x * b0.x + (double)a.y * b0.y + (double)a.z * b1.x + (double)a.w * b1.y;
-    }
-};
-
-// Row r of M dotted with x by one warp: 16-byte loads of M (VEC, when rows and x are aligned)
-// four in flight per lane, FP64 accumulation.
-template <typename MT, bool VEC>
-__device__ __forceinline__ double row_dot(const MT* __restrict__ row, const double* __restrict__ x, uint32_t n,
-                                          uint32_t lane)
-{
-    double s = 0.0;
-    uint32_t j0 = 0;
-    if (VEC) {
-        constexpr int V = Vec16<MT>::kN;
-        const uint32_t nv = n / V;
-        uint32_t v = lane;
-        for (; v + 96 < nv; v += 128) {
-            const double a0 = Vec16<MT>::dot(row + (size_t)v * V, x + (size_t)v * V);
-            const double a1 = Vec16<MT>::dot(row + (size_t)(v + 32) * V, x + (size_t)(v + 32) * V);
-            const double a2 = Vec16<MT>::dot(row + (size_t)(v + 64) * V, x + (size_t)(v + 64) * V);
-            const double a3 = Vec16<MT>::dot(row + (size_t)(v + 96) * V, x + (size_t)(v + 96) * V);
-            s += (a0 + a1) + (a2 + a3);
-        }
-        for (; v < nv; v += 32)
-            s += Vec16<MT>::dot(row + (size_t)v * V, x + (size_t)v * V);
-        j0 = nv * V;
-    }
-    for (uint32_t j = j0 + lane; j < n; j += 32)
-        s += (double)row[j] * x[j];
-    for (int o = 16; o > 0; o >>= 1)
-        s += __shfl_xor_sync(0xffffffffu, s, o);
-    return s;
-}
-
-// y = alpha * M x + beta * y, one warp per row (FP64 or FP32 matrix, FP64 vectors/accumulation).
-template <typename MT, bool VEC>
-__global__ void __launch_bounds__(256) gemv_kernel(uint32_t rows, uint32_t cols, double alpha,
-                                                   const MT* __restrict__ M, uint32_t ld,
-                                                   const double* __restrict__ x, double beta,
-                                                   double* __restrict__ y)
-{
-    const uint32_t r = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-    if (r >= rows)
-        return;
-    const double s = row_dot<MT, VEC>(M + (size_t)r * ld, x, cols, lane);
-    if (lane == 0)
-        y[r] = beta == 0.0 ? alpha * s : alpha * s + beta * y[r];
-}
-
-template <typename MT>
-void launch_gemv(uint32_t rows, uint32_t cols, double alpha, const MT* M, uint32_t ld, const double* x, double beta,
-                 double* y, cudaStream_t st)
-{
-    constexpr int V = Vec16<MT>::kN;
-    const bool vec = (ld % V) == 0 && (((uintptr_t)M | (uintptr_t)x) & 15u) == 0;
-    if (vec)
-        gemv_kernel<MT, true><<<blocks_for(rows, 8), 256, 0, st>>>(rows, cols, alpha, M, ld, x, beta, y);
-    else
-        gemv_kernel<MT, false><<<blocks_for(rows, 8), 256, 0, st>>>(rows, cols, alpha, M, ld, x, beta, y);
-}
 
 // c[i] = V_i . w for i < k (one CTA per basis vector).
 __global__ void __launch_bounds__(256) basis_dots_kernel(uint32_t n, const double* __restrict__ V, uint32_t ldv,
@@ -191,7 +113,8 @@ extern "C" int pvl_gemv_f64(uint32_t rows, uint32_t cols, double alpha, const do
     if (rows == 0)
         return PVL_OK;
     PVL_REQUIRE(A); PVL_REQUIRE(x); PVL_REQUIRE(y);
-    launch_gemv<double>(rows, cols, alpha, A, lda, x, beta, y, (cudaStream_t)stream);
+    pvl::launch_gemv<double, double>(rows, cols, alpha, A, lda, x, 0, beta, beta == 0.0 ? nullptr : y, y, 0, nullptr,
+                                     (cudaStream_t)stream);
     PVL_LAUNCH_CHECK();
     return PVL_OK;
 }
@@ -202,7 +125,20 @@ extern "C" int pvl_gemv_f32mat(uint32_t rows, uint32_t cols, double alpha, const
     if (rows == 0)
         return PVL_OK;
     PVL_REQUIRE(M); PVL_REQUIRE(x); PVL_REQUIRE(y);
-    launch_gemv<float>(rows, cols, alpha, M, ldm, x, beta, y, (cudaStream_t)stream);
+    pvl::launch_gemv<float, double>(rows, cols, alpha, M, ldm, x, 0, beta, beta == 0.0 ? nullptr : y, y, 0, nullptr,
+                                    (cudaStream_t)stream);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_gemv_f32(uint32_t rows, uint32_t cols, double alpha, const float* M, uint32_t ldm, const float* x,
+                            double beta, double* y, void* stream)
+{
+    if (rows == 0)
+        return PVL_OK;
+    PVL_REQUIRE(M); PVL_REQUIRE(x); PVL_REQUIRE(y);
+    pvl::launch_gemv<float, float>(rows, cols, alpha, M, ldm, x, 0, beta, beta == 0.0 ? nullptr : y, y, 0, nullptr,
+                                   (cudaStream_t)stream);
     PVL_LAUNCH_CHECK();
     return PVL_OK;
 }

@@ -581,6 +581,48 @@ __global__ void __launch_bounds__(kSolveThreads) trsv_wavefront_kernel(uint32_t 
         st_release(flags + b, 1);
 }
 
+// Blocked substitution with one launch per step and no inter-CTA waits (so that it can sit in a
+// conditional body of a CUDA graph, where the wavefront's co-resident launch is not available):
+// x_b = inv(D_bb) x_b for one diagonal block (one CTA), then the block's column slice updates
+// the rows still to be solved (one warp per row).  Same inverted diagonal blocks as the wavefront.
+template <bool LOWER>
+__global__ void __launch_bounds__(kRB) diag_apply_kernel(uint32_t n, uint32_t b, const double* __restrict__ inv,
+                                                         double* __restrict__ x)
+{
+    __shared__ double s[kRB];
+    const uint32_t r0 = b * kRB, rows = min((uint32_t)kRB, n - r0), t = threadIdx.x;
+    s[t] = t < rows ? x[r0 + t] : 0.0;
+    __syncthreads();
+    if (t < rows) {
+        const double* D = inv + ((size_t)b * 2 + (LOWER ? 0 : 1)) * kRB * kRB + (size_t)t * kRB;
+        double acc = 0.0;
+#pragma unroll 8
+        for (int c = 0; c < kRB; ++c)
+            acc = fma(D[c], s[c], acc);
+        x[r0 + t] = acc;
+    }
+}
+
+template <bool LOWER>
+__global__ void __launch_bounds__(256) block_update_kernel(uint32_t n, uint32_t b, const double* __restrict__ M,
+                                                           uint32_t lda, double* __restrict__ x)
+{
+    const uint32_t c0 = b * kRB, cols = min((uint32_t)kRB, n - c0);
+    const uint32_t first = LOWER ? c0 + cols : 0, count = LOWER ? n - first : c0;
+    const uint32_t i = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (i >= count)
+        return;
+    const uint32_t r = first + i;
+    const double* row = M + (size_t)r * lda + c0;
+    double s = 0.0;
+    for (uint32_t c = lane; c < cols; c += 32)
+        s = fma(row[c], x[c0 + c], s);
+    for (int o = 16; o > 0; o >>= 1)
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0)
+        x[r] -= s;
+}
+
 int coresident_blocks(const void* fn, int threads)
 {
     int dev = 0, sms = 0, per = 0;
@@ -683,6 +725,41 @@ extern "C" int pvl_lu_solve(uint32_t n, const double* LU, uint32_t lda, const in
         const void* fn = pass == 0 ? (const void*)trsv_wavefront_kernel<true> : (const void*)trsv_wavefront_kernel<false>;
         PVL_CUDA_CHECK(cudaLaunchCooperativeKernel(fn, dim3(nblk), dim3(kSolveThreads), args, 0, st));
         pvl_count_launch();
+    }
+    PVL_CUDA_CHECK(cudaMemcpyAsync(b, w.tmp, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    return PVL_OK;
+}
+
+extern "C" int pvl_lu_solve_blocked(uint32_t n, const double* LU, uint32_t lda, const int32_t* ipiv, double* b,
+                                    void* ws, size_t ws_bytes, void* stream)
+{
+    if (n == 0)
+        return PVL_OK;
+    if (!LU || !ipiv || !b || !ws)
+        return pvl_fail(PVL_ERR_ARG, "pvl_lu_solve_blocked: null pointer argument");
+    if (ws_bytes < lu_ws_bytes(n))
+        return pvl_fail(PVL_ERR_ALLOC, "pvl_lu_solve_blocked: workspace too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    LuWs w = carve(ws, n);
+    const uint32_t nblk = (n + kRB - 1) / kRB;
+    gather_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, ipiv + n, b, w.tmp);
+    PVL_LAUNCH_CHECK();
+    for (uint32_t k = 0; k < nblk; ++k) {
+        diag_apply_kernel<true><<<1, kRB, 0, st>>>(n, k, w.inv, w.tmp);
+        PVL_LAUNCH_CHECK();
+        const uint32_t below = n - std::min(n, (k + 1) * kRB);
+        if (below) {
+            block_update_kernel<true><<<blocks_for(below, 8), 256, 0, st>>>(n, k, LU, lda, w.tmp);
+            PVL_LAUNCH_CHECK();
+        }
+    }
+    for (uint32_t k = nblk; k-- > 0;) {
+        diag_apply_kernel<false><<<1, kRB, 0, st>>>(n, k, w.inv, w.tmp);
+        PVL_LAUNCH_CHECK();
+        if (k) {
+            block_update_kernel<false><<<blocks_for(k * kRB, 8), 256, 0, st>>>(n, k, LU, lda, w.tmp);
+            PVL_LAUNCH_CHECK();
+        }
     }
     PVL_CUDA_CHECK(cudaMemcpyAsync(b, w.tmp, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
     return PVL_OK;

@@ -25,6 +25,8 @@ the device (double-buffered) and are copied out only on request.
 
 from __future__ import annotations
 
+import ctypes
+from collections import deque
 from dataclasses import dataclass
 
 import numpy as np
@@ -33,6 +35,11 @@ import torch
 from . import _lib
 from .cvl import INVALID_ID, Mesh
 from .device import ptr, require_cuda, stream_ptr, to_device, to_device_u32
+
+# pvl_gmres_status (include/pvl_b200.h) and the number of solves whose status may be in flight
+_GMRES_STATUS = np.dtype([("iterations", "<u4"), ("converged", "<u4"), ("initial_rel_residual", "<f8"),
+                          ("final_rel_residual", "<f8")])
+_STATUS_RING = 64
 
 
 def wake_ring_connectivity(line_rows: int, n_shed: int, bordering_nodes=None) -> np.ndarray:
@@ -427,12 +434,15 @@ class MixedSolverEngine(SolverEngine):
     * The solve is right-preconditioned GMRES with FP64 vectors and FP64 residuals against the
       FP64 matrix.  The preconditioner is the explicit inverse of an FP32 LU factorisation of
       the system (trailing updates and the triangular inversion's rank-64 updates on the
-      tensor cores in TF32, pvl_lu32_factor / pvl_lu32_inverse), refreshed every ``refresh``
-      steps (earlier when a solve needed ``refresh_on_iters`` iterations; built on a side
-      stream while the steps go on) and applied as one FP32 matrix-vector product per
-      iteration.  If GMRES has not
-      reached ``gmres_tol`` (relative residual) after ``max_iter`` iterations the step falls
-      back to the plain FP64 factorisation.
+      tensor cores in TF32, pvl_lu32_factor / pvl_lu32_inverse), applied as one FP32
+      matrix-vector product per iteration.  It is rebuilt (on a side stream while the steps go
+      on) when it has gone stale: at once when a solve needed ``refresh_on_iters``
+      iterations, or when the iterations above the best count since the last rebuild add up
+      to ``refresh_excess`` (a rebuild costs as much as a few hundred Krylov columns, so a
+      preconditioner that costs one extra column per step is kept for a while), and in any
+      case every ``refresh`` steps when that is set.  If GMRES has not reached ``gmres_tol``
+      (relative residual) after ``max_iter`` iterations the step falls back to the plain FP64
+      factorisation.
     * The explicit wake term runs in FP64 for the wake rows below ``near_rows`` and in FP32
       beyond.  The default keeps every row FP64: the far wake still carries a large share of
       the normal wash (co-located segments of neighbouring strips and the long trailing
@@ -444,11 +454,16 @@ class MixedSolverEngine(SolverEngine):
     """
 
     def __init__(self, mesh: Mesh, freestream, tol: float, wake: WakeSpec | None = None, closed_groups=None,
-                 refresh: int = 25, near_rows: int | None = None, advect_near_rows: int = 8,
+                 refresh: int | None = None, near_rows: int | None = None, advect_near_rows: int = 8,
                  gmres_tol: float = 1e-12, max_iter: int = 20, async_refresh: bool = True,
-                 refresh_on_iters: int = 5, use_graphs: bool = True, wake_self_induction: bool = False):
+                 refresh_on_iters: int = 5, use_graphs: bool = True, wake_self_induction: bool = False,
+                 device_solve: bool = True, refresh_excess: int = 64):
         super().__init__(mesh, freestream, tol, wake, closed_groups, wake_self_induction)
-        self.refresh = int(refresh)
+        self.refresh = None if refresh is None else int(refresh)
+        self.refresh_excess = int(refresh_excess)
+        self._iters_seen = 0      # solves the refresh policy has looked at
+        self._iters_best = None   # fewest iterations of a solve since the last rebuild
+        self._iters_excess = 0    # iterations above that since the last rebuild
         self.gmres_tol = float(gmres_tol)
         self.max_iter = int(max_iter)
         n = self.N
@@ -485,8 +500,20 @@ class MixedSolverEngine(SolverEngine):
         self.b_saved = torch.zeros(n, **f64)
         self.have_precond = False
         self.steps_since_refresh = 0
-        self.stats = {"gmres_iters": [], "fallbacks": 0, "refreshes": 0, "initial_rel_residual": [],
-                      "final_rel_residual": [], "judge": []}
+        self._stats = {"gmres_iters": [], "fallbacks": 0, "refreshes": 0, "initial_rel_residual": [],
+                       "final_rel_residual": [], "judge": []}
+        # device-driven solve (pvl_gmres_graph_*): buffers captured by the graph, status ring
+        self.device_solve = bool(device_solve)
+        if self.device_solve and self.max_iter > int(_lib.query("pvl_gmres_max_iter")):
+            raise ValueError(f"max_iter {self.max_iter} > {int(_lib.query('pvl_gmres_max_iter'))} of the device solve")
+        self.v32 = torch.zeros(n, dtype=torch.float32, device=self.dev)
+        self.ctl = torch.zeros(int(_lib.query("pvl_gmres_ctl_bytes")), dtype=torch.uint8, device=self.dev)
+        self.status_dev = torch.zeros(_GMRES_STATUS.itemsize, dtype=torch.uint8, device=self.dev)
+        self._status_ring = torch.zeros((_STATUS_RING, _GMRES_STATUS.itemsize), dtype=torch.uint8, pin_memory=True)
+        self._pending: deque = deque()
+        self._next_slot = 0
+        self._graph = 0
+        self._graph_key = None
         need = 0
         if self.wake is not None:
             need = max(need, self._init_row_major_wake(near_rows, advect_near_rows))
@@ -588,7 +615,9 @@ class MixedSolverEngine(SolverEngine):
                 self.refresh_done.record()
         self.have_precond = True
         self.steps_since_refresh = 0
-        self.stats["refreshes"] += 1
+        self._iters_best = None
+        self._iters_excess = 0
+        self._stats["refreshes"] += 1
 
     def _adopt_refresh(self) -> None:
         """Switch to the side stream's new inverse once it is complete (no host wait).  It is
@@ -657,14 +686,7 @@ class MixedSolverEngine(SolverEngine):
         previous solve needed and then column by column, applies the Givens rotations and forms
         the update.  The true FP64 residual b - A x decides convergence."""
         n = self.N
-        self._adopt_refresh()
-        if not self.have_precond:
-            self.refresh_preconditioner(wait=True)
-        elif self.steps_since_refresh >= self.refresh or (
-                self.refresh_done is None and self.stats["gmres_iters"]
-                and self.stats["gmres_iters"][-1] >= self.refresh_on_iters and self.steps_since_refresh >= 2):
-            self.refresh_preconditioner(wait=not self.async_refresh)
-        self.steps_since_refresh += 1
+        self._maybe_refresh()
         x = self.x
         if x0 is not None:
             x.copy_(x0.reshape(-1)[:n])
@@ -688,7 +710,7 @@ class MixedSolverEngine(SolverEngine):
             torch.cuda.current_stream().synchronize()
             if first:
                 bnorm, beta = float(self.h_sc[0]), float(self.h_sc[1])
-                self.stats["initial_rel_residual"].append(beta / max(bnorm, 1e-300))
+                self._stats["initial_rel_residual"].append(beta / max(bnorm, 1e-300))
                 target = self.gmres_tol * bnorm
                 g[0] = beta
                 first = False
@@ -723,18 +745,116 @@ class MixedSolverEngine(SolverEngine):
         # the true FP64 residual decides
         self._replay(("finish", k), lambda: self._gmres_finish(k))
         rel = float(sc[0].item()) / max(bnorm, 1e-300)
-        self.stats["gmres_iters"].append(k)
-        self.stats["final_rel_residual"].append(rel)
+        self._stats["gmres_iters"].append(k)
+        self._stats["final_rel_residual"].append(rel)
         return rel <= self.gmres_tol
 
+    def _maybe_refresh(self) -> None:
+        """Adopt a finished refresh; start a new one when the preconditioner has gone stale
+        (the policy of the class docstring)."""
+        self._adopt_refresh()
+        its = self._stats["gmres_iters"]
+        for k in its[self._iters_seen:]:
+            self._iters_best = k if self._iters_best is None else min(self._iters_best, k)
+            self._iters_excess += k - self._iters_best
+        self._iters_seen = len(its)
+        idle = self.refresh_done is None
+        if not self.have_precond:
+            self.refresh_preconditioner(wait=True)
+        elif (self.refresh is not None and self.steps_since_refresh >= self.refresh) or (
+                idle and self.steps_since_refresh >= 2
+                and (its[-1] >= self.refresh_on_iters or self._iters_excess >= self.refresh_excess)):
+            self.refresh_preconditioner(wait=not self.async_refresh)
+        self.steps_since_refresh += 1
+
+    # ------------------------------------------------------------------ device-driven solve
+    def _ensure_graph(self) -> None:
+        key = (int(self.ws.data_ptr()), self._ws_bytes)
+        if self._graph and self._graph_key == key:
+            return
+        self._destroy_graph()
+        n = self.N
+        h = ctypes.c_uint64(0)
+        _lib.call("pvl_gmres_graph_create", n, ptr(self.A), n, ptr(self.Xinv), self.npad, ptr(self.rhs), ptr(self.x),
+                  ptr(self.V), ptr(self.Z), ptr(self.wv), ptr(self.v32), ptr(self.ctl), self.max_iter,
+                  self.gmres_tol, ptr(self.ipiv), ptr(self.info), ptr(self.ws), self._ws_bytes, ptr(self.gamma),
+                  self.P, self.m, ptr(self.goff) if self.m else None, ptr(self.status_dev), ctypes.byref(h))
+        self._graph = int(h.value)
+        self._graph_key = key
+
+    def _destroy_graph(self) -> None:
+        if self._graph:
+            self._collect_status(block=True)
+            _lib.call("pvl_gmres_graph_destroy", self._graph)
+            self._graph = 0
+
+    def __del__(self):
+        try:
+            self._destroy_graph()
+        except Exception:
+            pass
+
+    def _collect_status(self, block: bool) -> None:
+        """Move the status records of finished device solves into the statistics."""
+        while self._pending:
+            slot, ev = self._pending[0]
+            if block:
+                ev.synchronize()
+            elif not ev.query():
+                break
+            self._pending.popleft()
+            rec = np.frombuffer(self._status_ring[slot].numpy().tobytes(), dtype=_GMRES_STATUS)[0]
+            it, ok = int(rec["iterations"]), bool(rec["converged"])
+            st = self._stats
+            st["gmres_iters"].append(it)
+            st["initial_rel_residual"].append(float(rec["initial_rel_residual"]))
+            st["final_rel_residual"].append(float(rec["final_rel_residual"]))
+            if not ok:
+                st["fallbacks"] += 1
+            _lib.call("pvl_gmres_graph_account", self._graph, it, 0 if ok else 1)
+
+    @property
+    def stats(self) -> dict:
+        """Solve statistics (waits for the device solves still in flight)."""
+        self._collect_status(block=True)
+        return self._stats
+
+    def _solve_device(self, x0: torch.Tensor | None) -> None:
+        """The whole solve as one graph launch (pvl_gmres_graph_create): GMRES driven by the
+        device to convergence, the FP64 fallback inside the graph; no host synchronisation.
+        The status of each solve is read back later (``stats``); the host waits here for the
+        previous solve's record (long done while the GPU works through the wake update and this
+        step's assembly), so that the refresh policy sees every iteration count in time."""
+        self._collect_status(block=True)
+        self._maybe_refresh()
+        if x0 is not None:
+            self.x.copy_(x0.reshape(-1)[: self.N])
+        else:
+            self.x[: self.P].copy_(self.gamma)  # the previous step's circulation
+        self._ensure_graph()
+        while len(self._pending) >= _STATUS_RING:
+            slot, ev = self._pending[0]
+            ev.synchronize()
+            self._collect_status(block=False)
+        _lib.call("pvl_gmres_graph_launch", self._graph, stream_ptr())
+        slot = self._next_slot
+        self._next_slot = (slot + 1) % _STATUS_RING
+        self._status_ring[slot].copy_(self.status_dev, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record()
+        self._pending.append((slot, ev))
+
     def solve(self, x0: torch.Tensor | None = None) -> None:
+        if self.device_solve:
+            self._solve_device(x0)
+            return
         self.b_saved.copy_(self.rhs)
         if self.solve_mixed(x0):
             self.gamma.copy_(self.x[: self.P])
             if self.m:
                 _lib.call("pvl_group_mean_remove", self.m, ptr(self.goff), ptr(self.gamma), stream_ptr())
             return
-        self.stats["fallbacks"] += 1
+        self._stats["fallbacks"] += 1
         self.rhs.copy_(self.b_saved)
         super().solve()
 
@@ -774,7 +894,7 @@ class MixedSolverEngine(SolverEngine):
         ref = self.gamma.clone()
         self.gamma.copy_(mixed)
         err = float((torch.linalg.vector_norm(mixed - ref) / torch.linalg.vector_norm(ref)).item())
-        self.stats["judge"].append(err)
+        self._stats["judge"].append(err)
         return err
 
     def step_judged(self, time: float, positions, velocities, x0: torch.Tensor | None = None) -> float:

@@ -236,8 +236,8 @@ def test_gmres_graph_replay_is_bitwise_identical():
     from pyvl_b200.workloads import flapping
 
     case = flapping(ns=32, nc=8, line_rows=12)
-    a = _mixed_engine(case, refresh=5, use_graphs=False)
-    b = _mixed_engine(case, refresh=5, use_graphs=True)
+    a = _mixed_engine(case, refresh=5, use_graphs=False, device_solve=False)
+    b = _mixed_engine(case, refresh=5, use_graphs=True, device_solve=False)
     for k in range(14):
         t = k * case.dt
         p, v = case.positions_at(t), case.velocities_at(t)
@@ -245,3 +245,57 @@ def test_gmres_graph_replay_is_bitwise_identical():
         b.step(t, p, v)
         assert np.array_equal(a.gamma_host(), b.gamma_host()), k
     assert len(b.graphs) > 2
+
+
+def test_device_solve_against_host_driven_gmres():
+    """The solve driven by the device (one graph launch, conditional WHILE over the Krylov
+    columns) and the host-driven GMRES reach the same circulations; both judged against FP64."""
+    from pyvl_b200.workloads import flapping
+
+    case = flapping(ns=64, nc=16, line_rows=30)
+    dev = _mixed_engine(case, refresh=10)
+    host = _mixed_engine(case, refresh=10, device_solve=False)
+    assert dev.device_solve and not host.device_solve
+    worst = 0.0
+    for k in range(30):
+        t = k * case.dt
+        p, v = case.positions_at(t), case.velocities_at(t)
+        if k % 10 == 9:
+            assert dev.step_judged(t, p, v) <= MIXED_TOL
+            assert host.step_judged(t, p, v) <= MIXED_TOL
+        else:
+            dev.step(t, p, v)
+            host.step(t, p, v)
+        a, b = dev.gamma_host(), host.gamma_host()
+        worst = max(worst, float(np.linalg.norm(a - b) / np.linalg.norm(b)))
+    sd, sh = dev.stats, host.stats
+    print("device iterations", sd["gmres_iters"], "host iterations", sh["gmres_iters"], "worst", worst)
+    assert worst <= 1e-9, worst
+    assert sd["fallbacks"] == 0 and len(sd["gmres_iters"]) == 30
+    assert max(sd["final_rel_residual"]) <= 1e-12
+    assert abs(sum(sd["gmres_iters"]) - sum(sh["gmres_iters"])) <= 6
+
+
+def test_device_solve_fallback_runs_fp64_lu():
+    """With a tolerance GMRES cannot meet in one column, every solve takes the FP64 fallback
+    inside the graph (conditional IF: LU factorisation + blocked substitution): the
+    circulations are the plain FP64 engine's."""
+    from pyvl_b200.cvl import Mesh
+    from pyvl_b200.engine import SolverEngine, wake_spec_from_te
+    from pyvl_b200.workloads import flapping
+
+    case = flapping(ns=32, nc=8, line_rows=10)
+    mesh = Mesh(case.n_points, case.elements)
+    plain = SolverEngine(mesh, case.freestream, case.tol,
+                         wake_spec_from_te(mesh, case.te_node_pairs, case.line_rows, case.t0))
+    mixed = _mixed_engine(case, max_iter=1, gmres_tol=1e-300, refresh=5)
+    for k in range(8):
+        t = k * case.dt
+        p, v = case.positions_at(t), case.velocities_at(t)
+        plain.step(t, p, v)
+        mixed.step(t, p, v)
+        a, b = mixed.gamma_host(), plain.gamma_host()
+        assert float(np.linalg.norm(a - b) / np.linalg.norm(b)) <= 1e-11, k
+    st = mixed.stats
+    assert st["fallbacks"] == 8 and st["gmres_iters"] == [1] * 8
+    mixed.check_status()
