@@ -153,12 +153,6 @@ int pvl_induction_normal_tiled(uint32_t n_points, uint32_t n_lines, const uint32
                                uint32_t max_tile_lines, uint32_t n_cp, const double* cps, const double* normals,
                                double tol, double* out, uint32_t ld, void* ws, size_t ws_bytes, void* stream);
 
-/* Points per thread (1, 2 or 4; default 1) of the segment sweeps behind pvl_line_velocity,
- * pvl_wake_node_velocity(_cols) and the no-alloc entry, process-wide; returns the previous
- * value (or a negative status).  A tile-shape knob for autotuning; results do not depend on it.
- * No reference counterpart. */
-int pvl_set_sweep_points_per_thread(int ppt);
-
 size_t pvl_line_velocity_workspace(uint32_t n_lines, uint32_t n_pts, int precision);
 
 /* Velocity induced at points by segments carrying circulations:

@@ -48,7 +48,6 @@ SIGNATURES = {
     "pvl_induction_normal_tiled": (_I, [_U, _U, _P, _P, _U, _P, _P, _P, _P, _P, _U, _U, _P, _P, _D, _P, _U, _P, _Z,
                                         _P]),
     "pvl_induction_normal": (_I, [_I, _U, _U, _P, _P, _U, _P, _P, _U, _P, _P, _D, _P, _U, _P, _Z, _P]),
-    "pvl_set_sweep_points_per_thread": (_I, [_I]),
     "pvl_line_velocity_workspace": (_Z, [_U, _U, _I]),
     "pvl_line_velocity": (_I, [_I, _U, _U, _P, _P, _P, _U, _P, _P, _D, _D, _D, _P, _P, _Z, _P]),
     "pvl_line_circulation": (_I, [_U, _P, _P, _P, _U, _P, _P]),

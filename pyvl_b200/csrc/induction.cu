@@ -21,8 +21,6 @@ namespace {
 
 constexpr int kSegTile = 128;   // segments per shared-memory tile
 constexpr int kSumThreads = 128;
-constexpr int kSumPPT = 2;      // nominal points per thread of the N-body sweep (sizes its range split)
-int g_sum_ppt = 1;              // points per thread the sweep runs with (measured best; pvl_set_sweep_points_per_thread)
 constexpr int kRingThreads = 128;
 constexpr int kRingCPB = 8;     // control points per CTA row-block in ring matrices
 
@@ -207,64 +205,149 @@ __global__ void __launch_bounds__(kRingThreads) line_matrix_kernel(uint32_t n_li
     }
 }
 
-// N-body sweep: partial[(split*n_pts + p)*3 + c] = sum over this split's segments of gamma_k u_k(p).
-// Point p of the sweep is pts[col(p / group) * stride + p % group + in_off] with col(c) =
+// Point p of a sweep is pts[col(p / group) * stride + p % group + in_off] with col(c) =
 // cols ? cols[c] : c: group == stride == n_pts is a plain array; group = a range of wake
 // rows, stride = rows + 1, in_off = first row walks those rows of the listed wake node
-// columns (strip side s * 2 + side).
-template <typename T, int PPT>
-__global__ void __launch_bounds__(kSumThreads) line_sum_kernel(const Segment<T>* __restrict__ seg, uint32_t n_lines,
-                                                               uint32_t lines_per_split,
-                                                               const double* __restrict__ pts, uint32_t n_pts,
-                                                               uint32_t group, uint32_t stride, uint32_t in_off,
-                                                               const uint32_t* __restrict__ cols, uint32_t col_limit,
-                                                               T tol2, T* __restrict__ partial)
+// columns (strip side s * 2 + side).  A listed column at or past col_limit is no point.
+__device__ __forceinline__ bool sweep_point(uint32_t p, uint32_t n_pts, uint32_t group, uint32_t stride,
+                                            uint32_t in_off, const uint32_t* __restrict__ cols, uint32_t col_limit,
+                                            size_t& q)
 {
-    __shared__ Segment<T> s_seg[kSegTile];
+    bool ok = p < n_pts;
+    uint32_t col = ok ? (cols ? cols[p / group] : p / group) : 0;
+    if (col >= col_limit)
+        ok = false;
+    q = ok ? (size_t)col * stride + p % group + in_off : 0;
+    return ok;
+}
+
+// A segment of the FP64 sweep in Pluecker form about the CTA's origin o:
+// d (unit direction), m = (r1 - o) x d, e = d . (r1 - o), len, len^2, gamma, gamma len.
+struct __align__(16) SweepSeg {
+    double dx, dy, dz, mx, my, mz, e, len, len2, glen, gamma, pad;
+};
+
+struct SweepGeo {
+    double cx, cy, cz, hsq, x, r, w;
+};
+
+// For a point p' = p - o: t1 = d . p' - e = d . (p - r1) and c = p' x d - m = (p - r1) x d,
+// the quantities of segment_induction (pvl_common.cuh) from 9 FMAs instead of 3 differences
+// and 9 products; rounding is relative to |p - o| + |r1 - o| instead of |p - r1|, and o is the
+// centroid of the CTA's points, which are neighbours (ring or wake-node order).
+__device__ __forceinline__ SweepGeo sweep_geo(const SweepSeg& s, double px, double py, double pz)
+{
+    SweepGeo g;
+    const double t1 = fma(s.dz, pz, fma(s.dy, py, fma(s.dx, px, -s.e)));
+    g.cx = fma(py, s.dz, -fma(pz, s.dy, s.mx));
+    g.cy = fma(pz, s.dx, -fma(px, s.dz, s.my));
+    g.cz = fma(px, s.dy, -fma(py, s.dx, s.mz));
+    g.hsq = g.cx * g.cx + g.cy * g.cy + g.cz * g.cz;
+    g.x = g.hsq + t1 * (t1 - s.len);
+    g.r = pvl::FarSeries<double>::rcp(g.x);
+    g.w = g.hsq * s.len2 * (g.r * g.r);
+    return g;
+}
+
+// The rest of segment_induction<double, true>: far pairs by the arctangent series (selected,
+// no branch), the rare near pairs by atan2 in a branch, pairs inside the cut-off skipped.
+__device__ __forceinline__ void sweep_add(const SweepSeg& s, const SweepGeo& g, double tol2, Vec3<double>& acc)
+{
+    const bool ok = !pvl::lt_nn(g.hsq, tol2);
+    const bool far = ok && pvl::pos(g.x) && pvl::le_nn(g.w, pvl::FarSeries<double>::kW);
+    double mag = far ? -s.glen * g.r * pvl::FarSeries<double>::sum(g.w) : 0.0;
+    if (ok && !far) {
+        const double rh = rsqrt(g.hsq);
+        const double h = g.hsq * rh;
+        mag = s.gamma * atan2(-h * s.len, g.x) * rh;
+    }
+    acc.x += g.cx * mag;
+    acc.y += g.cy * mag;
+    acc.z += g.cz * mag;
+}
+
+// FP64 N-body sweep: partial[(split*n_pts + p)*3 + c] = sum over this split's segments of
+// gamma_k u_k(p).  One point per thread; segments stream through shared memory in tiles of
+// kSegTile, converted to the Pluecker form about the CTA's origin as they are staged, and
+// are evaluated two at a time (two independent dependency chains per thread).
+__global__ void __launch_bounds__(kSumThreads, 8) line_sum_f64_kernel(
+    const Segment<double>* __restrict__ seg, uint32_t n_lines, uint32_t lines_per_split,
+    const double* __restrict__ pts, uint32_t n_pts, uint32_t group, uint32_t stride, uint32_t in_off,
+    const uint32_t* __restrict__ cols, uint32_t col_limit, double tol2, double* __restrict__ partial)
+{
+    __shared__ SweepSeg s_seg[kSegTile + 1];
+    __shared__ double s_red[kSumThreads / 32][4];
+    __shared__ double s_o[3];
     const uint32_t split = blockIdx.y;
     const uint32_t l_begin = split * lines_per_split;
     const uint32_t l_end = min(n_lines, l_begin + lines_per_split);
-    T px[PPT], py[PPT], pz[PPT];
-    Vec3<T> acc[PPT];
+    const uint32_t p = blockIdx.x * kSumThreads + threadIdx.x;
+    size_t q;
+    const bool ok = sweep_point(p, n_pts, group, stride, in_off, cols, col_limit, q);
+    double px = ok ? pts[3 * q] : 0.0, py = ok ? pts[3 * q + 1] : 0.0, pz = ok ? pts[3 * q + 2] : 0.0;
+    {  // origin: centroid of the CTA's points
+        double v[4] = {px, py, pz, ok ? 1.0 : 0.0};
 #pragma unroll
-    for (int t = 0; t < PPT; ++t) {
-        const uint32_t p = blockIdx.x * (kSumThreads * PPT) + t * kSumThreads + threadIdx.x;
-        bool ok = p < n_pts;
-        uint32_t col = ok ? (cols ? cols[p / group] : p / group) : 0;
-        if (col >= col_limit) {  // a listed column outside the point array: skip the point
-            ok = false;
-            col = 0;
+        for (int c = 0; c < 4; ++c)
+            for (int o = 16; o > 0; o >>= 1)
+                v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+        if ((threadIdx.x & 31) == 0)
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                s_red[threadIdx.x >> 5][c] = v[c];
+        __syncthreads();
+        if (threadIdx.x < 3) {
+            double t = 0.0, n = 0.0;
+            for (int w = 0; w < kSumThreads / 32; ++w) {
+                t += s_red[w][threadIdx.x];
+                n += s_red[w][3];
+            }
+            s_o[threadIdx.x] = n > 0.0 ? t / n : 0.0;
         }
-        const size_t q = ok ? (size_t)col * stride + p % group + in_off : 0;
-        px[t] = ok ? T(pts[3 * q]) : T(0);
-        py[t] = ok ? T(pts[3 * q + 1]) : T(0);
-        pz[t] = ok ? T(pts[3 * q + 2]) : T(0);
-        acc[t] = Vec3<T>{T(0), T(0), T(0)};
+        __syncthreads();
     }
+    px -= s_o[0];
+    py -= s_o[1];
+    pz -= s_o[2];
+    Vec3<double> acc{0.0, 0.0, 0.0};
+    if (threadIdx.x == 0)
+        s_seg[kSegTile] = SweepSeg{};  // the partner of an odd last segment: d = 0, nothing induced
     for (uint32_t l0 = l_begin; l0 < l_end; l0 += kSegTile) {
         const uint32_t l = l0 + threadIdx.x;
-        if (threadIdx.x < kSegTile && l < l_end)
-            s_seg[threadIdx.x] = seg[l];
+        SweepSeg t{};
+        if (threadIdx.x < kSegTile && l < l_end) {
+            const Segment<double> g = seg[l];
+            const double rx = g.r1x - s_o[0], ry = g.r1y - s_o[1], rz = g.r1z - s_o[2];
+            t.dx = g.dx;
+            t.dy = g.dy;
+            t.dz = g.dz;
+            t.mx = ry * g.dz - rz * g.dy;
+            t.my = rz * g.dx - rx * g.dz;
+            t.mz = rx * g.dy - ry * g.dx;
+            t.e = g.dx * rx + g.dy * ry + g.dz * rz;
+            t.len = g.len;
+            t.len2 = g.len2;
+            t.glen = g.glen;
+            t.gamma = g.gamma;
+        }
+        if (threadIdx.x < kSegTile)
+            s_seg[threadIdx.x] = t;
         __syncthreads();
         const int cnt = (int)min((uint32_t)kSegTile, l_end - l0);
 #pragma unroll 1
-        for (int k = 0; k < cnt; ++k) {
-            const Segment<T> s = s_seg[k];
-#pragma unroll
-            for (int t = 0; t < PPT; ++t)
-                pvl::segment_induction<T, true>(s, px[t], py[t], pz[t], tol2, s.gamma, acc[t]);
+        for (int k = 0; k < cnt; k += 2) {
+            const SweepSeg a = s_seg[k], b = s_seg[k + 1];
+            const SweepGeo ga = sweep_geo(a, px, py, pz), gb = sweep_geo(b, px, py, pz);
+            sweep_add(a, ga, tol2, acc);
+            sweep_add(b, gb, tol2, acc);
         }
         __syncthreads();
     }
-#pragma unroll
-    for (int t = 0; t < PPT; ++t) {
-        const uint32_t p = blockIdx.x * (kSumThreads * PPT) + t * kSumThreads + threadIdx.x;
-        if (p < n_pts) {
-            T* o = partial + 3 * ((size_t)split * n_pts + p);
-            o[0] = acc[t].x;
-            o[1] = acc[t].y;
-            o[2] = acc[t].z;
-        }
+    if (p < n_pts) {
+        double* o = partial + 3 * ((size_t)split * n_pts + p);
+        o[0] = acc.x;
+        o[1] = acc.y;
+        o[2] = acc.z;
     }
 }
 
@@ -295,13 +378,8 @@ __global__ void __launch_bounds__(kSumThreads) line_sum_f32x2_kernel(const Segme
     for (int t = 0; t < 2; ++t) {
         const uint32_t p = blockIdx.x * (kSumThreads * 2) + t * kSumThreads + threadIdx.x;
         pid[t] = p;
-        bool ok = p < n_pts;
-        uint32_t col = ok ? (cols ? cols[p / group] : p / group) : 0;
-        if (col >= col_limit) {
-            ok = false;
-            col = 0;
-        }
-        const size_t q = ok ? (size_t)col * stride + p % group + in_off : 0;
+        size_t q;
+        const bool ok = sweep_point(p, n_pts, group, stride, in_off, cols, col_limit, q);
         pv[t][0] = ok ? float(pts[3 * q]) : 0.0f;
         pv[t][1] = ok ? float(pts[3 * q + 1]) : 0.0f;
         pv[t][2] = ok ? float(pts[3 * q + 2]) : 0.0f;
@@ -555,12 +633,16 @@ int prep_segments(uint32_t n_points, uint32_t n_lines, const uint32_t* lines, co
     return PVL_OK;
 }
 
-// Number of segment ranges the N-body sweep is split into: enough CTAs to fill the
-// 148 SMs several times over, at least two tiles of segments per range.
-uint32_t sum_splits(uint32_t n_lines, uint32_t n_pts)
+// Points per CTA of the sweeps: one per thread in FP64, two per thread (FP32x2) in FP32.
+inline uint32_t sweep_points_per_cta(int precision) { return precision == PVL_F32 ? 2 * kSumThreads : kSumThreads; }
+
+// Number of segment ranges a sweep is split into: enough CTAs to fill the 148 SMs many times
+// over (FP64: 32 per SM, so that the last of the ~4 resident waves is short; FP32x2: 8 per SM),
+// at least two tiles of segments per range.
+uint32_t sum_splits(uint32_t n_lines, uint32_t n_pts, int precision)
 {
-    const uint64_t ctas_x = (n_pts + kSumThreads * kSumPPT - 1) / (kSumThreads * kSumPPT);
-    const uint64_t want = 148ull * 8;
+    const uint64_t ctas_x = (n_pts + sweep_points_per_cta(precision) - 1) / sweep_points_per_cta(precision);
+    const uint64_t want = 148ull * (precision == PVL_F32 ? 8 : 32);
     uint64_t s = (want + ctas_x - 1) / std::max<uint64_t>(ctas_x, 1);
     const uint64_t max_s = std::max<uint64_t>(1, (n_lines + 2 * kSegTile - 1) / (2 * kSegTile));
     s = std::min(std::max<uint64_t>(s, 1), max_s);
@@ -764,7 +846,8 @@ extern "C" int pvl_induction_normal_tiled(uint32_t n_points, uint32_t n_lines, c
 extern "C" size_t pvl_line_velocity_workspace(uint32_t n_lines, uint32_t n_pts, int precision)
 {
     const size_t el = precision == PVL_F32 ? sizeof(float) : sizeof(double);
-    return pvl_segments_workspace(n_lines, precision) + align256((size_t)sum_splits(n_lines, n_pts) * n_pts * 3 * el);
+    return pvl_segments_workspace(n_lines, precision) +
+           align256((size_t)sum_splits(n_lines, n_pts, precision) * n_pts * 3 * el);
 }
 
 namespace {
@@ -791,31 +874,18 @@ int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint3
     if (ws_bytes < pvl_line_velocity_workspace(n_lines, n_pts, precision))
         return pvl_fail(PVL_ERR_ALLOC, "%s: workspace %zu < %zu", who, ws_bytes,
                         pvl_line_velocity_workspace(n_lines, n_pts, precision));
-    const uint32_t n_split = sum_splits(n_lines, n_pts);
+    const uint32_t n_split = sum_splits(n_lines, n_pts, precision);
     const uint32_t per = (n_lines + n_split - 1) / n_split;
     const uint32_t n_split_used = (n_lines + per - 1) / per;
-    const int ppt = g_sum_ppt;
-    dim3 grid(blocks_for(n_pts, kSumThreads * ppt), n_split_used);
-    dim3 grid_x2(blocks_for(n_pts, kSumThreads * 2), n_split_used);
+    dim3 grid(blocks_for(n_pts, sweep_points_per_cta(precision)), n_split_used);
     char* base = static_cast<char*>(ws);
-    auto sweep = [&](auto tag, const auto* seg, auto* part, auto tol2) -> void {
-        using T = decltype(tag);
-        if (ppt == 1)
-            line_sum_kernel<T, 1><<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off,
-                                                                 cols, col_limit, tol2, part);
-        else if (ppt == 4)
-            line_sum_kernel<T, 4><<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off,
-                                                                 cols, col_limit, tol2, part);
-        else
-            line_sum_kernel<T, 2><<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off,
-                                                                 cols, col_limit, tol2, part);
-    };
     if (precision == PVL_F64) {
         auto* seg = reinterpret_cast<Segment<double>*>(base);
         auto* part = reinterpret_cast<double*>(base + pvl_segments_workspace(n_lines, PVL_F64));
         if (int r = prep_segments<double>(n_points, n_lines, lines, positions, line_gamma, tol, seg, st))
             return r;
-        sweep(double(0), seg, part, pvl::cutoff2<double>(tol));
+        line_sum_f64_kernel<<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off, cols,
+                                                          col_limit, pvl::cutoff2<double>(tol), part);
         PVL_LAUNCH_CHECK();
         reduce_partials_kernel<double><<<blocks_for(n_pts, 256), 256, 0, st>>>(
             n_pts, n_split_used, part, normals, alpha, beta, ux, uy, uz, group, out_stride, out_off, out);
@@ -824,7 +894,7 @@ int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint3
         auto* part = reinterpret_cast<float*>(base + pvl_segments_workspace(n_lines, PVL_F32));
         if (int r = prep_segments<float>(n_points, n_lines, lines, positions, line_gamma, tol, seg, st))
             return r;
-        line_sum_f32x2_kernel<<<grid_x2, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off,
+        line_sum_f32x2_kernel<<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off,
                                                                cols, col_limit, pvl::cutoff2<float>(tol), part);
         PVL_LAUNCH_CHECK();
         reduce_partials_kernel<float><<<blocks_for(n_pts, 256), 256, 0, st>>>(
@@ -835,15 +905,6 @@ int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint3
 }
 
 }  // namespace
-
-extern "C" int pvl_set_sweep_points_per_thread(int ppt)
-{
-    if (ppt != 1 && ppt != 2 && ppt != 4)
-        return pvl_fail(PVL_ERR_ARG, "pvl_set_sweep_points_per_thread: 1, 2 or 4 (got %d)", ppt);
-    const int old = g_sum_ppt;
-    g_sum_ppt = ppt;
-    return old;
-}
 
 extern "C" int pvl_line_velocity(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
                                  const double* positions, const double* line_gamma, uint32_t n_pts, const double* pts,
