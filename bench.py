@@ -533,6 +533,7 @@ def main() -> None:
         n0 = len(getattr(eng, "stats", {}).get("gmres_iters", []))
         launches0 = _lib.lib().pvl_launch_count()
         ms = timed(eng, warm, W, K, host=False)
+        getattr(eng, "stats", None)  # the mixed engine counts its solves' Krylov columns as their status arrives
         launches = _lib.lib().pvl_launch_count() - launches0
         ms_e2e = timed(eng, warm, W + K, K, host=True)
         eng.check_status()
@@ -595,7 +596,7 @@ def main() -> None:
     peak = flops / (p0.elapsed_time(p1) * 1e-3) / 1e12
     del eng
     traffic = None
-    prof = ROOT / "profiles" / "line_sum_flapping_wake_term.md"
+    prof = ROOT / "profiles" / "line_sum_f64_flapping_wake_term.md"
     if prof.exists():
         for line in prof.read_text().splitlines():
             if line.startswith("traffic_bytes_per_launch:"):
@@ -637,7 +638,7 @@ def main() -> None:
                          "how": "after the timed steps, each judged step's mixed circulation vs the same state "
                                 "assembled in FP64 and solved by FP64 LU"},
             "e2e": {"value": sps_e2e, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "roofline": {"bound": "fp64", "kernel": "line_sum_kernel<double> (explicit wake term)",
+            "roofline": {"bound": "fp64", "kernel": "line_sum_f64_kernel (explicit wake term)",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "traffic": traffic, "ms_per_launch": kms, "pairs_per_launch": pairs,
                          "peak_source": "FP64 FMA throughput measured live (pvl_fma_probe); 45 FLOP per pair"},
