@@ -13,8 +13,10 @@
 #include <cstdint>
 
 #include "pvl_common.cuh"
+#include "sweep.cuh"
 
 using pvl::Segment;
+using pvl::SweepSeg;
 using pvl::Vec3;
 
 namespace {
@@ -221,51 +223,6 @@ __device__ __forceinline__ bool sweep_point(uint32_t p, uint32_t n_pts, uint32_t
     return ok;
 }
 
-// A segment of the FP64 sweep in Pluecker form about the CTA's origin o:
-// d (unit direction), m = (r1 - o) x d, e = d . (r1 - o), len, len^2, gamma, gamma len.
-struct __align__(16) SweepSeg {
-    double dx, dy, dz, mx, my, mz, e, len, len2, glen, gamma, pad;
-};
-
-struct SweepGeo {
-    double cx, cy, cz, hsq, x, r, w;
-};
-
-// For a point p' = p - o: t1 = d . p' - e = d . (p - r1) and c = p' x d - m = (p - r1) x d,
-// the quantities of segment_induction (pvl_common.cuh) from 9 FMAs instead of 3 differences
-// and 9 products; rounding is relative to |p - o| + |r1 - o| instead of |p - r1|, and o is the
-// centroid of the CTA's points, which are neighbours (ring or wake-node order).
-__device__ __forceinline__ SweepGeo sweep_geo(const SweepSeg& s, double px, double py, double pz)
-{
-    SweepGeo g;
-    const double t1 = fma(s.dz, pz, fma(s.dy, py, fma(s.dx, px, -s.e)));
-    g.cx = fma(py, s.dz, -fma(pz, s.dy, s.mx));
-    g.cy = fma(pz, s.dx, -fma(px, s.dz, s.my));
-    g.cz = fma(px, s.dy, -fma(py, s.dx, s.mz));
-    g.hsq = g.cx * g.cx + g.cy * g.cy + g.cz * g.cz;
-    g.x = g.hsq + t1 * (t1 - s.len);
-    g.r = pvl::FarSeries<double>::rcp(g.x);
-    g.w = g.hsq * s.len2 * (g.r * g.r);
-    return g;
-}
-
-// The rest of segment_induction<double, true>: far pairs by the arctangent series (selected,
-// no branch), the rare near pairs by atan2 in a branch, pairs inside the cut-off skipped.
-__device__ __forceinline__ void sweep_add(const SweepSeg& s, const SweepGeo& g, double tol2, Vec3<double>& acc)
-{
-    const bool ok = !pvl::lt_nn(g.hsq, tol2);
-    const bool far = ok && pvl::pos(g.x) && pvl::le_nn(g.w, pvl::FarSeries<double>::kW);
-    double mag = far ? -s.glen * g.r * pvl::FarSeries<double>::sum(g.w) : 0.0;
-    if (ok && !far) {
-        const double rh = rsqrt(g.hsq);
-        const double h = g.hsq * rh;
-        mag = s.gamma * atan2(-h * s.len, g.x) * rh;
-    }
-    acc.x += g.cx * mag;
-    acc.y += g.cy * mag;
-    acc.z += g.cz * mag;
-}
-
 // FP64 N-body sweep: partial[(split*n_pts + p)*3 + c] = sum over this split's segments of
 // gamma_k u_k(p).  One point per thread; segments stream through shared memory in tiles of
 // kSegTile, converted to the Pluecker form about the CTA's origin as they are staged, and
@@ -285,27 +242,7 @@ __global__ void __launch_bounds__(kSumThreads, 8) line_sum_f64_kernel(
     size_t q;
     const bool ok = sweep_point(p, n_pts, group, stride, in_off, cols, col_limit, q);
     double px = ok ? pts[3 * q] : 0.0, py = ok ? pts[3 * q + 1] : 0.0, pz = ok ? pts[3 * q + 2] : 0.0;
-    {  // origin: centroid of the CTA's points
-        double v[4] = {px, py, pz, ok ? 1.0 : 0.0};
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-            for (int o = 16; o > 0; o >>= 1)
-                v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
-        if ((threadIdx.x & 31) == 0)
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
-                s_red[threadIdx.x >> 5][c] = v[c];
-        __syncthreads();
-        if (threadIdx.x < 3) {
-            double t = 0.0, n = 0.0;
-            for (int w = 0; w < kSumThreads / 32; ++w) {
-                t += s_red[w][threadIdx.x];
-                n += s_red[w][3];
-            }
-            s_o[threadIdx.x] = n > 0.0 ? t / n : 0.0;
-        }
-        __syncthreads();
-    }
+    pvl::cta_centroid<kSumThreads>(px, py, pz, ok ? 1.0 : 0.0, s_red, s_o);  // px.. are 0 when !ok
     px -= s_o[0];
     py -= s_o[1];
     pz -= s_o[2];
@@ -314,22 +251,7 @@ __global__ void __launch_bounds__(kSumThreads, 8) line_sum_f64_kernel(
         s_seg[kSegTile] = SweepSeg{};  // the partner of an odd last segment: d = 0, nothing induced
     for (uint32_t l0 = l_begin; l0 < l_end; l0 += kSegTile) {
         const uint32_t l = l0 + threadIdx.x;
-        SweepSeg t{};
-        if (threadIdx.x < kSegTile && l < l_end) {
-            const Segment<double> g = seg[l];
-            const double rx = g.r1x - s_o[0], ry = g.r1y - s_o[1], rz = g.r1z - s_o[2];
-            t.dx = g.dx;
-            t.dy = g.dy;
-            t.dz = g.dz;
-            t.mx = ry * g.dz - rz * g.dy;
-            t.my = rz * g.dx - rx * g.dz;
-            t.mz = rx * g.dy - ry * g.dx;
-            t.e = g.dx * rx + g.dy * ry + g.dz * rz;
-            t.len = g.len;
-            t.len2 = g.len2;
-            t.glen = g.glen;
-            t.gamma = g.gamma;
-        }
+        const SweepSeg t = threadIdx.x < kSegTile && l < l_end ? pvl::sweep_seg(seg[l], s_o) : SweepSeg{};
         if (threadIdx.x < kSegTile)
             s_seg[threadIdx.x] = t;
         __syncthreads();
@@ -337,9 +259,9 @@ __global__ void __launch_bounds__(kSumThreads, 8) line_sum_f64_kernel(
 #pragma unroll 1
         for (int k = 0; k < cnt; k += 2) {
             const SweepSeg a = s_seg[k], b = s_seg[k + 1];
-            const SweepGeo ga = sweep_geo(a, px, py, pz), gb = sweep_geo(b, px, py, pz);
-            sweep_add(a, ga, tol2, acc);
-            sweep_add(b, gb, tol2, acc);
+            const pvl::SweepGeo ga = pvl::sweep_geo(a, px, py, pz), gb = pvl::sweep_geo(b, px, py, pz);
+            pvl::sweep_add(a, ga, tol2, acc);
+            pvl::sweep_add(b, gb, tol2, acc);
         }
         __syncthreads();
     }
@@ -357,7 +279,7 @@ __global__ void __launch_bounds__(kSumThreads, 8) line_sum_f64_kernel(
 // issue, not by the FMA pipe).  Both lanes take the far-field series of segment_induction; a
 // lane inside the cut-off contributes zero (selected, not computed), and a lane that needs the
 // near-field atan2 form takes a scalar side path.  Same function and layout as
-// line_sum_kernel<float>; points p and p + 128 of each 256-point block.
+// line_sum_f64_kernel; points p and p + 128 of each 256-point block.
 __device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
 
 __global__ void __launch_bounds__(kSumThreads) line_sum_f32x2_kernel(const Segment<float>* __restrict__ seg,
