@@ -10,8 +10,9 @@ One :meth:`SolverEngine.step` is one iteration of the reference's solver loop
 3. wake corrections for iteration > 0 (solver.py:217-220):
    implicit first wake row folded into the TE-adjacent columns, explicit rows contracted
    with the wake circulations into the RHS (wake_models.py:199-223)
-                                                            -> pvl_induction_normal on the
-   first-row rings, pvl_wake_fold_implicit, pvl_line_circulation + pvl_line_velocity
+                                                            -> pvl_induction_normal_tiled on
+   the first-row rings, pvl_wake_fold_implicit, pvl_line_circulation + pvl_line_velocity over the
+   lines of the rows shed so far
 4. dense solve (solver.py:223-227)                         -> pvl_lu_factor / pvl_lu_solve
    closed bodies: the bordered zero-mean system, then the mean removal of solver.py:229-233
 5. wake update (solver.py:236-239, wake_models.py:111-157): node velocities from the body
@@ -204,13 +205,9 @@ class SolverEngine:
         # each ring adjacent to at most one shedding line side: the fold may run in parallel
         self._fold_fn = ("pvl_wake_fold_implicit_distinct" if np.unique(valid).size == valid.size
                          else "pvl_wake_fold_implicit")
-        # first-row rings (r = 0) as their own CSR over the wake's lines
-        row0 = wake_row0_mesh(wmesh, S, R)
-        off0, sl0 = row0.surface_offsets, row0.surface_lines
         f64 = dict(dtype=torch.float64, device=self.dev)
         self.wake = {
             "S": S, "R": R, "mesh": wmesh, "d": wmesh.device_arrays(),
-            "off0": to_device_u32(off0, self.dev), "sl0": to_device_u32(sl0, self.dev),
             "adj": to_device_u32(adj.astype(np.uint32), self.dev),
             "bn": to_device_u32(bn.astype(np.uint32), self.dev),
             "pos": [torch.zeros((S, 2, R + 1, 3), **f64), torch.zeros((S, 2, R + 1, 3), **f64)],
@@ -222,12 +219,26 @@ class SolverEngine:
             "slot": to_device_u32(slot, self.dev),
             "n_cols": int(cols.size),
             "node_vel": torch.zeros((int(cols.size), R, 3), **f64),
-            "line_gamma": torch.zeros(max(wmesh.n_lines, 1), **f64),
             "self_line_gamma": torch.zeros(max(wmesh.n_lines, 1), **f64),
             "node_vel_self": torch.zeros((int(cols.size), R, 3), **f64),
             "time": float(w.time),
             "step_count": 0,
         }
+        # The explicit wake term runs over the same wake in row-major ring order (ring r*S + s):
+        # lines are then numbered row band by row band, so the lines of rows < k are the first
+        # lines_upto[k], and a wake that has shed k rows is swept over that prefix only (rows
+        # not yet shed carry no circulation).  Its first S rings are row 0, the implicit block.
+        rc = wake_ring_connectivity(R, S, bn).reshape(S, R, 4).transpose(1, 0, 2).reshape(-1, 4)
+        rm = Mesh(2 * (R + 1) * S, rc)
+        off_rm, ids = rm.surface_offsets, (rm.surface_lines & 0x7FFFFFFF).astype(np.int64)
+        run = np.maximum.accumulate(ids) + 1
+        self.wake.update({
+            "rm": rm, "rm_d": rm.device_arrays(),
+            "lines_upto": [0] + [int(run[int(off_rm[k * S]) - 1]) for k in range(1, R + 1)],
+            "circ_rs": torch.zeros((R, S), **f64),
+            "rm_line_gamma": torch.zeros(max(rm.n_lines, 1), **f64),
+        })
+        self.n_near_lines = rm.n_lines  # lines of the explicit term evaluated in FP64 (all)
 
     def _workspace_bytes(self) -> int:
         L = self.mesh.n_lines
@@ -323,24 +334,42 @@ class SolverEngine:
             self._wake_corrections()
         self.border()
 
-    def _wake_corrections(self) -> None:
-        """Implicit first row into A, explicit rows into the RHS (wake_models.py:199-223)."""
+    def _wake_corrections(self, fp64_only: bool = False) -> None:
+        """Implicit first row into A, explicit rows into the RHS (wake_models.py:199-223).
+
+        Both over the row-major wake: the implicit block is its first S rings (row 0 of every
+        strip, in strip order) at the control points, folded into the columns of the rings
+        that shed them; the explicit term sweeps the lines of the rows shed so far with the
+        line circulations of rows >= 1, in FP64 for the first ``n_near_lines`` lines and in
+        FP32 beyond (all FP64 unless a subclass says otherwise, or with ``fp64_only``)."""
         s = stream_ptr()
         w = self.wake
         S, R = w["S"], w["R"]
-        wm, wd = w["mesh"], w["d"]
+        rm, d = w["rm"], w["rm_d"]
         wpos = self.wake_positions.reshape(-1, 3)
         ws, nb = ptr(self.ws), self._ws_bytes
-        _lib.call("pvl_induction_normal", _lib.PVL_F64, wm.n_points, wm.n_lines, ptr(wd["lines"]), ptr(wpos), S,
-                  ptr(w["off0"]), ptr(w["sl0"]), self.P, ptr(self.cps), ptr(self.nrm), self.tol, ptr(w["implicit"]),
-                  S, ws, nb, s)
+        _lib.call("pvl_induction_normal_tiled", rm.n_points, rm.n_lines, ptr(d["lines"]), ptr(wpos), S,
+                  ptr(d["offsets"]), ptr(d["surface_lines"]), ptr(d["tile_offsets"]), ptr(d["tile_lines"]),
+                  ptr(d["sl_local"]), d["tile_max"], self.P, ptr(self.cps), ptr(self.nrm), self.tol,
+                  ptr(w["implicit"]), S, ws, nb, s)
         _lib.call(self._fold_fn, self.P, S, ptr(w["implicit"]), ptr(w["adj"]), ptr(self.A), self.N, s)
-        if R > 1:
-            _lib.call("pvl_line_circulation", wm.n_lines, ptr(wd["map_offsets"]), ptr(wd["map_entries"]),
-                      ptr(self.wake_circulation), R, ptr(w["line_gamma"]), s)
-            _lib.call("pvl_line_velocity", _lib.PVL_F64, wm.n_points, wm.n_lines, ptr(wd["lines"]), ptr(wpos),
-                      ptr(w["line_gamma"]), self.P, ptr(self.cps), ptr(self.nrm), self.tol, 1.0, 1.0, ptr(self.rhs),
-                      ws, nb, s)
+        active = w["lines_upto"][min(w["step_count"], R)]
+        if R <= 1 or active == 0:
+            return
+        crs = w["circ_rs"]
+        crs.copy_(self.wake_circulation.t())
+        crs[0].zero_()  # row 0 is implicit
+        lg = w["rm_line_gamma"]
+        _lib.call("pvl_line_circulation", rm.n_lines, ptr(d["map_offsets"]), ptr(d["map_entries"]), ptr(crs), 0,
+                  ptr(lg), s)
+        near = active if fp64_only else min(self.n_near_lines, active)
+        lines = d["lines"]
+        _lib.call("pvl_line_velocity", _lib.PVL_F64, rm.n_points, near, ptr(lines), ptr(wpos), ptr(lg), self.P,
+                  ptr(self.cps), ptr(self.nrm), self.tol, 1.0, 1.0, ptr(self.rhs), ws, nb, s)
+        if active > near:
+            _lib.call("pvl_line_velocity", _lib.PVL_F32, rm.n_points, active - near, lines.data_ptr() + 8 * near,
+                      ptr(wpos), lg.data_ptr() + 8 * near, self.P, ptr(self.cps), ptr(self.nrm), self.tol, 1.0, 1.0,
+                      ptr(self.rhs), ws, nb, s)
 
     def solve(self) -> None:
         s = stream_ptr()
@@ -523,20 +552,13 @@ class MixedSolverEngine(SolverEngine):
 
     # ------------------------------------------------------------------ wake in row-major ring order
     def _init_row_major_wake(self, near_rows: int | None, advect_near_rows: int) -> int:
+        """Precision bands of the wake terms and their workspace."""
         w = self.wake
         S, R = w["S"], w["R"]
-        bn = self.wake["bn"].cpu().numpy().astype(np.int64)
-        rc = wake_ring_connectivity(R, S, bn).reshape(S, R, 4).transpose(1, 0, 2).reshape(-1, 4)
-        rm = Mesh(2 * (R + 1) * S, rc)  # ring r*S + s: lines are numbered row band by row band
+        rm = w["rm"]
         self.near_rows = R if near_rows is None else max(1, min(int(near_rows), R))
         self.advect_near_rows = max(0, min(int(advect_near_rows), R))
-        off, sl = rm.surface_offsets, rm.surface_lines
-        ids = sl[: int(off[self.near_rows * S])] & 0x7FFFFFFF
-        self.n_near_lines = int(ids.max()) + 1  # lines of rows < near_rows come first
-        w["rm"] = rm
-        w["rm_d"] = rm.device_arrays()
-        w["circ_rs"] = torch.zeros((R, S), dtype=torch.float64, device=self.dev)
-        w["rm_line_gamma"] = torch.zeros(max(rm.n_lines, 1), dtype=torch.float64, device=self.dev)
+        self.n_near_lines = w["lines_upto"][self.near_rows]  # lines of rows < near_rows come first
         L, P = self.mesh.n_lines, self.P
         need = [_lib.query("pvl_segments_workspace", rm.n_lines, _lib.PVL_F64),
                 _lib.query("pvl_line_velocity_workspace", self.n_near_lines, P, _lib.PVL_F64),
@@ -549,36 +571,6 @@ class MixedSolverEngine(SolverEngine):
             if c > nr:
                 need.append(_lib.query("pvl_line_velocity_workspace", L, nc * (c - nr), _lib.PVL_F32))
         return max(need)
-
-    def _wake_corrections(self) -> None:
-        s = stream_ptr()
-        w = self.wake
-        S, R = w["S"], w["R"]
-        rm, d = w["rm"], w["rm_d"]
-        wpos = self.wake_positions.reshape(-1, 3)
-        ws, nb = ptr(self.ws), self._ws_bytes
-        # implicit: the first S rings of the row-major mesh are row 0 of every strip, in strip order
-        _lib.call("pvl_induction_normal_tiled", rm.n_points, rm.n_lines, ptr(d["lines"]), ptr(wpos), S,
-                  ptr(d["offsets"]), ptr(d["surface_lines"]), ptr(d["tile_offsets"]), ptr(d["tile_lines"]),
-                  ptr(d["sl_local"]), d["tile_max"], self.P, ptr(self.cps), ptr(self.nrm), self.tol,
-                  ptr(w["implicit"]), S, ws, nb, s)
-        _lib.call(self._fold_fn, self.P, S, ptr(w["implicit"]), ptr(w["adj"]), ptr(self.A), self.N, s)
-        if R <= 1:
-            return
-        crs = w["circ_rs"]
-        crs.copy_(self.wake_circulation.t())
-        crs[0].zero_()  # row 0 is implicit
-        lg = w["rm_line_gamma"]
-        _lib.call("pvl_line_circulation", rm.n_lines, ptr(d["map_offsets"]), ptr(d["map_entries"]), ptr(crs), 0,
-                  ptr(lg), s)
-        Ln = self.n_near_lines
-        lines = d["lines"]
-        _lib.call("pvl_line_velocity", _lib.PVL_F64, rm.n_points, Ln, ptr(lines), ptr(wpos), ptr(lg), self.P,
-                  ptr(self.cps), ptr(self.nrm), self.tol, 1.0, 1.0, ptr(self.rhs), ws, nb, s)
-        if rm.n_lines > Ln:
-            _lib.call("pvl_line_velocity", _lib.PVL_F32, rm.n_points, rm.n_lines - Ln, lines.data_ptr() + 8 * Ln,
-                      ptr(wpos), lg.data_ptr() + 8 * Ln, self.P, ptr(self.cps), ptr(self.nrm), self.tol, 1.0, 1.0,
-                      ptr(self.rhs), ws, nb, s)
 
     # ------------------------------------------------------------------ preconditioner
     def refresh_preconditioner(self, wait: bool = True) -> None:
@@ -888,7 +880,7 @@ class MixedSolverEngine(SolverEngine):
         mixed = self.gamma.clone()
         self.assemble_body_only()
         if self.wake is not None and self.iteration > 0:
-            SolverEngine._wake_corrections(self)
+            self._wake_corrections(fp64_only=True)
         self.border()
         SolverEngine.solve(self)
         ref = self.gamma.clone()
