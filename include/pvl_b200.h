@@ -471,11 +471,13 @@ int pvl_batch_ring_matrix(int cpb, const void* jobs, const uint32_t* job_item, u
 
 /* Segment sweeps of every job into per-job partials (FP64); tile = (threads, points per
  * thread) in {(128,1),(128,2),(128,4),(256,1),(256,2)}; rows: device uint32 (the step's row
- * count for jobs whose point count grows with the wake). */
+ * count for jobs whose point count grows with the wake).  A job with seg_rows set has its
+ * segments in row order and sweeps only the first seg_upto[seg_rows + min(*rows, rows_max)]
+ * of them (seg_upto: device table of the row prefixes; NULL sweeps every segment). */
 int pvl_batch_sweep(int threads, int ppt, const void* jobs, const uint32_t* job_item, uint32_t n_jobs,
-                    uint32_t n_items, uint32_t* counter, const uint32_t* rows, const void* segments,
-                    const double* pts, const uint32_t* pidx, double tol, double* partials, uint32_t n_ctas,
-                    void* stream);
+                    uint32_t n_items, uint32_t* counter, const uint32_t* rows, const uint32_t* seg_upto,
+                    uint32_t rows_max, const void* segments, const double* pts, const uint32_t* pidx, double tol,
+                    double* partials, uint32_t n_ctas, void* stream);
 
 /* Reduce the sweeps' partials: mode 0 jobs add n . v to out (the RHS), mode 1 jobs write
  * U_case + v (node velocities; uinf is (n_cases, 3)).  pt_item: first thread of each job. */

@@ -29,7 +29,8 @@ RING_JOB = np.dtype([("cp_begin", "<u4"), ("n_cp", "<u4"), ("ring_begin", "<u4")
                      ("out_begin", "<u8"), ("ld", "<u4"), ("item_begin", "<u4")])
 SWEEP_JOB = np.dtype([(k, "<u4") for k in ("seg_begin", "seg_count", "pt_begin", "pt_max", "pt_per_row",
                                           "out_begin", "n_split", "per", "part_begin", "item_begin", "mode",
-                                          "case_id")])
+                                          "case_id", "seg_rows")])
+NO_ROWS = 0xFFFFFFFF  # SweepJob.seg_rows of a job swept over all its segments
 WAKE_CASE = np.dtype({"names": ["P", "S", "n_cols", "ring_begin", "mat_begin", "imp_begin", "shed_begin",
                                 "pos_begin", "circ_begin", "vel_begin", "dt"],
                       "formats": ["<u4", "<u4", "<u4", "<u4", "<u8", "<u4", "<u4", "<u4", "<u4", "<u4", "<f8"],
@@ -140,8 +141,40 @@ class BatchEngine:
         self.row0_offsets = np.concatenate(
             [[0]] + [r.surface_offsets[1:].astype(np.int64) + off0[k] for k, r in enumerate(row0s)]).astype(np.uint32)
         self.row0_lines = np.concatenate(sl0).astype(np.uint32)
+        # The wake's lines in row order within each case (lines first used by row 0, then row 1,
+        # ...), so that the explicit wake term of a wake that has shed k rows sweeps a prefix of
+        # each case's lines: seg_upto[c * (R + 1) + k] of them.  The segment table, the line
+        # circulations (a permuted line -> ring map) and the row-0 rings all use this order.
+        wl = self.wake_mesh
+        w_off = wl.surface_offsets.astype(np.int64)
+        w_ids = (wl.surface_lines & np.uint32(0x7FFFFFFF)).astype(np.int64)
+        ring_row = np.arange(wl.n_surfaces, dtype=np.int64) % R  # rings s * R + r within each case
+        min_row = np.full(wl.n_lines, R, np.int64)
+        np.minimum.at(min_row, w_ids, np.repeat(ring_row, np.diff(w_off)))
+        line_case = np.repeat(np.arange(B), WL)
+        order = np.lexsort((np.arange(wl.n_lines), min_row, line_case))
+        inv = np.empty_like(order)
+        inv[order] = np.arange(order.size)
+        self.wake_lines_rm = np.asarray(wl._lines, np.uint32).reshape(-1, 2)[order]
+        m_off, m_ent = wl.ring_map()
+        m_off = m_off.astype(np.int64)
+        cnt = np.diff(m_off)[order]
+        self.wake_map_offsets_rm = np.concatenate([[0], np.cumsum(cnt)]).astype(np.uint32)
+        src = np.repeat(m_off[order] - self.wake_map_offsets_rm[:-1].astype(np.int64), cnt) + np.arange(int(cnt.sum()))
+        self.wake_map_entries_rm = np.asarray(m_ent, np.uint32)[src]
+        r0 = self.row0_lines.astype(np.int64)
+        self.row0_lines = ((inv[r0 & 0x7FFFFFFF]) | (r0 & 0x80000000)).astype(np.uint32)
+        self.seg_upto = np.zeros(B * (R + 1), np.uint32)
+        for k in range(B):
+            rows_k = np.sort(min_row[wline_off[k]:wline_off[k + 1]])
+            self.seg_upto[k * (R + 1):(k + 1) * (R + 1)] = np.searchsorted(rows_k, np.arange(R + 1), side="left")
         self.d_body = None if host_only else self.body.device_arrays()
-        self.d_wake = None if host_only else self.wake_mesh.device_arrays()
+        self.d_wake = None if host_only else {
+            "lines": to_device_u32(self.wake_lines_rm, dev),
+            "map_offsets": to_device_u32(self.wake_map_offsets_rm, dev),
+            "map_entries": to_device_u32(self.wake_map_entries_rm, dev),
+        }
+        self.d_seg_upto = to_device_u32(self.seg_upto, dev)
         self.d_row0 = {"offsets": to_device_u32(self.row0_offsets, dev), "lines": to_device_u32(self.row0_lines, dev)}
         n_wake_pts = int(wpt_off[-1])
         self.n_wake_pts = n_wake_pts
@@ -186,9 +219,10 @@ class BatchEngine:
         self.pidx = to_device_u32(np.concatenate(pidx).astype(np.uint32), dev)
         self._sweep_specs = {
             "wake": dict(seg_begin=wline_off[:-1], seg_count=WL, pt_begin=ring_off[:-1], pt_max=P,
-                         pt_per_row=[0] * B, out_begin=ring_off[:-1], mode=0),
+                         pt_per_row=[0] * B, out_begin=ring_off[:-1], mode=0, seg_rows=(R + 1) * np.arange(B)),
             "advect": dict(seg_begin=line_off[:-1], seg_count=L, pt_begin=R * np.concatenate([[0], np.cumsum(NC)[:-1]]),
-                           pt_max=np.asarray(NC) * R, pt_per_row=NC, out_begin=vel_off[:-1], mode=1),
+                           pt_max=np.asarray(NC) * R, pt_per_row=NC, out_begin=vel_off[:-1], mode=1,
+                           seg_rows=[NO_ROWS] * B),
         }
         self.sweep_tables: dict = {}
 
@@ -246,7 +280,7 @@ class BatchEngine:
         part_total = 0
         for name, sp in self._sweep_specs.items():
             jobs = np.zeros(B, SWEEP_JOB)
-            for k in ("seg_begin", "seg_count", "pt_begin", "pt_max", "pt_per_row", "out_begin"):
+            for k in ("seg_begin", "seg_count", "pt_begin", "pt_max", "pt_per_row", "out_begin", "seg_rows"):
                 jobs[k] = sp[k]
             jobs["mode"] = sp["mode"]
             jobs["case_id"] = np.arange(B)
@@ -277,8 +311,8 @@ class BatchEngine:
         s = stream_ptr()
         threads, ppt = self.tile["sweep"]
         _lib.call("pvl_batch_sweep", threads, ppt, ptr(jobs), ptr(items), self.B, n_items, ptr(self.counter),
-                  ptr(self.rows), ptr(segs), ptr(pts), ptr(pidx) if pidx is not None else None, self.tol,
-                  ptr(self.partials), 0, s)
+                  ptr(self.rows), ptr(self.d_seg_upto), self.R, ptr(segs), ptr(pts),
+                  ptr(pidx) if pidx is not None else None, self.tol, ptr(self.partials), 0, s)
         _lib.call("pvl_batch_sweep_reduce", ptr(jobs), ptr(pt_item), self.B, n_total, ptr(self.rows),
                   ptr(self.partials), ptr(self.nrm), ptr(self.uinf), ptr(out), s)
 

@@ -55,7 +55,12 @@ struct SweepJob {
     uint32_t item_begin;             // first work item; items = ceil(pt_max / pts_per_cta) * n_split
     uint32_t mode;                   // 0: normal output (out[o] += n . v); 1: vector output (out = U + v)
     uint32_t case_id;
+    uint32_t seg_rows;               // != kNoRows: the job's segments are in row order and only the first
+                                     // seg_upto[seg_rows + min(*rows, rows_max)] of them (the rows shed so
+                                     // far) are swept; the other ranges write zero partials
 };
+
+constexpr uint32_t kNoRows = 0xFFFFFFFFu;
 
 __device__ __forceinline__ uint32_t find_job(const uint32_t* __restrict__ item_begin, uint32_t n_jobs, uint32_t item)
 {
@@ -129,6 +134,8 @@ __global__ void __launch_bounds__(THREADS) batched_sweep_kernel(const SweepJob* 
                                                                 uint32_t n_jobs, uint32_t n_items,
                                                                 uint32_t* __restrict__ counter,
                                                                 const uint32_t* __restrict__ rows,
+                                                                const uint32_t* __restrict__ seg_upto,
+                                                                uint32_t rows_max,
                                                                 const Segment<double>* __restrict__ seg,
                                                                 const double* __restrict__ pts,
                                                                 const uint32_t* __restrict__ pidx, double tol2,
@@ -157,8 +164,11 @@ __global__ void __launch_bounds__(THREADS) batched_sweep_kernel(const SweepJob* 
             __syncthreads();
             continue;
         }
+        uint32_t seg_count = J.seg_count;
+        if (J.seg_rows != kNoRows && seg_upto)
+            seg_count = min(seg_count, seg_upto[J.seg_rows + min(rows[0], rows_max)]);
         const uint32_t l_begin = J.seg_begin + split * J.per;
-        const uint32_t l_end = J.seg_begin + min(J.seg_count, (split + 1) * J.per);
+        const uint32_t l_end = J.seg_begin + min(seg_count, (split + 1) * J.per);  // may be <= l_begin: zeros
         double px[PPT], py[PPT], pz[PPT];
         Vec3<double> acc[PPT];
 #pragma unroll
@@ -592,13 +602,13 @@ int launch_ring(const void* jobs, const uint32_t* job_item, uint32_t n_jobs, uin
 
 template <int THREADS, int PPT>
 int launch_sweep(const void* jobs, const uint32_t* job_item, uint32_t n_jobs, uint32_t n_items, uint32_t* counter,
-                 const uint32_t* rows, const void* seg, const double* pts, const uint32_t* pidx, double tol,
-                 double* part, uint32_t n_ctas, cudaStream_t st)
+                 const uint32_t* rows, const uint32_t* seg_upto, uint32_t rows_max, const void* seg, const double* pts,
+                 const uint32_t* pidx, double tol, double* part, uint32_t n_ctas, cudaStream_t st)
 {
     if (n_ctas == 0)
         n_ctas = persistent_ctas((const void*)batched_sweep_kernel<THREADS, PPT>, THREADS);
     batched_sweep_kernel<THREADS, PPT><<<n_ctas, THREADS, 0, st>>>(
-        static_cast<const SweepJob*>(jobs), job_item, n_jobs, n_items, counter, rows,
+        static_cast<const SweepJob*>(jobs), job_item, n_jobs, n_items, counter, rows, seg_upto, rows_max,
         static_cast<const Segment<double>*>(seg), pts, pidx, pvl::cutoff2<double>(tol), part);
     PVL_LAUNCH_CHECK();
     return PVL_OK;
@@ -638,9 +648,9 @@ extern "C" int pvl_batch_ring_matrix(int cpb, const void* jobs, const uint32_t* 
 }
 
 extern "C" int pvl_batch_sweep(int threads, int ppt, const void* jobs, const uint32_t* job_item, uint32_t n_jobs,
-                               uint32_t n_items, uint32_t* counter, const uint32_t* rows, const void* segments,
-                               const double* pts, const uint32_t* pidx, double tol, double* partials,
-                               uint32_t n_ctas, void* stream)
+                               uint32_t n_items, uint32_t* counter, const uint32_t* rows, const uint32_t* seg_upto,
+                               uint32_t rows_max, const void* segments, const double* pts, const uint32_t* pidx,
+                               double tol, double* partials, uint32_t n_ctas, void* stream)
 {
     if (n_items == 0)
         return PVL_OK;
@@ -650,16 +660,16 @@ extern "C" int pvl_batch_sweep(int threads, int ppt, const void* jobs, const uin
     PVL_CUDA_CHECK(cudaMemsetAsync(counter, 0, sizeof(uint32_t), st));
     const int key = threads * 10 + ppt;
     switch (key) {
-    case 1281: return launch_sweep<128, 1>(jobs, job_item, n_jobs, n_items, counter, rows, segments, pts, pidx, tol,
-                                           partials, n_ctas, st);
-    case 1282: return launch_sweep<128, 2>(jobs, job_item, n_jobs, n_items, counter, rows, segments, pts, pidx, tol,
-                                           partials, n_ctas, st);
-    case 1284: return launch_sweep<128, 4>(jobs, job_item, n_jobs, n_items, counter, rows, segments, pts, pidx, tol,
-                                           partials, n_ctas, st);
-    case 2561: return launch_sweep<256, 1>(jobs, job_item, n_jobs, n_items, counter, rows, segments, pts, pidx, tol,
-                                           partials, n_ctas, st);
-    case 2562: return launch_sweep<256, 2>(jobs, job_item, n_jobs, n_items, counter, rows, segments, pts, pidx, tol,
-                                           partials, n_ctas, st);
+    case 1281: return launch_sweep<128, 1>(jobs, job_item, n_jobs, n_items, counter, rows, seg_upto, rows_max,
+                                           segments, pts, pidx, tol, partials, n_ctas, st);
+    case 1282: return launch_sweep<128, 2>(jobs, job_item, n_jobs, n_items, counter, rows, seg_upto, rows_max,
+                                           segments, pts, pidx, tol, partials, n_ctas, st);
+    case 1284: return launch_sweep<128, 4>(jobs, job_item, n_jobs, n_items, counter, rows, seg_upto, rows_max,
+                                           segments, pts, pidx, tol, partials, n_ctas, st);
+    case 2561: return launch_sweep<256, 1>(jobs, job_item, n_jobs, n_items, counter, rows, seg_upto, rows_max,
+                                           segments, pts, pidx, tol, partials, n_ctas, st);
+    case 2562: return launch_sweep<256, 2>(jobs, job_item, n_jobs, n_items, counter, rows, seg_upto, rows_max,
+                                           segments, pts, pidx, tol, partials, n_ctas, st);
     default: return pvl_fail(PVL_ERR_ARG, "pvl_batch_sweep: unsupported tile (threads %d, points/thread %d)", threads,
                              ppt);
     }

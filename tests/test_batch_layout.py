@@ -50,6 +50,15 @@ def test_ring_jobs_cover_each_block_once(layout):
             assert int(J["out_begin"]) + int(J["n_cp"]) * int(J["ld"]) <= out_size
 
 
+def _active(e, J, rows):
+    """Segments a sweep job covers when the wake has `rows` rows (csrc/batch.cu, SweepJob)."""
+    from pyvl_b200.batch import NO_ROWS
+
+    if int(J["seg_rows"]) == NO_ROWS:
+        return int(J["seg_count"])
+    return min(int(J["seg_count"]), int(e.seg_upto[int(J["seg_rows"]) + min(rows, e.R)]))
+
+
 def test_sweep_jobs_in_bounds_and_cover_pairs(layout):
     from pyvl_b200.batch import SWEEP_JOB
 
@@ -73,14 +82,14 @@ def test_sweep_jobs_in_bounds_and_cover_pairs(layout):
                 split, pb = divmod(item - int(J["item_begin"]), blocks)
                 assert split < J["n_split"]
                 l0 = int(J["seg_begin"]) + split * int(J["per"])
-                l1 = int(J["seg_begin"]) + min(int(J["seg_count"]), (split + 1) * int(J["per"]))
+                l1 = int(J["seg_begin"]) + min(_active(e, J, rows), (split + 1) * int(J["per"]))
                 p0, p1 = pb * kpts, min(pb * kpts + kpts, n_pts)
                 if p0 < p1:
-                    cover[jb][p0:p1] += l1 - l0
+                    cover[jb][p0:p1] += max(0, l1 - l0)
             for J, cv in zip(jobs, cover):
                 n_pts = int(J["pt_max"]) if not J["pt_per_row"] else int(J["pt_per_row"]) * min(
                     rows, int(J["pt_max"]) // int(J["pt_per_row"]))
-                assert (cv[:n_pts] == int(J["seg_count"])).all()  # every point meets every segment once
+                assert (cv[:n_pts] == _active(e, J, rows)).all()  # every point meets every live segment once
                 assert (cv[n_pts:] == 0).all()
         for J in jobs:
             assert int(J["seg_begin"]) + int(J["seg_count"]) <= n_seg
@@ -104,12 +113,60 @@ def test_wake_tables_in_bounds(layout):
         a = adj[2 * o:2 * (o + S)]
         assert ((a == 0x7FFFFFFF) | (a < e.P[k])).all()
         o += S
-    # first-row rings of the implicit blocks are the merged wake mesh's rings s*R (row 0)
+    # first-row rings of the implicit blocks are the merged wake mesh's rings s*R (row 0), with
+    # their lines renumbered into the row order of the sweep (same node pairs, same orientation)
     off, sl = e.wake_mesh.surface_offsets, e.wake_mesh.surface_lines
+    old_lines = np.asarray(e.wake_mesh._lines, np.uint32).reshape(-1, 2)
     shed0 = 0
     for k in range(e.B):
         for s in range(int(e.S[k])):
             r = (shed0 + s) * e.R
             a0, a1 = e.row0_offsets[shed0 + s], e.row0_offsets[shed0 + s + 1]
-            assert np.array_equal(e.row0_lines[a0:a1], sl[off[r]:off[r + 1]])
+            new, old = e.row0_lines[a0:a1], sl[off[r]:off[r + 1]]
+            assert np.array_equal(new & 0x80000000, old & 0x80000000)
+            assert np.array_equal(e.wake_lines_rm[new & 0x7FFFFFFF], old_lines[old & 0x7FFFFFFF])
         shed0 += int(e.S[k])
+
+
+def test_row_ordered_wake_lines(layout):
+    """The wake's lines in row order per case: a permutation of the merged wake mesh's lines,
+    the line -> ring map and the row-0 rings follow it, and the lines of rows < k of a case
+    are exactly its first seg_upto[k] lines (so a sweep over that prefix misses no live line)."""
+    e, cases = layout
+    wl, R = e.wake_mesh, e.R
+    old_lines = np.asarray(wl._lines, np.uint32).reshape(-1, 2)
+    new_lines = e.wake_lines_rm
+    key = lambda a: set(map(tuple, a.tolist()))
+    assert len(new_lines) == len(old_lines) and key(new_lines) == key(old_lines)
+    # recover the permutation from the unique (start, end) node pairs
+    pos = {tuple(v): i for i, v in enumerate(old_lines.tolist())}
+    order = np.array([pos[tuple(v)] for v in new_lines.tolist()])
+    m_off, m_ent = wl.ring_map()
+    for i in range(0, len(order), max(1, len(order) // 300)):
+        o = order[i]
+        a = e.wake_map_entries_rm[e.wake_map_offsets_rm[i]:e.wake_map_offsets_rm[i + 1]]
+        assert np.array_equal(a, m_ent[m_off[o]:m_off[o + 1]])
+    # row-0 rings reference the same node pairs as before the renumbering
+    for g_new, g_old in zip(e.row0_lines[:200], np.concatenate(
+            [((wl.surface_lines[wl.surface_offsets[s * R]:wl.surface_offsets[s * R + 1]]))
+             for s in range(int(np.sum(e.S)))])[:200]):
+        assert (g_new & 0x80000000) == (g_old & 0x80000000)
+        assert tuple(new_lines[g_new & 0x7FFFFFFF]) == tuple(old_lines[g_old & 0x7FFFFFFF])
+    # prefix property per case
+    off, ids = wl.surface_offsets.astype(np.int64), (wl.surface_lines & 0x7FFFFFFF).astype(np.int64)
+    inv = np.empty_like(order)
+    inv[order] = np.arange(order.size)
+    per_case = e.seg_upto.reshape(e.B, R + 1)[:, R].astype(np.int64)  # every line has a row < R
+    assert per_case.sum() == wl.n_lines
+    line_off = np.concatenate([[0], np.cumsum(per_case)])
+    ring0 = 0
+    for c in range(e.B):
+        S = int(e.S[c])
+        up = e.seg_upto[c * (R + 1):(c + 1) * (R + 1)]
+        assert up[0] == 0 and np.all(np.diff(up.astype(np.int64)) >= 0)
+        for k in (1, 2, R):
+            rings = [ring0 + s * R + r for s in range(S) for r in range(k)]
+            used = np.unique(np.concatenate([ids[off[j]:off[j + 1]] for j in rings]))
+            new = inv[used] - line_off[c]
+            assert new.min() >= 0 and new.max() < up[k] and used.size == up[k]
+        ring0 += S * R
