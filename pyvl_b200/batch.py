@@ -38,7 +38,7 @@ WAKE_CASE = np.dtype({"names": ["P", "S", "n_cols", "ring_begin", "mat_begin", "
 SOLVE_CASE = np.dtype([("row_begin", "<u4"), ("n", "<u4"), ("mat_begin", "<u8")])
 
 SWEEP_TILES = [(128, 1), (128, 2), (128, 4), (256, 1), (256, 2)]
-RING_TILES = [4, 8, 16]
+RING_TILES = [8, 16, 32]
 
 
 def _check_layouts() -> None:
@@ -47,6 +47,30 @@ def _check_layouts() -> None:
         n = int(_lib.query(f"pvl_batch_{name}_bytes"))
         if n != dt.itemsize:
             raise RuntimeError(f"batch record {name}: library has {n} bytes, host layout {dt.itemsize}")
+
+
+def ring_tile_tables(offsets, surface_lines, n_rings, tile: int = 128):
+    """Column tiles of the ring jobs for pvl_batch_ring_matrix_tiled.  The CSR rows (rings) are
+    the jobs' rings back to back (job j owns n_rings[j] of them); each job's rings are cut into
+    tiles of `tile`.  Returns job_tile (first tile of each job), tile_offsets and tile_lines (the
+    distinct lines of every tile, ascending), sl_local (each CSR entry's position in its tile's
+    list) and the longest list."""
+    off = np.asarray(offsets, np.int64)
+    ids = (np.asarray(surface_lines, np.uint32) & np.uint32(0x7FFFFFFF)).astype(np.int64)
+    n_rings = np.asarray(n_rings, np.int64)
+    per_job = -(-n_rings // tile)
+    job_tile = np.concatenate([[0], np.cumsum(per_job)[:-1]]).astype(np.int64)
+    ring_job = np.repeat(np.arange(n_rings.size), n_rings)
+    ring_begin = np.concatenate([[0], np.cumsum(n_rings)[:-1]])
+    ring_tile = job_tile[ring_job] + (np.arange(ring_job.size) - ring_begin[ring_job]) // tile
+    entry_tile = np.repeat(ring_tile, np.diff(off))
+    base = int(ids.max()) + 1 if ids.size else 1
+    uniq, inv = np.unique(entry_tile * base + ids, return_inverse=True)
+    counts = np.bincount(uniq // base, minlength=int(per_job.sum()))
+    tile_off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    sl_local = inv.reshape(-1) - tile_off[entry_tile]
+    return (job_tile.astype(np.uint32), tile_off.astype(np.uint32), (uniq % base).astype(np.uint32),
+            sl_local.astype(np.uint32), int(counts.max()) if counts.size else 1)
 
 
 def _dev_records(arr: np.ndarray, dev) -> torch.Tensor:
@@ -89,7 +113,7 @@ class BatchEngine:
 
         self.static = bool(reuse_static_bodies) and all(isinstance(c.kinematics, Static) for c in self.cases)
         self.A_body = None
-        self.tile = dict(tile or {"sweep": (128, 2), "ring": 8})
+        self.tile = dict(tile or {"sweep": (128, 1), "ring": 16})
         dev = self.dev
         f64 = dict(dtype=torch.float64, device=dev)
 
@@ -207,6 +231,16 @@ class BatchEngine:
             "implicit": (S, shed_off[:-1], imp_off[:-1], S),
         }
         self.ring_tables: dict = {}
+        self.ring_tiles = {}  # per ring-job kind: column-tile tables (ring_tile_tables), host and device
+        for name, off_, sl_, n_ in (("body", self.body.surface_offsets, self.body.surface_lines, P),
+                                    ("implicit", self.row0_offsets, self.row0_lines, S)):
+            jt, toff, tl, sll, mx = ring_tile_tables(off_, sl_, n_)
+            self.ring_tiles[name] = {"job_tile": jt, "tile_offsets": toff, "tile_lines": tl, "sl_local": sll,
+                                     "max": mx}
+            if not host_only:
+                self.ring_tiles[name]["dev"] = {k: to_device_u32(v if v.size else np.zeros(1, np.uint32), dev)
+                                                for k, v in (("job_tile", jt), ("tile_offsets", toff),
+                                                             ("tile_lines", tl), ("sl_local", sll))}
 
         # sweep jobs: explicit wake term (points = control points, segments = the case's wake
         # lines) and advection (points = the case's distinct wake node columns, row by row)
@@ -302,9 +336,12 @@ class BatchEngine:
     # ------------------------------------------------------------------ pieces of a step
     def _ring(self, which: str, segs, off, sl, n_lines: int, out) -> None:
         jobs, items, n_items = self.ring_tables[which]
-        _lib.call("pvl_batch_ring_matrix", int(self.tile["ring"]), ptr(jobs), ptr(items), self.B, n_items,
-                  ptr(self.counter), ptr(off), ptr(sl), n_lines, ptr(segs), ptr(self.cps), ptr(self.nrm), self.tol,
-                  ptr(out), 0, stream_ptr())
+        t = self.ring_tiles[which]
+        td = t["dev"]
+        _lib.call("pvl_batch_ring_matrix_tiled", int(self.tile["ring"]), ptr(jobs), ptr(items), self.B, n_items,
+                  ptr(self.counter), ptr(off), ptr(sl), ptr(td["sl_local"]), ptr(td["job_tile"]),
+                  ptr(td["tile_offsets"]), ptr(td["tile_lines"]), t["max"], n_lines, ptr(segs), ptr(self.cps),
+                  ptr(self.nrm), self.tol, ptr(out), 0, stream_ptr())
 
     def _sweep(self, which: str, segs, pts, pidx, out) -> None:
         jobs, items, n_items, pt_item, n_total = self.sweep_tables[which]

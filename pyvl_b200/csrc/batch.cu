@@ -127,6 +127,82 @@ __global__ void __launch_bounds__(128) batched_ring_kernel(const RingJob* __rest
     }
 }
 
+// The same blocks with each line of a tile evaluated once per control point (as
+// pvl_induction_normal_tiled does for one mesh): work item (job, CPB control points, 128
+// rings); the tile's distinct lines (tile_lines[tile_off[t] ..], t = job_tile[job] + column
+// tile) are evaluated at the CTA's control points into shared memory, n_i . u_l(cp_i), and
+// each thread sums its ring's signed entries (sl_local: each CSR entry's position in its
+// tile's list), in CSR order.  Adjacent rings share lines, so a quad mesh needs ~0.57 line
+// evaluations per (point, ring line) instead of one.
+template <int CPB>
+__global__ void __launch_bounds__(128) batched_ring_tile_kernel(
+    const RingJob* __restrict__ jobs, const uint32_t* __restrict__ job_item, uint32_t n_jobs, uint32_t n_items,
+    uint32_t* __restrict__ counter, const uint32_t* __restrict__ off, const uint32_t* __restrict__ sl,
+    const uint32_t* __restrict__ sl_local, const uint32_t* __restrict__ job_tile,
+    const uint32_t* __restrict__ tile_off, const uint32_t* __restrict__ tile_lines, uint32_t tile_stride,
+    uint32_t n_lines, const Segment<double>* __restrict__ seg, const double* __restrict__ cps,
+    const double* __restrict__ nrm, double tol2, double* __restrict__ out)
+{
+    extern __shared__ double sV[];  // [CPB][tile_stride]
+    __shared__ uint32_t s_item;
+    __shared__ double s_p[CPB][3], s_n[CPB][3];
+    for (;;) {
+        if (threadIdx.x == 0)
+            s_item = atomicAdd(counter, 1u);
+        __syncthreads();
+        const uint32_t item = s_item;
+        if (item >= n_items)
+            return;
+        const uint32_t jb = find_job(job_item, n_jobs, item);
+        const RingJob J = jobs[jb];
+        const uint32_t col_tiles = (J.n_rings + 127) / 128;
+        const uint32_t local = item - J.item_begin;
+        const uint32_t rb = local / col_tiles, ct = local % col_tiles;
+        const uint32_t i0 = rb * CPB;
+        const int nq = (int)min((uint32_t)CPB, J.n_cp - i0);  // CTA-uniform, >= 1
+        if (threadIdx.x < CPB * 3) {
+            const uint32_t q = threadIdx.x / 3, c = threadIdx.x % 3;
+            const bool ok = (int)q < nq;
+            s_p[q][c] = ok ? cps[3 * (size_t)(J.cp_begin + i0 + q) + c] : 0.0;
+            s_n[q][c] = ok ? nrm[3 * (size_t)(J.cp_begin + i0 + q) + c] : 0.0;
+        }
+        __syncthreads();
+        const uint32_t t = job_tile[jb] + ct;
+        const uint32_t L0 = tile_off[t], nl = min(tile_off[t + 1] - L0, tile_stride);
+        for (uint32_t l = threadIdx.x; l < nl; l += 128) {
+            const uint32_t g = tile_lines[L0 + l];
+            Segment<double> sg;
+            if (g < n_lines) {
+                sg = seg[g];
+            } else {  // d = 0: nothing induced
+                sg.r1x = sg.r1y = sg.r1z = sg.dx = sg.dy = sg.dz = 0.0;
+                sg.len = sg.len2 = sg.gamma = sg.glen = sg.pad0 = sg.pad1 = 0.0;
+            }
+#pragma unroll 4
+            for (int q = 0; q < nq; ++q) {
+                Vec3<double> acc{0.0, 0.0, 0.0};
+                pvl::segment_induction(sg, s_p[q][0], s_p[q][1], s_p[q][2], tol2, 1.0, acc);
+                sV[q * tile_stride + l] = acc.x * s_n[q][0] + acc.y * s_n[q][1] + acc.z * s_n[q][2];
+            }
+        }
+        __syncthreads();
+        const uint32_t j = ct * 128 + threadIdx.x;
+        if (j < J.n_rings) {
+            const uint32_t r = J.ring_begin + j, k0 = off[r], k1 = off[r + 1];
+            for (int q = 0; q < nq; ++q) {
+                double v = 0.0;
+                for (uint32_t k = k0; k < k1; ++k) {
+                    const uint32_t e = sl_local[k];
+                    const double x = e < tile_stride ? sV[q * tile_stride + e] : 0.0;
+                    v += PVL_REV(sl[k]) ? -x : x;
+                }
+                out[J.out_begin + (size_t)(i0 + q) * J.ld + j] = v;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------------ sweep jobs
 template <int THREADS, int PPT>
 __global__ void __launch_bounds__(THREADS) batched_sweep_kernel(const SweepJob* __restrict__ jobs,
@@ -600,6 +676,35 @@ int launch_ring(const void* jobs, const uint32_t* job_item, uint32_t n_jobs, uin
     return PVL_OK;
 }
 
+template <int CPB>
+int launch_ring_tiled(const void* jobs, const uint32_t* job_item, uint32_t n_jobs, uint32_t n_items,
+                      uint32_t* counter, const uint32_t* off, const uint32_t* sl, const uint32_t* sl_local,
+                      const uint32_t* job_tile, const uint32_t* tile_off, const uint32_t* tile_lines,
+                      uint32_t tile_stride, uint32_t n_lines, const void* seg, const double* cps, const double* nrm,
+                      double tol, double* out, uint32_t n_ctas, cudaStream_t st)
+{
+    const size_t smem = (size_t)CPB * tile_stride * sizeof(double);
+    if (smem > 200 * 1024)
+        return pvl_fail(PVL_ERR_ARG, "pvl_batch_ring_matrix_tiled: %u lines in one tile x %d control points exceed "
+                        "shared memory", tile_stride, CPB);
+    const void* fn = (const void*)batched_ring_tile_kernel<CPB>;
+    PVL_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (n_ctas == 0) {
+        int dev = 0, sms = 0, per = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, 128, smem) != cudaSuccess)
+            return pvl_fail(PVL_ERR_CUDA, "pvl_batch_ring_matrix_tiled: occupancy query failed");
+        n_ctas = (uint32_t)std::max(1, sms * std::max(1, per));
+    }
+    batched_ring_tile_kernel<CPB><<<n_ctas, 128, smem, st>>>(
+        static_cast<const RingJob*>(jobs), job_item, n_jobs, n_items, counter, off, sl, sl_local, job_tile, tile_off,
+        tile_lines, tile_stride, n_lines, static_cast<const Segment<double>*>(seg), cps, nrm,
+        pvl::cutoff2<double>(tol), out);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
 template <int THREADS, int PPT>
 int launch_sweep(const void* jobs, const uint32_t* job_item, uint32_t n_jobs, uint32_t n_items, uint32_t* counter,
                  const uint32_t* rows, const uint32_t* seg_upto, uint32_t rows_max, const void* seg, const double* pts,
@@ -644,6 +749,37 @@ extern "C" int pvl_batch_ring_matrix(int cpb, const void* jobs, const uint32_t* 
     case 16: return launch_ring<16>(jobs, job_item, n_jobs, n_items, counter, offsets, surface_lines, n_lines,
                                     segments, cps, normals, tol, out, n_ctas, st);
     default: return pvl_fail(PVL_ERR_ARG, "pvl_batch_ring_matrix: control points per CTA must be 4, 8 or 16");
+    }
+}
+
+extern "C" int pvl_batch_ring_matrix_tiled(int cpb, const void* jobs, const uint32_t* job_item, uint32_t n_jobs,
+                                           uint32_t n_items, uint32_t* counter, const uint32_t* offsets,
+                                           const uint32_t* surface_lines, const uint32_t* sl_local,
+                                           const uint32_t* job_tile, const uint32_t* tile_offsets,
+                                           const uint32_t* tile_lines, uint32_t max_tile_lines, uint32_t n_lines,
+                                           const void* segments, const double* cps, const double* normals, double tol,
+                                           double* out, uint32_t n_ctas, void* stream)
+{
+    if (n_items == 0)
+        return PVL_OK;
+    if (!jobs || !job_item || !counter || !offsets || !surface_lines || !sl_local || !job_tile || !tile_offsets ||
+        !tile_lines || !segments || !cps || !normals || !out)
+        return pvl_fail(PVL_ERR_ARG, "pvl_batch_ring_matrix_tiled: null pointer argument");
+    if (max_tile_lines == 0)
+        return pvl_fail(PVL_ERR_ARG, "pvl_batch_ring_matrix_tiled: max_tile_lines is 0");
+    cudaStream_t st = (cudaStream_t)stream;
+    PVL_CUDA_CHECK(cudaMemsetAsync(counter, 0, sizeof(uint32_t), st));
+    switch (cpb) {
+#define PVL_RING_TILED(C)                                                                                           \
+    case C:                                                                                                         \
+        return launch_ring_tiled<C>(jobs, job_item, n_jobs, n_items, counter, offsets, surface_lines, sl_local,     \
+                                    job_tile, tile_offsets, tile_lines, max_tile_lines, n_lines, segments, cps,     \
+                                    normals, tol, out, n_ctas, st);
+        PVL_RING_TILED(8)
+        PVL_RING_TILED(16)
+        PVL_RING_TILED(32)
+#undef PVL_RING_TILED
+    default: return pvl_fail(PVL_ERR_ARG, "pvl_batch_ring_matrix_tiled: control points per CTA must be 8, 16 or 32");
     }
 }
 

@@ -170,3 +170,27 @@ def test_row_ordered_wake_lines(layout):
             new = inv[used] - line_off[c]
             assert new.min() >= 0 and new.max() < up[k] and used.size == up[k]
         ring0 += S * R
+
+
+def test_ring_tile_tables(layout):
+    """Column tiles of the tiled ring kernel: every tile lists exactly the distinct lines of its
+    (up to) 128 rings, every CSR entry points at its own line in its tile's list, and the
+    shared-memory stride covers the longest list."""
+    e, cases = layout
+    for name, off, sl, n_rings in (("body", e.body.surface_offsets, e.body.surface_lines, e.P),
+                                   ("implicit", e.row0_offsets, e.row0_lines, e.S)):
+        t = e.ring_tiles[name]
+        off = np.asarray(off, np.int64)
+        ids = np.asarray(sl, np.uint32) & 0x7FFFFFFF
+        toff, tl, sll = t["tile_offsets"].astype(np.int64), t["tile_lines"], t["sl_local"]
+        assert len(sll) == len(ids) and t["max"] == int(np.diff(toff).max())
+        r0 = 0
+        for j, n in enumerate(np.asarray(n_rings, np.int64)):
+            for ct in range(-(-int(n) // 128)):
+                tile = int(t["job_tile"][j]) + ct
+                a, b = off[r0 + ct * 128], off[r0 + min(ct * 128 + 128, int(n))]
+                lines = tl[toff[tile]:toff[tile + 1]]
+                assert np.array_equal(lines, np.unique(ids[a:b]))
+                assert np.array_equal(lines[sll[a:b]], ids[a:b])
+            r0 += int(n)
+        assert r0 == len(off) - 1

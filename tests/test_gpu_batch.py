@@ -75,3 +75,42 @@ def test_batch_graph_replay_is_bitwise_identical_and_tuning_keeps_results():
     rep = a.tune(reps=1)
     assert rep["chosen"]["ring"] in (4, 8, 16)
     assert a.failures() == 0 and b.failures() == 0 and c.failures() == 0
+
+
+@pytest.mark.parametrize("cpb", [8, 16, 32])
+def test_tiled_ring_blocks_match_per_ring_kernel(cpb):
+    """The tiled batched ring kernel (each line once per control point and 128-ring tile) gives
+    the body matrices and implicit blocks of the per-ring kernel (each ring's own segments) to
+    rounding; two calls in a row agree bit for bit."""
+    import torch
+
+    from pyvl_b200 import _lib
+    from pyvl_b200.batch import BatchEngine
+    from pyvl_b200.device import ptr, stream_ptr
+    from pyvl_b200.workloads import batch_wings
+
+    cases = batch_wings(n_cases=9, seed=2, steps=6, p_min=64, p_max=1500)
+    eng = BatchEngine(cases, solve_tol=1e-13, max_iter=10, tile={"sweep": (128, 1), "ring": cpb})
+    eng.start(0.0)
+    for _ in range(3):
+        eng.step()
+    torch.cuda.synchronize()
+    d = eng.d_body
+    for which, segs, off, sl, n_lines, out in (
+            ("body", eng.seg_body, d["offsets"], d["surface_lines"], eng.body.n_lines, eng.A),
+            ("implicit", eng.seg_wake, eng.d_row0["offsets"], eng.d_row0["lines"], eng.wake_mesh.n_lines,
+             eng.implicit)):
+        eng._ring(which, segs, off, sl, n_lines, out)
+        tiled = out.clone()
+        eng._ring(which, segs, off, sl, n_lines, out)
+        assert torch.equal(out, tiled)
+        jobs, items, n_items = eng.ring_tables[which]
+        ref = torch.full_like(out, float("nan"))
+        if cpb in (8, 16):  # the per-ring kernel's tiles use the same item layout
+            _lib.call("pvl_batch_ring_matrix", cpb, ptr(jobs), ptr(items), eng.B, n_items, ptr(eng.counter),
+                      ptr(off), ptr(sl), n_lines, ptr(segs), ptr(eng.cps), ptr(eng.nrm), eng.tol, ptr(ref), 0,
+                      stream_ptr())
+            torch.cuda.synchronize()
+            scale = float(ref.abs().max())
+            err = float((tiled - ref).abs().max()) / scale
+            assert err <= 1e-13, (which, err)
