@@ -472,13 +472,17 @@ int pvl_batch_ring_matrix(int cpb, const void* jobs, const uint32_t* job_item, u
  * point (the batched form of pvl_induction_normal_tiled): job_tile[j] = first tile of job j
  * (its column tiles are consecutive), tile_offsets / tile_lines = the tiles' distinct lines,
  * sl_local = each CSR entry's position in its tile's list, max_tile_lines = the longest list;
- * cpb = 8, 16 or 32 control points per CTA (shared memory cpb * max_tile_lines doubles). */
+ * cpb = 8, 16 or 32 control points per CTA (shared memory cpb * max_tile_lines doubles).
+ * fold_adj != NULL (implicit wake blocks): instead of storing entry (i, j), fold it into the
+ * case's matrix (out_begin, ld of the jobs = the matrix) as pvl_batch_fold_implicit does,
+ * A[i, adj[2r + 1]] -= v, A[i, adj[2r]] += v with r the ring's CSR row (its shedding line);
+ * only when no body ring is adjacent to two shedding-line sides of its case. */
 int pvl_batch_ring_matrix_tiled(int cpb, const void* jobs, const uint32_t* job_item, uint32_t n_jobs,
                                 uint32_t n_items, uint32_t* counter, const uint32_t* offsets,
                                 const uint32_t* surface_lines, const uint32_t* sl_local, const uint32_t* job_tile,
                                 const uint32_t* tile_offsets, const uint32_t* tile_lines, uint32_t max_tile_lines,
                                 uint32_t n_lines, const void* segments, const double* cps, const double* normals,
-                                double tol, double* out, uint32_t n_ctas, void* stream);
+                                double tol, const uint32_t* fold_adj, double* out, uint32_t n_ctas, void* stream);
 
 /* Segment sweeps of every job into per-job partials (FP64); tile = (threads, points per
  * thread) in {(128,1),(128,2),(128,4),(256,1),(256,2)}; rows: device uint32 (the step's row

@@ -97,7 +97,7 @@ SIGNATURES = {
     "pvl_prep_segments": (_I, [_I, _U, _U, _P, _P, _P, _D, _P, _P]),
     "pvl_batch_ring_matrix": (_I, [_I, _P, _P, _U, _U, _P, _P, _P, _U, _P, _P, _P, _D, _P, _U, _P]),
     "pvl_batch_ring_matrix_tiled": (_I, [_I, _P, _P, _U, _U, _P, _P, _P, _P, _P, _P, _P, _U, _U, _P, _P, _P, _D,
-                                         _P, _U, _P]),
+                                         _P, _P, _U, _P]),
     "pvl_batch_sweep": (_I, [_I, _I, _P, _P, _U, _U, _P, _P, _P, _U, _P, _P, _P, _D, _P, _U, _P]),
     "pvl_batch_sweep_reduce": (_I, [_P, _P, _U, _U, _P, _P, _P, _P, _P, _P]),
     "pvl_batch_fold_implicit": (_I, [_P, _P, _U, _P, _P, _P, _P]),

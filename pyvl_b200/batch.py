@@ -229,7 +229,12 @@ class BatchEngine:
         self._ring_job_args = {
             "body": (P, ring_off[:-1], mat_off[:-1], P),
             "implicit": (S, shed_off[:-1], imp_off[:-1], S),
+            "implicit_fold": (S, shed_off[:-1], mat_off[:-1], P),  # folded straight into the matrices
         }
+        # the implicit blocks can be folded by the ring kernel itself when no ring of a case is
+        # adjacent to two shedding-line sides (no two threads then update one matrix entry)
+        self.fold_in_ring = all(np.unique(a[a != 0x7FFFFFFF]).size == int((a != 0x7FFFFFFF).sum())
+                                for a in adj_all)
         self.ring_tables: dict = {}
         self.ring_tiles = {}  # per ring-job kind: column-tile tables (ring_tile_tables), host and device
         for name, off_, sl_, n_ in (("body", self.body.surface_offsets, self.body.surface_lines, P),
@@ -336,12 +341,13 @@ class BatchEngine:
     # ------------------------------------------------------------------ pieces of a step
     def _ring(self, which: str, segs, off, sl, n_lines: int, out) -> None:
         jobs, items, n_items = self.ring_tables[which]
-        t = self.ring_tiles[which]
+        t = self.ring_tiles["implicit" if which == "implicit_fold" else which]
         td = t["dev"]
         _lib.call("pvl_batch_ring_matrix_tiled", int(self.tile["ring"]), ptr(jobs), ptr(items), self.B, n_items,
                   ptr(self.counter), ptr(off), ptr(sl), ptr(td["sl_local"]), ptr(td["job_tile"]),
                   ptr(td["tile_offsets"]), ptr(td["tile_lines"]), t["max"], n_lines, ptr(segs), ptr(self.cps),
-                  ptr(self.nrm), self.tol, ptr(out), 0, stream_ptr())
+                  ptr(self.nrm), self.tol, ptr(self.adj) if which == "implicit_fold" else None, ptr(out), 0,
+                  stream_ptr())
 
     def _sweep(self, which: str, segs, pts, pidx, out) -> None:
         jobs, items, n_items, pt_item, n_total = self.sweep_tables[which]
@@ -378,10 +384,14 @@ class BatchEngine:
                   ptr(self.wcirc), self.R, ptr(self.wake_line_gamma), s)
         _lib.call("pvl_prep_segments", _lib.PVL_F64, self.n_wake_pts, self.wake_mesh.n_lines, ptr(w["lines"]),
                   ptr(wpos), ptr(self.wake_line_gamma), self.tol, ptr(self.seg_wake), s)
-        self._ring("implicit", self.seg_wake, self.d_row0["offsets"], self.d_row0["lines"], self.wake_mesh.n_lines,
-                   self.implicit)
-        _lib.call("pvl_batch_fold_implicit", ptr(self.wake_cases), ptr(self.row_case), self.n_rings,
-                  ptr(self.implicit), ptr(self.adj), ptr(self.A), s)
+        if self.fold_in_ring:
+            self._ring("implicit_fold", self.seg_wake, self.d_row0["offsets"], self.d_row0["lines"],
+                       self.wake_mesh.n_lines, self.A)
+        else:
+            self._ring("implicit", self.seg_wake, self.d_row0["offsets"], self.d_row0["lines"],
+                       self.wake_mesh.n_lines, self.implicit)
+            _lib.call("pvl_batch_fold_implicit", ptr(self.wake_cases), ptr(self.row_case), self.n_rings,
+                      ptr(self.implicit), ptr(self.adj), ptr(self.A), s)
         self._sweep("wake", self.seg_wake, self.cps, None, self.rhs)
 
     def _solve(self) -> None:

@@ -134,14 +134,19 @@ __global__ void __launch_bounds__(128) batched_ring_kernel(const RingJob* __rest
 // each thread sums its ring's signed entries (sl_local: each CSR entry's position in its
 // tile's list), in CSR order.  Adjacent rings share lines, so a quad mesh needs ~0.57 line
 // evaluations per (point, ring line) instead of one.
-template <int CPB>
+// FOLD (implicit wake blocks): the block is not stored; the value of control point i and
+// first-row ring j (shedding line shed = J.ring_begin + j) is folded straight into the case's
+// system matrix, A[i, adj[2 shed + 1]] -= v and A[i, adj[2 shed]] += v (out_begin / ld = the
+// matrix), the arithmetic of the fold kernel.  Only for cases in which every body ring is
+// adjacent to at most one shedding-line side, so that no two threads touch one entry.
+template <int CPB, bool FOLD>
 __global__ void __launch_bounds__(128) batched_ring_tile_kernel(
     const RingJob* __restrict__ jobs, const uint32_t* __restrict__ job_item, uint32_t n_jobs, uint32_t n_items,
     uint32_t* __restrict__ counter, const uint32_t* __restrict__ off, const uint32_t* __restrict__ sl,
     const uint32_t* __restrict__ sl_local, const uint32_t* __restrict__ job_tile,
     const uint32_t* __restrict__ tile_off, const uint32_t* __restrict__ tile_lines, uint32_t tile_stride,
     uint32_t n_lines, const Segment<double>* __restrict__ seg, const double* __restrict__ cps,
-    const double* __restrict__ nrm, double tol2, double* __restrict__ out)
+    const double* __restrict__ nrm, double tol2, const uint32_t* __restrict__ fold_adj, double* __restrict__ out)
 {
     extern __shared__ double sV[];  // [CPB][tile_stride]
     __shared__ uint32_t s_item;
@@ -196,7 +201,16 @@ __global__ void __launch_bounds__(128) batched_ring_tile_kernel(
                     const double x = e < tile_stride ? sV[q * tile_stride + e] : 0.0;
                     v += PVL_REV(sl[k]) ? -x : x;
                 }
-                out[J.out_begin + (size_t)(i0 + q) * J.ld + j] = v;
+                if (FOLD) {
+                    double* arow = out + J.out_begin + (size_t)(i0 + q) * J.ld;
+                    const uint32_t a1 = fold_adj[2 * (size_t)r + 1], a0 = fold_adj[2 * (size_t)r];
+                    if (a1 != PVL_INVALID && a1 < J.ld)
+                        arow[a1] -= v;
+                    if (a0 != PVL_INVALID && a0 < J.ld)
+                        arow[a0] += v;
+                } else {
+                    out[J.out_begin + (size_t)(i0 + q) * J.ld + j] = v;
+                }
             }
         }
         __syncthreads();
@@ -681,13 +695,14 @@ int launch_ring_tiled(const void* jobs, const uint32_t* job_item, uint32_t n_job
                       uint32_t* counter, const uint32_t* off, const uint32_t* sl, const uint32_t* sl_local,
                       const uint32_t* job_tile, const uint32_t* tile_off, const uint32_t* tile_lines,
                       uint32_t tile_stride, uint32_t n_lines, const void* seg, const double* cps, const double* nrm,
-                      double tol, double* out, uint32_t n_ctas, cudaStream_t st)
+                      double tol, const uint32_t* fold_adj, double* out, uint32_t n_ctas, cudaStream_t st)
 {
     const size_t smem = (size_t)CPB * tile_stride * sizeof(double);
     if (smem > 200 * 1024)
         return pvl_fail(PVL_ERR_ARG, "pvl_batch_ring_matrix_tiled: %u lines in one tile x %d control points exceed "
                         "shared memory", tile_stride, CPB);
-    const void* fn = (const void*)batched_ring_tile_kernel<CPB>;
+    const void* fn = fold_adj ? (const void*)batched_ring_tile_kernel<CPB, true>
+                              : (const void*)batched_ring_tile_kernel<CPB, false>;
     PVL_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (n_ctas == 0) {
         int dev = 0, sms = 0, per = 0;
@@ -697,10 +712,18 @@ int launch_ring_tiled(const void* jobs, const uint32_t* job_item, uint32_t n_job
             return pvl_fail(PVL_ERR_CUDA, "pvl_batch_ring_matrix_tiled: occupancy query failed");
         n_ctas = (uint32_t)std::max(1, sms * std::max(1, per));
     }
-    batched_ring_tile_kernel<CPB><<<n_ctas, 128, smem, st>>>(
-        static_cast<const RingJob*>(jobs), job_item, n_jobs, n_items, counter, off, sl, sl_local, job_tile, tile_off,
-        tile_lines, tile_stride, n_lines, static_cast<const Segment<double>*>(seg), cps, nrm,
-        pvl::cutoff2<double>(tol), out);
+    auto* J = static_cast<const RingJob*>(jobs);
+    auto* sg = static_cast<const Segment<double>*>(seg);
+    if (fold_adj)
+        batched_ring_tile_kernel<CPB, true><<<n_ctas, 128, smem, st>>>(J, job_item, n_jobs, n_items, counter, off, sl,
+                                                                        sl_local, job_tile, tile_off, tile_lines,
+                                                                        tile_stride, n_lines, sg, cps, nrm,
+                                                                        pvl::cutoff2<double>(tol), fold_adj, out);
+    else
+        batched_ring_tile_kernel<CPB, false><<<n_ctas, 128, smem, st>>>(J, job_item, n_jobs, n_items, counter, off,
+                                                                         sl, sl_local, job_tile, tile_off, tile_lines,
+                                                                         tile_stride, n_lines, sg, cps, nrm,
+                                                                         pvl::cutoff2<double>(tol), nullptr, out);
     PVL_LAUNCH_CHECK();
     return PVL_OK;
 }
@@ -758,7 +781,7 @@ extern "C" int pvl_batch_ring_matrix_tiled(int cpb, const void* jobs, const uint
                                            const uint32_t* job_tile, const uint32_t* tile_offsets,
                                            const uint32_t* tile_lines, uint32_t max_tile_lines, uint32_t n_lines,
                                            const void* segments, const double* cps, const double* normals, double tol,
-                                           double* out, uint32_t n_ctas, void* stream)
+                                           const uint32_t* fold_adj, double* out, uint32_t n_ctas, void* stream)
 {
     if (n_items == 0)
         return PVL_OK;
@@ -774,7 +797,7 @@ extern "C" int pvl_batch_ring_matrix_tiled(int cpb, const void* jobs, const uint
     case C:                                                                                                         \
         return launch_ring_tiled<C>(jobs, job_item, n_jobs, n_items, counter, offsets, surface_lines, sl_local,     \
                                     job_tile, tile_offsets, tile_lines, max_tile_lines, n_lines, segments, cps,     \
-                                    normals, tol, out, n_ctas, st);
+                                    normals, tol, fold_adj, out, n_ctas, st);
         PVL_RING_TILED(8)
         PVL_RING_TILED(16)
         PVL_RING_TILED(32)

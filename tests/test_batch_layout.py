@@ -25,7 +25,8 @@ def test_ring_jobs_cover_each_block_once(layout):
     e, cases = layout
     cpb = e.tile["ring"]
     for name, n_cols, csr_rows, out_size in (("body", e.P, e.n_rings, e.A.numel()),
-                                             ("implicit", e.S, len(e.row0_offsets) - 1, e.implicit.numel())):
+                                             ("implicit", e.S, len(e.row0_offsets) - 1, e.implicit.numel()),
+                                             ("implicit_fold", e.S, len(e.row0_offsets) - 1, e.A.numel())):
         jobs_t, items_t, n_items = e.ring_tables[name]
         jobs = _records(jobs_t, RING_JOB)
         items = items_t.numpy().view(np.uint32)

@@ -114,3 +114,35 @@ def test_tiled_ring_blocks_match_per_ring_kernel(cpb):
             scale = float(ref.abs().max())
             err = float((tiled - ref).abs().max()) / scale
             assert err <= 1e-13, (which, err)
+
+
+def test_implicit_fold_in_ring_kernel_matches_fold_kernel():
+    """Folding the implicit wake blocks inside the tiled ring kernel gives, bit for bit, the
+    matrices of the implicit block stored first and folded by pvl_batch_fold_implicit."""
+    import torch
+
+    from pyvl_b200 import _lib
+    from pyvl_b200.batch import BatchEngine
+    from pyvl_b200.device import ptr, stream_ptr
+    from pyvl_b200.workloads import batch_wings
+
+    cases = batch_wings(n_cases=9, seed=4, steps=6, p_min=64, p_max=1500)
+    eng = BatchEngine(cases, solve_tol=1e-13, max_iter=10)
+    assert eng.fold_in_ring
+    eng.start(0.0)
+    for _ in range(3):
+        eng.step()
+    torch.cuda.synchronize()
+    d = eng.d_body
+    body = lambda: eng._ring("body", eng.seg_body, d["offsets"], d["surface_lines"], eng.body.n_lines, eng.A)
+    row0 = (eng.d_row0["offsets"], eng.d_row0["lines"], eng.wake_mesh.n_lines)
+    body()
+    eng._ring("implicit_fold", eng.seg_wake, *row0, eng.A)
+    fused = eng.A.clone()
+    body()
+    eng._ring("implicit", eng.seg_wake, *row0, eng.implicit)
+    _lib.call("pvl_batch_fold_implicit", ptr(eng.wake_cases), ptr(eng.row_case), eng.n_rings, ptr(eng.implicit),
+              ptr(eng.adj), ptr(eng.A), stream_ptr())
+    torch.cuda.synchronize()
+    assert torch.equal(fused, eng.A)
+    assert float(eng.implicit.abs().max()) > 0.0
