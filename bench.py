@@ -60,8 +60,8 @@ def parse():
                     help="flapping: the deforming wing (headline); batch: 256 ragged wings x 50 steps; "
                          "swept: pitching swept wing, 200 steps; sphere: closed 5120-ring sphere")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile-kernel", choices=["line_sum", "advect_f32", "wake_term", "lu", "lu32", "mixed_step",
-                                                 "batch_step"],
+    ap.add_argument("--profile-kernel", choices=["line_sum", "advect_f32", "wake_term", "body", "gemv", "lu", "lu32",
+                                                 "mixed_step", "batch_step"],
                     default=None,
                     help="set up the workload, launch only that kernel family twice and exit (for ncu captures)")
     ap.add_argument("--fraction", type=int, default=16,
@@ -232,6 +232,19 @@ def profile_kernel(args) -> None:
             _lib.call("pvl_line_velocity", _lib.PVL_F64, rm.n_points, rm.n_lines, ptr(d["lines"]),
                       ptr(eng.wake_positions.reshape(-1, 3)), ptr(lg), eng.P, ptr(eng.cps), ptr(eng.nrm), case.tol,
                       1.0, 0.0, ptr(eng.rhs), ptr(eng.ws), eng._ws_bytes, stream_ptr())
+    elif args.profile_kernel == "body":  # the body matrix (tiled ring kernel)
+        for _ in range(2):
+            eng.assemble_body_only()
+    elif args.profile_kernel == "gemv":  # the solve's matrix-vector products on the benchmark system
+        eng.assemble()
+        n = eng.N
+        x = torch.randn(n, dtype=torch.float64, device="cuda")
+        x32 = x.float()
+        y = torch.zeros(n, dtype=torch.float64, device="cuda")
+        M32 = eng.A.float()
+        for _ in range(2):
+            _lib.call("pvl_gemv_f64", n, n, 1.0, ptr(eng.A), n, ptr(x), 0.0, ptr(y), stream_ptr())
+            _lib.call("pvl_gemv_f32", n, n, 1.0, ptr(M32), n, ptr(x32), 0.0, ptr(y), stream_ptr())
     elif args.profile_kernel == "lu":
         eng.assemble()
         A0 = eng.A.clone()
