@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(kRingThreads) ring_matrix_kernel(
 // tile's line list) in CSR order.  Adjacent rings share lines, so a structured wing needs
 // ~0.57 line evaluations per (point, ring line) instead of one.
 constexpr int kRingTile = 128;
-constexpr int kTileCPB = 16;
+constexpr int kTileCPB = 8;   // control points per CTA (8: 231 us, 16: 272 us on the 4096-ring body)
 
 __global__ void __launch_bounds__(kRingTile) ring_tile_kernel(uint32_t n_surfaces, const uint32_t* __restrict__ off,
                                                               const uint32_t* __restrict__ sl,
@@ -560,13 +560,14 @@ inline uint32_t sweep_points_per_cta(int precision) { return precision == PVL_F3
 
 // Number of segment ranges a sweep is split into: enough CTAs to fill the 148 SMs many times
 // over (FP64: 32 per SM, so that the last of the ~4 resident waves is short; FP32x2: 8 per SM),
-// at least two tiles of segments per range.
+// at least one tile of segments per range in FP64 (two in FP32).
 uint32_t sum_splits(uint32_t n_lines, uint32_t n_pts, int precision)
 {
     const uint64_t ctas_x = (n_pts + sweep_points_per_cta(precision) - 1) / sweep_points_per_cta(precision);
     const uint64_t want = 148ull * (precision == PVL_F32 ? 8 : 32);
     uint64_t s = (want + ctas_x - 1) / std::max<uint64_t>(ctas_x, 1);
-    const uint64_t max_s = std::max<uint64_t>(1, (n_lines + 2 * kSegTile - 1) / (2 * kSegTile));
+    const uint64_t min_range = precision == PVL_F32 ? 2 * kSegTile : kSegTile;
+    const uint64_t max_s = std::max<uint64_t>(1, (n_lines + min_range - 1) / min_range);
     s = std::min(std::max<uint64_t>(s, 1), max_s);
     return (uint32_t)std::min<uint64_t>(s, 65535);
 }
