@@ -542,6 +542,8 @@ def main() -> None:
         eng, warm = make(kind)
         for k in range(W):
             drive_step(eng, warm, times[k], dpos[k], dvel[k])
+        if hasattr(eng, "wait_refresh"):  # a preconditioner rebuild started in the warm-up ends in it
+            eng.wait_refresh()
         eng.check_status()
         n0 = len(getattr(eng, "stats", {}).get("gmres_iters", []))
         launches0 = _lib.lib().pvl_launch_count()

@@ -18,13 +18,24 @@ def require_cuda() -> torch.device:
     return torch.device("cuda", torch.cuda.current_device())
 
 
-def stream_ptr(stream: torch.cuda.Stream | None = None) -> ctypes.c_void_p:
-    s = stream if stream is not None else torch.cuda.current_stream()
-    return ctypes.c_void_p(s.cuda_stream)
+_raw_stream = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+_cur_device = getattr(torch._C, "_cuda_getDevice", None)
 
 
-def ptr(t: torch.Tensor | None) -> ctypes.c_void_p | None:
-    return None if t is None else ctypes.c_void_p(t.data_ptr())
+def stream_ptr(stream: torch.cuda.Stream | None = None) -> int:
+    """The stream handle as an integer for a void* argument (the current stream by default;
+    read through torch's raw-stream query, which costs far less per call than building a
+    Stream object: a step makes dozens of these calls)."""
+    if stream is not None:
+        return stream.cuda_stream
+    if _raw_stream is not None and _cur_device is not None:
+        return _raw_stream(_cur_device())
+    return torch.cuda.current_stream().cuda_stream
+
+
+def ptr(t: torch.Tensor | None) -> int | None:
+    """Device address of a tensor as an integer for a void* argument (None -> NULL)."""
+    return None if t is None else t.data_ptr()
 
 
 def to_device(a, dtype=torch.float64, device=None) -> torch.Tensor:

@@ -40,7 +40,7 @@ from .device import ptr, require_cuda, stream_ptr, to_device, to_device_u32
 # pvl_gmres_status (include/pvl_b200.h) and the number of solves whose status may be in flight
 _GMRES_STATUS = np.dtype([("iterations", "<u4"), ("converged", "<u4"), ("initial_rel_residual", "<f8"),
                           ("final_rel_residual", "<f8")])
-_STATUS_RING = 64
+_STATUS_RING = 4  # at most one record is pending when a solve is launched
 
 
 def wake_ring_connectivity(line_rows: int, n_shed: int, bordering_nodes=None) -> np.ndarray:
@@ -617,6 +617,12 @@ class MixedSolverEngine(SolverEngine):
         if self.refresh_done is not None and self.refresh_done.query():
             self._finish_refresh()
 
+    def wait_refresh(self) -> None:
+        """Make the current stream wait for a preconditioner rebuild still running on the side
+        stream and adopt it (e.g. at the end of a warm-up, so that a rebuild started there is
+        not timed as part of the steps that follow)."""
+        self._finish_refresh()
+
     def _finish_refresh(self) -> None:
         """Adopt a refresh still in flight, making the current stream wait for it."""
         if self.refresh_done is not None:
@@ -815,8 +821,9 @@ class MixedSolverEngine(SolverEngine):
         """The whole solve as one graph launch (pvl_gmres_graph_create): GMRES driven by the
         device to convergence, the FP64 fallback inside the graph; no host synchronisation.
         The status of each solve is read back later (``stats``); the host waits here for the
-        previous solve's record (long done while the GPU works through the wake update and this
-        step's assembly), so that the refresh policy sees every iteration count in time."""
+        previous solve's record (finished by the time the GPU works through the wake update and
+        this step's assembly, which are queued behind it), so that the refresh policy sees every
+        iteration count in time."""
         self._collect_status(block=True)
         self._maybe_refresh()
         if x0 is not None:
@@ -824,10 +831,6 @@ class MixedSolverEngine(SolverEngine):
         else:
             self.x[: self.P].copy_(self.gamma)  # the previous step's circulation
         self._ensure_graph()
-        while len(self._pending) >= _STATUS_RING:
-            slot, ev = self._pending[0]
-            ev.synchronize()
-            self._collect_status(block=False)
         _lib.call("pvl_gmres_graph_launch", self._graph, stream_ptr())
         slot = self._next_slot
         self._next_slot = (slot + 1) % _STATUS_RING

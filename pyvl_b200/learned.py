@@ -149,6 +149,12 @@ class WarmStart:
         self.record = record
         self.rec_X: list[torch.Tensor] = []
         self.rec_target: list[torch.Tensor] = []
+        if mlp is not None and not record:
+            # One inference on the (zero) buffers now: the forward kernel and the scaling are first
+            # needed only once three steps of history exist, and a kernel's first launch in a
+            # process loads its code (milliseconds) -- that belongs to the set-up, not to a step.
+            torch.mul(self.rnorm, 1.0, out=self.step_scale)
+            self.mlp.predict(self.X, self.base, self.seed, self.step_scale)
 
     def prepare(self) -> torch.Tensor | None:
         eng = self.eng
