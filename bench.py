@@ -19,7 +19,8 @@ Paths (both are timed; ``value`` is the one named by --path, default mixed):
 
 * ``value``: steps/s with each step's body positions/velocities already in HBM.
 * ``e2e``: steps/s through the public stepping API with positions/velocities copied from
-  pinned host memory and the circulations copied back every step.
+  pinned host memory and the circulations copied back every step (gamma_host_async: step k+1
+  is enqueued before step k's circulations are read, every copy inside the timed region).
 * ``roofline``: the dominant kernel (the FP64 segment sweep of the explicit wake term) timed
   live with CUDA events; 45 FLOP per segment-point pair (the reference kernel's arithmetic)
   against the FP64 FMA throughput measured live by pvl_fma_probe on the same GPU.
@@ -526,12 +527,18 @@ def main() -> None:
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
+        pending = None
         for k in range(first, first + count):
-            if host:
+            if host:  # host inputs in, the step's circulations out; step k+1 is enqueued before k is read
                 drive_step(eng, warm, times[k], hpos[k], hvel[k])
-                eng.gamma_host()
+                res = eng.gamma_host_async()
+                if pending is not None:
+                    pending.result()
+                pending = res
             else:
                 drive_step(eng, warm, times[k], dpos[k], dvel[k])
+        if pending is not None:
+            pending.result()
         e1.record()
         barrier()
         return max_over_ranks(e0.elapsed_time(e1))

@@ -41,6 +41,18 @@ from .device import ptr, require_cuda, stream_ptr, to_device, to_device_u32
 _GMRES_STATUS = np.dtype([("iterations", "<u4"), ("converged", "<u4"), ("initial_rel_residual", "<f8"),
                           ("final_rel_residual", "<f8")])
 _STATUS_RING = 4  # at most one record is pending when a solve is launched
+_HOST_RING = 4    # pinned result buffers of gamma_host_async
+
+
+class HostResult:
+    """A device-to-host copy in flight (SolverEngine.gamma_host_async)."""
+
+    def __init__(self, buf: torch.Tensor, event: torch.cuda.Event):
+        self._buf, self._event = buf, event
+
+    def result(self) -> np.ndarray:
+        self._event.synchronize()
+        return self._buf.numpy().copy()
 
 
 def wake_ring_connectivity(line_rows: int, n_shed: int, bordering_nodes=None) -> np.ndarray:
@@ -446,6 +458,22 @@ class SolverEngine:
         self.h_gamma.copy_(self.gamma, non_blocking=True)
         torch.cuda.current_stream().synchronize()
         return self.h_gamma.numpy().copy()
+
+    def gamma_host_async(self) -> "HostResult":
+        """Start copying this step's circulations to the host and return at once; the returned
+        object's ``result()`` waits for that copy only.  A caller can enqueue the next step
+        before reading this one, so the GPU does not idle while the host reads the result.
+        Results come from a small ring of pinned buffers: read each one before starting more
+        than ``_HOST_RING - 1`` further copies."""
+        if not hasattr(self, "_h_ring"):
+            self._h_ring = [torch.empty(self.P, dtype=torch.float64, pin_memory=True) for _ in range(_HOST_RING)]
+            self._h_next = 0
+        buf = self._h_ring[self._h_next]
+        self._h_next = (self._h_next + 1) % _HOST_RING
+        buf.copy_(self.gamma, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record()
+        return HostResult(buf, ev)
 
     def check_status(self) -> None:
         """Raise if the last solve reported a zero pivot or a timed-out wait."""
