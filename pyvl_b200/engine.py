@@ -493,11 +493,11 @@ class MixedSolverEngine(SolverEngine):
       the system (trailing updates and the triangular inversion's rank-64 updates on the
       tensor cores in TF32, pvl_lu32_factor / pvl_lu32_inverse), applied as one FP32
       matrix-vector product per iteration.  It is rebuilt (on a side stream while the steps go
-      on) when it has gone stale: at once when a solve needed ``refresh_on_iters``
-      iterations, or when the iterations above the best count since the last rebuild add up
-      to ``refresh_excess`` (a rebuild costs as much as a few hundred Krylov columns, so a
-      preconditioner that costs one extra column per step is kept for a while), and in any
-      case every ``refresh`` steps when that is set.  If GMRES has not reached ``gmres_tol``
+      on) when it has gone stale: at once when a solve needed ``refresh_on_iters`` iterations
+      and at least 3 more than the best count since the last rebuild, or when the iterations
+      above that best count add up to ``refresh_excess`` (a rebuild costs as much as a few
+      hundred Krylov columns, so a preconditioner that costs one extra column per step is kept
+      for a while), and in any case every ``refresh`` steps when that is set.  If GMRES has not reached ``gmres_tol``
       (relative residual) after ``max_iter`` iterations the step falls back to the plain FP64
       factorisation.
     * The explicit wake term runs in FP64 for the wake rows below ``near_rows`` and in FP32
@@ -514,7 +514,7 @@ class MixedSolverEngine(SolverEngine):
                  refresh: int | None = None, near_rows: int | None = None, advect_near_rows: int = 8,
                  gmres_tol: float = 1e-12, max_iter: int = 20, async_refresh: bool = True,
                  refresh_on_iters: int = 5, use_graphs: bool = True, wake_self_induction: bool = False,
-                 device_solve: bool = True, refresh_excess: int = 64):
+                 device_solve: bool = True, refresh_excess: int = 128):
         super().__init__(mesh, freestream, tol, wake, closed_groups, wake_self_induction)
         self.refresh = None if refresh is None else int(refresh)
         self.refresh_excess = int(refresh_excess)
@@ -785,11 +785,15 @@ class MixedSolverEngine(SolverEngine):
             self._iters_excess += k - self._iters_best
         self._iters_seen = len(its)
         idle = self.refresh_done is None
+        # a slow solve triggers a rebuild only when it is well above the best count since the
+        # last rebuild: a system whose iteration count just wanders (a growing wake) is left to
+        # the accumulated-excess rule, since a rebuild costs as much as hundreds of columns
+        slow = bool(its) and its[-1] >= self.refresh_on_iters and (
+            self._iters_best is None or its[-1] >= self._iters_best + 3)
         if not self.have_precond:
             self.refresh_preconditioner(wait=True)
         elif (self.refresh is not None and self.steps_since_refresh >= self.refresh) or (
-                idle and self.steps_since_refresh >= 2
-                and (its[-1] >= self.refresh_on_iters or self._iters_excess >= self.refresh_excess)):
+                idle and self.steps_since_refresh >= 2 and (slow or self._iters_excess >= self.refresh_excess)):
             self.refresh_preconditioner(wait=not self.async_refresh)
         self.steps_since_refresh += 1
 
