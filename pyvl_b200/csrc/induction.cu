@@ -559,12 +559,12 @@ int prep_segments(uint32_t n_points, uint32_t n_lines, const uint32_t* lines, co
 inline uint32_t sweep_points_per_cta(int precision) { return precision == PVL_F32 ? 2 * kSumThreads : kSumThreads; }
 
 // Number of segment ranges a sweep is split into: enough CTAs to fill the 148 SMs many times
-// over (FP64: 32 per SM, so that the last of the ~4 resident waves is short; FP32x2: 8 per SM),
-// at least one tile of segments per range in FP64 (two in FP32).
+// over (32 per SM, so that the last resident wave is short), at least one tile of segments per
+// range in FP64 (two in FP32).
 uint32_t sum_splits(uint32_t n_lines, uint32_t n_pts, int precision)
 {
     const uint64_t ctas_x = (n_pts + sweep_points_per_cta(precision) - 1) / sweep_points_per_cta(precision);
-    const uint64_t want = 148ull * (precision == PVL_F32 ? 8 : 32);
+    const uint64_t want = 148ull * 32;
     uint64_t s = (want + ctas_x - 1) / std::max<uint64_t>(ctas_x, 1);
     const uint64_t min_range = precision == PVL_F32 ? 2 * kSegTile : kSegTile;
     const uint64_t max_s = std::max<uint64_t>(1, (n_lines + min_range - 1) / min_range);
