@@ -553,10 +553,11 @@ def main() -> None:
             eng.wait_refresh()
         eng.check_status()
         n0 = len(getattr(eng, "stats", {}).get("gmres_iters", []))
-        launches0 = _lib.lib().pvl_launch_count()
+        launches0 = _lib.lib().pvl_launch_count() + eng.replayed_kernels
         ms = timed(eng, warm, W, K, host=False)
         getattr(eng, "stats", None)  # the mixed engine counts its solves' Krylov columns as their status arrives
-        launches = _lib.lib().pvl_launch_count() - launches0
+        # this library's kernels: direct launches plus those run by replays of captured step pieces
+        launches = _lib.lib().pvl_launch_count() + eng.replayed_kernels - launches0
         ms_e2e = timed(eng, warm, W + K, K, host=True)
         eng.check_status()
         rec = {"ms": ms, "ms_e2e": ms_e2e, "launches": launches}

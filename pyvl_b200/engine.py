@@ -167,6 +167,11 @@ class SolverEngine:
         self.m = len(self.groups)
         self.N = self.P + self.m
         self.iteration = 0
+        # pieces of a step that touch only fixed buffers run as CUDA graphs captured on first use
+        # (one replay instead of a launch per kernel from Python)
+        self.capture_steps = True
+        self._step_graphs: dict = {}
+        self.replayed_kernels = 0  # this library's kernels run by those replays
         f64 = dict(dtype=torch.float64, device=self.dev)
         d = mesh.device_arrays()
         self.d_body = d
@@ -310,9 +315,35 @@ class SolverEngine:
             self._h2d_done = torch.cuda.Event()
             self._h2d_done.record()
 
+    def captured(self, key, fn, store: dict | None = None) -> None:
+        """Run ``fn`` (launches on fixed buffers only, no host reads) as the CUDA graph captured
+        under ``key`` on its first use (kept in ``store``, by default the engine's own table);
+        directly when ``capture_steps`` is off."""
+        if not self.capture_steps:
+            fn()
+            return
+        graphs = self._step_graphs if store is None else store
+        entry = graphs.get(key)
+        if entry is None:
+            n0 = _lib.lib().pvl_launch_count()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                fn()
+            entry = (g, int(_lib.lib().pvl_launch_count() - n0))
+            graphs[key] = entry
+        entry[0].replay()
+        self.replayed_kernels += entry[1]
+
     def assemble_body_only(self, buf: dict | None = None) -> None:
         """Control points, normals, RHS for a uniform stream and the body matrix (into ``buf``,
-        a set of pos/vel/cps/cpv/nrm/rhs/A/ws buffers, or the engine's own)."""
+        a set of pos/vel/cps/cpv/nrm/rhs/A/ws buffers, or the engine's own: then as one
+        captured graph)."""
+        if buf is None:
+            self.captured("body", lambda: self._assemble_body(None))
+        else:
+            self._assemble_body(buf)
+
+    def _assemble_body(self, buf: dict | None) -> None:
         s = stream_ptr()
         d, P = self.d_body, self.P
         msh = self.mesh

@@ -147,6 +147,7 @@ class WarmStart:
         self.ready = False
         self.have_base = False
         self.record = record
+        self._graphs: dict = {}  # captured prepare / finish pieces (SolverEngine.captured)
         self.rec_X: list[torch.Tensor] = []
         self.rec_target: list[torch.Tensor] = []
         if mlp is not None and not record:
@@ -158,12 +159,23 @@ class WarmStart:
 
     def prepare(self) -> torch.Tensor | None:
         eng = self.eng
-        P = eng.P
-        self.rhs_cur.copy_(eng.rhs[:P])
         self.have_base = self.n_hist >= 1
         self.ready = self.n_hist >= 3  # g1, rem0 and rem1 hold real history
-        if not self.have_base:
-            return None
+        infer = self.have_base and self.mlp is not None and not self.record and self.ready
+        run = lambda: self._prepare_ops(self.have_base, infer)
+        if self.record:
+            run()
+        else:  # fixed buffers: one captured graph per state (engine.captured)
+            scale = self.mlp.out_scale if infer else 0.0  # a host value the graph keeps
+            eng.captured(("prepare", self.have_base, infer, scale), run, self._graphs)
+        return self.seed if infer else None
+
+    def _prepare_ops(self, have_base: bool, infer: bool) -> None:
+        eng = self.eng
+        P = eng.P
+        self.rhs_cur.copy_(eng.rhs[:P])
+        if not have_base:
+            return
         s = stream_ptr()
         g0, g1 = self.hist
         self.resid.copy_(self.rhs_cur)
@@ -172,13 +184,11 @@ class WarmStart:
         mean, inv = (self.mlp.mean, self.mlp.inv_std) if self.mlp is not None and not self.record else \
             (self.raw_mean, self.raw_inv)
         _lib.call("pvl_mlp_features", P, ptr(g0), ptr(g1), ptr(self.rem[0]), ptr(self.rem[1]), ptr(self.resid),
-                  ptr(self.rnorm), ptr(eng.A), eng.N, ptr(self.rhs_cur), ptr(self.rhs_prev), ptr(eng.nrm), ptr(eng.cpv), ptr(mean),
-                  ptr(inv), ptr(self.X), ptr(self.base), s)
-        if self.mlp is None or self.record or not self.ready:
-            return None
-        torch.mul(self.rnorm, 1.0 / float(np.sqrt(P)), out=self.step_scale)
-        self.mlp.predict(self.X, self.base, self.seed, self.step_scale)
-        return self.seed
+                  ptr(self.rnorm), ptr(eng.A), eng.N, ptr(self.rhs_cur), ptr(self.rhs_prev), ptr(eng.nrm), ptr(eng.cpv),
+                  ptr(mean), ptr(inv), ptr(self.X), ptr(self.base), s)
+        if infer:
+            torch.mul(self.rnorm, 1.0 / float(np.sqrt(P)), out=self.step_scale)
+            self.mlp.predict(self.X, self.base, self.seed, self.step_scale)
 
     def finish(self) -> None:
         eng = self.eng
@@ -186,17 +196,26 @@ class WarmStart:
             s = torch.clamp(self.rnorm / float(np.sqrt(eng.P)), min=1e-300)
             self.rec_X.append(self.X.clone())
             self.rec_target.append((eng.gamma - self.base) / s)
+        have_base = self.have_base
+        run = lambda: self._finish_ops(have_base)
+        if self.record:
+            run()
+        else:
+            eng.captured(("finish", have_base), run, self._graphs)
+        self.n_hist += 1
+
+    def _finish_ops(self, have_base: bool) -> None:
+        eng = self.eng
         g0, g1 = self.hist
         r0, r1 = self.rem
         r1.copy_(r0)
-        if self.have_base:
+        if have_base:
             torch.sub(eng.gamma, self.base, out=r0)
         else:
             r0.zero_()
         g1.copy_(g0)
         g0.copy_(eng.gamma)
         self.rhs_prev.copy_(self.rhs_cur)
-        self.n_hist += 1
 
     def training_data(self) -> tuple[torch.Tensor, torch.Tensor]:
         """Raw inputs (n, 12) and raw targets gamma - base (n,) of the recorded steps."""
