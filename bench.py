@@ -617,6 +617,58 @@ def main() -> None:
     p1.record()
     torch.cuda.synchronize()
     peak = flops / (p0.elapsed_time(p1) * 1e-3) / 1e12
+
+    def time_call(name, args, reps=5):
+        for _ in range(2):
+            _lib.call(name, *args)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            _lib.call(name, *args)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    # secondary rooflines: the FP32x2 advection sweep against the FP32 FMA peak, the body
+    # matrix against the FP64 peak and the HBM write bandwidth
+    S, R, L = w["S"], w["R"], mesh.n_lines
+    r_near = eng.advect_near_rows
+    eng.body_line_gamma.fill_(1e-2)
+    ams = time_call("pvl_wake_node_velocity_cols", (
+        _lib.PVL_F32, mesh.n_points, L, ptr(eng.d_body["lines"]), ptr(eng.pos), ptr(eng.body_line_gamma), S, R, R,
+        r_near, R, w["n_cols"], ptr(w["cols"]), ptr(eng.wake_positions), 1.0, 0.0, 0.0, case.tol,
+        ptr(w["node_vel"]), ptr(eng.ws), eng._ws_bytes, stream_ptr()))
+    a_pairs = L * w["n_cols"] * (R - r_near)
+    sink32 = torch.zeros(148 * 8, dtype=torch.float32, device="cuda")
+    _lib.lib().pvl_fma_probe(_lib.PVL_F32, 148 * 8, 2000, ptr(sink32), stream_ptr())
+    torch.cuda.synchronize()
+    p0.record()
+    flops32 = _lib.lib().pvl_fma_probe(_lib.PVL_F32, 148 * 8, 20000, ptr(sink32), stream_ptr())
+    p1.record()
+    torch.cuda.synchronize()
+    peak32 = flops32 / (p0.elapsed_time(p1) * 1e-3) / 1e12
+    db = eng.d_body
+    bms = time_call("pvl_induction_normal_tiled", (
+        mesh.n_points, L, ptr(db["lines"]), ptr(eng.pos), eng.P, ptr(db["offsets"]), ptr(db["surface_lines"]),
+        ptr(db["tile_offsets"]), ptr(db["tile_lines"]), ptr(db["sl_local"]), db["tile_max"], eng.P, ptr(eng.cps),
+        ptr(eng.nrm), case.tol, ptr(eng.A), eng.N, ptr(eng.ws), eng._ws_bytes, stream_ptr()))
+    b_pairs = eng.P * int(mesh.ring_tiles()[1].size)  # (control point, distinct tile line) pairs
+    hbm_peak = None
+    mp = ROOT / "MEASURED_PEAKS.json"
+    if mp.exists():
+        hbm_peak = json.loads(mp.read_text()).get("hbm_gbs")
+    secondary = {
+        "advection_fp32x2": {"kernel": "line_sum_f32x2_kernel (wake rows %d..%d)" % (r_near, R - 1),
+                             "ms_per_call": ams, "pairs": a_pairs,
+                             "achieved": a_pairs * PAIR_FLOPS / (ams * 1e-3) / 1e12, "peak": peak32,
+                             "unit": "TFLOP/s", "frac": a_pairs * PAIR_FLOPS / (ams * 1e-3) / 1e12 / peak32,
+                             "peak_source": "FP32 FMA throughput measured live (pvl_fma_probe)"},
+        "body_matrix": {"kernel": "ring_tile_kernel", "ms_per_call": bms, "pairs": b_pairs,
+                        "achieved": b_pairs * PAIR_FLOPS / (bms * 1e-3) / 1e12, "peak": peak, "unit": "TFLOP/s",
+                        "frac": b_pairs * PAIR_FLOPS / (bms * 1e-3) / 1e12 / peak,
+                        "hbm_write_gbs": 8.0 * eng.P * eng.P / (bms * 1e-3) / 1e9, "hbm_peak_gbs": hbm_peak},
+    }
     del eng
     traffic = None
     prof = ROOT / "profiles" / "line_sum_f64_flapping_wake_term.md"
@@ -664,7 +716,9 @@ def main() -> None:
             "roofline": {"bound": "fp64", "kernel": "line_sum_f64_kernel (explicit wake term)",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "traffic": traffic, "ms_per_launch": kms, "pairs_per_launch": pairs,
-                         "peak_source": "FP64 FMA throughput measured live (pvl_fma_probe); 45 FLOP per pair"},
+                         "peak_source": "FP64 FMA throughput measured live (pvl_fma_probe); 45 FLOP per pair",
+                         "timed": "pvl_line_velocity: segment table, the sweep and the partial-sum reduction"},
+            "rooflines_secondary": secondary,
             "cpu_baseline": base,
             "gpu_launches": int(head["launches"]),
             "clocks": clocks,
