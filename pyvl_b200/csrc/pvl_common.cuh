@@ -48,8 +48,9 @@ template <typename T> struct Vec3 { T x, y, z; };
 //   atan(z) = z (1 - w/3 + w^2/5 - w^3/7 + ...),  w = z^2,
 // gives ang / h = -(len / x) S(w) with w = h^2 len^2 / x^2 -- no square root and no atan2.
 // The series is used only for w <= kW, where the first omitted term bounds the relative
-// truncation error: double, 8 terms for w <= 0.01 (0.01^8 / 17 < 1e-17) and 5 terms for
-// w <= 1e-4 (1e-20 / 11 < 1e-21); float, 6 terms for w <= 0.04 (0.04^6 / 13 < 4e-10).
+// truncation error: double, 16 terms for w <= 0.1 (0.1^16 / 33 < 4e-18), 8 terms for
+// w <= 0.01 (0.01^8 / 17 < 1e-17) and 5 terms for w <= 1e-4 (1e-20 / 11 < 1e-21); float,
+// 6 terms for w <= 0.04 (0.04^6 / 13 < 4e-10).
 // Closer pairs (larger w, or x <= 0) take the atan2 form.
 // Comparisons of non-negative values (or +NaN) through their bit patterns: for IEEE numbers of
 // one sign, the order of the bit patterns is the order of the values, and the integer compare
@@ -65,7 +66,7 @@ __device__ __forceinline__ bool pos(float x) { return x > 0.0f; }
 
 template <typename T> struct FarSeries;
 template <> struct FarSeries<double> {
-    static constexpr double kW = 0.01;
+    static constexpr double kW = 0.1;
     // 1/x by Newton-Raphson refinement, r <- r + r (1 - x r), of the hardware's approximate
     // reciprocal (rcp.approx.ftz.f64, a seed good to ~2^-22): two steps reach full double
     // precision (the relative error squares each step), within an ulp of the rounded quotient.
@@ -85,8 +86,21 @@ template <> struct FarSeries<double> {
         double s;
         if (le_nn(w, 1e-4)) {  // most pairs of a wake sweep: the five-term series is exact to 1e-21
             s = 1.0 / 9.0;
-        } else {
+        } else if (le_nn(w, 0.01)) {  // eight terms: 0.01^8 / 17 < 1e-17
             s = -1.0 / 15.0;
+            s = fma(s, w, 1.0 / 13.0);
+            s = fma(s, w, -1.0 / 11.0);
+            s = fma(s, w, 1.0 / 9.0);
+        } else {  // sixteen terms for w <= 0.1: 0.1^16 / 33 < 4e-18 (pairs 3 to 10 lengths away)
+            s = -1.0 / 31.0;
+            s = fma(s, w, 1.0 / 29.0);
+            s = fma(s, w, -1.0 / 27.0);
+            s = fma(s, w, 1.0 / 25.0);
+            s = fma(s, w, -1.0 / 23.0);
+            s = fma(s, w, 1.0 / 21.0);
+            s = fma(s, w, -1.0 / 19.0);
+            s = fma(s, w, 1.0 / 17.0);
+            s = fma(s, w, -1.0 / 15.0);
             s = fma(s, w, 1.0 / 13.0);
             s = fma(s, w, -1.0 / 11.0);
             s = fma(s, w, 1.0 / 9.0);
