@@ -193,14 +193,11 @@ __global__ void __launch_bounds__(128) batched_ring_tile_kernel(
         __syncthreads();
         const uint32_t j = ct * 128 + threadIdx.x;
         if (j < J.n_rings) {
-            const uint32_t r = J.ring_begin + j, k0 = off[r], k1 = off[r + 1];
+            const uint32_t r = J.ring_begin + j;
+            pvl::RingEntries re;
+            re.load(sl, sl_local, off[r], off[r + 1]);
             for (int q = 0; q < nq; ++q) {
-                double v = 0.0;
-                for (uint32_t k = k0; k < k1; ++k) {
-                    const uint32_t e = sl_local[k];
-                    const double x = e < tile_stride ? sV[q * tile_stride + e] : 0.0;
-                    v += PVL_REV(sl[k]) ? -x : x;
-                }
+                const double v = re.sum(sV + q * tile_stride, tile_stride, sl, sl_local);
                 if (FOLD) {
                     double* arow = out + J.out_begin + (size_t)(i0 + q) * J.ld;
                     const uint32_t a1 = fold_adj[2 * (size_t)r + 1], a0 = fold_adj[2 * (size_t)r];

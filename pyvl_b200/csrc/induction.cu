@@ -164,16 +164,12 @@ __global__ void __launch_bounds__(kRingTile) ring_tile_kernel(uint32_t n_surface
     const uint32_t j = tile * kRingTile + threadIdx.x;
     if (j >= n_surfaces)
         return;
-    const uint32_t k0 = off[j], k1 = off[j + 1];
+    pvl::RingEntries re;
+    re.load(sl, sl_local, off[j], off[j + 1]);
     for (int q = 0; q < kTileCPB; ++q) {
         if (i0 + q >= n_cp)
             break;
-        double v = 0.0;
-        for (uint32_t k = k0; k < k1; ++k) {
-            const double x = sV[q * tile_stride + sl_local[k]];
-            v += PVL_REV(sl[k]) ? -x : x;
-        }
-        out[(size_t)(i0 + q) * ld + j] = v;
+        out[(size_t)(i0 + q) * ld + j] = re.sum(sV + q * tile_stride, tile_stride, sl, sl_local);
     }
 }
 

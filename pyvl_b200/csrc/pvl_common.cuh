@@ -225,6 +225,52 @@ struct RingSegments {
     }
 };
 
+// The signed entries of one ring in its tile's line list (tiled ring kernels), held in
+// registers for rings of up to kMax lines (quads and triangles), so that summing the ring at
+// every control point of a CTA reads its CSR entries once; larger rings read them per point.
+// sum() adds +-row[e] in CSR order (the reference's order); an entry at or past `stride` adds 0.
+struct RingEntries {
+    static constexpr int kMax = 4;
+    uint32_t e[kMax];
+    bool neg[kMax];
+    uint32_t k0, k1;
+
+    __device__ __forceinline__ void load(const uint32_t* __restrict__ sl, const uint32_t* __restrict__ sl_local,
+                                         uint32_t k0_, uint32_t k1_)
+    {
+        k0 = k0_;
+        k1 = k1_;
+#pragma unroll
+        for (int u = 0; u < kMax; ++u) {
+            const bool ok = k1 - k0 <= (uint32_t)kMax && k0 + u < k1;
+            e[u] = ok ? sl_local[k0 + u] : 0u;
+            neg[u] = ok ? PVL_REV(sl[k0 + u]) != 0 : false;
+        }
+    }
+
+    __device__ __forceinline__ double sum(const double* __restrict__ row, uint32_t stride,
+                                          const uint32_t* __restrict__ sl, const uint32_t* __restrict__ sl_local) const
+    {
+        double v = 0.0;
+        if (k1 - k0 <= (uint32_t)kMax) {
+#pragma unroll
+            for (int u = 0; u < kMax; ++u) {
+                if (k0 + u < k1) {
+                    const double x = e[u] < stride ? row[e[u]] : 0.0;
+                    v += neg[u] ? -x : x;
+                }
+            }
+        } else {
+            for (uint32_t k = k0; k < k1; ++k) {
+                const uint32_t ek = sl_local[k];
+                const double x = ek < stride ? row[ek] : 0.0;
+                v += PVL_REV(sl[k]) ? -x : x;
+            }
+        }
+        return v;
+    }
+};
+
 }  // namespace pvl
 
 #define PVL_CUDA_CHECK(expr)                                                                   \
