@@ -22,6 +22,8 @@ using pvl::Vec3;
 namespace {
 
 constexpr int kSegTile = 128;   // segments per shared-memory tile
+constexpr int kReducePts = 32;    // points per CTA of the partial-sum reduction
+constexpr int kReduceGroups = 8;  // rows of threads (split groups) per CTA
 constexpr int kSumThreads = 128;
 constexpr int kRingThreads = 128;
 constexpr int kRingCPB = 8;     // control points per CTA row-block in ring matrices
@@ -372,22 +374,38 @@ __global__ void __launch_bounds__(kSumThreads) line_sum_f32x2_kernel(const Segme
 // Point p is written at o = (p / group) * out_stride + p % group + out_off (normals are
 // indexed by p: normal output is always a plain array).
 template <typename T>
-__global__ void reduce_partials_kernel(uint32_t n_pts, uint32_t n_split, const T* __restrict__ partial,
-                                       const double* __restrict__ normals, double alpha, double beta, double ux,
-                                       double uy, double uz, uint32_t group, uint32_t out_stride, uint32_t out_off,
-                                       double* __restrict__ out)
+__global__ void __launch_bounds__(kReducePts * kReduceGroups) reduce_partials_kernel(
+    uint32_t n_pts, uint32_t n_split, const T* __restrict__ partial, const double* __restrict__ normals, double alpha,
+    double beta, double ux, double uy, double uz, uint32_t group, uint32_t out_stride, uint32_t out_off,
+    double* __restrict__ out)
 {
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n_pts)
-        return;
-    const size_t op = (size_t)(p / group) * out_stride + p % group + out_off;
+    // kReducePts consecutive points per CTA (their partials are contiguous for every split, so a
+    // row of threads reads them coalesced); kReduceGroups rows of threads take every
+    // kReduceGroups-th split, and the rows' sums are added in row order (deterministic).
+    __shared__ double s_v[kReduceGroups][kReducePts][3];
+    const uint32_t tx = threadIdx.x % kReducePts, ty = threadIdx.x / kReducePts;
+    const uint32_t p = blockIdx.x * kReducePts + tx;
     double vx = 0, vy = 0, vz = 0;
-    for (uint32_t s = 0; s < n_split; ++s) {
-        const T* q = partial + 3 * ((size_t)s * n_pts + p);
-        vx += double(q[0]);
-        vy += double(q[1]);
-        vz += double(q[2]);
+    if (p < n_pts) {
+        for (uint32_t s = ty; s < n_split; s += kReduceGroups) {
+            const T* q = partial + 3 * ((size_t)s * n_pts + p);
+            vx += double(q[0]);
+            vy += double(q[1]);
+            vz += double(q[2]);
+        }
     }
+    s_v[ty][tx][0] = vx;
+    s_v[ty][tx][1] = vy;
+    s_v[ty][tx][2] = vz;
+    __syncthreads();
+    if (ty != 0 || p >= n_pts)
+        return;
+    for (int g = 1; g < kReduceGroups; ++g) {
+        vx += s_v[g][tx][0];
+        vy += s_v[g][tx][1];
+        vz += s_v[g][tx][2];
+    }
+    const size_t op = (size_t)(p / group) * out_stride + p % group + out_off;
     if (normals) {
         const double v = vx * normals[3 * (size_t)p] + vy * normals[3 * (size_t)p + 1] + vz * normals[3 * (size_t)p + 2];
         out[p] = beta == 0.0 ? alpha * v : beta * out[p] + alpha * v;
@@ -782,9 +800,8 @@ int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint3
     if (precision != PVL_F64 && precision != PVL_F32)
         return pvl_fail(PVL_ERR_ARG, "%s: unknown precision %d", who, precision);
     if (n_lines == 0) {
-        reduce_partials_kernel<double><<<blocks_for(n_pts, 256), 256, 0, st>>>(n_pts, 0, nullptr, normals, alpha,
-                                                                               beta, ux, uy, uz, group, out_stride,
-                                                                               out_off, out);
+        reduce_partials_kernel<double><<<blocks_for(n_pts, kReducePts), kReducePts * kReduceGroups, 0, st>>>(
+            n_pts, 0, nullptr, normals, alpha, beta, ux, uy, uz, group, out_stride, out_off, out);
         PVL_LAUNCH_CHECK();
         return PVL_OK;
     }
@@ -806,7 +823,7 @@ int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint3
         line_sum_f64_kernel<<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off, cols,
                                                           col_limit, pvl::cutoff2<double>(tol), part);
         PVL_LAUNCH_CHECK();
-        reduce_partials_kernel<double><<<blocks_for(n_pts, 256), 256, 0, st>>>(
+        reduce_partials_kernel<double><<<blocks_for(n_pts, kReducePts), kReducePts * kReduceGroups, 0, st>>>(
             n_pts, n_split_used, part, normals, alpha, beta, ux, uy, uz, group, out_stride, out_off, out);
     } else {
         auto* seg = reinterpret_cast<Segment<float>*>(base);
@@ -816,7 +833,7 @@ int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint3
         line_sum_f32x2_kernel<<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off,
                                                                cols, col_limit, pvl::cutoff2<float>(tol), part);
         PVL_LAUNCH_CHECK();
-        reduce_partials_kernel<float><<<blocks_for(n_pts, 256), 256, 0, st>>>(
+        reduce_partials_kernel<float><<<blocks_for(n_pts, kReducePts), kReducePts * kReduceGroups, 0, st>>>(
             n_pts, n_split_used, part, normals, alpha, beta, ux, uy, uz, group, out_stride, out_off, out);
     }
     PVL_LAUNCH_CHECK();
