@@ -331,9 +331,9 @@ int pvl_gemv_f32(uint32_t rows, uint32_t cols, double alpha, const float* M, uin
 /* Outcome of one solve of the GMRES graph, written by the device. */
 typedef struct pvl_gmres_status {
     uint32_t iterations;          /* Krylov columns used */
-    uint32_t converged;           /* 1: the true FP64 residual met tol; 0: the FP64 fallback ran */
+    uint32_t converged;           /* 1: the final FP64 residual met tol; 0: the FP64 fallback ran */
     double initial_rel_residual;  /* ||b - A x0|| / ||b|| */
-    double final_rel_residual;    /* ||b - A x|| / ||b|| before any fallback */
+    double final_rel_residual;    /* ||r0 - sum_j y_j A z_j|| / ||b|| (= ||b - A x||) before any fallback */
 } pvl_gmres_status;
 
 /* Bytes of the device control block (8-byte aligned) and the largest max_iter. */
@@ -343,17 +343,18 @@ uint32_t pvl_gmres_max_iter(void);
 /* Capture the whole mixed solve as one CUDA graph: r = b - A x (x holds the seed), right-
  * preconditioned flexible GMRES with the FP32 approximate inverse Minv (ldm) inside a
  * conditional WHILE node that the device ends (rotated residual <= tol ||b||, exhausted Krylov
- * space, or max_iter columns), x += Z y, the true residual, the status record, and in a
+ * space, or max_iter columns), x += Z y, the FP64 residual r0 - sum_j y_j W_j from the stored
+ * products W_j = A z_j (b - A x without another pass over A), the status record, and in a
  * conditional IF node the FP64 fallback when that residual missed tol (pvl_lu_factor of A
  * in place and pvl_lu_solve_blocked of b in place, x = b).  Then gamma = x[0..n_gamma) and,
  * with n_groups, pvl_group_mean_remove.  Buffers (all device, fixed for the graph's life):
- * V (max_iter + 1) x n, Z max_iter x n, w n doubles, v32 n floats (16-byte aligned), ctl of
+ * V (max_iter + 1) x n, Z and W max_iter x n, r0 and w n doubles, v32 n floats (16-byte aligned), ctl of
  * pvl_gmres_ctl_bytes(), ipiv 2n, info 1, ws >= pvl_lu_workspace(n).  *graph_out receives an
  * opaque handle.  No reference counterpart (the reference factorises every step,
  * python/pyvl/solver.py:223-227). */
 int pvl_gmres_graph_create(uint32_t n, double* A, uint32_t lda, const float* Minv, uint32_t ldm, double* b,
-                           double* x, double* V, double* Z, double* w, float* v32, void* ctl, uint32_t max_iter,
-                           double tol, int32_t* ipiv, int32_t* info, void* ws, size_t ws_bytes, double* gamma,
+                           double* x, double* V, double* Z, double* W, double* r0, double* w, float* v32, void* ctl,
+                           uint32_t max_iter, double tol, int32_t* ipiv, int32_t* info, void* ws, size_t ws_bytes, double* gamma,
                            uint32_t n_gamma, uint32_t n_groups, const uint32_t* group_offsets,
                            pvl_gmres_status* status, uint64_t* graph_out);
 /* Enqueue one solve on stream; counts the graph's fixed kernels in pvl_launch_count(). */

@@ -75,8 +75,8 @@ SIGNATURES = {
     "pvl_lu_solve_blocked": (_I, [_U, _P, _U, _P, _P, _P, _Z, _P]),
     "pvl_gmres_ctl_bytes": (_Z, []),
     "pvl_gmres_max_iter": (_U, []),
-    "pvl_gmres_graph_create": (_I, [_U, _P, _U, _P, _U, _P, _P, _P, _P, _P, _P, _P, _U, _D, _P, _P, _P, _Z, _P, _U,
-                                    _U, _P, _P, _P]),
+    "pvl_gmres_graph_create": (_I, [_U, _P, _U, _P, _U, _P, _P, _P, _P, _P, _P, _P, _P, _P, _U, _D, _P, _P, _P, _Z,
+                                    _P, _U, _U, _P, _P, _P]),
     "pvl_gmres_graph_launch": (_I, [ctypes.c_uint64, _P]),
     "pvl_gmres_graph_account": (_I, [ctypes.c_uint64, _U, _U]),
     "pvl_gmres_graph_destroy": (_I, [ctypes.c_uint64]),

@@ -9,10 +9,12 @@
 // The columns run inside a conditional WHILE node whose condition the single-CTA kernel
 // sets: the loop ends when the rotated residual meets tol ||b||, the Krylov space is
 // exhausted, or max_iter columns are done (the column counter rises by one every pass, so
-// the loop always ends).  After it: the triangular solve for y, x += Z y, the true FP64
-// residual b - A x, and a status record.  A conditional IF node then runs the FP64
-// factorisation and a blocked triangular solve when the true residual missed tol, so the
-// returned x always meets it without the host looking at the iteration in between.
+// the loop always ends).  After it: the triangular solve for y, x += Z y, the FP64 residual
+// r = r0 - sum_j y_j (A z_j) from the stored products A z_j (the vector b - A x, which a
+// further pass over A would recompute; the two differ by the rounding of the x update), and a
+// status record.  A conditional IF node then runs the FP64 factorisation and a blocked
+// triangular solve when that residual missed tol, so the returned x meets it without the host
+// looking at the iteration in between.
 //
 // The host only launches the graph; the status record (iterations, residuals, whether the
 // FP64 fallback ran) is read back whenever the host wants it.  This removes the host round
@@ -71,9 +73,10 @@ __device__ double block_sum(double v, double* red)
 
 // ||b||, beta = ||r|| (r = b - A x already in w), v_0 = r / beta and its FP32 copy.
 __global__ void __launch_bounds__(kCta) gmres_start_kernel(uint32_t n, const double* __restrict__ b,
-                                                           const double* __restrict__ r, double* __restrict__ V,
-                                                           float* __restrict__ v32, Ctl* __restrict__ ctl, double tol,
-                                                           uint32_t max_iter, cudaGraphConditionalHandle loop)
+                                                           const double* __restrict__ r, double* __restrict__ r0,
+                                                           double* __restrict__ V, float* __restrict__ v32,
+                                                           Ctl* __restrict__ ctl, double tol, uint32_t max_iter,
+                                                           cudaGraphConditionalHandle loop)
 {
     __shared__ double red[33];
     double sb = 0.0, sr = 0.0;
@@ -86,6 +89,7 @@ __global__ void __launch_bounds__(kCta) gmres_start_kernel(uint32_t n, const dou
     const double inv = be > 0.0 ? 1.0 / be : 0.0;
     for (uint32_t e = threadIdx.x; e < n; e += kCta) {
         const double v = r[e] * inv;
+        r0[e] = r[e];
         V[e] = v;
         v32[e] = (float)v;
     }
@@ -101,18 +105,21 @@ __global__ void __launch_bounds__(kCta) gmres_start_kernel(uint32_t n, const dou
     }
 }
 
-// Column j = ctl->j after w = A z_j: Gram-Schmidt (two classical passes), normalisation,
-// Givens rotation, convergence test; sets the loop condition.
+// Column j = ctl->j after W_j = A z_j: w = W_j (W_j stays for the final residual), Gram-Schmidt
+// (two classical passes), normalisation, Givens rotation, convergence test; sets the loop
+// condition.
 __global__ void __launch_bounds__(kCta) gmres_arnoldi_kernel(uint32_t n, double* __restrict__ V,
-                                                             double* __restrict__ w, float* __restrict__ v32,
-                                                             Ctl* __restrict__ ctl, uint32_t max_iter,
-                                                             cudaGraphConditionalHandle loop)
+                                                             const double* __restrict__ W, double* __restrict__ w,
+                                                             float* __restrict__ v32, Ctl* __restrict__ ctl,
+                                                             uint32_t max_iter, cudaGraphConditionalHandle loop)
 {
     __shared__ double red[32][kMaxIter + 1];
     __shared__ double tot[33];
     const uint32_t j = ctl->j;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double* h = ctl->H[j];
+    for (uint32_t e = threadIdx.x; e < n; e += kCta)  // each thread works on its own entries only
+        w[e] = W[(size_t)j * n + e];
     for (int pass = 0; pass < 2; ++pass) {
         for (uint32_t i = 0; i <= j; ++i) {
             const double* vi = V + (size_t)i * n;
@@ -174,11 +181,17 @@ __global__ void __launch_bounds__(kCta) gmres_arnoldi_kernel(uint32_t n, double*
     }
 }
 
-// y from the rotated Hessenberg system, x += Z y.
+// y from the rotated Hessenberg system, x += Z y, r = r0 - W y (held in r), rel = ||r|| / ||b||,
+// the status record and the fallback condition.
 __global__ void __launch_bounds__(kCta) gmres_update_kernel(uint32_t n, const double* __restrict__ Z,
-                                                            double* __restrict__ x, const Ctl* __restrict__ ctl)
+                                                            const double* __restrict__ W,
+                                                            const double* __restrict__ r0, double* __restrict__ x,
+                                                            double* __restrict__ r, const Ctl* __restrict__ ctl,
+                                                            double tol, pvl_gmres_status* __restrict__ status,
+                                                            cudaGraphConditionalHandle fallback)
 {
     __shared__ double y[kMaxIter];
+    __shared__ double red[33];
     const uint32_t k = ctl->j;
     if (threadIdx.x == 0) {
         for (uint32_t i = k; i-- > 0;) {  // back substitution (rows of R = rotated H)
@@ -190,30 +203,23 @@ __global__ void __launch_bounds__(kCta) gmres_update_kernel(uint32_t n, const do
         }
     }
     __syncthreads();
+    double q = 0.0;
     for (uint32_t e = threadIdx.x; e < n; e += kCta) {
-        double s = x[e];
-        for (uint32_t i = 0; i < k; ++i)
+        double s = x[e], t = r0[e];
+        for (uint32_t i = 0; i < k; ++i) {
             s = fma(y[i], Z[(size_t)i * n + e], s);
+            t = fma(-y[i], W[(size_t)i * n + e], t);
+        }
         x[e] = s;
+        r[e] = t;
+        q = fma(t, t, q);
     }
-}
-
-// rel = ||b - A x|| / ||b|| (the residual in r); status; the fallback condition.
-__global__ void __launch_bounds__(kCta) gmres_status_kernel(uint32_t n, const double* __restrict__ r,
-                                                            const Ctl* __restrict__ ctl, double tol,
-                                                            pvl_gmres_status* __restrict__ status,
-                                                            cudaGraphConditionalHandle fallback)
-{
-    __shared__ double red[33];
-    double s = 0.0;
-    for (uint32_t e = threadIdx.x; e < n; e += kCta)
-        s = fma(r[e], r[e], s);
-    const double rn = sqrt(block_sum(s, red));
+    const double rn = sqrt(block_sum(q, red));
     if (threadIdx.x == 0) {
         const double bn = fmax(ctl->bnorm, 1e-300);
         const double rel = rn / bn;
         const uint32_t ok = rel <= tol;  // false for NaN
-        status->iterations = ctl->j;
+        status->iterations = k;
         status->converged = ok;
         status->initial_rel_residual = ctl->beta / bn;
         status->final_rel_residual = rel;
@@ -255,8 +261,8 @@ int add_conditional(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraphCondi
 }
 
 int capture_graph(SolverGraph* sg, cudaStream_t s, cudaStream_t s2, uint32_t n, double* A, uint32_t lda,
-                  const float* Minv, uint32_t ldm, double* b, double* x, double* V, double* Z, double* w, float* v32,
-                  Ctl* ctl, uint32_t max_iter, double tol, int32_t* ipiv, int32_t* info, void* ws, size_t ws_bytes,
+                  const float* Minv, uint32_t ldm, double* b, double* x, double* V, double* Z, double* W, double* r0,
+                  double* w, float* v32, Ctl* ctl, uint32_t max_iter, double tol, int32_t* ipiv, int32_t* info, void* ws, size_t ws_bytes,
                   double* gamma, uint32_t n_gamma, uint32_t n_groups, const uint32_t* group_offsets,
                   pvl_gmres_status* status)
 {
@@ -270,7 +276,7 @@ int capture_graph(SolverGraph* sg, cudaStream_t s, cudaStream_t s2, uint32_t n, 
     // r = b - A x, v_0
     pvl::launch_gemv<double, double>(n, n, -1.0, A, lda, x, 0, 1.0, b, w, 0, nullptr, s);
     PVL_LAUNCH_CHECK();
-    gmres_start_kernel<<<1, kCta, 0, s>>>(n, b, w, V, v32, ctl, tol, max_iter, loop);
+    gmres_start_kernel<<<1, kCta, 0, s>>>(n, b, w, r0, V, v32, ctl, tol, max_iter, loop);
     PVL_LAUNCH_CHECK();
     // the Krylov columns
     cudaGraph_t body;
@@ -280,9 +286,9 @@ int capture_graph(SolverGraph* sg, cudaStream_t s, cudaStream_t s2, uint32_t n, 
     PVL_CUDA_CHECK(cudaStreamBeginCaptureToGraph(s2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     pvl::launch_gemv<float, float>(n, n, 1.0, Minv, ldm, v32, 0, 0.0, nullptr, Z, n, &ctl->j, s2);
     pvl_count_launch();
-    pvl::launch_gemv<double, double>(n, n, 1.0, A, lda, Z, n, 0.0, nullptr, w, 0, &ctl->j, s2);
+    pvl::launch_gemv<double, double>(n, n, 1.0, A, lda, Z, n, 0.0, nullptr, W, n, &ctl->j, s2);
     pvl_count_launch();
-    gmres_arnoldi_kernel<<<1, kCta, 0, s2>>>(n, V, w, v32, ctl, max_iter, loop);
+    gmres_arnoldi_kernel<<<1, kCta, 0, s2>>>(n, V, W, w, v32, ctl, max_iter, loop);
     pvl_count_launch();
     const cudaError_t eb = cudaGetLastError();
     cudaGraph_t body_out = nullptr;
@@ -291,12 +297,8 @@ int capture_graph(SolverGraph* sg, cudaStream_t s, cudaStream_t s2, uint32_t n, 
         return pvl_fail(PVL_ERR_CUDA, "gmres graph: column body: %s", cudaGetErrorString(eb != cudaSuccess ? eb : ee));
     sg->column_kernels = pvl_launch_count() - c1;
     const unsigned long long c2 = pvl_launch_count();
-    // x += Z y, the true residual, the status
-    gmres_update_kernel<<<1, kCta, 0, s>>>(n, Z, x, ctl);
-    PVL_LAUNCH_CHECK();
-    pvl::launch_gemv<double, double>(n, n, -1.0, A, lda, x, 0, 1.0, b, w, 0, nullptr, s);
-    PVL_LAUNCH_CHECK();
-    gmres_status_kernel<<<1, kCta, 0, s>>>(n, w, ctl, tol, status, fallback);
+    // x += Z y, the residual r0 - W y, the status
+    gmres_update_kernel<<<1, kCta, 0, s>>>(n, Z, W, r0, x, w, ctl, tol, status, fallback);
     PVL_LAUNCH_CHECK();
     // the FP64 fallback: factorise A in place, solve for b in place, x = b
     if (int r = add_conditional(s, fallback, cudaGraphCondTypeIf, &body))
@@ -333,15 +335,15 @@ extern "C" size_t pvl_gmres_ctl_bytes(void) { return sizeof(Ctl); }
 extern "C" uint32_t pvl_gmres_max_iter(void) { return kMaxIter; }
 
 extern "C" int pvl_gmres_graph_create(uint32_t n, double* A, uint32_t lda, const float* Minv, uint32_t ldm, double* b,
-                                      double* x, double* V, double* Z, double* w, float* v32, void* ctl,
-                                      uint32_t max_iter, double tol, int32_t* ipiv, int32_t* info, void* ws,
+                                      double* x, double* V, double* Z, double* W, double* r0, double* w,
+                                      float* v32, void* ctl, uint32_t max_iter, double tol, int32_t* ipiv, int32_t* info, void* ws,
                                       size_t ws_bytes, double* gamma, uint32_t n_gamma, uint32_t n_groups,
                                       const uint32_t* group_offsets, pvl_gmres_status* status, uint64_t* graph_out)
 {
     if (!graph_out)
         return pvl_fail(PVL_ERR_ARG, "pvl_gmres_graph_create: graph_out is NULL");
     *graph_out = 0;
-    if (n == 0 || !A || !Minv || !b || !x || !V || !Z || !w || !v32 || !ctl || !ipiv || !info || !ws || !status)
+    if (n == 0 || !A || !Minv || !b || !x || !V || !Z || !W || !r0 || !w || !v32 || !ctl || !ipiv || !info || !ws || !status)
         return pvl_fail(PVL_ERR_ARG, "pvl_gmres_graph_create: empty system or null pointer argument");
     if (max_iter == 0 || max_iter > kMaxIter)
         return pvl_fail(PVL_ERR_ARG, "pvl_gmres_graph_create: max_iter %u outside 1..%u", max_iter, kMaxIter);
@@ -362,7 +364,7 @@ extern "C" int pvl_gmres_graph_create(uint32_t n, double* A, uint32_t lda, const
     } else if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         rc = pvl_fail(PVL_ERR_CUDA, "pvl_gmres_graph_create: capture failed to start");
     } else {
-        rc = capture_graph(sg, s, s2, n, A, lda, Minv, ldm, b, x, V, Z, w, v32, static_cast<Ctl*>(ctl), max_iter, tol,
+        rc = capture_graph(sg, s, s2, n, A, lda, Minv, ldm, b, x, V, Z, W, r0, w, v32, static_cast<Ctl*>(ctl), max_iter, tol,
                            ipiv, info, ws, ws_bytes, gamma, n_gamma, n_groups, group_offsets, status);
         cudaGraph_t g = nullptr;
         const cudaError_t e = cudaStreamEndCapture(s, &g);

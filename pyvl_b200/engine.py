@@ -574,6 +574,8 @@ class MixedSolverEngine(SolverEngine):
         m = self.max_iter
         self.V = torch.zeros((m + 1, n), **f64)
         self.Z = torch.zeros((m, n), **f64)
+        self.W = torch.zeros((m, n), **f64)  # A z_j of the device-driven solve
+        self.r0 = torch.zeros(n, **f64)
         self.wv = torch.zeros(n, **f64)
         self.Hd = torch.zeros((m, 2 * (m + 2)), **f64)  # column j: h[0..j+1] and basis_project scratch
         self.h_H = torch.zeros((m, 2 * (m + 2)), dtype=torch.float64, pin_memory=True)
@@ -837,8 +839,8 @@ class MixedSolverEngine(SolverEngine):
         n = self.N
         h = ctypes.c_uint64(0)
         _lib.call("pvl_gmres_graph_create", n, ptr(self.A), n, ptr(self.Xinv), self.npad, ptr(self.rhs), ptr(self.x),
-                  ptr(self.V), ptr(self.Z), ptr(self.wv), ptr(self.v32), ptr(self.ctl), self.max_iter,
-                  self.gmres_tol, ptr(self.ipiv), ptr(self.info), ptr(self.ws), self._ws_bytes, ptr(self.gamma),
+                  ptr(self.V), ptr(self.Z), ptr(self.W), ptr(self.r0), ptr(self.wv), ptr(self.v32), ptr(self.ctl),
+                  self.max_iter, self.gmres_tol, ptr(self.ipiv), ptr(self.info), ptr(self.ws), self._ws_bytes, ptr(self.gamma),
                   self.P, self.m, ptr(self.goff) if self.m else None, ptr(self.status_dev), ctypes.byref(h))
         self._graph = int(h.value)
         self._graph_key = key
