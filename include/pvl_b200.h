@@ -547,6 +547,12 @@ unsigned long long pvl_launch_count(void);
  * counterpart (measurement helper). */
 double pvl_fma_probe(int precision, uint32_t n_blocks, uint32_t iters, void* sink, void* stream);
 
+/* rcp[i] = the FP64 pair kernels' 1/x[i] (hardware seed and one third-order refinement) and
+ * sum[i] = their arctangent series sum_k (-w)^k / (2k + 1) at w[i] (w in [0, 0.1]), for n
+ * device values; lets a test hold the far-field arithmetic to its error bounds.  No reference
+ * counterpart (the reference calls atan2 for every pair, src/core/flow_solver.c:113-135). */
+int pvl_far_series_eval(uint32_t n, const double* x, const double* w, double* rcp, double* sum, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -117,6 +117,7 @@ SIGNATURES = {
     "pvl_mlp_to_bf16": (_I, [_P, _P, _P]),
     "pvl_launch_count": (ctypes.c_ulonglong, []),
     "pvl_fma_probe": (_D, [_I, _U, _U, _P, _P]),
+    "pvl_far_series_eval": (_I, [_U, _P, _P, _P, _P, _P]),
 }
 
 _lib = None

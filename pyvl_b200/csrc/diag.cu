@@ -1,10 +1,13 @@
-// Measurement helpers of the C ABI: a kernel-launch counter and an FMA-throughput probe.
+// Measurement helpers of the C ABI: a kernel-launch counter, an FMA-throughput probe and an
+// evaluator of the far-field arithmetic.
 //
 // pvl_launch_count() counts every kernel enqueued through the ABI (incremented at each
 // launch site), so a caller can state how many of this library's kernels ran in a timed
 // region.  pvl_fma_probe() enqueues a kernel of independent FMA chains whose FLOP count
 // is known exactly; timing it gives the FP64 / FP32 non-tensor peak that the
-// compute-bound pair kernels are measured against.
+// compute-bound pair kernels are measured against.  pvl_far_series_eval() runs the FP64
+// reciprocal and arctangent series of the pair kernels on given arguments, so that a test
+// can hold them to their error bounds.
 #include <atomic>
 #include <cstdint>
 
@@ -36,6 +39,15 @@ __global__ void __launch_bounds__(kProbeThreads) fma_probe_kernel(uint32_t iters
     if (s == T(-1.2345))  // never true for the chains above; keeps the work observable
         sink[blockIdx.x] = s;
 }
+__global__ void far_series_kernel(uint32_t n, const double* __restrict__ x, const double* __restrict__ w,
+                                  double* __restrict__ rcp, double* __restrict__ sum)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        rcp[i] = pvl::FarSeries<double>::rcp(x[i]);
+        sum[i] = pvl::FarSeries<double>::sum(w[i]);
+    }
+}
 }  // namespace
 
 void pvl_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
@@ -59,4 +71,16 @@ extern "C" double pvl_fma_probe(int precision, uint32_t n_blocks, uint32_t iters
         return -1.0;
     }
     return 2.0 * kChains * (double)iters * kProbeThreads * n_blocks;
+}
+
+extern "C" int pvl_far_series_eval(uint32_t n, const double* x, const double* w, double* rcp, double* sum,
+                                   void* stream)
+{
+    if (n == 0)
+        return PVL_OK;
+    if (!x || !w || !rcp || !sum)
+        return pvl_fail(PVL_ERR_ARG, "pvl_far_series_eval: null pointer argument");
+    far_series_kernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(n, x, w, rcp, sum);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
 }

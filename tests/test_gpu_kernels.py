@@ -195,3 +195,31 @@ def test_tiled_ring_matrix_matches_ring_matrix(factory):
               ptr(d["sl_local"]), d["tile_max"], P, ptr(cps), ptr(nrm), case.tol, ptr(b), P, ws, nb, s)
     torch.cuda.synchronize()
     assert (torch.linalg.norm(a - b) / torch.linalg.norm(a)).item() <= 1e-14
+
+
+def test_far_field_reciprocal_and_series_bounds(torch_cuda):
+    """The FP64 pair kernels' far-field arithmetic held to its error bounds: 1/x from the
+    hardware seed and one third-order step within an ulp of the rounded quotient; the
+    arctangent series (four, eight or sixteen terms by w) within a few ulps of atan(q)/q,
+    q = sqrt(w), evaluated in extended precision."""
+    torch = torch_cuda
+    from pyvl_b200 import _lib
+    from pyvl_b200.device import ptr, stream_ptr
+
+    rng = np.random.default_rng(3)
+    n = 1 << 20
+    x = np.ldexp(rng.uniform(1.0, 2.0, n), rng.integers(-900, 900, n))
+    x[:4] = [1.0, 1.5, 2.0 - 2.0**-52, 3.0]
+    w = np.concatenate([rng.uniform(0.0, 0.1, n // 2), 10.0 ** rng.uniform(-12, -1, n // 2)])
+    w[:6] = [0.0, 1e-4, np.nextafter(1e-4, 1.0), 0.01, np.nextafter(0.01, 1.0), 0.1]
+    dx, dw = torch.as_tensor(x, device="cuda"), torch.as_tensor(w, device="cuda")
+    rcp, ssum = torch.empty_like(dx), torch.empty_like(dw)
+    _lib.call("pvl_far_series_eval", n, ptr(dx), ptr(dw), ptr(rcp), ptr(ssum), stream_ptr())
+    torch.cuda.synchronize()
+    r, s = rcp.cpu().numpy(), ssum.cpu().numpy()
+    want_r = 1.0 / x  # correctly rounded
+    assert np.all(np.abs(r - want_r) <= np.spacing(want_r))
+    q = np.sqrt(w.astype(np.longdouble))
+    want_s = np.where(q > 0, np.arctan(q) / np.where(q > 0, q, 1), 1).astype(np.longdouble)
+    err = np.abs(s.astype(np.longdouble) - want_s) / want_s
+    assert float(err.max()) <= 4 * 2.0**-53
