@@ -273,12 +273,49 @@ __global__ void __launch_bounds__(kSumThreads, 8) line_sum_f64_kernel(
 
 // The FP32 sweep with Blackwell's packed FP32x2 arithmetic (__ffma2_rn / __fadd2_rn /
 // __fmul2_rn): each thread evaluates every segment at two points held in the two lanes of
-// float2 registers, so one instruction serves two pairs (the FP32 sweep is bound by instruction
-// issue, not by the FMA pipe).  Both lanes take the far-field series of segment_induction; a
-// lane inside the cut-off contributes zero (selected, not computed), and a lane that needs the
-// near-field atan2 form takes a scalar side path.  Same function and layout as
-// line_sum_f64_kernel; points p and p + 128 of each 256-point block.
+// float2 registers, so one instruction serves two pairs.  The pair arithmetic is the Pluecker
+// form of sweep.cuh about the CTA's centroid o (t1 = d . p' - e, c = p' x d - m, p' = p - o;
+// m and e formed in FP64 when the tile is staged; -d, -m, -e, -len and -gamma len staged too,
+// so that no operand is negated in the loop): 26 packed instructions per two pairs on the FMA
+// pipe, which bounds this kernel.  (Staging every operand already broadcast to both lanes as
+// float2 was slower: 112 instead of 64 bytes of shared loads per segment.)  Both lanes take
+// the far-field series of segment_induction; a lane inside the cut-off contributes zero
+// (selected, not computed), and a lane that needs the near-field atan2 form takes a scalar
+// side path.  Same function and layout as line_sum_f64_kernel; points p and p + 128 of each
+// 256-point block.
 __device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
+
+struct __align__(16) SweepSeg2 {
+    float dx, dy, dz, ndx, ndy, ndz;  // d and -d
+    float nmx, nmy, nmz, ne;          // -m and -e about the CTA's origin
+    float nlen, len2, nglen;          // -len, len^2, -gamma len
+    float gamma, len;                 // the near-field side path
+    float pad;
+};
+
+__device__ __forceinline__ SweepSeg2 sweep_seg2(const Segment<float>& g, const double* o)
+{
+    const double rx = (double)g.r1x - o[0], ry = (double)g.r1y - o[1], rz = (double)g.r1z - o[2];
+    const double dx = g.dx, dy = g.dy, dz = g.dz;
+    SweepSeg2 t;
+    t.dx = g.dx;
+    t.dy = g.dy;
+    t.dz = g.dz;
+    t.ndx = -g.dx;
+    t.ndy = -g.dy;
+    t.ndz = -g.dz;
+    t.nmx = (float)(rz * dy - ry * dz);
+    t.nmy = (float)(rx * dz - rz * dx);
+    t.nmz = (float)(ry * dx - rx * dy);
+    t.ne = (float)-(dx * rx + dy * ry + dz * rz);
+    t.nlen = -g.len;
+    t.len2 = g.len2;
+    t.nglen = -g.glen;
+    t.gamma = g.gamma;
+    t.len = g.len;
+    t.pad = 0.0f;
+    return t;
+}
 
 __global__ void __launch_bounds__(kSumThreads) line_sum_f32x2_kernel(const Segment<float>* __restrict__ seg,
                                                                      uint32_t n_lines, uint32_t lines_per_split,
@@ -288,56 +325,61 @@ __global__ void __launch_bounds__(kSumThreads) line_sum_f32x2_kernel(const Segme
                                                                      uint32_t col_limit, float tol2,
                                                                      float* __restrict__ partial)
 {
-    __shared__ Segment<float> s_seg[kSegTile];
+    __shared__ SweepSeg2 s_seg[kSegTile];
+    __shared__ double s_red[kSumThreads / 32][4];
+    __shared__ double s_o[3];
     const uint32_t split = blockIdx.y;
     const uint32_t l_begin = split * lines_per_split;
     const uint32_t l_end = min(n_lines, l_begin + lines_per_split);
-    float pv[2][3];
+    double pv[2][3];
     uint32_t pid[2];
+    double cs[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (int t = 0; t < 2; ++t) {
         const uint32_t p = blockIdx.x * (kSumThreads * 2) + t * kSumThreads + threadIdx.x;
         pid[t] = p;
         size_t q;
         const bool ok = sweep_point(p, n_pts, group, stride, in_off, cols, col_limit, q);
-        pv[t][0] = ok ? float(pts[3 * q]) : 0.0f;
-        pv[t][1] = ok ? float(pts[3 * q + 1]) : 0.0f;
-        pv[t][2] = ok ? float(pts[3 * q + 2]) : 0.0f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            pv[t][c] = ok ? pts[3 * q + c] : 0.0;
+            cs[c] += pv[t][c];
+        }
+        cs[3] += ok ? 1.0 : 0.0;
     }
-    const float2 px = make_float2(pv[0][0], pv[1][0]), py = make_float2(pv[0][1], pv[1][1]),
-                 pz = make_float2(pv[0][2], pv[1][2]);
+    pvl::cta_centroid<kSumThreads>(cs[0], cs[1], cs[2], cs[3], s_red, s_o);
+    const float2 px = make_float2((float)(pv[0][0] - s_o[0]), (float)(pv[1][0] - s_o[0])),
+                 py = make_float2((float)(pv[0][1] - s_o[1]), (float)(pv[1][1] - s_o[1])),
+                 pz = make_float2((float)(pv[0][2] - s_o[2]), (float)(pv[1][2] - s_o[2]));
     float2 accx = bc2(0.0f), accy = bc2(0.0f), accz = bc2(0.0f);
     constexpr float kW = pvl::FarSeries<float>::kW;
     for (uint32_t l0 = l_begin; l0 < l_end; l0 += kSegTile) {
         const uint32_t l = l0 + threadIdx.x;
         if (threadIdx.x < kSegTile && l < l_end)
-            s_seg[threadIdx.x] = seg[l];
+            s_seg[threadIdx.x] = sweep_seg2(seg[l], s_o);
         __syncthreads();
         const int cnt = (int)min((uint32_t)kSegTile, l_end - l0);
 #pragma unroll 1
         for (int k = 0; k < cnt; ++k) {
-            const Segment<float> s = s_seg[k];
-            const float2 ax = __fadd2_rn(px, bc2(-s.r1x)), ay = __fadd2_rn(py, bc2(-s.r1y)),
-                         az = __fadd2_rn(pz, bc2(-s.r1z));
-            float2 t1 = __fmul2_rn(bc2(s.dx), ax);
-            t1 = __ffma2_rn(bc2(s.dy), ay, t1);
-            t1 = __ffma2_rn(bc2(s.dz), az, t1);
-            const float2 cx = __ffma2_rn(az, bc2(-s.dy), __fmul2_rn(ay, bc2(s.dz)));
-            const float2 cy = __ffma2_rn(ax, bc2(-s.dz), __fmul2_rn(az, bc2(s.dx)));
-            const float2 cz = __ffma2_rn(ay, bc2(-s.dx), __fmul2_rn(ax, bc2(s.dy)));
+            const SweepSeg2 s = s_seg[k];
+            float2 t1 = __ffma2_rn(bc2(s.dx), px, bc2(s.ne));
+            t1 = __ffma2_rn(bc2(s.dy), py, t1);
+            t1 = __ffma2_rn(bc2(s.dz), pz, t1);
+            const float2 cx = __ffma2_rn(py, bc2(s.dz), __ffma2_rn(pz, bc2(s.ndy), bc2(s.nmx)));
+            const float2 cy = __ffma2_rn(pz, bc2(s.dx), __ffma2_rn(px, bc2(s.ndz), bc2(s.nmy)));
+            const float2 cz = __ffma2_rn(px, bc2(s.dy), __ffma2_rn(py, bc2(s.ndx), bc2(s.nmz)));
             float2 hsq = __fmul2_rn(cx, cx);
             hsq = __ffma2_rn(cy, cy, hsq);
             hsq = __ffma2_rn(cz, cz, hsq);
-            const float2 x = __ffma2_rn(t1, __fadd2_rn(t1, bc2(-s.len)), hsq);
-            const float2 r = make_float2(__fdividef(1.0f, x.x), __fdividef(1.0f, x.y));
+            const float2 x = __ffma2_rn(t1, __fadd2_rn(t1, bc2(s.nlen)), hsq);
+            const float2 r = make_float2(pvl::FarSeries<float>::rcp(x.x), pvl::FarSeries<float>::rcp(x.y));
             const float2 w = __fmul2_rn(__fmul2_rn(hsq, bc2(s.len2)), __fmul2_rn(r, r));
-            float2 S = bc2(-1.0f / 11.0f);
-            S = __ffma2_rn(S, w, bc2(1.0f / 9.0f));
+            float2 S = bc2(1.0f / 9.0f);  // FarSeries<float>::sum, packed
             S = __ffma2_rn(S, w, bc2(-1.0f / 7.0f));
             S = __ffma2_rn(S, w, bc2(1.0f / 5.0f));
             S = __ffma2_rn(S, w, bc2(-1.0f / 3.0f));
             S = __ffma2_rn(S, w, bc2(1.0f));
-            float2 mag = __fmul2_rn(__fmul2_rn(bc2(-s.glen), r), S);
+            float2 mag = __fmul2_rn(__fmul2_rn(bc2(s.nglen), r), S);
             const bool cut0 = hsq.x < tol2, cut1 = hsq.y < tol2;
             const bool far0 = x.x > 0.0f && w.x <= kW, far1 = x.y > 0.0f && w.y <= kW;
             if (!(cut0 || far0) || !(cut1 || far1)) {  // rare: a lane in the near field

@@ -1,16 +1,17 @@
-// Pair arithmetic of the FP64 N-body sweeps (single-case line_sum_f64_kernel and the batched
-// sweep), sm_100a.
+// Pair arithmetic of the FP64 N-body sweep (line_sum_f64_kernel), sm_100a.
 //
 // The quantities of segment_induction (pvl_common.cuh) in Pluecker form about an origin o
 // that the CTA chooses (the centroid of its points): a segment is staged once per CTA as
-//   d (unit direction), m = (r1 - o) x d, e = d . (r1 - o), len, len^2, gamma, gamma len,
-// and for a point p' = p - o
+//   d (unit direction), m = (r1 - o) x d, e = d . (r1 - o), len, gamma len, gamma
+// (80 bytes, five 16-byte shared loads per pair; gamma is read only by the near pairs), and
+// for a point p' = p - o
 //   t1 = d . p' - e = d . (p - r1),   c = p' x d - m = (p - r1) x d
 // from 9 FMAs instead of 3 differences and 9 products per pair.  Rounding is relative to
 // |p - o| + |r1 - o| instead of |p - r1|; the points of one CTA are neighbours (ring or
 // wake-node order, or one case of a batch), so |p - o| stays of the order of the body.
 // Everything after c and t1 -- h^2, x = h^2 + t1 t2, the far-field series with the Newton
-// reciprocal, the atan2 form for near pairs, the cut-off -- is segment_induction<double, true>.
+// reciprocal, the atan2 form for near pairs, the cut-off -- is segment_induction<double, true>,
+// with w = h^2 len^2 / x^2 formed as h^2 (len / x)^2.
 #pragma once
 
 #include <cstdint>
@@ -20,7 +21,7 @@
 namespace pvl {
 
 struct __align__(16) SweepSeg {
-    double dx, dy, dz, mx, my, mz, e, len, len2, glen, gamma, pad;
+    double dx, dy, dz, mx, my, mz, e, len, glen, gamma;
 };
 
 struct SweepGeo {
@@ -40,10 +41,8 @@ __device__ __forceinline__ SweepSeg sweep_seg(const Segment<double>& g, const do
     t.mz = rx * g.dy - ry * g.dx;
     t.e = g.dx * rx + g.dy * ry + g.dz * rz;
     t.len = g.len;
-    t.len2 = g.len2;
     t.glen = g.glen;
     t.gamma = g.gamma;
-    t.pad = 0.0;
     return t;
 }
 
@@ -57,7 +56,8 @@ __device__ __forceinline__ SweepGeo sweep_geo(const SweepSeg& s, double px, doub
     g.hsq = g.cx * g.cx + g.cy * g.cy + g.cz * g.cz;
     g.x = g.hsq + t1 * (t1 - s.len);
     g.r = FarSeries<double>::rcp(g.x);
-    g.w = g.hsq * s.len2 * (g.r * g.r);
+    const double a = s.len * g.r;
+    g.w = g.hsq * (a * a);
     return g;
 }
 
