@@ -266,6 +266,31 @@ def profile_kernel(args) -> None:
     print("profile-kernel done", args.profile_kernel)
 
 
+def lift_at_state(case, mesh, spec, eng, pos, vel, gamma) -> float:
+    """CL of the ring circulations ``gamma`` at the engine's body positions and wake state
+    before its wake update (circulatory_forces, python/pyvl/postprocess/forces.py:10-42: line
+    forces with the freestream, the body's and the wake's induced velocity at the nodes minus
+    the motion, then the wake's trailing-edge correction, wake_models.py:293-330)."""
+    from types import SimpleNamespace
+
+    from pyvl_b200.cvl import Mesh
+    from pyvl_b200.postprocess import lift_coefficient
+    from pyvl_b200.wake_models import WakeModelLineExplicitUnsteady
+
+    wm = WakeModelLineExplicitUnsteady(spec.bordering_nodes, spec.shedding_lines, spec.adjacent_surfaces, case.tol,
+                                       0.0, spec.line_rows)
+    wm.wake_positions[...] = eng.wake_positions.cpu().numpy()
+    wm.circulation[...] = eng.wake_circulation.cpu().numpy()
+    u = np.asarray(case.freestream, np.float64)
+    flow = SimpleNamespace(get_velocity=lambda t, p: np.tile(u, (np.asarray(p).reshape(-1, 3).shape[0], 1)))
+    pos = np.ascontiguousarray(pos, np.float64)
+    induced = mesh.induced_velocity(case.tol, pos, pos, gamma) + wm.get_velocity(pos)
+    forces = Mesh.line_forces(mesh, mesh.compute_dual(), gamma / (2 * np.pi), pos,
+                              flow.get_velocity(0.0, pos) + induced - np.asarray(vel, np.float64))
+    wm.correct_forces(forces, SimpleNamespace(mesh=mesh), pos, gamma, flow)
+    return lift_coefficient(forces, u, case.s_ref)
+
+
 def train_warm_start(mesh, case, t0: float, n_steps: int, seed: int = 0):
     """The learned warm start, trained on n_steps plain FP64 steps that end just before t0."""
     import torch
@@ -568,17 +593,20 @@ def main() -> None:
             rec["fallbacks"] = st["fallbacks"]
             rec["refreshes"] = st["refreshes"]
             # accuracy: the next steps judged against the all-FP64 step of the same state
-            errs = []
+            errs, cls = [], []
             for k in range(W + 2 * K, W + 2 * K + 3):
                 eng.load_inputs(dpos[k], dvel[k])
                 eng.assemble()
                 x0 = warm.prepare()
                 eng.solve(x0)
                 errs.append(eng.judge())
+                cls.append([lift_at_state(case, mesh, spec, eng, hpos[k], hvel[k], g.cpu().numpy())
+                            for g in (eng.gamma, eng.last_judge_ref)])
                 warm.finish()
                 eng.wake_update(times[k])
                 eng.iteration += 1
             rec["judge"] = errs
+            rec["cl"] = cls
             rec["initial_rel_residual_median"] = float(np.median(st["initial_rel_residual"][n0:n0 + K]))
         results[kind] = rec
         del eng, warm
@@ -709,9 +737,13 @@ def main() -> None:
                 "speedup_mixed_over_plain": results["plain"]["ms"] / mx["ms"],
             },
             "accuracy": {"gamma_rel_err_vs_fp64_max": max(mx["judge"]), "judged_steps": len(mx["judge"]),
+                         "cl_rel_err_vs_fp64_max": max(abs(a - b) / abs(b) for a, b in mx["cl"]),
+                         "cl_mixed_fp64_last": mx["cl"][-1],
                          "tolerance": 1e-10,
                          "how": "after the timed steps, each judged step's mixed circulation vs the same state "
-                                "assembled in FP64 and solved by FP64 LU"},
+                                "assembled in FP64 and solved by FP64 LU; CL of both circulations at that state "
+                                "through the line-force path (body + wake velocity at the nodes, trailing-edge "
+                                "correction)"},
             "e2e": {"value": sps_e2e, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp64", "kernel": "line_sum_f64_kernel (explicit wake term)",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,

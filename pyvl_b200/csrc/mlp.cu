@@ -5,8 +5,9 @@
 // Kernels:
 //   features_kernel -- the 12 normalised inputs of each panel and the base of the prediction
 //                      (previous circulation + one Jacobi correction of the new system);
-//   forward_kernel  -- inference: one CTA of 128 threads per tile of 32 panels, thread j owns
-//                      hidden unit j; W2 staged transposed in shared memory (conflict-free);
+//   forward_kernel  -- inference: one CTA of 128 threads per tile of 8 panels, thread j owns
+//                      hidden unit j; W2 staged transposed in shared memory (a row of W2
+//                      per thread: conflict-free both when staged and when read);
 //   train_kernel    -- forward + backward of the mean squared error over a batch, persistent
 //                      CTAs, each accumulating its gradient in shared memory (FP32) and
 //                      writing one partial gradient row; reduce_kernel sums the rows in a
@@ -26,10 +27,12 @@ namespace {
 
 constexpr int kIn = 12;
 constexpr int kH = 128;
-constexpr int kTile = 32;  // panels per tile
+constexpr int kTile = 32;     // panels per tile of training
+constexpr int kFwdTile = 8;   // panels per tile of inference (n / 8 CTAs: 512 at 4096 panels)
 constexpr int kThreads = kH;
 constexpr int oW1 = 0, oB1 = oW1 + kH * kIn, oW2 = oB1 + kH, oB2 = oW2 + kH * kH, oW3 = oB2 + kH, oB3 = oW3 + kH;
 constexpr int kParams = oB3 + 1;
+static_assert(oW2 % 8 == 0 && kH % 8 == 0 && kThreads == kH, "W2 is staged in 16-byte vectors, a row per thread");
 constexpr int kDW2Stride = kH + 1;  // padded rows of the W2 gradient (conflict-free row-per-thread updates)
 
 inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
@@ -37,19 +40,21 @@ inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1)
 __device__ __forceinline__ float bf(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 __device__ __forceinline__ float ldb(const __nv_bfloat16* p) { return __bfloat162float(*p); }
 
-struct FwdSmem {
+template <int T> struct FwdSmemT {
     __nv_bfloat16 w2t[kH][kH];  // w2t[k][j] = W2[j][k]
-    float x[kTile][kIn];
-    float h1[kTile][kH];
-    float red[kThreads / 32][kTile];
+    float x[T][kIn];
+    float h1[T][kH];
+    float red[kThreads / 32][T];
 };
+using FwdSmem = FwdSmemT<kTile>;
 
 // Layers 1 and 2 for one tile; returns h2[s] (BF16-rounded) for this thread's unit j in h2.
-__device__ __forceinline__ void tile_forward(const FwdSmem& sm, float (&h1s)[kTile][kH], const float (&w1)[kIn],
-                                             float b1, float b2, int ns, float (&h2)[kTile])
+template <int T>
+__device__ __forceinline__ void tile_forward(const FwdSmemT<T>& sm, float (&h1s)[T][kH], const float (&w1)[kIn],
+                                             float b1, float b2, int ns, float (&h2)[T])
 {
     const int j = threadIdx.x;
-    for (int s = 0; s < kTile; ++s) {
+    for (int s = 0; s < T; ++s) {
         float a = b1;
 #pragma unroll
         for (int i = 0; i < kIn; ++i)
@@ -58,7 +63,7 @@ __device__ __forceinline__ void tile_forward(const FwdSmem& sm, float (&h1s)[kTi
     }
     __syncthreads();
 #pragma unroll
-    for (int s = 0; s < kTile; ++s)
+    for (int s = 0; s < T; ++s)
         h2[s] = b2;
     for (int k = 0; k < kH; k += 4) {
         float w[4];
@@ -66,22 +71,23 @@ __device__ __forceinline__ void tile_forward(const FwdSmem& sm, float (&h1s)[kTi
         for (int q = 0; q < 4; ++q)
             w[q] = __bfloat162float(sm.w2t[k + q][j]);
 #pragma unroll
-        for (int s = 0; s < kTile; ++s) {
+        for (int s = 0; s < T; ++s) {
             const float4 h = *reinterpret_cast<const float4*>(&h1s[s][k]);
             h2[s] = fmaf(w[0], h.x, fmaf(w[1], h.y, fmaf(w[2], h.z, fmaf(w[3], h.w, h2[s]))));
         }
     }
 #pragma unroll
-    for (int s = 0; s < kTile; ++s)
+    for (int s = 0; s < T; ++s)
         h2[s] = bf(fmaxf(h2[s], 0.0f));
 }
 
 // y[s] = b3 + sum_j w3[j] h2[s][j] for the tile (all threads take part; result in red[0][s]).
-__device__ __forceinline__ void tile_output(FwdSmem& sm, float w3, const float (&h2)[kTile])
+template <int T>
+__device__ __forceinline__ void tile_output(FwdSmemT<T>& sm, float w3, const float (&h2)[T])
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int s = 0; s < kTile; ++s) {
+    for (int s = 0; s < T; ++s) {
         float v = w3 * h2[s];
         for (int o = 16; o > 0; o >>= 1)
             v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -91,19 +97,37 @@ __device__ __forceinline__ void tile_output(FwdSmem& sm, float w3, const float (
     __syncthreads();
 }
 
-__device__ __forceinline__ void load_x_tile(FwdSmem& sm, const float* __restrict__ X, uint64_t s0, int ns)
+template <int T>
+__device__ __forceinline__ void load_x_tile(FwdSmemT<T>& sm, const float* __restrict__ X, uint64_t s0, int ns)
 {
-    for (int e = threadIdx.x; e < kTile * kIn; e += kThreads) {
+    for (int e = threadIdx.x; e < T * kIn; e += kThreads) {
         const int s = e / kIn, i = e % kIn;
         sm.x[s][i] = s < ns ? bf(X[(s0 + s) * kIn + i]) : 0.0f;
     }
 }
 
-__device__ __forceinline__ void load_w2t(FwdSmem& sm, const __nv_bfloat16* __restrict__ P)
+// W2 into shared memory, transposed: thread j loads row j of W2 as sixteen 16-byte vectors,
+// eight in flight before their stores (the 32 KB arrive in two rounds of L2 latency), and
+// writes column j of w2t: the 32 lanes of a store write 32 consecutive entries of one row.
+template <int T>
+__device__ __forceinline__ void load_w2t(FwdSmemT<T>& sm, const __nv_bfloat16* __restrict__ P)
 {
-    for (int e = threadIdx.x; e < kH * kH; e += kThreads) {
-        const int j = e / kH, k = e % kH;
-        sm.w2t[k][j] = P[oW2 + e];
+    constexpr int kVec = 8, kBatch = 8, kPer = kH / kVec;  // 16 vectors per row
+    const int j = threadIdx.x;
+    const uint4* __restrict__ row = reinterpret_cast<const uint4*>(P + oW2) + j * kPer;  // oW2 % 8 == 0
+#pragma unroll
+    for (int b0 = 0; b0 < kPer; b0 += kBatch) {
+        uint4 q[kBatch];
+#pragma unroll
+        for (int b = 0; b < kBatch; ++b)
+            q[b] = __ldg(row + b0 + b);
+#pragma unroll
+        for (int b = 0; b < kBatch; ++b) {
+            const __nv_bfloat16* w = reinterpret_cast<const __nv_bfloat16*>(&q[b]);
+#pragma unroll
+            for (int i = 0; i < kVec; ++i)
+                sm.w2t[(b0 + b) * kVec + i][j] = w[i];
+        }
     }
 }
 
@@ -114,7 +138,7 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(uint32_t n, const flo
                                                            const double* __restrict__ base, double* __restrict__ out)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    FwdSmem& sm = *reinterpret_cast<FwdSmem*>(smem_raw);
+    FwdSmemT<kFwdTile>& sm = *reinterpret_cast<FwdSmemT<kFwdTile>*>(smem_raw);
     const int j = threadIdx.x;
     load_w2t(sm, P);
     float w1[kIn];
@@ -123,12 +147,12 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(uint32_t n, const flo
         w1[i] = ldb(P + oW1 + j * kIn + i);
     const float b1 = ldb(P + oB1 + j), b2 = ldb(P + oB2 + j), w3 = ldb(P + oW3 + j), b3 = ldb(P + oB3);
     const double sc = mul ? scale * mul[0] : scale;
-    for (uint64_t s0 = (uint64_t)blockIdx.x * kTile; s0 < n; s0 += (uint64_t)gridDim.x * kTile) {
-        const int ns = (int)(n - s0 < (uint64_t)kTile ? n - s0 : (uint64_t)kTile);
+    for (uint64_t s0 = (uint64_t)blockIdx.x * kFwdTile; s0 < n; s0 += (uint64_t)gridDim.x * kFwdTile) {
+        const int ns = (int)(n - s0 < (uint64_t)kFwdTile ? n - s0 : (uint64_t)kFwdTile);
         __syncthreads();
         load_x_tile(sm, X, s0, ns);
         __syncthreads();
-        float h2[kTile];
+        float h2[kFwdTile];
         tile_forward(sm, sm.h1, w1, b1, b2, ns, h2);
         tile_output(sm, w3, h2);
         if (j < ns) {
@@ -358,7 +382,7 @@ int set_attrs()
     if (g_attr_done)
         return PVL_OK;
     PVL_CUDA_CHECK(cudaFuncSetAttribute(forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)sizeof(FwdSmem)));
+                                        (int)sizeof(FwdSmemT<kFwdTile>)));
     PVL_CUDA_CHECK(cudaFuncSetAttribute(train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)sizeof(TrainSmem)));
     g_attr_done = true;
@@ -405,8 +429,8 @@ extern "C" int pvl_mlp_forward(uint32_t n, const float* X, const void* params_bf
         return pvl_fail(PVL_ERR_ARG, "pvl_mlp_forward: null pointer argument");
     if (int r = set_attrs())
         return r;
-    const unsigned grid = (unsigned)std::min<uint64_t>(blocks_for(n, kTile), 148ull * 4);
-    forward_kernel<<<grid, kThreads, sizeof(FwdSmem), (cudaStream_t)stream>>>(
+    const unsigned grid = (unsigned)std::min<uint64_t>(blocks_for(n, kFwdTile), 148ull * 6);
+    forward_kernel<<<grid, kThreads, sizeof(FwdSmemT<kFwdTile>), (cudaStream_t)stream>>>(
         n, X, static_cast<const __nv_bfloat16*>(params_bf16), scale, mul, base, out);
     PVL_LAUNCH_CHECK();
     return PVL_OK;

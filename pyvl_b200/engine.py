@@ -952,6 +952,7 @@ class MixedSolverEngine(SolverEngine):
         self.border()
         SolverEngine.solve(self)
         ref = self.gamma.clone()
+        self.last_judge_ref = ref  # the all-FP64 circulation of the judged state
         self.gamma.copy_(mixed)
         err = float((torch.linalg.vector_norm(mixed - ref) / torch.linalg.vector_norm(ref)).item())
         self._stats["judge"].append(err)
