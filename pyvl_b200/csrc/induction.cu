@@ -119,11 +119,15 @@ __global__ void __launch_bounds__(kRingThreads) ring_matrix_kernel(
 // its tile (tile_lines[tile_offsets[t] ..]) at its CPB control points into shared memory,
 // then each thread sums its ring's signed entries (sl_local: each CSR entry's position in its
 // tile's line list) in CSR order.  Adjacent rings share lines, so a structured wing needs
-// ~0.57 line evaluations per (point, ring line) instead of one.
+// ~0.57 line evaluations per (point, ring line) instead of one.  The CTA has THREADS >=
+// kRingTile threads (chosen per launch from the largest tile's line count, so that the line
+// loop's last round is not mostly idle: 292 lines take two rounds of 160 threads instead of
+// three of 128); the first kRingTile of them sum the rings.
 constexpr int kRingTile = 128;
 constexpr int kTileCPB = 8;   // control points per CTA (8: 231 us, 16: 272 us on the 4096-ring body)
 
-__global__ void __launch_bounds__(kRingTile) ring_tile_kernel(uint32_t n_surfaces, const uint32_t* __restrict__ off,
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) ring_tile_kernel(uint32_t n_surfaces, const uint32_t* __restrict__ off,
                                                               const uint32_t* __restrict__ sl,
                                                               const uint32_t* __restrict__ sl_local,
                                                               const uint32_t* __restrict__ tile_off,
@@ -145,7 +149,7 @@ __global__ void __launch_bounds__(kRingTile) ring_tile_kernel(uint32_t n_surface
     }
     __syncthreads();
     const uint32_t L0 = tile_off[tile], nl = tile_off[tile + 1] - L0;
-    for (uint32_t l = threadIdx.x; l < nl; l += kRingTile) {
+    for (uint32_t l = threadIdx.x; l < nl; l += THREADS) {
         const uint32_t g = tile_lines[L0 + l];
         const bool ok = g < n_lines;
         Segment<double> sg;
@@ -164,7 +168,7 @@ __global__ void __launch_bounds__(kRingTile) ring_tile_kernel(uint32_t n_surface
     }
     __syncthreads();
     const uint32_t j = tile * kRingTile + threadIdx.x;
-    if (j >= n_surfaces)
+    if (threadIdx.x >= kRingTile || j >= n_surfaces)
         return;
     pvl::RingEntries re;
     re.load(sl, sl_local, off[j], off[j + 1]);
@@ -785,6 +789,46 @@ extern "C" int pvl_induction_normal(int precision, uint32_t n_points, uint32_t n
     return PVL_OK;
 }
 
+namespace {
+
+// Threads of a ring-tile CTA: the candidate with the fewest idle lane-slots in the line loop
+// (rounds x threads - lines), ties to fewer threads.
+int ring_tile_threads(uint32_t max_tile_lines)
+{
+    int best = kRingTile;
+    uint64_t best_slots = ~0ull;
+    for (int t : {128, 160, 192, 256}) {
+        const uint64_t slots = (uint64_t)((max_tile_lines + t - 1) / t) * (uint64_t)t;
+        if (slots < best_slots) {
+            best = t;
+            best_slots = slots;
+        }
+    }
+    return best;
+}
+
+template <int THREADS>
+int launch_ring_tile(dim3 grid, size_t smem, cudaStream_t st, uint32_t n_surfaces, const uint32_t* offsets,
+                     const uint32_t* surface_lines, const uint32_t* sl_local, const uint32_t* tile_offsets,
+                     const uint32_t* tile_lines, uint32_t max_tile_lines, uint32_t n_lines,
+                     const Segment<double>* seg, uint32_t n_cp, const double* cps, const double* normals, double tol,
+                     double* out, uint32_t ld)
+{
+    static size_t attr = 0;
+    if (smem > attr) {
+        PVL_CUDA_CHECK(cudaFuncSetAttribute(ring_tile_kernel<THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem));
+        attr = smem;
+    }
+    ring_tile_kernel<THREADS><<<grid, THREADS, smem, st>>>(n_surfaces, offsets, surface_lines, sl_local,
+                                                           tile_offsets, tile_lines, max_tile_lines, n_lines, seg,
+                                                           n_cp, cps, normals, pvl::cutoff2<double>(tol), out, ld);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+}  // namespace
+
 extern "C" int pvl_induction_normal_tiled(uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
                                           const double* positions, uint32_t n_surfaces, const uint32_t* offsets,
                                           const uint32_t* surface_lines, const uint32_t* tile_offsets,
@@ -810,17 +854,21 @@ extern "C" int pvl_induction_normal_tiled(uint32_t n_points, uint32_t n_lines, c
     auto* seg = static_cast<Segment<double>*>(ws);
     if (int r = prep_segments<double>(n_points, n_lines, lines, positions, nullptr, tol, seg, st))
         return r;
-    static size_t attr = 0;
-    if (smem > attr) {
-        PVL_CUDA_CHECK(cudaFuncSetAttribute(ring_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr = smem;
-    }
     dim3 grid((n_surfaces + kRingTile - 1) / kRingTile, (n_cp + kTileCPB - 1) / kTileCPB);
-    ring_tile_kernel<<<grid, kRingTile, smem, st>>>(n_surfaces, offsets, surface_lines, sl_local, tile_offsets,
-                                                    tile_lines, max_tile_lines, n_lines, seg, n_cp, cps, normals,
-                                                    pvl::cutoff2<double>(tol), out, ld);
-    PVL_LAUNCH_CHECK();
-    return PVL_OK;
+    switch (ring_tile_threads(max_tile_lines)) {
+    case 160:
+        return launch_ring_tile<160>(grid, smem, st, n_surfaces, offsets, surface_lines, sl_local, tile_offsets,
+                                     tile_lines, max_tile_lines, n_lines, seg, n_cp, cps, normals, tol, out, ld);
+    case 192:
+        return launch_ring_tile<192>(grid, smem, st, n_surfaces, offsets, surface_lines, sl_local, tile_offsets,
+                                     tile_lines, max_tile_lines, n_lines, seg, n_cp, cps, normals, tol, out, ld);
+    case 256:
+        return launch_ring_tile<256>(grid, smem, st, n_surfaces, offsets, surface_lines, sl_local, tile_offsets,
+                                     tile_lines, max_tile_lines, n_lines, seg, n_cp, cps, normals, tol, out, ld);
+    default:
+        return launch_ring_tile<128>(grid, smem, st, n_surfaces, offsets, surface_lines, sl_local, tile_offsets,
+                                     tile_lines, max_tile_lines, n_lines, seg, n_cp, cps, normals, tol, out, ld);
+    }
 }
 
 extern "C" size_t pvl_line_velocity_workspace(uint32_t n_lines, uint32_t n_pts, int precision)
