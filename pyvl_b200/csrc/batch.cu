@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(128) batched_ring_tile_kernel(
 #pragma unroll 4
             for (int q = 0; q < nq; ++q) {
                 Vec3<double> acc{0.0, 0.0, 0.0};
-                pvl::segment_induction(sg, s_p[q][0], s_p[q][1], s_p[q][2], tol2, 1.0, acc);
+                pvl::segment_induction<double, false, true>(sg, s_p[q][0], s_p[q][1], s_p[q][2], tol2, 1.0, acc);
                 sV[q * tile_stride + l] = acc.x * s_n[q][0] + acc.y * s_n[q][1] + acc.z * s_n[q][2];
             }
         }

@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(THREADS) ring_tile_kernel(uint32_t n_surfaces,
 #pragma unroll 4
         for (int q = 0; q < kTileCPB; ++q) {
             Vec3<double> acc{0.0, 0.0, 0.0};
-            pvl::segment_induction(sg, s_p[q][0], s_p[q][1], s_p[q][2], tol2, 1.0, acc);
+            pvl::segment_induction<double, false, true>(sg, s_p[q][0], s_p[q][1], s_p[q][2], tol2, 1.0, acc);
             sV[q * tile_stride + l] = acc.x * s_n[q][0] + acc.y * s_n[q][1] + acc.z * s_n[q][2];
         }
     }
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(kSumThreads, 8) line_sum_f64_kernel(
 // the far-field series of segment_induction; a lane inside the cut-off contributes zero
 // (selected, not computed), and a lane that needs the near-field atan2 form takes a scalar
 // side path.  Same function and layout as line_sum_f64_kernel; points p and p + 128 of each
-// 256-point block.
+// 256-point block.  40 registers, 12 CTAs per SM (541 us; 48 registers, 10 CTAs: 547 us).
 __device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
 
 struct __align__(16) SweepSeg2 {
@@ -321,7 +321,7 @@ __device__ __forceinline__ SweepSeg2 sweep_seg2(const Segment<float>& g, const d
     return t;
 }
 
-__global__ void __launch_bounds__(kSumThreads) line_sum_f32x2_kernel(const Segment<float>* __restrict__ seg,
+__global__ void __launch_bounds__(kSumThreads, 12) line_sum_f32x2_kernel(const Segment<float>* __restrict__ seg,
                                                                      uint32_t n_lines, uint32_t lines_per_split,
                                                                      const double* __restrict__ pts, uint32_t n_pts,
                                                                      uint32_t group, uint32_t stride, uint32_t in_off,

@@ -113,6 +113,27 @@ template <> struct FarSeries<double> {
         s = fma(s, w, -1.0 / 3.0);
         return fma(s, w, 1.0);
     }
+    // The same series with the tier voted over the lanes that call it together: each lane
+    // gets at least the terms it needs, and the warp runs one tier instead of up to three
+    // (kernels whose lanes hold different segments at one point, at spread-out distances).
+    static __device__ __forceinline__ double sum_uniform(double w)
+    {
+        const unsigned m = __activemask();
+        if (__any_sync(m, !le_nn(w, 0.01)))
+            return sum_tier<16>(w);
+        if (__any_sync(m, !le_nn(w, 1e-4)))
+            return sum_tier<8>(w);
+        return sum_tier<4>(w);
+    }
+    // sum_{k < N} (-w)^k / (2k + 1) by Horner's rule (the tiers of sum(), without the branches)
+    template <int N> static __device__ __forceinline__ double sum_tier(double w)
+    {
+        double s = ((N - 1) % 2 ? -1.0 : 1.0) / (2 * N - 1);
+#pragma unroll
+        for (int k = N - 2; k >= 0; --k)
+            s = fma(s, w, (k % 2 ? -1.0 : 1.0) / (2 * k + 1));
+        return s;
+    }
 };
 template <> struct FarSeries<float> {
     static constexpr float kW = 0.04f;
@@ -126,6 +147,7 @@ template <> struct FarSeries<float> {
         s = fmaf(s, w, -1.0f / 3.0f);
         return fmaf(s, w, 1.0f);
     }
+    static __device__ __forceinline__ float sum_uniform(float w) { return sum(w); }
 };
 
 // Induction of one straight segment at point p, scaled by `scale`, added to `acc`.
@@ -142,7 +164,8 @@ template <> struct FarSeries<float> {
 //   * far pairs evaluate ang / h by the arctangent series of FarSeries (no sqrt, no atan2).
 // GAMMA: the scale is the segment's own circulation (sweeps), so that gamma * len comes
 // precomputed from the table; otherwise `scale` (ring sums: +-1).
-template <typename T, bool GAMMA = false>
+// UNIFORM: the series tier is voted over the warp (FarSeries::sum_uniform).
+template <typename T, bool GAMMA = false, bool UNIFORM = false>
 __device__ __forceinline__ void segment_induction(const Segment<T>& s, T px, T py, T pz, T tol2, T scale,
                                                   Vec3<T>& acc)
 {
@@ -157,7 +180,8 @@ __device__ __forceinline__ void segment_induction(const Segment<T>& s, T px, T p
     const T w = hsq * s.len2 * (r * r);  // >= +0, or +NaN
     T mag;
     if (pos(x) && le_nn(w, FarSeries<T>::kW)) {
-        mag = (GAMMA ? -s.glen : -scale * s.len) * r * FarSeries<T>::sum(w);
+        const T S = UNIFORM ? FarSeries<T>::sum_uniform(w) : FarSeries<T>::sum(w);
+        mag = (GAMMA ? -s.glen : -scale * s.len) * r * S;
     } else {
         // one reciprocal square root gives both h and 1/h (no separate sqrt and division)
         const T rh = rsqrt(hsq);
