@@ -181,6 +181,109 @@ __global__ void __launch_bounds__(kCta) gmres_arnoldi_kernel(uint32_t n, double*
     }
 }
 
+// The same column step with this thread's PER entries of w (e = threadIdx.x + i * kCta) held in
+// registers, the projections and the Givens inputs in shared memory: the only global-memory
+// round trips left are the loads of W_j and of the basis rows.  For n <= PER * kCta.
+template <int PER>
+__global__ void __launch_bounds__(kCta) gmres_arnoldi_reg_kernel(uint32_t n, double* __restrict__ V,
+                                                                 const double* __restrict__ W,
+                                                                 float* __restrict__ v32, Ctl* __restrict__ ctl,
+                                                                 uint32_t max_iter, cudaGraphConditionalHandle loop)
+{
+    __shared__ double red[32][kMaxIter + 1];
+    __shared__ double tot[33];
+    __shared__ double hs[kMaxIter + 2], hp[kMaxIter + 1], cs[kMaxIter], sn[kMaxIter];
+    const uint32_t j = ctl->j;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x < j) {  // the previous rotations, for the Givens step at the end
+        cs[threadIdx.x] = ctl->cs[threadIdx.x];
+        sn[threadIdx.x] = ctl->sn[threadIdx.x];
+    }
+    double w[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const uint32_t e = threadIdx.x + q * kCta;
+        w[q] = e < n ? W[(size_t)j * n + e] : 0.0;
+    }
+    for (int pass = 0; pass < 2; ++pass) {
+        for (uint32_t i = 0; i <= j; ++i) {
+            const double* vi = V + (size_t)i * n;
+            double t = 0.0;
+#pragma unroll
+            for (int q = 0; q < PER; ++q) {
+                const uint32_t e = threadIdx.x + q * kCta;
+                if (e < n)
+                    t = fma(vi[e], w[q], t);
+            }
+            t = warp_sum(t);
+            if (lane == 0)
+                red[warp][i] = t;
+        }
+        __syncthreads();
+        if (threadIdx.x <= j) {
+            double c = 0.0;
+            for (int q = 0; q < kCta / 32; ++q)
+                c += red[q][threadIdx.x];
+            hp[threadIdx.x] = c;
+            hs[threadIdx.x] = pass == 0 ? c : hs[threadIdx.x] + c;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            const uint32_t e = threadIdx.x + q * kCta;
+            if (e < n) {
+                double t = w[q];
+                for (uint32_t i = 0; i <= j; ++i)
+                    t = fma(-hp[i], V[(size_t)i * n + e], t);
+                w[q] = t;
+            }
+        }
+        __syncthreads();  // hp is rewritten by the next pass
+    }
+    double ss = 0.0;
+#pragma unroll
+    for (int q = 0; q < PER; ++q)
+        ss = fma(w[q], w[q], ss);
+    const double hn = sqrt(block_sum(ss, tot));
+    const double inv = hn > 0.0 ? 1.0 / hn : 0.0;
+    double* vn = V + (size_t)(j + 1) * n;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const uint32_t e = threadIdx.x + q * kCta;
+        if (e < n) {
+            const double v = w[q] * inv;
+            vn[e] = v;
+            v32[e] = (float)v;
+        }
+    }
+    if (threadIdx.x == 0) {
+        double gj = ctl->g[j];
+        hs[j + 1] = hn;
+        for (uint32_t i = 0; i < j; ++i) {  // the previous rotations
+            const double t = cs[i] * hs[i] + sn[i] * hs[i + 1];
+            hs[i + 1] = -sn[i] * hs[i] + cs[i] * hs[i + 1];
+            hs[i] = t;
+        }
+        const double den = hypot(hs[j], hs[j + 1]);
+        const double c = den == 0.0 ? 1.0 : hs[j] / den, sg = den == 0.0 ? 0.0 : hs[j + 1] / den;
+        hs[j] = c * hs[j] + sg * hs[j + 1];
+        hs[j + 1] = 0.0;
+        double* h = ctl->H[j];
+        for (uint32_t i = 0; i <= j + 1; ++i)
+            h[i] = hs[i];
+        ctl->cs[j] = c;
+        ctl->sn[j] = sg;
+        const double gn = -sg * gj;
+        ctl->g[j + 1] = gn;
+        ctl->g[j] = c * gj;
+        const uint32_t jn = j + 1;
+        ctl->j = jn;
+        const uint32_t done = !(fabs(gn) > ctl->target) || hn == 0.0 || jn >= max_iter;
+        ctl->done = done;
+        cudaGraphSetConditional(loop, done ? 0u : 1u);
+    }
+}
+
 // y from the rotated Hessenberg system, x += Z y, r = r0 - W y (held in r), rel = ||r|| / ||b||,
 // the status record and the fallback condition.
 __global__ void __launch_bounds__(kCta) gmres_update_kernel(uint32_t n, const double* __restrict__ Z,
@@ -192,13 +295,22 @@ __global__ void __launch_bounds__(kCta) gmres_update_kernel(uint32_t n, const do
 {
     __shared__ double y[kMaxIter];
     __shared__ double red[33];
+    __shared__ double R[kMaxIter][kMaxIter + 1], gs[kMaxIter];  // R[l][i] = rotated H, column l
     const uint32_t k = ctl->j;
+    for (uint32_t e = threadIdx.x; e < k * k; e += kCta) {  // the triangle, loaded in parallel
+        const uint32_t l = e / k, i = e % k;
+        if (i <= l)
+            R[l][i] = ctl->H[l][i];
+    }
+    if (threadIdx.x < k)
+        gs[threadIdx.x] = ctl->g[threadIdx.x];
+    __syncthreads();
     if (threadIdx.x == 0) {
-        for (uint32_t i = k; i-- > 0;) {  // back substitution (rows of R = rotated H)
-            double s = ctl->g[i];
+        for (uint32_t i = k; i-- > 0;) {  // back substitution (rows of R)
+            double s = gs[i];
             for (uint32_t l = i + 1; l < k; ++l)
-                s -= ctl->H[l][i] * y[l];
-            const double d = ctl->H[i][i];
+                s -= R[l][i] * y[l];
+            const double d = R[i][i];
             y[i] = d != 0.0 ? s / d : 0.0;
         }
     }
@@ -288,7 +400,18 @@ int capture_graph(SolverGraph* sg, cudaStream_t s, cudaStream_t s2, uint32_t n, 
     pvl_count_launch();
     pvl::launch_gemv<double, double>(n, n, 1.0, A, lda, Z, n, 0.0, nullptr, W, n, &ctl->j, s2);
     pvl_count_launch();
-    gmres_arnoldi_kernel<<<1, kCta, 0, s2>>>(n, V, W, w, v32, ctl, max_iter, loop);
+    if (n <= 1u * kCta)
+        gmres_arnoldi_reg_kernel<1><<<1, kCta, 0, s2>>>(n, V, W, v32, ctl, max_iter, loop);
+    else if (n <= 2u * kCta)
+        gmres_arnoldi_reg_kernel<2><<<1, kCta, 0, s2>>>(n, V, W, v32, ctl, max_iter, loop);
+    else if (n <= 4u * kCta)
+        gmres_arnoldi_reg_kernel<4><<<1, kCta, 0, s2>>>(n, V, W, v32, ctl, max_iter, loop);
+    else if (n <= 8u * kCta)
+        gmres_arnoldi_reg_kernel<8><<<1, kCta, 0, s2>>>(n, V, W, v32, ctl, max_iter, loop);
+    else if (n <= 16u * kCta)
+        gmres_arnoldi_reg_kernel<16><<<1, kCta, 0, s2>>>(n, V, W, v32, ctl, max_iter, loop);
+    else
+        gmres_arnoldi_kernel<<<1, kCta, 0, s2>>>(n, V, W, w, v32, ctl, max_iter, loop);
     pvl_count_launch();
     const cudaError_t eb = cudaGetLastError();
     cudaGraph_t body_out = nullptr;
