@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(THREADS) ring_tile_kernel(uint32_t n_surfaces,
             sg.r1x = sg.r1y = sg.r1z = sg.dx = sg.dy = sg.dz = 0.0;
             sg.len = sg.len2 = sg.gamma = sg.glen = sg.pad0 = sg.pad1 = 0.0;
         }
-#pragma unroll 4
+#pragma unroll  // all 8 control points: 232 vs 236 us for the body (unroll 4), no spills
         for (int q = 0; q < kTileCPB; ++q) {
             Vec3<double> acc{0.0, 0.0, 0.0};
             pvl::segment_induction<double, false, true>(sg, s_p[q][0], s_p[q][1], s_p[q][2], tol2, 1.0, acc);
