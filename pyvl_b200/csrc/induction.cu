@@ -22,8 +22,8 @@ using pvl::Vec3;
 namespace {
 
 constexpr int kSegTile = 128;   // segments per shared-memory tile
-constexpr int kReducePts = 32;    // points per CTA of the partial-sum reduction
-constexpr int kReduceGroups = 8;  // rows of threads (split groups) per CTA
+constexpr int kReducePts = 16;     // points per CTA of the partial-sum reduction (256 CTAs at 4096)
+constexpr int kReduceGroups = 16;  // rows of threads (split groups) per CTA
 constexpr int kSumThreads = 128;
 constexpr int kRingThreads = 128;
 constexpr int kRingCPB = 8;     // control points per CTA row-block in ring matrices
