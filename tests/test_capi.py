@@ -127,3 +127,50 @@ def test_wake_node_columns_merge_shared_trailing_edge_nodes():
     # per strip: R + 1 spanwise and 2 R streamwise lines; two shared columns save 2 R lines
     assert plain.n_lines == S * (3 * R + 1)
     assert merged.n_lines == plain.n_lines - 2 * R
+
+
+def test_argument_errors_are_reported_before_any_device_work():
+    """Null pointers, bad sizes and short workspaces come back as the reference's exception
+    types with a message, from the host-side checks that run before any CUDA call (so they
+    hold without a GPU).  Fake device addresses stand in where a pointer must be non-null."""
+    fake = 1 << 20  # 16-byte aligned, never dereferenced: every call below fails before use
+    # the far-field evaluator
+    _lib.call("pvl_far_series_eval", 0, None, None, None, None, None)  # nothing to do
+    with pytest.raises(ValueError, match="null pointer"):
+        _lib.call("pvl_far_series_eval", 8, None, fake, fake, fake, None)
+    # the segment-sum velocity
+    with pytest.raises(ValueError, match="pts is NULL"):
+        _lib.call("pvl_line_velocity", _lib.PVL_F64, 4, 2, fake, fake, fake, 5, None, None, 1e-6, 1.0, 0.0, fake,
+                  fake, 1 << 20, None)
+    with pytest.raises(ValueError, match="unknown precision"):
+        _lib.call("pvl_line_velocity", 7, 4, 2, fake, fake, fake, 5, fake, None, 1e-6, 1.0, 0.0, fake, fake,
+                  1 << 20, None)
+    need = _lib.query("pvl_line_velocity_workspace", 2, 5, _lib.PVL_F64)
+    with pytest.raises(_lib.PvlError, match="workspace"):
+        _lib.call("pvl_line_velocity", _lib.PVL_F64, 4, 2, fake, fake, fake, 5, fake, None, 1e-6, 1.0, 0.0, fake,
+                  fake, need - 1, None)
+    # the device-driven GMRES graph
+    n = 64
+    args = dict(n=n, A=fake, lda=n, Minv=fake, ldm=n, b=fake, x=fake, V=fake, Z=fake, W=fake, r0=fake, w=fake,
+                v32=fake, ctl=fake, max_iter=8, tol=1e-12, ipiv=fake, info=fake, ws=fake,
+                ws_bytes=_lib.query("pvl_lu_workspace", n), gamma=None, n_gamma=0, n_groups=0, group_offsets=None,
+                status=fake)
+    h = ctypes.c_uint64(7)
+
+    def create(**kw):
+        a = dict(args, **kw)
+        _lib.call("pvl_gmres_graph_create", *a.values(), ctypes.byref(h))
+
+    with pytest.raises(ValueError, match="graph_out is NULL"):
+        _lib.call("pvl_gmres_graph_create", *args.values(), None)
+    with pytest.raises(ValueError, match="null pointer"):
+        create(W=None)
+    assert h.value == 0  # cleared before the checks
+    with pytest.raises(ValueError, match="max_iter"):
+        create(max_iter=_lib.query("pvl_gmres_max_iter") + 1)
+    with pytest.raises(ValueError, match="inconsistent sizes"):
+        create(lda=n - 1)
+    with pytest.raises(ValueError, match="aligned"):
+        create(v32=fake + 4)
+    with pytest.raises(_lib.PvlError, match="workspace"):
+        create(ws_bytes=args["ws_bytes"] - 1)
