@@ -515,6 +515,45 @@ class SolverEngine:
             raise _lib.PvlError(_lib.PVL_ERR_SINGULAR, f"exactly singular system: U[{info - 1},{info - 1}] == 0")
 
 
+class RefreshPolicy:
+    """When the mixed solve rebuilds its FP32 preconditioner, from the Krylov iteration counts
+    of the solves since the last rebuild (host logic only).
+
+    A rebuild is due every ``period`` steps when that is set; otherwise, with no rebuild in
+    flight and at least two steps since the last one, when the latest solve needed
+    ``on_iters`` iterations and at least 3 more than the fewest since the last rebuild (a
+    stale preconditioner), or when the iterations above that fewest count add up to
+    ``excess`` (a preconditioner that costs one extra column per step is kept for a while: a
+    rebuild costs as much as a few hundred columns)."""
+
+    def __init__(self, on_iters: int, excess: int, period: int | None = None):
+        self.on_iters = int(on_iters)
+        self.excess_limit = int(excess)
+        self.period = None if period is None else int(period)
+        self.best: int | None = None  # fewest iterations of a solve since the last rebuild
+        self.excess = 0               # iterations above that since the last rebuild
+        self.last: int | None = None  # the latest solve's count
+
+    def observe(self, counts) -> None:
+        """Take the iteration counts of further solves, in order."""
+        for k in counts:
+            k = int(k)
+            self.best = k if self.best is None else min(self.best, k)
+            self.excess += k - self.best
+            self.last = k
+
+    def rebuilt(self) -> None:
+        self.best = None
+        self.excess = 0
+
+    def due(self, steps_since_rebuild: int, idle: bool) -> bool:
+        if self.period is not None and steps_since_rebuild >= self.period:
+            return True
+        slow = self.last is not None and self.last >= self.on_iters and (
+            self.best is None or self.last >= self.best + 3)
+        return idle and steps_since_rebuild >= 2 and (slow or self.excess >= self.excess_limit)
+
+
 class MixedSolverEngine(SolverEngine):
     """The mixed-precision step: the FP64 system solved to FP64 accuracy with cheaper arithmetic.
 
@@ -550,8 +589,6 @@ class MixedSolverEngine(SolverEngine):
         self.refresh = None if refresh is None else int(refresh)
         self.refresh_excess = int(refresh_excess)
         self._iters_seen = 0      # solves the refresh policy has looked at
-        self._iters_best = None   # fewest iterations of a solve since the last rebuild
-        self._iters_excess = 0    # iterations above that since the last rebuild
         self.gmres_tol = float(gmres_tol)
         self.max_iter = int(max_iter)
         n = self.N
@@ -566,6 +603,7 @@ class MixedSolverEngine(SolverEngine):
                                device=self.dev)
         self.async_refresh = bool(async_refresh)
         self.refresh_on_iters = int(refresh_on_iters)  # a solve that needed this many iterations refreshes early
+        self.policy = RefreshPolicy(self.refresh_on_iters, self.refresh_excess, self.refresh)
         self.side = torch.cuda.Stream(device=self.dev)
         self.refresh_done = None
         self.ipiv32 = torch.zeros(2 * self.npad, dtype=torch.int32, device=self.dev)
@@ -668,8 +706,7 @@ class MixedSolverEngine(SolverEngine):
                 self.refresh_done.record()
         self.have_precond = True
         self.steps_since_refresh = 0
-        self._iters_best = None
-        self._iters_excess = 0
+        self.policy.rebuilt()
         self._stats["refreshes"] += 1
 
     def _adopt_refresh(self) -> None:
@@ -813,20 +850,11 @@ class MixedSolverEngine(SolverEngine):
         (the policy of the class docstring)."""
         self._adopt_refresh()
         its = self._stats["gmres_iters"]
-        for k in its[self._iters_seen:]:
-            self._iters_best = k if self._iters_best is None else min(self._iters_best, k)
-            self._iters_excess += k - self._iters_best
+        self.policy.observe(its[self._iters_seen:])
         self._iters_seen = len(its)
-        idle = self.refresh_done is None
-        # a slow solve triggers a rebuild only when it is well above the best count since the
-        # last rebuild: a system whose iteration count just wanders (a growing wake) is left to
-        # the accumulated-excess rule, since a rebuild costs as much as hundreds of columns
-        slow = bool(its) and its[-1] >= self.refresh_on_iters and (
-            self._iters_best is None or its[-1] >= self._iters_best + 3)
         if not self.have_precond:
             self.refresh_preconditioner(wait=True)
-        elif (self.refresh is not None and self.steps_since_refresh >= self.refresh) or (
-                idle and self.steps_since_refresh >= 2 and (slow or self._iters_excess >= self.refresh_excess)):
+        elif self.policy.due(self.steps_since_refresh, idle=self.refresh_done is None):
             self.refresh_preconditioner(wait=not self.async_refresh)
         self.steps_since_refresh += 1
 
