@@ -11,10 +11,11 @@ is one iteration of the solver loop.
 
 Paths (both are timed; ``value`` is the one named by --path, default mixed):
 * mixed (+ learned): FP64 assembly and wake terms, GMRES with FP64 residuals preconditioned by
-  the inverse of an FP32 tensor-core LU refreshed every 25 steps, seeded by the per-panel MLP
-  (trained beforehand, outside the timed region, on 64 earlier steps of the plain engine),
-  FP32 far-row advection.  Its circulation is judged after the timed steps against the
-  all-FP64 step of the same state (``accuracy``).
+  the inverse of an FP32 tensor-core LU rebuilt when it goes stale (engine.RefreshPolicy),
+  seeded by the per-panel MLP (trained beforehand, outside the timed region, on 64 earlier
+  steps of the plain engine), FP32 far-row advection.  Its circulation, and the lift
+  coefficient from it, are judged after the timed steps against the all-FP64 step of the same
+  state (``accuracy``).
 * plain: FP64 assembly, FP64 LU every step.
 
 * ``value``: steps/s with each step's body positions/velocities already in HBM.
