@@ -2,7 +2,7 @@
 // and FP32 accumulation (tcgen05.mma kind::tf32, accumulator in tensor memory).
 //
 // Used by the low-precision preconditioner (the approximate inverse of the system matrix,
-// refreshed every few steps, and the trailing update of the FP32 LU).  Row-major A (M x K),
+// rebuilt when it goes stale, and the trailing update of the FP32 LU).  Row-major A (M x K),
 // B (K x N), C (M x N); any M and N (rows and columns past the edge of a tile are staged as
 // zeros and not stored), K a multiple of 32, leading dimensions multiples of 4 floats,
 // 16-byte aligned bases.

@@ -49,8 +49,8 @@ template <typename T> struct Vec3 { T x, y, z; };
 // gives ang / h = -(len / x) S(w) with w = h^2 len^2 / x^2 -- no square root and no atan2.
 // The series is used only for w <= kW, where the first omitted term bounds the relative
 // truncation error: double, 16 terms for w <= 0.1 (0.1^16 / 33 < 4e-18), 8 terms for
-// w <= 0.01 (0.01^8 / 17 < 1e-17) and 5 terms for w <= 1e-4 (1e-20 / 11 < 1e-21); float,
-// 6 terms for w <= 0.04 (0.04^6 / 13 < 4e-10).
+// w <= 0.01 (0.01^8 / 17 < 1e-17) and 4 terms for w <= 1e-4 (1e-16 / 9 < 1.2e-17); float,
+// 5 terms for w <= 0.04 (0.04^5 / 11 < 1e-8).
 // Closer pairs (larger w, or x <= 0) take the atan2 form.
 // Comparisons of non-negative values (or +NaN) through their bit patterns: for IEEE numbers of
 // one sign, the order of the bit patterns is the order of the values, and the integer compare
