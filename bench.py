@@ -267,6 +267,25 @@ def profile_kernel(args) -> None:
     print("profile-kernel done", args.profile_kernel)
 
 
+def reduce_max_over_ranks(x: float, dist, device: str) -> float:
+    """The largest of the ranks' values (every rank gets it); x itself without a process group.
+    Each rank's timed region is measured on its own device, and the job's time is the slowest
+    rank's."""
+    if dist is None:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(steps: int, ms_max: float, world: int) -> float:
+    """Whole-job steps/s of ``world`` independent replicas that each ran ``steps`` steps, the
+    slowest in ``ms_max`` milliseconds (weak scaling: the work grows with the ranks)."""
+    return world * steps / (ms_max * 1e-3)
+
+
 def lift_at_state(case, mesh, spec, eng, pos, vel, gamma) -> float:
     """CL of the ring circulations ``gamma`` at the engine's body positions and wake state
     before its wake update (circulatory_forces, python/pyvl/postprocess/forces.py:10-42: line
@@ -532,11 +551,7 @@ def main() -> None:
             dist.barrier()
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max_over_ranks(x, dist, "cuda")
 
     def make(kind):
         if kind == "plain":
@@ -706,8 +721,8 @@ def main() -> None:
             if line.startswith("traffic_bytes_per_launch:"):
                 traffic = float(line.split(":", 1)[1].split()[0])
     head = results[args.path]
-    sps = world * K / (head["ms"] * 1e-3)
-    sps_e2e = world * K / (head["ms_e2e"] * 1e-3)
+    sps = replica_throughput(K, head["ms"], world)
+    sps_e2e = replica_throughput(K, head["ms_e2e"], world)
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline()
@@ -726,11 +741,11 @@ def main() -> None:
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "per-step working set (134 MB matrix + wake) exceeds the 126 MB L2"},
             "paths": {
-                "plain_fp64": {"steps_per_s": world * K / (results["plain"]["ms"] * 1e-3),
+                "plain_fp64": {"steps_per_s": replica_throughput(K, results["plain"]["ms"], world),
                                "ms_per_step": results["plain"]["ms"] / K,
-                               "e2e_steps_per_s": world * K / (results["plain"]["ms_e2e"] * 1e-3)},
-                "mixed_learned": {"steps_per_s": world * K / (mx["ms"] * 1e-3), "ms_per_step": mx["ms"] / K,
-                                  "e2e_steps_per_s": world * K / (mx["ms_e2e"] * 1e-3),
+                               "e2e_steps_per_s": replica_throughput(K, results["plain"]["ms_e2e"], world)},
+                "mixed_learned": {"steps_per_s": replica_throughput(K, mx["ms"], world), "ms_per_step": mx["ms"] / K,
+                                  "e2e_steps_per_s": replica_throughput(K, mx["ms_e2e"], world),
                                   "gmres_iters_mean": mx["gmres_iters_mean"], "fallbacks": mx["fallbacks"],
                                   "preconditioner_refreshes": mx["refreshes"],
                                   "initial_rel_residual_median": mx["initial_rel_residual_median"],
