@@ -35,7 +35,8 @@ enum {
     PVL_ERR_SINGULAR = -4,      /* exactly zero pivot met by the LU factorisation */
     PVL_ERR_NOT_CONVERGED = -5, /* an iterative solve missed its tolerance */
     PVL_ERR_TOPOLOGY = -6,      /* topology construction failed (RuntimeError in the reference) */
-    PVL_ERR_TIMEOUT = -7        /* a device-side wait gave up (bounded spin) */
+    PVL_ERR_TIMEOUT = -7,       /* a device-side wait gave up (bounded spin) */
+    PVL_ERR_NONFINITE = -8      /* a NaN or infinity reached the system (set by pvl_rhs through its status word) */
 };
 
 enum { PVL_F64 = 0, PVL_F32 = 1 };
@@ -103,10 +104,13 @@ int pvl_surface_average(uint32_t n_surfaces, const uint32_t* surface_offsets,
                         const double* values, double* out, void* stream);
 
 /* No-penetration right-hand side b_i = n_i . (-(U_i - v_i)) with U_i = flow[i] when
- * flow != NULL else (ux, uy, uz); cp_velocity may be NULL (zero).
- * Replaces python/pyvl/solver.py:199-206. */
+ * flow != NULL else (ux, uy, uz); cp_velocity may be NULL (zero).  When `nonfinite` is not
+ * NULL, any b_i that is a NaN or an infinity (a NaN or infinity in a position, a velocity or the
+ * stream of an element) sets *nonfinite = 1; the word is never cleared here, so it holds the
+ * error until the caller reads and resets it.
+ * Replaces python/pyvl/solver.py:199-206 (where a NaN propagates silently). */
 int pvl_rhs(uint32_t n, const double* normals, const double* flow, double ux, double uy,
-            double uz, const double* cp_velocity, double* rhs_out, void* stream);
+            double uz, const double* cp_velocity, double* rhs_out, int32_t* nonfinite, void* stream);
 
 /* ------------------------------------------------------------------ induction */
 
@@ -301,14 +305,16 @@ int pvl_border_groups(uint32_t n, uint32_t m, const uint32_t* group_offsets, dou
 
 /* ------------------------------------------------------------------ tensor cores */
 
-/* C = alpha * A * B + beta * C on the 5th-generation tensor cores (tcgen05, accumulator in
- * tensor memory): FP32 storage, TF32 multiplication, FP32 accumulation.  Row-major A (M x K),
- * B (K x N), C (M x N); any M and N, K a multiple of 32, leading dimensions multiples of
- * 4 floats, 16-byte aligned bases.  err (device int32) is set to 1 if an
- * internal wait timed out.  No reference counterpart: it builds the low-precision
- * preconditioner that replaces the per-step FP64 factorisation in the mixed path. */
+/* C = alpha * A * B + beta * C on the 5th-generation tensor cores (tcgen05, accumulators in
+ * tensor memory, operands brought in by TMA): FP32 storage, TF32 multiplication, FP32
+ * accumulation.  Row-major A (M x K); B given as its transpose Bt (N x K, row-major), so that
+ * both operands are K-major; row-major C (M x N).  Any M and N, K a positive multiple of 32,
+ * leading dimensions multiples of 4 floats (and >= K, resp. N), 16-byte aligned bases.
+ * err (device int32) is set to 1 if an internal wait timed out.  No reference counterpart: it
+ * builds the low-precision preconditioner that replaces the per-step FP64 factorisation in
+ * the mixed path. */
 int pvl_gemm_tf32(uint32_t M, uint32_t N, uint32_t K, float alpha, const float* A, uint32_t lda,
-                  const float* B, uint32_t ldb, float beta, float* C, uint32_t ldc, int32_t* err,
+                  const float* Bt, uint32_t ldbt, float beta, float* C, uint32_t ldc, int32_t* err,
                   void* stream);
 
 /* ------------------------------------------------------------------ mixed-precision solve */
@@ -539,19 +545,6 @@ int pvl_line_forces(uint32_t n_lines, const uint32_t* primal_lines, const uint32
 /* Number of kernels this library has enqueued since it was loaded (all threads).  No
  * reference counterpart: it lets a benchmark state how many of the library's kernels ran. */
 unsigned long long pvl_launch_count(void);
-
-/* Enqueue a kernel of n_blocks x 256 threads, each running 8 independent FMA chains of
- * `iters` steps in `precision`; returns the exact FLOP count it performs (2 per FMA), or a
- * negative value on error.  `sink` is a device buffer of n_blocks elements (never written in
- * practice).  Timing it with events gives the non-tensor FMA peak of the GPU.  No reference
- * counterpart (measurement helper). */
-double pvl_fma_probe(int precision, uint32_t n_blocks, uint32_t iters, void* sink, void* stream);
-
-/* rcp[i] = the FP64 pair kernels' 1/x[i] (hardware seed and one third-order refinement) and
- * sum[i] = their arctangent series sum_k (-w)^k / (2k + 1) at w[i] (w in [0, 0.1]), for n
- * device values; lets a test hold the far-field arithmetic to its error bounds.  No reference
- * counterpart (the reference calls atan2 for every pair, src/core/flow_solver.c:113-135). */
-int pvl_far_series_eval(uint32_t n, const double* x, const double* w, double* rcp, double* sum, void* stream);
 
 #ifdef __cplusplus
 }

@@ -2,7 +2,11 @@
 # Compile the reference's own C extension (`pyvl.cvl`) from its sources, where they
 # lie, into oracle/_ref/.  Test infrastructure only: the product never loads it.
 #
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default: /root/reference)
+# Usage: oracle/build_ref.sh [--if-present] [REFERENCE_ROOT]
+#
+# REFERENCE_ROOT defaults to $PYVL_REFERENCE_ROOT, else to the checkout this build recipe
+# was written against (/root/reference).  With --if-present a missing tree is not an error
+# (the prebuilt oracle/_ref, if any, is kept).
 #
 # The output, oracle/_ref/cvl<EXT_SUFFIX>, is the unmodified reference induction,
 # topology and line-force code (src/core/*.c + src/*.c, built the way the
@@ -10,12 +14,20 @@
 # and travels to the GPU host as a prebuilt file; nothing here needs the reference
 # tree at run time.
 set -euo pipefail
-REF="${1:-/root/reference}"
+IF_PRESENT=0
+if [ "${1:-}" = "--if-present" ]; then
+  IF_PRESENT=1
+  shift
+fi
+REF="${1:-${PYVL_REFERENCE_ROOT:-/root/reference}}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 OUT="$HERE/_ref"
 PY="${PYTHON:-python3}"
 if [ ! -d "$REF/src/core" ]; then
   echo "reference sources not found under $REF" >&2
+  if [ "$IF_PRESENT" = 1 ]; then
+    exit 0
+  fi
   exit 1
 fi
 EXT_SUFFIX="$($PY -c 'import sysconfig;print(sysconfig.get_config_var("EXT_SUFFIX"))')"

@@ -12,6 +12,7 @@ from __future__ import annotations
 
 import importlib.machinery
 import importlib.util
+import os
 import sys
 import sysconfig
 from pathlib import Path
@@ -39,9 +40,18 @@ def load_cvl():
     return mod
 
 
-def load_pyvl(reference_root: str | Path = "/root/reference"):
+def reference_root(given: str | Path | None = None) -> Path:
+    """The reference checkout: ``given``, else $PYVL_REFERENCE_ROOT."""
+    if given is None:
+        given = os.environ.get("PYVL_REFERENCE_ROOT")
+    if not given:
+        raise FileNotFoundError("the reference checkout is not known: pass its path or set PYVL_REFERENCE_ROOT")
+    return Path(given)
+
+
+def load_pyvl(reference_root_dir: str | Path | None = None):
     """Import the reference Python package on top of the compiled extension."""
-    root = Path(reference_root) / "python"
+    root = reference_root(reference_root_dir) / "python"
     if not (root / "pyvl" / "__init__.py").exists():
         raise FileNotFoundError(f"reference python package not found under {root}")
     load_cvl()

@@ -35,7 +35,8 @@ def wake_ring_connectivity(line_rows: int, n_lines: int) -> np.ndarray:
 class OracleWake:
     """State and operations of WakeModelLineExplicitUnsteady (wake_models.py:17-330)."""
 
-    def __init__(self, bordering_nodes, shedding_lines, adjacent_surfaces, vortex_tol, time, line_rows):
+    def __init__(self, bordering_nodes, shedding_lines, adjacent_surfaces, vortex_tol, time, line_rows,
+                 mesh_cls=OracleMesh):
         # wake_models.py:54-81
         self.shedding_lines = np.array(shedding_lines, np.uint64)
         S = self.shedding_lines.size
@@ -45,7 +46,7 @@ class OracleWake:
         self.adjacent_surfaces = np.array(adjacent_surfaces, np.uint64)
         self.vortex_tol = float(vortex_tol)
         self.circulation = np.zeros((S, line_rows), np.float64)
-        self.wake_mesh = OracleMesh(2 * (line_rows + 1) * S, wake_ring_connectivity(line_rows, S))
+        self.wake_mesh = mesh_cls(2 * (line_rows + 1) * S, wake_ring_connectivity(line_rows, S))
         self.current_time = float(time)
         self.step_count = 0
 
@@ -155,17 +156,20 @@ def bordered_solve(A, b, groups):
 
 
 class OracleRun:
-    """One run of the reference solver loop (solver.py:175-263) on a workload Case."""
+    """One run of the reference solver loop (solver.py:175-263) on a workload Case.
 
-    def __init__(self, case, closed_mode: str = "reference", wake_self_induction: bool = False):
+    ``mesh_cls`` supplies the pair kernels: OracleMesh (the C restatement, oracle.c) by default;
+    oracle/refbench.py passes an adapter over the reference's own compiled extension."""
+
+    def __init__(self, case, closed_mode: str = "reference", wake_self_induction: bool = False, mesh_cls=OracleMesh):
         self.case = case
         self.wake_self_induction = wake_self_induction
-        self.mesh = OracleMesh(case.n_points, case.elements)
+        self.mesh = mesh_cls(case.n_points, case.elements)
         self.closed_mode = closed_mode
         self.wake = None
         if case.line_rows > 0 and len(case.te_node_pairs):
             shed, nodes, adj = shedding_setup(self.mesh, case.te_node_pairs)
-            self.wake = OracleWake(nodes, shed, adj, case.tol, case.t0, case.line_rows)
+            self.wake = OracleWake(nodes, shed, adj, case.tol, case.t0, case.line_rows, mesh_cls)
         self.iteration = 0
         self.history = []
 

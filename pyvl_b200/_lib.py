@@ -21,6 +21,7 @@ PVL_ERR_SINGULAR = -4
 PVL_ERR_NOT_CONVERGED = -5
 PVL_ERR_TOPOLOGY = -6
 PVL_ERR_TIMEOUT = -7
+PVL_ERR_NONFINITE = -8
 PVL_F64 = 0
 PVL_F32 = 1
 INVALID_ID = 0x7FFFFFFF
@@ -41,7 +42,7 @@ SIGNATURES = {
     "pvl_line_ring_map": (_I, [_U, _U, _P, _P, _P, _P]),
     "pvl_surface_normal": (_I, [_U, _P, _P, _P, _P, _P, _P]),
     "pvl_surface_average": (_I, [_U, _P, _P, _P, _P, _P, _P]),
-    "pvl_rhs": (_I, [_U, _P, _P, _D, _D, _D, _P, _P, _P]),
+    "pvl_rhs": (_I, [_U, _P, _P, _D, _D, _D, _P, _P, _P, _P]),
     "pvl_segments_workspace": (_Z, [_U, _I]),
     "pvl_line_induction": (_I, [_U, _U, _P, _P, _U, _P, _D, _P, _P, _Z, _P]),
     "pvl_induction_matrix": (_I, [_U, _U, _P, _P, _U, _P, _P, _U, _P, _D, _P, _P, _Z, _P]),
@@ -116,8 +117,6 @@ SIGNATURES = {
                           _P]),
     "pvl_mlp_to_bf16": (_I, [_P, _P, _P]),
     "pvl_launch_count": (ctypes.c_ulonglong, []),
-    "pvl_fma_probe": (_D, [_I, _U, _U, _P, _P]),
-    "pvl_far_series_eval": (_I, [_U, _P, _P, _P, _P, _P]),
 }
 
 _lib = None

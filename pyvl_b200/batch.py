@@ -192,6 +192,12 @@ class BatchEngine:
         for k in range(B):
             rows_k = np.sort(min_row[wline_off[k]:wline_off[k + 1]])
             self.seg_upto[k * (R + 1):(k + 1) * (R + 1)] = np.searchsorted(rows_k, np.arange(R + 1), side="left")
+        # segment-point pairs of the two sweeps once every wake has all R rows: the explicit wake
+        # term (each case's wake lines at its control points) and the advection (each case's body
+        # lines at its distinct wake node columns, every row)
+        full = self.seg_upto.reshape(B, R + 1)[:, R].astype(np.int64)
+        self.sweep_pairs_full = {"wake": int(np.sum(full * np.asarray(P, np.int64))),
+                                 "advect": int(np.sum(np.asarray(L, np.int64) * np.asarray(NC, np.int64) * R))}
         self.d_body = None if host_only else self.body.device_arrays()
         self.d_wake = None if host_only else {
             "lines": to_device_u32(self.wake_lines_rm, dev),
@@ -368,7 +374,7 @@ class BatchEngine:
                   ptr(self.vel), ptr(self.cpv), s)
         _lib.call("pvl_surface_normal", NR, ptr(d["offsets"]), ptr(d["surface_lines"]), ptr(d["lines"]),
                   ptr(self.pos), ptr(self.nrm), s)
-        _lib.call("pvl_rhs", NR, ptr(self.nrm), ptr(self.flow), 0.0, 0.0, 0.0, ptr(self.cpv), ptr(self.rhs), s)
+        _lib.call("pvl_rhs", NR, ptr(self.nrm), ptr(self.flow), 0.0, 0.0, 0.0, ptr(self.cpv), ptr(self.rhs), None, s)
         if self.static and self.A_body is not None:
             self.A.copy_(self.A_body)
         else:
@@ -425,6 +431,26 @@ class BatchEngine:
         """Body node positions of every case (list of (n_points_c, 3) arrays)."""
         self.pos.copy_(torch.as_tensor(np.concatenate([np.asarray(p, np.float64) for p in positions]),
                                        device=self.dev))
+
+    def load_positions_host(self, flat: torch.Tensor) -> None:
+        """All cases' node positions, concatenated ((n_points, 3) FP64, pinned host memory), copied
+        in asynchronously on the current stream; the captured step reads them from there."""
+        self.pos.copy_(flat.reshape(self.pos.shape), non_blocking=True)
+
+    def gamma_host_async(self):
+        """Start copying every case's circulations (concatenated in case order) to pinned host
+        memory; the returned object's result() waits for that copy only."""
+        from .engine import HostResult
+
+        if not hasattr(self, "_h_ring"):
+            self._h_ring = [torch.empty(self.gamma.shape, dtype=torch.float64, pin_memory=True) for _ in range(4)]
+            self._h_next = 0
+        buf = self._h_ring[self._h_next]
+        self._h_next = (self._h_next + 1) % len(self._h_ring)
+        buf.copy_(self.gamma, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record()
+        return HostResult(buf, ev)
 
     def start(self, time: float = 0.0) -> None:
         """Positions at ``time`` and the wake pinned to the trailing edges (first wake update)."""

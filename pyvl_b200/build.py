@@ -4,7 +4,9 @@
 
 The library is compiled from pyvl_b200/csrc/*.cu and *.cpp with
 ``-gencode arch=compute_100a,code=sm_100a`` and lands next to this file, where the
-Python layer loads it.  nvcc cross-compiles without a GPU.
+Python layer loads it.  nvcc cross-compiles without a GPU.  Beside it, libpvl_probe.so
+(pyvl_b200/probe: an FMA-throughput probe and test hooks) is built for benchmarks and tests;
+the product never loads it.
 """
 
 from __future__ import annotations
@@ -14,11 +16,14 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 LIB = HERE / "libpvl_b200.so"
+PROBE_SRC = HERE / "probe"
+PROBE_LIB = HERE / "libpvl_probe.so"  # measurement and test probes, not part of the product ABI
 BUILD_DIR = HERE.parent / "_build"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -34,22 +39,38 @@ def sources() -> list[Path]:
     return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
 
 
-def needs_build() -> bool:
-    if not LIB.exists():
+def _headers() -> list[Path]:
+    return sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + [HERE.parent / "include" / "pvl_b200.h"]
+
+
+def needs_build(lib: Path = LIB, srcs: list[Path] | None = None) -> bool:
+    if not lib.exists():
         return True
-    t = LIB.stat().st_mtime
-    deps = sources() + sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + [HERE.parent / "include" / "pvl_b200.h"]
+    t = lib.stat().st_mtime
+    deps = (sources() if srcs is None else srcs) + _headers() + sorted(PROBE_SRC.glob("*.h"))
     return any(p.stat().st_mtime > t for p in deps)
 
 
 def build(verbose: bool = False, force: bool = False) -> Path:
-    if not force and not needs_build():
-        return LIB
+    """Build libpvl_b200.so and the probe library beside it; returns the product library."""
+    _build_lib(LIB, sources(), "", verbose, force)
+    # the probes reach internal launchers of the product library: link it, found beside them
+    _build_lib(PROBE_LIB, sorted(PROBE_SRC.glob("*.cu")), "probe_", verbose, force,
+               ["-L", str(HERE), "-lpvl_b200", "-Xlinker", "-rpath=$ORIGIN"], after=LIB)
+    return LIB
+
+
+def _build_lib(lib: Path, srcs: list[Path], prefix: str, verbose: bool, force: bool, link: list[str] | None = None,
+               after: Path | None = None) -> Path:
+    stale = after is not None and lib.exists() and after.stat().st_mtime > lib.stat().st_mtime
+    if not force and not stale and not needs_build(lib, srcs):
+        return lib
     BUILD_DIR.mkdir(exist_ok=True)
-    objs = []
-    common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(HERE.parent / "include"), "-I", str(CSRC)]
-    for src in sources():
-        obj = BUILD_DIR / (src.name + ".o")
+    common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(HERE.parent / "include"), "-I", str(CSRC),
+              "-I", str(PROBE_SRC)]
+
+    def compile_one(src: Path) -> str:
+        obj = BUILD_DIR / (prefix + src.name + ".o")
         cmd = [nvcc(), *common, *ARCH, "-lineinfo", "-c", str(src), "-o", str(obj)]
         if verbose and src.suffix == ".cu":
             cmd += ["-Xptxas", "-v"]
@@ -58,15 +79,19 @@ def build(verbose: bool = False, force: bool = False) -> Path:
             sys.stderr.write(r.stdout + r.stderr)
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed on {src.name}")
-        objs.append(str(obj))
-    tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart_static", "-lrt", "-ldl", "-lpthread"]
+        return str(obj)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(srcs), os.cpu_count() or 1))) as pool:
+        objs = list(pool.map(compile_one, srcs))
+    tmp = lib.with_suffix(".so.tmp")
+    cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, *(link or []), "-lcudart_static", "-lrt", "-ldl",
+           "-lpthread"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("link failed")
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib)
+    return lib
 
 
 def main() -> None:

@@ -700,7 +700,7 @@ int launch_ring_tiled(const void* jobs, const uint32_t* job_item, uint32_t n_job
                         "shared memory", tile_stride, CPB);
     const void* fn = fold_adj ? (const void*)batched_ring_tile_kernel<CPB, true>
                               : (const void*)batched_ring_tile_kernel<CPB, false>;
-    PVL_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PVL_SMEM_OPTIN(fn, smem);
     if (n_ctas == 0) {
         int dev = 0, sms = 0, per = 0;
         if (cudaGetDevice(&dev) != cudaSuccess ||

@@ -557,7 +557,8 @@ __global__ void surface_average_kernel(uint32_t n_surfaces, const uint32_t* __re
 
 // python/pyvl/solver.py:199-206
 __global__ void rhs_kernel(uint32_t n, const double* __restrict__ normals, const double* __restrict__ flow, double ux,
-                           double uy, double uz, const double* __restrict__ cpv, double* __restrict__ rhs)
+                           double uy, double uz, const double* __restrict__ cpv, double* __restrict__ rhs,
+                           int32_t* __restrict__ nonfinite)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
@@ -569,7 +570,10 @@ __global__ void rhs_kernel(uint32_t n, const double* __restrict__ normals, const
         ey -= cpv[3 * (size_t)i + 1];
         ez -= cpv[3 * (size_t)i + 2];
     }
-    rhs[i] = normals[3 * (size_t)i] * -ex + normals[3 * (size_t)i + 1] * -ey + normals[3 * (size_t)i + 2] * -ez;
+    const double b = normals[3 * (size_t)i] * -ex + normals[3 * (size_t)i + 1] * -ey + normals[3 * (size_t)i + 2] * -ez;
+    rhs[i] = b;
+    if (nonfinite && !isfinite(b))
+        atomicExch(nonfinite, 1);
 }
 
 // src/meshobject.c:1368-1393
@@ -696,13 +700,13 @@ extern "C" int pvl_surface_average(uint32_t n_surfaces, const uint32_t* off, con
 }
 
 extern "C" int pvl_rhs(uint32_t n, const double* normals, const double* flow, double ux, double uy, double uz,
-                       const double* cp_velocity, double* rhs_out, void* stream)
+                       const double* cp_velocity, double* rhs_out, int32_t* nonfinite, void* stream)
 {
     if (n == 0)
         return PVL_OK;
     PVL_REQUIRE(normals); PVL_REQUIRE(rhs_out);
     rhs_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(n, normals, flow, ux, uy, uz, cp_velocity,
-                                                                     rhs_out);
+                                                                     rhs_out, nonfinite);
     PVL_LAUNCH_CHECK();
     return PVL_OK;
 }
@@ -814,12 +818,7 @@ int launch_ring_tile(dim3 grid, size_t smem, cudaStream_t st, uint32_t n_surface
                      const Segment<double>* seg, uint32_t n_cp, const double* cps, const double* normals, double tol,
                      double* out, uint32_t ld)
 {
-    static size_t attr = 0;
-    if (smem > attr) {
-        PVL_CUDA_CHECK(cudaFuncSetAttribute(ring_tile_kernel<THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)smem));
-        attr = smem;
-    }
+    PVL_SMEM_OPTIN(ring_tile_kernel<THREADS>, smem);
     ring_tile_kernel<THREADS><<<grid, THREADS, smem, st>>>(n_surfaces, offsets, surface_lines, sl_local,
                                                            tile_offsets, tile_lines, max_tile_lines, n_lines, seg,
                                                            n_cp, cps, normals, pvl::cutoff2<double>(tol), out, ld);

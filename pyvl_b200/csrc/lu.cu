@@ -29,16 +29,17 @@
 #include <cstdint>
 
 #include "pvl_common.cuh"
+#include "dmma.cuh"
+#include "trsv.cuh"
 
 namespace {
 
 constexpr int NB = 64;               // panel width
 constexpr int kSlabRows = 64;        // rows below the top block per CTA in panel_spec_kernel
-constexpr int kGemmTile = 128;       // trailing update tile (M and N)
-constexpr int kGemmThreads = 256;    // 16 x 16 threads, 8 x 8 outputs each
 constexpr int kRB = 64;              // rows per block in the wavefront solves
-constexpr int kSolveThreads = 256;
-constexpr long long kSpinLimit = 20000000;  // bounded waits: ~2 s at 100 ns per poll
+static_assert(kRB == pvl::trsv::kRB, "the solve's row blocks are the inverted diagonal blocks");
+static_assert(NB == pvl::dmma::K, "the tensor-core products have K = the panel width");
+constexpr int kSolveThreads = pvl::trsv::kThreads;
 
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
@@ -51,6 +52,9 @@ struct LuWs {
     int32_t* flags;         // wavefront flags (solve)
     double* tmp;            // (n) solve vector
     double* inv;            // (n_blocks, 2, kRB, kRB): inverses of the diagonal blocks of L and U
+    double* backup_row;     // (NB, n) copy of the panel's row block right of it (FP64 path)
+    double* linv;           // (NB, NB) inverse of the panel's unit-lower L11 (FP64 path)
+    double* uinv;           // (NB, NB) inverse of the panel's U11 (FP64 path)
 };
 
 size_t lu_ws_bytes(uint32_t n)
@@ -58,7 +62,8 @@ size_t lu_ws_bytes(uint32_t n)
     return align256((size_t)n * NB * sizeof(double)) + align256((size_t)NB * NB * sizeof(double)) +
            align256(((size_t)n / NB + 2) * sizeof(int32_t)) +
            align256(((size_t)n / NB + 2) * sizeof(int32_t)) + align256(((size_t)n / kRB + 2) * sizeof(int32_t)) +
-           align256((size_t)n * sizeof(double)) + align256(((size_t)n + kRB - 1) / kRB * 2 * kRB * kRB * sizeof(double));
+           align256((size_t)n * sizeof(double)) + align256(((size_t)n + kRB - 1) / kRB * 2 * kRB * kRB * sizeof(double)) +
+           align256((size_t)NB * n * sizeof(double)) + 2 * align256((size_t)NB * NB * sizeof(double));
 }
 
 LuWs carve(void* ws, uint32_t n)
@@ -78,6 +83,12 @@ LuWs carve(void* ws, uint32_t n)
     w.tmp = reinterpret_cast<double*>(p);
     p += align256((size_t)n * sizeof(double));
     w.inv = reinterpret_cast<double*>(p);
+    p += align256(((size_t)n + kRB - 1) / kRB * 2 * kRB * kRB * sizeof(double));
+    w.backup_row = reinterpret_cast<double*>(p);
+    p += align256((size_t)NB * n * sizeof(double));
+    w.linv = reinterpret_cast<double*>(p);
+    p += align256((size_t)NB * NB * sizeof(double));
+    w.uinv = reinterpret_cast<double*>(p);
     return w;
 }
 
@@ -175,7 +186,8 @@ __global__ void __launch_bounds__(1024) panel_pivot_kernel(uint32_t n, uint32_t 
                                                            const int32_t* __restrict__ reject,
                                                            int32_t* __restrict__ ok, uint32_t panel,
                                                            int32_t* __restrict__ ipiv, int32_t* __restrict__ perm,
-                                                           int32_t* __restrict__ info)
+                                                           int32_t* __restrict__ info,
+                                                           const T* __restrict__ backup_row)
 {
     __shared__ T s_val[32];
     __shared__ uint32_t s_idx[32];
@@ -201,6 +213,11 @@ __global__ void __launch_bounds__(1024) panel_pivot_kernel(uint32_t n, uint32_t 
         const uint32_t r = (uint32_t)(t / nb) + nb, c = (uint32_t)(t % nb);
         A[(size_t)(k0 + r) * lda + k0 + c] = backup[(size_t)r * NB + c];
     }
+    if (backup_row)  // the FP64 path also replaced the row block right of the panel by U12
+        for (size_t t = threadIdx.x; t < (size_t)nb * (n - k0 - nb); t += blockDim.x) {
+            const uint32_t r = (uint32_t)(t / (n - k0 - nb)), c = k0 + nb + (uint32_t)(t % (n - k0 - nb));
+            A[(size_t)(k0 + r) * lda + c] = backup_row[(size_t)r * n + c];
+        }
     __syncthreads();
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (uint32_t j = 0; j < nb; ++j) {
@@ -285,8 +302,10 @@ template <typename T>
 __global__ void __launch_bounds__(kTrsmCols, 1) trsm_kernel(uint32_t n, uint32_t k0, uint32_t nb,
                                                             T* __restrict__ A, uint32_t lda,
                                                             const int32_t* __restrict__ ok, uint32_t panel,
-                                                            const int32_t* __restrict__ ipiv)
+                                                            const int32_t* __restrict__ ipiv, int fast_u12)
 {
+    if (fast_u12 && ok[panel])
+        return;  // the FP64 path formed U12 = L11^-1 A12 already and nothing was interchanged
     extern __shared__ double tsm_raw[];
     T* tsm = reinterpret_cast<T*>(tsm_raw);
     T(*L)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(tsm);                        // [NB][NB + 1]
@@ -344,92 +363,147 @@ __global__ void __launch_bounds__(kTrsmCols, 1) trsm_kernel(uint32_t n, uint32_t
     }
 }
 
-// ---------------------------------------------------------------- 4. trailing update
-// A22 -= L21 U12 (FP64, K = nb <= 64): 128 x 128 tile per CTA, 16 x 16 threads.  Thread
-// (ty, tx) owns rows {2ty, 2ty+1} + 32 p and columns {2tx, 2tx+1} + 32 q (p, q = 0..3).
-// L21 is staged row-major (row stride 66 doubles: conflict-free stores, 16-byte aligned rows)
-// and read two k at a time per row (each load is a broadcast: two rows per warp); U12 is
-// staged row-major and read as 16 consecutive pairs per half-warp (conflict-free).  Per two
-// k steps: 16 128-bit shared loads for 128 FMAs.
-constexpr int kAStride = NB + 2;
+// ---------------------------------------------------------------- FP64 panel on the tensor cores
+// The FP64 factorisation first factors each panel without interchanges and then checks that
+// partial pivoting would have made none: with no interchange before column j, GEPP keeps the
+// diagonal in column j exactly when no entry below it is larger in magnitude at that moment,
+// i.e. when every multiplier l_ij (i > j) has |l_ij| <= 1 (LAPACK's idamax returns the first
+// maximal entry, and the diagonal comes first).  The multipliers are formed by blocks:
+//   top_factor_kernel   L11 U11 = A11 (one CTA, the 64 x 64 diagonal block, in shared memory),
+//                       the check inside the block, and L11^-1, U11^-1;
+//   panel_apply_kernel  L21 = A21 U11^-1 (with the check on every multiplier) and
+//                       U12 = L11^-1 A12, both as FP64 tensor-core tiles (dmma.cuh), the
+//                       overwritten operands backed up;
+//   panel_pivot_kernel  commits the top block -- or, if any check failed, restores the panel and
+//                       its row block and refactors the panel with explicit partial pivoting in
+//                       getf2 order, after which trsm_kernel applies the interchanges and forms
+//                       U12 by substitution;
+//   dmma_update_kernel  A22 -= L21 U12 on the FP64 tensor cores, two 128 x 64 tiles per SM.
+// Every product has K = 64, the panel width; the multipliers and U12 are the blocked forms of
+// getf2's and trsm's, equal to them up to rounding.
+constexpr int kTopThreads = 256;
 
-__global__ void __launch_bounds__(kGemmThreads) gemm_update_kernel(uint32_t n, uint32_t k0, uint32_t nb,
-                                                                   double* __restrict__ A, uint32_t lda)
+__global__ void __launch_bounds__(kTopThreads) top_factor_kernel(uint32_t k0, uint32_t nb,
+                                                                 const double* __restrict__ A, uint32_t lda,
+                                                                 double* __restrict__ top_out,
+                                                                 double* __restrict__ linv,
+                                                                 double* __restrict__ uinv,
+                                                                 int32_t* __restrict__ reject)
 {
-    extern __shared__ double2 gsm2[];
-    double* As = reinterpret_cast<double*>(gsm2);   // [kGemmTile][kAStride]: As[i][k] = L21[i][k]
-    double* Bs = As + kGemmTile * kAStride;         // [NB][kGemmTile]:       Bs[k][j] = U12[k][j]
-    const uint32_t base = k0 + nb;
-    const uint32_t i0 = base + blockIdx.y * kGemmTile, j0 = base + blockIdx.x * kGemmTile;
-    const uint32_t tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    for (uint32_t t = threadIdx.x; t < kGemmTile * NB; t += kGemmThreads) {
-        const uint32_t i = t / NB, k = t % NB;
-        As[i * kAStride + k] = (i0 + i < n && k < nb) ? A[(size_t)(i0 + i) * lda + k0 + k] : 0.0;
-    }
-    for (uint32_t t = threadIdx.x; t < NB * kGemmTile; t += kGemmThreads) {
-        const uint32_t k = t / kGemmTile, j = t % kGemmTile;
-        Bs[k * kGemmTile + j] = (j0 + j < n && k < nb) ? A[(size_t)(k0 + k) * lda + j0 + j] : 0.0;
+    __shared__ double T[NB][NB + 1];
+    const uint32_t tid = threadIdx.x;
+    for (uint32_t e = tid; e < NB * NB; e += kTopThreads) {
+        const uint32_t r = e / NB, c = e % NB;
+        T[r][c] = (r < nb && c < nb) ? A[(size_t)(k0 + r) * lda + k0 + c] : (r == c ? 1.0 : 0.0);
     }
     __syncthreads();
-    double acc[8][8];
-#pragma unroll
-    for (int r = 0; r < 8; ++r)
-#pragma unroll
-        for (int c = 0; c < 8; ++c)
-            acc[r][c] = 0.0;
-    const double2* A2 = reinterpret_cast<const double2*>(As);
-    const double2* B2 = reinterpret_cast<const double2*>(Bs);
+    bool bad = false;
+    const uint32_t tx = tid & 15, ty = tid >> 4;  // 16 x 16 threads for the rank-1 updates
 #pragma unroll 1
-    for (uint32_t k = 0; k < NB; k += 2) {
-        double2 a[8];
-#pragma unroll
-        for (int p = 0; p < 4; ++p)
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-                a[2 * p + h] = A2[((2 * ty + 32 * p + h) * kAStride + k) / 2];
-#pragma unroll
-        for (int kk = 0; kk < 2; ++kk) {
-            double b[8];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const double2 vb = B2[((k + kk) * kGemmTile + 2 * tx + 32 * q) / 2];
-                b[2 * q] = vb.x;
-                b[2 * q + 1] = vb.y;
-            }
-#pragma unroll
-            for (int r = 0; r < 8; ++r) {
-                const double ar = kk ? a[r].y : a[r].x;
-#pragma unroll
-                for (int c = 0; c < 8; ++c)
-                    acc[r][c] = fma(ar, b[c], acc[r][c]);
-            }
+    for (uint32_t j = 0; j < NB; ++j) {
+        const double piv = T[j][j];
+        if (tid == 0)
+            bad |= !(fabs(piv) > 0.0);  // zero or NaN pivot
+        const double rcp = 1.0 / piv;   // getf2 scales by the reciprocal of the pivot
+        if (tid > j && tid < NB) {
+            const double l = T[tid][j] * rcp;
+            bad |= !(fabs(l) < pvl::dmma::kMultLimit);
+            T[tid][j] = l;
         }
+        __syncthreads();
+        for (uint32_t i = j + 1 + ty; i < NB; i += 16) {
+            const double l = T[i][j];
+            for (uint32_t c = j + 1 + tx; c < NB; c += 16)
+                T[i][c] = fma(-l, T[j][c], T[i][c]);
+        }
+        __syncthreads();
     }
+    if (__syncthreads_or(bad) && tid == 0)
+        atomicExch(reject, 1);
+    for (uint32_t e = tid; e < NB * NB; e += kTopThreads) {
+        const uint32_t r = e / NB, c = e % NB;
+        if (r < nb && c < nb)
+            top_out[(size_t)r * NB + c] = T[r][c];
+    }
+    // inverses: threads 0..63 column c of L11^-1 (unit lower), threads 64..127 column c of U11^-1
+    if (tid < 2 * NB) {
+        const bool lower = tid < NB;
+        const int c = (int)(tid & (NB - 1));
+        double y[NB];
 #pragma unroll
-    for (int p = 0; p < 4; ++p)
+        for (int r = 0; r < NB; ++r)
+            y[r] = r == c ? 1.0 : 0.0;
+        if (lower) {
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const uint32_t i = i0 + 2 * ty + 32 * p + h;
-            if (i >= n)
-                continue;
-            double* crow = A + (size_t)i * lda;
+            for (int q = 0; q < NB - 1; ++q) {
+                const double yq = y[q];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const uint32_t j = j0 + 2 * tx + 32 * q;
-                if (j + 1 < n && ((lda & 1u) == 0)) {
-                    double2* c2 = reinterpret_cast<double2*>(crow + j);
-                    double2 v = *c2;
-                    v.x -= acc[2 * p + h][2 * q];
-                    v.y -= acc[2 * p + h][2 * q + 1];
-                    *c2 = v;
-                } else {
-                    if (j < n)
-                        crow[j] -= acc[2 * p + h][2 * q];
-                    if (j + 1 < n)
-                        crow[j + 1] -= acc[2 * p + h][2 * q + 1];
-                }
+                for (int r = q + 1; r < NB; ++r)
+                    y[r] = fma(-T[r][q], yq, y[r]);
+            }
+        } else {
+#pragma unroll
+            for (int q = NB - 1; q >= 0; --q) {
+                const double yq = y[q] / T[q][q];
+                y[q] = yq;
+#pragma unroll
+                for (int r = 0; r < q; ++r)
+                    y[r] = fma(-T[r][q], yq, y[r]);
             }
         }
+        double* out = lower ? linv : uinv;
+#pragma unroll
+        for (int r = 0; r < NB; ++r)
+            out[(size_t)r * NB + c] = y[r];
+    }
+}
+
+constexpr int kApplyRows = 32;  // L21 tile: 32 rows x 64
+constexpr int kApplyCols = 32;  // U12 tile: 64 x 32 columns
+constexpr size_t kApplySmem = sizeof(pvl::dmma::Smem<64, 32>) > sizeof(pvl::dmma::Smem<32, 64>)
+                                  ? sizeof(pvl::dmma::Smem<64, 32>) : sizeof(pvl::dmma::Smem<32, 64>);
+
+// CTAs 0 .. n_ltiles-1: a 32-row tile of L21 = A21 U11^-1; the rest: a 32-column tile of
+// U12 = L11^-1 A12.  Both in place, the old values backed up for the pivoting fallback.
+template <bool VEC>
+__global__ void __launch_bounds__(pvl::dmma::kThreads) panel_apply_kernel(uint32_t n, uint32_t k0,
+                                                                          double* __restrict__ A, uint32_t lda,
+                                                                          const double* __restrict__ linv,
+                                                                          const double* __restrict__ uinv,
+                                                                          double* __restrict__ backup,
+                                                                          double* __restrict__ backup_row,
+                                                                          int32_t* __restrict__ reject,
+                                                                          uint32_t n_ltiles)
+{
+    using namespace pvl::dmma;
+    extern __shared__ __align__(16) double apply_smem[];
+    const uint32_t base = k0 + NB;
+    if (blockIdx.x < n_ltiles) {
+        auto& sm = *reinterpret_cast<Smem<kApplyRows, 64>*>(apply_smem);
+        const uint32_t r0 = base + blockIdx.x * kApplyRows;
+        tile<kApplyRows, 64, kLowerMul, VEC>(sm, A, lda, r0, k0, uinv, NB, 0, 0, A, lda, r0, k0,
+                                             min((uint32_t)kApplyRows, n - r0), NB, backup, k0, 0, 0, reject);
+    } else {
+        auto& sm = *reinterpret_cast<Smem<64, kApplyCols>*>(apply_smem);
+        const uint32_t c0 = base + (blockIdx.x - n_ltiles) * kApplyCols;
+        tile<64, kApplyCols, kUpperMul, VEC>(sm, linv, NB, 0, 0, A, lda, k0, c0, A, lda, k0, c0, NB,
+                                             min((uint32_t)kApplyCols, n - c0), backup_row, 0, 0, n, nullptr);
+    }
+}
+
+constexpr int kUpdM = 128, kUpdN = 64;  // trailing-update tile; two CTAs per SM
+
+template <bool VEC>
+__global__ void __launch_bounds__(pvl::dmma::kThreads, 2) dmma_update_kernel(uint32_t n, uint32_t k0,
+                                                                             double* __restrict__ A, uint32_t lda)
+{
+    using namespace pvl::dmma;
+    extern __shared__ __align__(16) double upd_smem[];
+    auto& sm = *reinterpret_cast<Smem<kUpdM, kUpdN>*>(upd_smem);
+    const uint32_t base = k0 + NB;
+    const uint32_t i0 = base + blockIdx.y * kUpdM, j0 = base + blockIdx.x * kUpdN;
+    tile<kUpdM, kUpdN, kUpdate, VEC>(sm, A, lda, i0, k0, A, lda, k0, j0, A, lda, i0, j0, min((uint32_t)kUpdM, n - i0),
+                                     min((uint32_t)kUpdN, n - j0), nullptr, 0, 0, 0, nullptr);
 }
 
 // ---------------------------------------------------------------- diagonal-block inverses
@@ -489,96 +563,6 @@ __global__ void gather_kernel(uint32_t n, const int32_t* __restrict__ perm, cons
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n)
         out[i] = b[perm[i]];
-}
-
-__device__ __forceinline__ int32_t ld_acquire(const int32_t* p)
-{
-    int32_t v;
-    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ void st_release(int32_t* p, int32_t v)
-{
-    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-// Wavefront triangular solve over row blocks of kRB rows, one CTA per block.  LOWER:
-// unit-lower forward substitution, block b waits for blocks 0..b-1.  UPPER: backward
-// substitution with U's diagonal, block b waits for blocks nblk-1..b+1.  x holds the
-// right-hand side on entry and the solution on exit.  Each wait is bounded: on time-out
-// the CTA sets *err, publishes its flag so that no later block waits on it, and returns.
-template <bool LOWER>
-__global__ void __launch_bounds__(kSolveThreads) trsv_wavefront_kernel(uint32_t n, const double* __restrict__ M,
-                                                                       uint32_t lda,
-                                                                       const double* __restrict__ inv,
-                                                                       double* __restrict__ x,
-                                                                       int32_t* __restrict__ flags,
-                                                                       int32_t* __restrict__ err)
-{
-    __shared__ double s_acc[kRB];
-    __shared__ double s_r[kRB];
-    __shared__ int s_abort;
-    const uint32_t nblk = (n + kRB - 1) / kRB;
-    const uint32_t b = LOWER ? blockIdx.x : nblk - 1 - blockIdx.x;
-    const uint32_t r0 = b * kRB;
-    const uint32_t rows = min((uint32_t)kRB, n - r0);
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (threadIdx.x == 0)
-        s_abort = 0;
-    if (threadIdx.x < kRB)
-        s_acc[threadIdx.x] = 0.0;
-    __syncthreads();
-    const uint32_t n_dep = LOWER ? b : nblk - 1 - b;
-    for (uint32_t step = 0; step < n_dep; ++step) {
-        const uint32_t c = LOWER ? step : nblk - 1 - step;
-        if (threadIdx.x == 0) {
-            long long spins = 0;
-            while (ld_acquire(flags + c) == 0) {
-                if (++spins > kSpinLimit) {
-                    atomicExch(err, 1);
-                    s_abort = 1;
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __syncthreads();
-        if (s_abort) {
-            if (threadIdx.x == 0)
-                st_release(flags + b, 1);
-            return;
-        }
-        const uint32_t c0 = c * kRB;
-        const uint32_t ccols = min((uint32_t)kRB, n - c0);
-        const double x0 = lane < ccols ? __ldcg(x + c0 + lane) : 0.0;
-        const double x1 = lane + 32 < ccols ? __ldcg(x + c0 + lane + 32) : 0.0;
-        for (uint32_t r = warp; r < rows; r += kSolveThreads / 32) {
-            const double* mrow = M + (size_t)(r0 + r) * lda + c0;
-            double s = (lane < ccols ? mrow[lane] * x0 : 0.0) + (lane + 32 < ccols ? mrow[lane + 32] * x1 : 0.0);
-            for (int o = 16; o > 0; o >>= 1)
-                s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0)
-                s_acc[r] += s;
-        }
-        __syncthreads();
-    }
-    // diagonal block: x_b = inv(D_bb) (r_b - acc), one parallel matrix-vector product
-    if (threadIdx.x < kRB)
-        s_r[threadIdx.x] = threadIdx.x < rows ? __ldcg(x + r0 + threadIdx.x) - s_acc[threadIdx.x] : 0.0;
-    __syncthreads();
-    const double* D = inv + ((size_t)b * 2 + (LOWER ? 0 : 1)) * kRB * kRB;
-    for (uint32_t r = warp; r < rows; r += kSolveThreads / 32) {
-        double s = D[(size_t)r * kRB + lane] * s_r[lane] + D[(size_t)r * kRB + lane + 32] * s_r[lane + 32];
-        for (int o = 16; o > 0; o >>= 1)
-            s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0)
-            x[r0 + r] = s;
-    }
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0)
-        st_release(flags + b, 1);
 }
 
 // Blocked substitution with one launch per step and no inter-CTA waits (so that it can sit in a
@@ -652,16 +636,15 @@ extern "C" int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv,
         return pvl_fail(PVL_ERR_ALLOC, "pvl_lu_factor: workspace %zu < %zu", ws_bytes, lu_ws_bytes(n));
     cudaStream_t st = (cudaStream_t)stream;
     LuWs w = carve(ws, n);
-    const size_t gemm_smem = (size_t)(kGemmTile * kAStride + NB * kGemmTile) * sizeof(double);
     const size_t trsm_smem = (size_t)(NB * (NB + 1) + NB * (kTrsmCols + 1)) * sizeof(double);
-    static bool attr_done = false;
-    if (!attr_done) {
-        PVL_CUDA_CHECK(cudaFuncSetAttribute(gemm_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)gemm_smem));
-        PVL_CUDA_CHECK(cudaFuncSetAttribute(trsm_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)trsm_smem));
-        attr_done = true;
-    }
+    const size_t upd_smem = sizeof(pvl::dmma::Smem<kUpdM, kUpdN>);
+    // 16-byte operand copies and stores need even row strides and an even width
+    const bool vec = (lda % 2 == 0) && (n % 2 == 0) && (((uintptr_t)A & 15u) == 0);
+    const void* apply_fn = vec ? (const void*)panel_apply_kernel<true> : (const void*)panel_apply_kernel<false>;
+    const void* upd_fn = vec ? (const void*)dmma_update_kernel<true> : (const void*)dmma_update_kernel<false>;
+    PVL_SMEM_OPTIN(trsm_kernel<double>, trsm_smem);
+    PVL_SMEM_OPTIN(apply_fn, kApplySmem);
+    PVL_SMEM_OPTIN(upd_fn, upd_smem);
     int32_t* perm = ipiv + n;
     PVL_CUDA_CHECK(cudaMemsetAsync(info, 0, sizeof(int32_t), st));
     init_perm_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, perm);
@@ -671,23 +654,35 @@ extern "C" int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv,
     for (uint32_t p = 0; p < n_panels; ++p) {
         const uint32_t k0 = p * NB;
         const uint32_t nb = std::min<uint32_t>(NB, n - k0);
-        const uint32_t below = n - k0 - nb;
-        const uint32_t ctas = std::max<uint32_t>(1, (below + kSlabRows - 1) / kSlabRows);
-        panel_spec_kernel<double><<<ctas, 2 * kSlabRows, 0, st>>>(n, k0, nb, A, lda, w.backup, w.top_out,
-                                                                  w.reject + p);
+        const uint32_t below = n - k0 - nb;  // nonzero only for full panels (nb == NB)
+        top_factor_kernel<<<1, kTopThreads, 0, st>>>(k0, nb, A, lda, w.top_out, w.linv, w.uinv, w.reject + p);
         PVL_LAUNCH_CHECK();
+        if (below > 0) {
+            const uint32_t nl = blocks_for(below, kApplyRows), nu = blocks_for(below, kApplyCols);
+            double* bk = w.backup;
+            double* bkr = w.backup_row;
+            const double* li = w.linv;
+            const double* ui = w.uinv;
+            int32_t* rj = w.reject + p;
+            void* args[] = {(void*)&n, (void*)&k0, (void*)&A, (void*)&lda, (void*)&li, (void*)&ui, (void*)&bk,
+                            (void*)&bkr, (void*)&rj, (void*)&nl};
+            PVL_CUDA_CHECK(cudaLaunchKernel(apply_fn, dim3(nl + nu), dim3(pvl::dmma::kThreads), args, kApplySmem, st));
+            pvl_count_launch();
+        }
         panel_pivot_kernel<double><<<1, 1024, 0, st>>>(n, k0, nb, A, lda, w.backup, w.top_out, w.reject, w.ok, p, ipiv,
-                                                       perm, info);
+                                                       perm, info, below > 0 ? w.backup_row : nullptr);
         PVL_LAUNCH_CHECK();
         if (n > nb) {
             trsm_kernel<double><<<blocks_for(n - nb, kTrsmCols), kTrsmCols, trsm_smem, st>>>(n, k0, nb, A, lda, w.ok, p,
-                                                                                           ipiv);
+                                                                                           ipiv, 1);
             PVL_LAUNCH_CHECK();
         }
         if (below > 0) {
-            dim3 g(blocks_for(below, kGemmTile), blocks_for(below, kGemmTile));
-            gemm_update_kernel<<<g, kGemmThreads, gemm_smem, st>>>(n, k0, nb, A, lda);
-            PVL_LAUNCH_CHECK();
+            uint32_t kk = k0;
+            void* args[] = {(void*)&n, (void*)&kk, (void*)&A, (void*)&lda};
+            const dim3 g(blocks_for(below, kUpdN), blocks_for(below, kUpdM));
+            PVL_CUDA_CHECK(cudaLaunchKernel(upd_fn, g, dim3(pvl::dmma::kThreads), args, upd_smem, st));
+            pvl_count_launch();
         }
     }
     diag_inverse_kernel<double><<<(n + kRB - 1) / kRB, 2 * kRB, 0, st>>>(n, A, lda, w.inv);
@@ -707,8 +702,9 @@ extern "C" int pvl_lu_solve(uint32_t n, const double* LU, uint32_t lda, const in
     if (ws_bytes < lu_ws_bytes(n))
         return pvl_fail(PVL_ERR_ALLOC, "pvl_lu_solve: workspace too small");
     const uint32_t nblk = (n + kRB - 1) / kRB;
-    if ((int)nblk > coresident_blocks((const void*)trsv_wavefront_kernel<true>, kSolveThreads) ||
-        (int)nblk > coresident_blocks((const void*)trsv_wavefront_kernel<false>, kSolveThreads))
+    const void* fwd = (const void*)pvl::trsv::wavefront_kernel<true>;
+    const void* bwd = (const void*)pvl::trsv::wavefront_kernel<false>;
+    if ((int)nblk > coresident_blocks(fwd, kSolveThreads) || (int)nblk > coresident_blocks(bwd, kSolveThreads))
         return pvl_fail(PVL_ERR_ARG, "pvl_lu_solve: n = %u needs %u co-resident blocks", n, nblk);
     cudaStream_t st = (cudaStream_t)stream;
     LuWs w = carve(ws, n);
@@ -716,14 +712,16 @@ extern "C" int pvl_lu_solve(uint32_t n, const double* LU, uint32_t lda, const in
     PVL_CUDA_CHECK(cudaMemsetAsync(err, 0, sizeof(int32_t), st));
     gather_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, perm, b, w.tmp);
     PVL_LAUNCH_CHECK();
+    long long spin = pvl::trsv::kSpinLimit;
+    int32_t skip = -1;
     for (int pass = 0; pass < 2; ++pass) {
         PVL_CUDA_CHECK(cudaMemsetAsync(w.flags, 0, sizeof(int32_t) * (nblk + 1), st));
         double* xt = w.tmp;
         int32_t* fl = w.flags;
         const double* iv = w.inv;
-        void* args[] = {(void*)&n, (void*)&LU, (void*)&lda, (void*)&iv, (void*)&xt, (void*)&fl, (void*)&err};
-        const void* fn = pass == 0 ? (const void*)trsv_wavefront_kernel<true> : (const void*)trsv_wavefront_kernel<false>;
-        PVL_CUDA_CHECK(cudaLaunchCooperativeKernel(fn, dim3(nblk), dim3(kSolveThreads), args, 0, st));
+        void* args[] = {(void*)&n, (void*)&LU, (void*)&lda, (void*)&iv, (void*)&xt, (void*)&fl, (void*)&err,
+                        (void*)&spin, (void*)&skip};
+        PVL_CUDA_CHECK(cudaLaunchCooperativeKernel(pass == 0 ? fwd : bwd, dim3(nblk), dim3(kSolveThreads), args, 0, st));
         pvl_count_launch();
     }
     PVL_CUDA_CHECK(cudaMemcpyAsync(b, w.tmp, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
@@ -766,10 +764,10 @@ extern "C" int pvl_lu_solve_blocked(uint32_t n, const double* LU, uint32_t lda, 
 }
 
 // ================================================================ FP32 LU (TF32 trailing update)
-// The low-precision factorisation behind the mixed path's preconditioner.  Same panel,
-// pivot and TRSM kernels as the FP64 factorisation (instantiated for float), with the
-// trailing update A22 -= L21 U12 on the tensor cores (pvl_gemm_tf32: TF32 products, FP32
-// accumulation).  The explicit inverse U^-1 L^-1 is then formed from the factors by blocked
+// The low-precision factorisation behind the mixed path's preconditioner.  Speculative panel
+// (panel_spec_kernel), pivot and TRSM kernels instantiated for float, with the trailing update
+// A22 -= L21 U12 on the tensor cores (U12 transposed into a K-major operand, then
+// pvl_gemm_tf32: TMA-fed tcgen05 MMAs, TF32 products, FP32 accumulation).  The explicit inverse U^-1 L^-1 is then formed from the factors by blocked
 // triangular inversion: the 64 x 64 diagonal-block products on CUDA cores in FP32, every
 // rank-64 update on the tensor cores.  Applying the preconditioner is then one FP32
 // matrix-vector product per Krylov iteration instead of two latency-bound triangular solves.
@@ -825,11 +823,39 @@ __global__ void permute_columns_kernel(uint32_t n, const float* __restrict__ X, 
         out[(size_t)r * ldo + q] = X[(size_t)r * ldx + c];
 }
 
+// dst (cols x 64, row-major) = the transpose of the 64 x cols block src (leading dimension
+// lds): the K-major form of a rank-64 update's right operand for the tensor-core GEMM.
+__global__ void __launch_bounds__(256) transpose64_kernel(uint32_t cols, const float* __restrict__ src, uint32_t lds,
+                                                          float* __restrict__ dst)
+{
+    __shared__ float t[32][33];
+    const uint32_t c0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+    const uint32_t tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+    for (uint32_t k = ty; k < 32; k += 8)
+        t[k][tx] = c0 + tx < cols ? src[(size_t)(k0 + k) * lds + c0 + tx] : 0.0f;
+    __syncthreads();
+    for (uint32_t c = ty; c < 32; c += 8)
+        if (c0 + c < cols)
+            dst[(size_t)(c0 + c) * kRB + k0 + tx] = t[tx][c];
+}
+
 }  // namespace
 
 extern "C" int pvl_gemm_tf32(uint32_t M, uint32_t N, uint32_t K, float alpha, const float* A, uint32_t lda,
-                             const float* B, uint32_t ldb, float beta, float* C, uint32_t ldc, int32_t* err,
+                             const float* Bt, uint32_t ldbt, float beta, float* C, uint32_t ldc, int32_t* err,
                              void* stream);
+
+namespace {
+// C (M x cols) -= A (M x 64, lda) * B where B is the 64 x cols block at src (lds): B is
+// transposed into bt (cols x 64) first, then the tensor-core GEMM runs on K-major operands.
+int rank64_update(uint32_t M, uint32_t cols, const float* A, uint32_t lda, const float* src, uint32_t lds, float* bt,
+                  float* C, uint32_t ldc, int32_t* err, cudaStream_t st)
+{
+    transpose64_kernel<<<dim3(blocks_for(cols, 32), kRB / 32), 256, 0, st>>>(cols, src, lds, bt);
+    PVL_LAUNCH_CHECK();
+    return pvl_gemm_tf32(M, cols, kRB, -1.0f, A, lda, bt, kRB, 1.0f, C, ldc, err, st);
+}
+}  // namespace
 
 extern "C" size_t pvl_lu32_workspace(uint32_t n) { return lu_ws_bytes(n); }
 
@@ -849,13 +875,9 @@ extern "C" int pvl_lu32_factor(uint32_t n, float* A, uint32_t lda, int32_t* ipiv
     float* backup = reinterpret_cast<float*>(w.backup);
     float* top_out = reinterpret_cast<float*>(w.top_out);
     float* inv = reinterpret_cast<float*>(w.inv);
+    float* ut = reinterpret_cast<float*>(w.backup_row);  // U12 transposed for the tensor-core updates
     const size_t trsm_smem = (size_t)(NB * (NB + 1) + NB * (kTrsmCols + 1)) * sizeof(float);
-    static bool attr_done = false;
-    if (!attr_done) {
-        PVL_CUDA_CHECK(cudaFuncSetAttribute(trsm_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)trsm_smem));
-        attr_done = true;
-    }
+    PVL_SMEM_OPTIN(trsm_kernel<float>, trsm_smem);
     int32_t* perm = ipiv + n;
     PVL_CUDA_CHECK(cudaMemsetAsync(info, 0, sizeof(int32_t), st));
     PVL_CUDA_CHECK(cudaMemsetAsync(err, 0, sizeof(int32_t), st));
@@ -871,18 +893,18 @@ extern "C" int pvl_lu32_factor(uint32_t n, float* A, uint32_t lda, int32_t* ipiv
         panel_spec_kernel<float><<<ctas, 2 * kSlabRows, 0, st>>>(n, k0, nb, A, lda, backup, top_out, w.reject + p);
         PVL_LAUNCH_CHECK();
         panel_pivot_kernel<float><<<1, 1024, 0, st>>>(n, k0, nb, A, lda, backup, top_out, w.reject, w.ok, p, ipiv,
-                                                      perm, info);
+                                                      perm, info, nullptr);
         PVL_LAUNCH_CHECK();
         if (n > nb) {
             trsm_kernel<float><<<blocks_for(n - nb, kTrsmCols), kTrsmCols, trsm_smem, st>>>(n, k0, nb, A, lda, w.ok, p,
-                                                                                          ipiv);
+                                                                                          ipiv, 0);
             PVL_LAUNCH_CHECK();
         }
         if (below > 0) {
             // every panel with rows below it is a full NB = 64 wide, so K = 64 (a multiple of 32)
             float* a22 = A + (size_t)(k0 + nb) * lda + k0 + nb;
-            if (int r = pvl_gemm_tf32(below, below, nb, -1.0f, A + (size_t)(k0 + nb) * lda + k0, lda,
-                                      A + (size_t)k0 * lda + k0 + nb, lda, 1.0f, a22, lda, err, stream))
+            if (int r = rank64_update(below, below, A + (size_t)(k0 + nb) * lda + k0, lda, A + (size_t)k0 * lda + k0 + nb,
+                                      lda, ut, a22, lda, err, st))
                 return r;
         }
     }
@@ -910,6 +932,7 @@ extern "C" int pvl_lu32_inverse(uint32_t n, const float* LU, uint32_t lda, const
     cudaStream_t st = (cudaStream_t)stream;
     LuWs w = carve(ws, n);
     const float* inv = reinterpret_cast<const float*>(w.inv);  // written by pvl_lu32_factor
+    float* bt = reinterpret_cast<float*>(w.backup_row);         // transposed update operands
     const uint32_t nblk = n / kRB;
     // forward: Y = L^-1, with X as the working right-hand side (starts as I)
     set_identity_kernel<<<blocks_for((size_t)n * n, 256), 256, 0, st>>>(n, X, ldx);
@@ -921,8 +944,8 @@ extern "C" int pvl_lu32_inverse(uint32_t n, const float* LU, uint32_t lda, const
                                                                  X + (size_t)r0 * ldx, ldx, Y + (size_t)r0 * ldy, ldy);
         PVL_LAUNCH_CHECK();
         if (cols < n)
-            if (int r = pvl_gemm_tf32(n - cols, cols, kRB, -1.0f, LU + (size_t)cols * lda + r0, lda,
-                                      Y + (size_t)r0 * ldy, ldy, 1.0f, X + (size_t)cols * ldx, ldx, err, stream))
+            if (int r = rank64_update(n - cols, cols, LU + (size_t)cols * lda + r0, lda, Y + (size_t)r0 * ldy, ldy, bt,
+                                      X + (size_t)cols * ldx, ldx, err, st))
                 return r;
     }
     // backward: X = U^-1 Y, with Y as the working right-hand side
@@ -932,8 +955,7 @@ extern "C" int pvl_lu32_inverse(uint32_t n, const float* LU, uint32_t lda, const
                                                               Y + (size_t)r0 * ldy, ldy, X + (size_t)r0 * ldx, ldx);
         PVL_LAUNCH_CHECK();
         if (r0 > 0)
-            if (int r = pvl_gemm_tf32(r0, n, kRB, -1.0f, LU + r0, lda, X + (size_t)r0 * ldx, ldx, 1.0f, Y, ldy, err,
-                                      stream))
+            if (int r = rank64_update(r0, n, LU + r0, lda, X + (size_t)r0 * ldx, ldx, bt, Y, ldy, err, st))
                 return r;
     }
     if (perm) {

@@ -5,9 +5,8 @@
 // Kernels:
 //   features_kernel -- the 12 normalised inputs of each panel and the base of the prediction
 //                      (previous circulation + one Jacobi correction of the new system);
-//   forward_kernel  -- inference: one CTA of 128 threads per tile of 8 panels, thread j owns
-//                      hidden unit j; W2 staged transposed in shared memory (a row of W2
-//                      per thread: conflict-free both when staged and when read);
+//   forward_tc_kernel -- inference on the tensor cores (tcgen05.mma kind::f16, BF16 operands,
+//                      FP32 accumulators in tensor memory), one 128-panel tile per CTA;
 //   train_kernel    -- forward + backward of the mean squared error over a batch, persistent
 //                      CTAs, each accumulating its gradient in shared memory (FP32) and
 //                      writing one partial gradient row; reduce_kernel sums the rows in a
@@ -22,13 +21,13 @@
 #include <cstdint>
 
 #include "pvl_common.cuh"
+#include "umma.cuh"
 
 namespace {
 
 constexpr int kIn = 12;
 constexpr int kH = 128;
 constexpr int kTile = 32;     // panels per tile of training
-constexpr int kFwdTile = 8;   // panels per tile of inference (n / 8 CTAs: 512 at 4096 panels)
 constexpr int kThreads = kH;
 constexpr int oW1 = 0, oB1 = oW1 + kH * kIn, oW2 = oB1 + kH, oB2 = oW2 + kH * kH, oW3 = oB2 + kH, oB3 = oW3 + kH;
 constexpr int kParams = oB3 + 1;
@@ -131,37 +130,159 @@ __device__ __forceinline__ void load_w2t(FwdSmemT<T>& sm, const __nv_bfloat16* _
     }
 }
 
-// out[p] = base[p] + scale * mul[0] * y(p)   (base and mul may be NULL)
-__global__ void __launch_bounds__(kThreads) forward_kernel(uint32_t n, const float* __restrict__ X,
-                                                           const __nv_bfloat16* __restrict__ P, double scale,
-                                                           const double* __restrict__ mul,
-                                                           const double* __restrict__ base, double* __restrict__ out)
+// ---------------------------------------------------------------- inference on the tensor cores
+// One CTA of 128 threads per 128-panel tile (the tiles strided over the CTAs).  Layer 1:
+// acc1 (TMEM columns 0..127) = X W1^T with X the tile's inputs rounded to BF16 (K = 12 padded
+// to one K = 16 step); thread r (TMEM lane r, panel r of the tile) reads its row back, adds b1,
+// applies ReLU and rounds to BF16 into H1 in shared memory; layer 2: acc2 (columns 128..255) =
+// H1 W2^T, eight K = 16 steps; thread r then forms h2 = bf16(relu(acc2 + b2)) and
+// y = b3 + w3 . h2 in FP32.  Operands in the SW128 K-major layout (umma.cuh), MMAs issued by
+// one thread (tcgen05.mma kind::f16, BF16 x BF16 -> FP32), completion through mbarriers whose
+// waits are bounded: a wait that runs out leaves NaN in the tile's outputs (the seed is then
+// rejected by the solve, whose answer does not depend on it).
+constexpr int kTcTile = 128;
+struct FwdTcSmem {
+    unsigned char x[kTcTile * 128];       // X tile: 128 rows x 64 BF16 of K (0..11 used)
+    unsigned char w1[kH * 128];           // W1: N = 128 units x 64 BF16 of K (0..11 used)
+    unsigned char h1[2][kTcTile * 128];   // H1: K = 128 in two 64-wide column blocks
+    unsigned char w2[2][kH * 128];        // W2: N = 128 x K = 128 in two column blocks
+    float b1[kH], b2[kH], w3[kH];
+    uint64_t bar[2];
+    uint32_t tmem;
+    int fail;
+};
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    FwdSmemT<kFwdTile>& sm = *reinterpret_cast<FwdSmemT<kFwdTile>*>(smem_raw);
-    const int j = threadIdx.x;
-    load_w2t(sm, P);
-    float w1[kIn];
+    const uint32_t lo = __bfloat16_as_ushort(__float2bfloat16_rn(a));
+    const uint32_t hi = __bfloat16_as_ushort(__float2bfloat16_rn(b));
+    return lo | (hi << 16);
+}
+
+__global__ void __launch_bounds__(kTcTile) forward_tc_kernel(uint32_t n, const float* __restrict__ X,
+                                                             const __nv_bfloat16* __restrict__ P, double scale,
+                                                             const double* __restrict__ mul,
+                                                             const double* __restrict__ base,
+                                                             double* __restrict__ out)
+{
+    namespace um = pvl::umma;
+    extern __shared__ __align__(1024) unsigned char tc_raw[];
+    FwdTcSmem& sm = *reinterpret_cast<FwdTcSmem*>(tc_raw + ((1024u - (um::smem_u32(tc_raw) & 1023u)) & 1023u));
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    // weights into the SW128 layout: row j of W1 / W2 is unit j (the N index), K along the row
+    for (uint32_t e = tid; e < kH * 8; e += kTcTile) {  // W1: 8 chunks of 8 BF16 per row
+        const uint32_t j = e >> 3, c = e & 7u;
+        uint32_t w[4];
 #pragma unroll
-    for (int i = 0; i < kIn; ++i)
-        w1[i] = ldb(P + oW1 + j * kIn + i);
-    const float b1 = ldb(P + oB1 + j), b2 = ldb(P + oB2 + j), w3 = ldb(P + oW3 + j), b3 = ldb(P + oB3);
-    const double sc = mul ? scale * mul[0] : scale;
-    for (uint64_t s0 = (uint64_t)blockIdx.x * kFwdTile; s0 < n; s0 += (uint64_t)gridDim.x * kFwdTile) {
-        const int ns = (int)(n - s0 < (uint64_t)kFwdTile ? n - s0 : (uint64_t)kFwdTile);
-        __syncthreads();
-        load_x_tile(sm, X, s0, ns);
-        __syncthreads();
-        float h2[kFwdTile];
-        tile_forward(sm, sm.h1, w1, b1, b2, ns, h2);
-        tile_output(sm, w3, h2);
-        if (j < ns) {
-            float y = b3;
-            for (int w = 0; w < kThreads / 32; ++w)
-                y += sm.red[w][j];
-            out[s0 + j] = (base ? base[s0 + j] : 0.0) + sc * (double)y;
+        for (int q = 0; q < 4; ++q) {
+            const uint32_t k0 = c * 8 + 2 * q;
+            const float a = k0 < kIn ? __bfloat162float(P[oW1 + j * kIn + k0]) : 0.0f;
+            const float b = k0 + 1 < kIn ? __bfloat162float(P[oW1 + j * kIn + k0 + 1]) : 0.0f;
+            w[q] = pack_bf16x2(a, b);
         }
+        *reinterpret_cast<uint4*>(sm.w1 + um::sw128(j, c)) = make_uint4(w[0], w[1], w[2], w[3]);
     }
+    for (uint32_t e = tid; e < kH * 16; e += kTcTile) {  // W2: 16 chunks of 8 BF16 per row, two blocks
+        const uint32_t j = e >> 4, c = e & 15u;
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(P + oW2 + j * kH + c * 8));  // oW2 % 8 == 0
+        *reinterpret_cast<uint4*>(sm.w2[c >> 3] + um::sw128(j, c & 7u)) = v;
+    }
+    sm.b1[tid] = ldb(P + oB1 + tid);
+    sm.b2[tid] = ldb(P + oB2 + tid);
+    sm.w3[tid] = ldb(P + oW3 + tid);
+    const float b3 = ldb(P + oB3);
+    if (tid == 0) {
+        um::mbar_init(um::smem_u32(&sm.bar[0]), 1);
+        um::mbar_init(um::smem_u32(&sm.bar[1]), 1);
+        sm.fail = 0;
+    }
+    if (warp == 0)
+        um::tmem_alloc(&sm.tmem, 2 * kH);
+    um::fence_before_sync();
+    __syncthreads();
+    um::fence_after_sync();
+    const uint32_t tmem = sm.tmem;
+    const uint32_t lane_base = (32u * warp) << 16;  // this warp's TMEM lanes
+    const double sc = mul ? scale * mul[0] : scale;
+    constexpr uint32_t kId = pvl::umma::idesc_bf16(kTcTile, kH);
+    uint32_t phase = 0;
+    for (uint64_t s0 = (uint64_t)blockIdx.x * kTcTile; s0 < n; s0 += (uint64_t)gridDim.x * kTcTile, phase ^= 1u) {
+        // the tile's inputs, BF16, two 16-byte chunks per row (K 0..15, 12..15 zero)
+        {
+            const uint64_t s = s0 + tid;
+            float f[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                f[i] = (i < kIn && s < n) ? X[s * kIn + i] : 0.0f;
+            uint32_t w[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                w[q] = pack_bf16x2(f[2 * q], f[2 * q + 1]);
+            *reinterpret_cast<uint4*>(sm.x + um::sw128(tid, 0)) = make_uint4(w[0], w[1], w[2], w[3]);
+            *reinterpret_cast<uint4*>(sm.x + um::sw128(tid, 1)) = make_uint4(w[4], w[5], w[6], w[7]);
+        }
+        um::fence_proxy_async();
+        um::fence_before_sync();
+        __syncthreads();
+        if (tid == 0) {
+            um::fence_after_sync();
+            um::mma<false>(tmem, um::sw128_desc(um::smem_u32(sm.x)), um::sw128_desc(um::smem_u32(sm.w1)), kId, 0u);
+            um::commit(um::smem_u32(&sm.bar[0]));
+        }
+        bool ok = um::mbar_wait(um::smem_u32(&sm.bar[0]), phase);
+        um::fence_after_sync();
+        // H1 row tid: bf16(relu(acc1 + b1)), 16 columns at a time into the two K blocks
+#pragma unroll 1
+        for (uint32_t c0 = 0; c0 < kH; c0 += 16) {
+            float v[16];
+            __syncwarp();
+            um::tmem_ld16(tmem + lane_base + c0, v);
+            uint32_t w[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                w[q] = pack_bf16x2(fmaxf(v[2 * q] + sm.b1[c0 + 2 * q], 0.0f),
+                                   fmaxf(v[2 * q + 1] + sm.b1[c0 + 2 * q + 1], 0.0f));
+            unsigned char* blk = sm.h1[c0 >> 6];
+            const uint32_t ch = (c0 & 63u) >> 3;
+            *reinterpret_cast<uint4*>(blk + um::sw128(tid, ch)) = make_uint4(w[0], w[1], w[2], w[3]);
+            *reinterpret_cast<uint4*>(blk + um::sw128(tid, ch + 1)) = make_uint4(w[4], w[5], w[6], w[7]);
+        }
+        um::fence_proxy_async();
+        um::fence_before_sync();
+        if (__syncthreads_or(!ok))
+            ok = false;
+        if (tid == 0 && ok) {
+            um::fence_after_sync();
+#pragma unroll
+            for (uint32_t ks = 0; ks < kH / 16; ++ks) {  // K = 16 BF16 = 32 bytes per step
+                const uint32_t blk = ks >> 2, step = 2u * (ks & 3u);
+                um::mma<false>(tmem + kH, um::sw128_desc(um::smem_u32(sm.h1[blk])) + step,
+                               um::sw128_desc(um::smem_u32(sm.w2[blk])) + step, kId, ks ? 1u : 0u);
+            }
+        }
+        if (tid == 0)
+            um::commit(um::smem_u32(&sm.bar[1]));  // arrives even without MMAs (all earlier ones done)
+        ok = um::mbar_wait(um::smem_u32(&sm.bar[1]), phase) && ok;
+        um::fence_after_sync();
+        float y = b3;
+#pragma unroll 1
+        for (uint32_t c0 = 0; c0 < kH; c0 += 16) {
+            float v[16];
+            __syncwarp();
+            um::tmem_ld16(tmem + lane_base + kH + c0, v);
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                y = fmaf(sm.w3[c0 + i], bf(fmaxf(v[i] + sm.b2[c0 + i], 0.0f)), y);
+        }
+        const uint64_t s = s0 + tid;
+        if (s < n)
+            out[s] = ok ? (base ? base[s] : 0.0) + sc * (double)y : __longlong_as_double(0x7FF8000000000000ll);
+        um::fence_before_sync();
+        __syncthreads();
+    }
+    um::fence_after_sync();
+    if (warp == 0)
+        um::tmem_dealloc(tmem, 2 * kH);
 }
 
 struct TrainSmem {
@@ -375,17 +496,10 @@ __global__ void features_kernel(uint32_t n, const double* __restrict__ g0, const
     base[i] = g0[i] + jac;
 }
 
-bool g_attr_done = false;
-
 int set_attrs()
 {
-    if (g_attr_done)
-        return PVL_OK;
-    PVL_CUDA_CHECK(cudaFuncSetAttribute(forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)sizeof(FwdSmemT<kFwdTile>)));
-    PVL_CUDA_CHECK(cudaFuncSetAttribute(train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)sizeof(TrainSmem)));
-    g_attr_done = true;
+    PVL_SMEM_OPTIN(forward_tc_kernel, sizeof(FwdTcSmem) + 1024);
+    PVL_SMEM_OPTIN(train_kernel, sizeof(TrainSmem));
     return PVL_OK;
 }
 
@@ -429,8 +543,8 @@ extern "C" int pvl_mlp_forward(uint32_t n, const float* X, const void* params_bf
         return pvl_fail(PVL_ERR_ARG, "pvl_mlp_forward: null pointer argument");
     if (int r = set_attrs())
         return r;
-    const unsigned grid = (unsigned)std::min<uint64_t>(blocks_for(n, kFwdTile), 148ull * 6);
-    forward_kernel<<<grid, kThreads, sizeof(FwdSmemT<kFwdTile>), (cudaStream_t)stream>>>(
+    const unsigned grid = (unsigned)std::min<uint64_t>(blocks_for(n, kTcTile), 148ull * 2);
+    forward_tc_kernel<<<grid, kTcTile, sizeof(FwdTcSmem) + 1024, (cudaStream_t)stream>>>(
         n, X, static_cast<const __nv_bfloat16*>(params_bf16), scale, mul, base, out);
     PVL_LAUNCH_CHECK();
     return PVL_OK;

@@ -19,8 +19,11 @@
 //    safe.  The array keeps the contents of the last call; nothing in it needs to start at
 //    zero, because every byte the computation reads is written earlier in the same call;
 //  * the first call on each device looks up the array's device address with
-//    cudaGetSymbolAddress (once per device, with that device current).  Make that first
-//    call before any stream capture begins.
+//    cudaGetSymbolAddress (once per device and CUDA context, with that device current).  Make
+//    that first call before any stream capture begins.  A device reset or a new primary
+//    context reloads the module, possibly at another address: the lookup is redone when the
+//    current context differs from the one the address was found in.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -32,26 +35,56 @@ namespace {
 static __device__ __align__(256) unsigned char g_noalloc_scratch[PVL_NOALLOC_SCRATCH_BYTES];
 
 constexpr int kMaxDevices = 64;
-void* g_scratch_addr[kMaxDevices] = {};
+struct ScratchAddr {
+    CUcontext ctx;  // the context the address was looked up in
+    void* addr;
+};
+ScratchAddr g_scratch[kMaxDevices] = {};
 std::mutex g_scratch_mutex;
 
-// Device address of g_noalloc_scratch on the current device (looked up once per device).
+// The driver's cuCtxGetCurrent, reached through the runtime (the library links no libcuda).
+using CtxGetCurrent = CUresult (*)(CUcontext*);
+CtxGetCurrent ctx_get_current()
+{
+    static CtxGetCurrent fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<CtxGetCurrent>(p);
+    }();
+    return fn;
+}
+
+// Device address of g_noalloc_scratch on the current device, looked up once per device and
+// context (the caller has made the device current, so the runtime's context is current too).
 int scratch_for_current_device(void** out)
 {
     int dev = 0;
     PVL_CUDA_CHECK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices)
         return pvl_fail(PVL_ERR_ARG, "pvl_line_velocity_noalloc: device index %d out of range", dev);
+    CtxGetCurrent get = ctx_get_current();
+    if (!get)
+        return pvl_fail(PVL_ERR_CUDA, "pvl_line_velocity_noalloc: cuCtxGetCurrent is not available");
+    CUcontext ctx = nullptr;
+    if (get(&ctx) != CUDA_SUCCESS)
+        return pvl_fail(PVL_ERR_CUDA, "pvl_line_velocity_noalloc: cuCtxGetCurrent failed");
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_addr[dev]) {
+    ScratchAddr& s = g_scratch[dev];
+    if (!s.addr || !ctx || s.ctx != ctx) {
         void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);  // makes the primary context current
         if (e != cudaSuccess || !p)
             return pvl_fail(PVL_ERR_CUDA, "pvl_line_velocity_noalloc: cudaGetSymbolAddress failed: %s",
                             cudaGetErrorString(e));
-        g_scratch_addr[dev] = p;
+        if (!ctx && (get(&ctx) != CUDA_SUCCESS || !ctx))
+            return pvl_fail(PVL_ERR_CUDA, "pvl_line_velocity_noalloc: no current CUDA context");
+        s.ctx = ctx;
+        s.addr = p;
     }
-    *out = g_scratch_addr[dev];
+    *out = s.addr;
     return PVL_OK;
 }
 

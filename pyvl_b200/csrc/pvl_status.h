@@ -5,3 +5,15 @@
 
 // Record a formatted message for pvl_last_error() and return `code`.
 int pvl_fail(int code, const char* fmt, ...);
+
+#include <stddef.h>
+
+// Opt the kernel `fn` in to `bytes` of dynamic shared memory on the current device (once per
+// kernel and device; thread-safe).  Returns PVL_OK or a PVL_ERR_* code with the message set.
+int pvl_smem_optin(const void* fn, size_t bytes);
+#define PVL_SMEM_OPTIN(fn, bytes)                                                    \
+    do {                                                                             \
+        const int pvl_rc_ = pvl_smem_optin(reinterpret_cast<const void*>(fn), bytes); \
+        if (pvl_rc_ != PVL_OK)                                                       \
+            return pvl_rc_;                                                          \
+    } while (0)

@@ -1,6 +1,11 @@
 // Thread-local error reporting for the C ABI (pvl_last_error) and the ABI version.
 #include <cstdarg>
 #include <cstdio>
+#include <map>
+#include <mutex>
+#include <utility>
+
+#include <cuda_runtime.h>
 
 #include "pvl_status.h"
 
@@ -20,3 +25,24 @@ int pvl_fail(int code, const char* fmt, ...)
 extern "C" const char* pvl_last_error(void) { return g_last_error; }
 
 extern "C" int pvl_version(void) { return 100; }
+
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) is a per-device setting of a kernel: keep
+// the largest value set for each (kernel, device) and call the runtime only when a launch on
+// the current device needs more.  Thread-safe.
+int pvl_smem_optin(const void* fn, size_t bytes)
+{
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, size_t> done;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+        return pvl_fail(PVL_ERR_CUDA, "cudaGetDevice failed");
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& have = done[std::make_pair(fn, dev)];
+    if (have >= bytes)
+        return PVL_OK;
+    const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess)
+        return pvl_fail(PVL_ERR_CUDA, "cudaFuncSetAttribute(%zu bytes): %s", bytes, cudaGetErrorString(e));
+    have = bytes;
+    return PVL_OK;
+}

@@ -187,6 +187,8 @@ class SolverEngine:
         self.ipiv = torch.zeros(2 * self.N, dtype=torch.int32, device=self.dev)
         self.info = torch.zeros(1, dtype=torch.int32, device=self.dev)
         self.err = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        # set by the RHS kernel when a NaN or infinity reaches the system; held until check_status
+        self.nonfinite = torch.zeros(1, dtype=torch.int32, device=self.dev)
         if self.m:
             goff = np.array([a for a, _ in self.groups] + [self.groups[-1][1]], np.uint32)
             contiguous = all(self.groups[i][1] == self.groups[i + 1][0] for i in range(self.m - 1))
@@ -357,7 +359,7 @@ class SolverEngine:
                   ptr(b["pos"]), ptr(b["nrm"]), s)
         u = self.u_inf
         _lib.call("pvl_rhs", P, ptr(b["nrm"]), None, float(u[0]), float(u[1]), float(u[2]), ptr(b["cpv"]),
-                  ptr(b["rhs"]), s)
+                  ptr(b["rhs"]), ptr(self.nonfinite), s)
         ws = b["ws"]
         _lib.call("pvl_induction_normal_tiled", msh.n_points, msh.n_lines, ptr(d["lines"]), ptr(b["pos"]), P,
                   ptr(d["offsets"]), ptr(d["surface_lines"]), ptr(d["tile_offsets"]), ptr(d["tile_lines"]),
@@ -507,8 +509,13 @@ class SolverEngine:
         return HostResult(buf, ev)
 
     def check_status(self) -> None:
-        """Raise if the last solve reported a zero pivot or a timed-out wait."""
-        info, err = int(self.info.item()), int(self.err.item())
+        """Raise if a step since the last check met a NaN or infinity in its inputs, or if the
+        last solve reported a zero pivot or a timed-out wait (one host synchronisation)."""
+        info, err, bad = (int(v) for v in torch.cat([self.info, self.err, self.nonfinite]).tolist())
+        if bad:
+            self.nonfinite.zero_()
+            raise _lib.PvlError(_lib.PVL_ERR_NONFINITE,
+                                "a NaN or infinity reached the right-hand side (positions, velocities or stream)")
         if err:
             raise _lib.PvlError(_lib.PVL_ERR_TIMEOUT, "a wavefront wait in the triangular solve timed out")
         if info:
@@ -607,8 +614,12 @@ class MixedSolverEngine(SolverEngine):
         self.side = torch.cuda.Stream(device=self.dev)
         self.refresh_done = None
         self.ipiv32 = torch.zeros(2 * self.npad, dtype=torch.int32, device=self.dev)
-        self.info32 = torch.zeros(1, dtype=torch.int32, device=self.dev)
-        self.err32 = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        # status words of a rebuild (zero pivot of the FP32 factorisation, a tensor-core GEMM wait
+        # that ran out), side by side so that one copy brings both to the host
+        self.rstat = torch.zeros(2, dtype=torch.int32, device=self.dev)
+        self.info32, self.err32 = self.rstat[0:1], self.rstat[1:2]
+        self._h_rstat = torch.zeros(2, dtype=torch.int32, pin_memory=True)
+        self._precond_backoff = 0  # steps to wait after a rebuild that failed before trying again
         m = self.max_iter
         self.V = torch.zeros((m + 1, n), **f64)
         self.Z = torch.zeros((m, n), **f64)
@@ -628,8 +639,8 @@ class MixedSolverEngine(SolverEngine):
         self.b_saved = torch.zeros(n, **f64)
         self.have_precond = False
         self.steps_since_refresh = 0
-        self._stats = {"gmres_iters": [], "fallbacks": 0, "refreshes": 0, "initial_rel_residual": [],
-                       "final_rel_residual": [], "judge": []}
+        self._stats = {"gmres_iters": [], "fallbacks": 0, "refreshes": 0, "refresh_failures": 0,
+                       "initial_rel_residual": [], "final_rel_residual": [], "judge": []}
         # device-driven solve (pvl_gmres_graph_*): buffers captured by the graph, status ring
         self.device_solve = bool(device_solve)
         if self.device_solve and self.max_iter > int(_lib.query("pvl_gmres_max_iter")):
@@ -683,6 +694,7 @@ class MixedSolverEngine(SolverEngine):
         s = stream_ptr()
         n, npad = self.N, self.npad
         self._finish_refresh()  # never two refreshes in flight
+        self._stats["refreshes"] += 1  # rebuilds started (those that failed are refresh_failures)
         _lib.call("pvl_pad_convert_f32", n, ptr(self.A), self.N, ptr(self.A32), npad, npad, s)
         target = self.Xinv if wait else self.Xnew
 
@@ -693,9 +705,16 @@ class MixedSolverEngine(SolverEngine):
             perm = self.ipiv32.data_ptr() + 4 * npad
             _lib.call("pvl_lu32_inverse", npad, ptr(self.A32), npad, perm, ptr(target), npad, ptr(self.Yscr), npad,
                       ptr(self.err32), ws, nb, stream)
+            # the status words travel with the rebuild; the host reads them when it adopts it
+            self._h_rstat.copy_(self.rstat, non_blocking=True)
 
         if wait:
             build(s)
+            torch.cuda.current_stream().synchronize()
+            if not self._rebuild_ok():
+                self.have_precond = False
+                self._precond_backoff = 25
+                return
         else:
             converted = torch.cuda.Event()
             converted.record()
@@ -707,7 +726,6 @@ class MixedSolverEngine(SolverEngine):
         self.have_precond = True
         self.steps_since_refresh = 0
         self.policy.rebuilt()
-        self._stats["refreshes"] += 1
 
     def _adopt_refresh(self) -> None:
         """Switch to the side stream's new inverse once it is complete (no host wait).  It is
@@ -721,11 +739,32 @@ class MixedSolverEngine(SolverEngine):
         not timed as part of the steps that follow)."""
         self._finish_refresh()
 
+    def join_side_stream(self) -> None:
+        """Make the current stream wait for everything enqueued on the side stream so far (a
+        rebuild in flight stays in flight for the host): an event recorded after this covers
+        the side stream's work too."""
+        ev = torch.cuda.Event()
+        ev.record(self.side)
+        torch.cuda.current_stream().wait_event(ev)
+
+    def _rebuild_ok(self) -> bool:
+        """Whether the rebuild whose status words reached the host is usable: no exactly zero
+        FP32 pivot and no tensor-core wait that ran out.  A failed one is counted and dropped."""
+        info, err = (int(v) for v in self._h_rstat.tolist())
+        if info or err:
+            self._stats["refresh_failures"] += 1
+            return False
+        return True
+
     def _finish_refresh(self) -> None:
-        """Adopt a refresh still in flight, making the current stream wait for it."""
+        """Adopt a refresh still in flight: the host waits for its status words (long done when
+        the policy adopts it) and, if it succeeded, the current stream waits for it and copies
+        the new inverse into place; a failed rebuild leaves the previous inverse in use."""
         if self.refresh_done is not None:
-            torch.cuda.current_stream().wait_event(self.refresh_done)
-            self.Xinv.copy_(self.Xnew)
+            self.refresh_done.synchronize()
+            if self._rebuild_ok():
+                torch.cuda.current_stream().wait_event(self.refresh_done)
+                self.Xinv.copy_(self.Xnew)
             self.refresh_done = None
 
     # ------------------------------------------------------------------ GMRES
@@ -783,6 +822,8 @@ class MixedSolverEngine(SolverEngine):
         the update.  The true FP64 residual b - A x decides convergence."""
         n = self.N
         self._maybe_refresh()
+        if not self.have_precond:
+            return False  # the caller falls back to the FP64 LU
         x = self.x
         if x0 is not None:
             x.copy_(x0.reshape(-1)[:n])
@@ -852,7 +893,9 @@ class MixedSolverEngine(SolverEngine):
         its = self._stats["gmres_iters"]
         self.policy.observe(its[self._iters_seen:])
         self._iters_seen = len(its)
-        if not self.have_precond:
+        if self._precond_backoff > 0:
+            self._precond_backoff -= 1
+        elif not self.have_precond:
             self.refresh_preconditioner(wait=True)
         elif self.policy.due(self.steps_since_refresh, idle=self.refresh_done is None):
             self.refresh_preconditioner(wait=not self.async_refresh)
@@ -919,6 +962,10 @@ class MixedSolverEngine(SolverEngine):
         iteration count in time."""
         self._collect_status(block=True)
         self._maybe_refresh()
+        if not self.have_precond:  # no usable preconditioner (its rebuild failed): the FP64 LU
+            self._stats["fallbacks"] += 1
+            SolverEngine.solve(self)
+            return
         if x0 is not None:
             self.x.copy_(x0.reshape(-1)[: self.N])
         else:

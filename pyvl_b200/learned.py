@@ -124,11 +124,14 @@ class WarmStart:
     only (the inputs are per panel; a bordered closed-body system keeps its multipliers).
     """
 
-    def __init__(self, engine, mlp: WarmStartMLP | None = None, record: bool = False):
+    def __init__(self, engine, mlp: WarmStartMLP | None = None, record: bool = False, jacobi: bool = False):
         if getattr(engine, "m", 0):
             raise ValueError("the learned warm start is for open meshes")
+        if jacobi and (mlp is not None or record):
+            raise ValueError("jacobi=True is the seed without a network")
         self.eng = engine
         self.mlp = mlp
+        self.jacobi = bool(jacobi)  # seed with the Jacobi correction alone (the method without the network)
         P, dev = engine.P, engine.dev
         f64 = dict(dtype=torch.float64, device=dev)
         self.hist = [torch.zeros(P, **f64) for _ in range(2)]  # g0 (last step), g1
@@ -168,6 +171,8 @@ class WarmStart:
         else:  # fixed buffers: one captured graph per state (engine.captured)
             scale = self.mlp.out_scale if infer else 0.0  # a host value the graph keeps
             eng.captured(("prepare", self.have_base, infer, scale), run, self._graphs)
+        if self.jacobi and self.have_base:
+            return self.base
         return self.seed if infer else None
 
     def _prepare_ops(self, have_base: bool, infer: bool) -> None:
@@ -182,7 +187,7 @@ class WarmStart:
         _lib.call("pvl_gemv_f64", P, P, -1.0, ptr(eng.A), eng.N, ptr(g0), 1.0, ptr(self.resid), s)
         _lib.call("pvl_normalize", P, ptr(self.resid), None, ptr(self.rnorm), s)
         mean, inv = (self.mlp.mean, self.mlp.inv_std) if self.mlp is not None and not self.record else \
-            (self.raw_mean, self.raw_inv)
+            (self.raw_mean, self.raw_inv)  # (the Jacobi seed uses base only; X is not read)
         _lib.call("pvl_mlp_features", P, ptr(g0), ptr(g1), ptr(self.rem[0]), ptr(self.rem[1]), ptr(self.resid),
                   ptr(self.rnorm), ptr(eng.A), eng.N, ptr(self.rhs_cur), ptr(self.rhs_prev), ptr(eng.nrm), ptr(eng.cpv),
                   ptr(mean), ptr(inv), ptr(self.X), ptr(self.base), s)

@@ -2,7 +2,7 @@
 
 Run here (where the reference tree is mounted) after oracle/build_ref.sh:
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py [--reference REFERENCE_ROOT]   (default: $PYVL_REFERENCE_ROOT)
 
 It imports the reference's compiled extension (oracle/_ref) and its Python package
 and records, for small seeded inputs:
@@ -348,7 +348,7 @@ def make_checkpoint(pyvl):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=None, help="reference checkout (default: $PYVL_REFERENCE_ROOT)")
     ap.add_argument("--only", default=None)
     args = ap.parse_args()
     pyvl = ref.load_pyvl(args.reference)

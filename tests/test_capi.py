@@ -8,7 +8,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from pyvl_b200 import _lib
+from pyvl_b200 import _lib, _probe
 from pyvl_b200.cvl import Mesh
 
 ROOT = Path(__file__).resolve().parent.parent
@@ -29,6 +29,17 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
     # every declared symbol has a ctypes signature in the binding
     assert not [n for n in names if n not in _lib.SIGNATURES], [n for n in names if n not in _lib.SIGNATURES]
+    # measurement and test probes live in their own library, outside the product ABI
+    assert not [n for n in names if "probe" in n]
+
+
+def test_probe_library_exports_its_header():
+    text = (ROOT / "pyvl_b200" / "probe" / "pvl_probe.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = sorted(set(re.findall(r"\b(pvl_[a-z0-9_]+)\s*\(", text)))
+    lib = ctypes.CDLL(str(_probe.LIB_PATH))
+    assert names and not [n for n in names if not hasattr(lib, n)]
+    assert sorted(_probe.SIGNATURES) == names
 
 
 def test_version_and_error_string():
@@ -134,10 +145,10 @@ def test_argument_errors_are_reported_before_any_device_work():
     types with a message, from the host-side checks that run before any CUDA call (so they
     hold without a GPU).  Fake device addresses stand in where a pointer must be non-null."""
     fake = 1 << 20  # 16-byte aligned, never dereferenced: every call below fails before use
-    # the far-field evaluator
-    _lib.call("pvl_far_series_eval", 0, None, None, None, None, None)  # nothing to do
+    # the far-field evaluator of the probe library
+    _probe.call("pvl_probe_far_series", 0, None, None, None, None, None)  # nothing to do
     with pytest.raises(ValueError, match="null pointer"):
-        _lib.call("pvl_far_series_eval", 8, None, fake, fake, fake, None)
+        _probe.call("pvl_probe_far_series", 8, None, fake, fake, fake, None)
     # the segment-sum velocity
     with pytest.raises(ValueError, match="pts is NULL"):
         _lib.call("pvl_line_velocity", _lib.PVL_F64, 4, 2, fake, fake, fake, 5, None, None, 1e-6, 1.0, 0.0, fake,

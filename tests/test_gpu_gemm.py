@@ -22,7 +22,8 @@ def test_gemm_tf32_matches_torch(M, N, K, alpha, beta):
     C = torch.randn(M, N, device="cuda", generator=g)
     want = alpha * (A.double() @ B.double()) + beta * C.double()
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
-    _lib.call("pvl_gemm_tf32", M, N, K, alpha, ptr(A), K, ptr(B), N, beta, ptr(C), N, ptr(err), stream_ptr())
+    Bt = B.t().contiguous()  # the right operand is passed K-major (transposed)
+    _lib.call("pvl_gemm_tf32", M, N, K, alpha, ptr(A), K, ptr(Bt), K, beta, ptr(C), N, ptr(err), stream_ptr())
     torch.cuda.synchronize()
     assert int(err.item()) == 0
     rel = (torch.linalg.norm(C.double() - want) / torch.linalg.norm(want)).item()
@@ -40,16 +41,16 @@ def test_gemm_tf32_ragged_submatrix(M, N, K):
 
     g = torch.Generator(device="cuda").manual_seed(7 * M + N)
     n4 = (N + 3) // 4 * 4  # leading dimensions: multiples of 4 floats, blocks 16-byte aligned
-    lda, ldb, ldc = K + 8, n4 + 12, n4 + 20
+    lda, ldbt, ldc = K + 8, K + 12, n4 + 20
     A = torch.randn(M + 3, lda, device="cuda", generator=g)
-    B = torch.randn(K + 2, ldb, device="cuda", generator=g)
+    Bt = torch.randn(N + 2, ldbt, device="cuda", generator=g)
     C = torch.randn(M + 5, ldc, device="cuda", generator=g)
     C0 = C.clone()
-    a, b = A[1:1 + M, 4:4 + K], B[2:2 + K, 4:4 + N]
+    a, bt = A[1:1 + M, 4:4 + K], Bt[2:2 + N, 4:4 + K]  # bt: B transposed, inside a larger buffer
     c = C[2:2 + M, 8:8 + N]
-    want = -(a.double() @ b.double()) + c.double()
+    want = -(a.double() @ bt.double().t()) + c.double()
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
-    _lib.call("pvl_gemm_tf32", M, N, K, -1.0, a.data_ptr(), lda, b.data_ptr(), ldb, 1.0, c.data_ptr(), ldc, ptr(err),
+    _lib.call("pvl_gemm_tf32", M, N, K, -1.0, a.data_ptr(), lda, bt.data_ptr(), ldbt, 1.0, c.data_ptr(), ldc, ptr(err),
               stream_ptr())
     torch.cuda.synchronize()
     assert int(err.item()) == 0
@@ -67,5 +68,31 @@ def test_gemm_tf32_rejects_bad_shapes():
 
     x = torch.zeros(16, device="cuda")
     with pytest.raises(ValueError):  # K not a multiple of 32: rejected before any launch
-        _lib.call("pvl_gemm_tf32", 128, 128, 20, 1.0, x.data_ptr(), 32, x.data_ptr(), 128, 0.0, x.data_ptr(), 128,
+        _lib.call("pvl_gemm_tf32", 128, 128, 20, 1.0, x.data_ptr(), 32, x.data_ptr(), 32, 0.0, x.data_ptr(), 128,
                   x.data_ptr(), None)
+
+
+def test_gemm_tf32_waits_run_out_without_its_copies():
+    """The probe runs the same kernel with a short wait limit and a producer that issues no
+    copies: every bounded wait runs out, the kernel returns, frees its tensor memory and sets
+    the error word; a regular GEMM on the same stream follows and is right."""
+    import torch
+
+    from pyvl_b200 import _lib, _probe
+    from pyvl_b200.device import ptr, stream_ptr
+
+    A = torch.randn(256, 64, device="cuda")
+    Bt = torch.randn(256, 64, device="cuda")
+    C = torch.zeros(256, 256, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    _probe.call("pvl_probe_gemm_timeout", 256, 256, 64, ptr(A), 64, ptr(Bt), 64, ptr(C), 256, ptr(err), 4000,
+                stream_ptr())
+    torch.cuda.synchronize()
+    assert int(err.item()) == 1
+    assert torch.count_nonzero(C).item() == 0  # no accumulator reached the epilogue
+    err.zero_()
+    _lib.call("pvl_gemm_tf32", 256, 256, 64, 1.0, ptr(A), 64, ptr(Bt), 64, 0.0, ptr(C), 256, ptr(err), stream_ptr())
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    want = A.double() @ Bt.double().t()
+    assert (torch.linalg.norm(C.double() - want) / torch.linalg.norm(want)).item() <= 3e-3

@@ -203,7 +203,7 @@ def test_far_field_reciprocal_and_series_bounds(torch_cuda):
     arctangent series (four, eight or sixteen terms by w) within a few ulps of atan(q)/q,
     q = sqrt(w), evaluated in extended precision."""
     torch = torch_cuda
-    from pyvl_b200 import _lib
+    from pyvl_b200 import _probe
     from pyvl_b200.device import ptr, stream_ptr
 
     rng = np.random.default_rng(3)
@@ -214,7 +214,7 @@ def test_far_field_reciprocal_and_series_bounds(torch_cuda):
     w[:6] = [0.0, 1e-4, np.nextafter(1e-4, 1.0), 0.01, np.nextafter(0.01, 1.0), 0.1]
     dx, dw = torch.as_tensor(x, device="cuda"), torch.as_tensor(w, device="cuda")
     rcp, ssum = torch.empty_like(dx), torch.empty_like(dw)
-    _lib.call("pvl_far_series_eval", n, ptr(dx), ptr(dw), ptr(rcp), ptr(ssum), stream_ptr())
+    _probe.call("pvl_probe_far_series", n, ptr(dx), ptr(dw), ptr(rcp), ptr(ssum), stream_ptr())
     torch.cuda.synchronize()
     r, s = rcp.cpu().numpy(), ssum.cpu().numpy()
     want_r = 1.0 / x  # correctly rounded

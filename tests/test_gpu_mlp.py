@@ -112,7 +112,8 @@ def test_training_fits_a_smooth_target():
 
 def test_warm_start_gain_in_mixed_solve():
     """Trained on plain-engine steps, the network's seed starts GMRES closer to the answer than
-    the previous circulation (the method without it) and than one Jacobi correction."""
+    the previous circulation and than one Jacobi correction (the methods without it), and needs
+    no more Krylov iterations than either."""
     import torch
 
     from pyvl_b200.cvl import Mesh
@@ -140,10 +141,8 @@ def test_warm_start_gain_in_mixed_solve():
         warm = None
         if mode == "learned":
             warm = WarmStart(eng, mlp)
-        elif mode == "jacobi":
-            zero = WarmStartMLP(torch.device("cuda"))
-            zero.out_scale = 0.0
-            warm = WarmStart(eng, zero)
+        elif mode == "jacobi":  # the same seed without the network
+            warm = WarmStart(eng, jacobi=True)
         for t in test_t:
             drive_step(eng, warm, t, case.positions_at(t), case.velocities_at(t))
         st = eng.stats
@@ -154,3 +153,4 @@ def test_warm_start_gain_in_mixed_solve():
     assert results["learned"][0] < 0.5 * results["previous"][0]
     assert results["learned"][0] < results["jacobi"][0]
     assert results["learned"][1] <= results["previous"][1]
+    assert results["learned"][1] <= results["jacobi"][1]

@@ -36,11 +36,19 @@ def test_noalloc_matches_workspace_entry_point_twice():
         ws, nb = Workspace.get(_lib.query("pvl_line_velocity_workspace", mesh.n_lines, 5000, _lib.PVL_F64))
         _lib.call("pvl_line_velocity", _lib.PVL_F64, mesh.n_points, mesh.n_lines, ptr(d["lines"]), ptr(pos), ptr(lg),
                   5000, ptr(pts), ptr(normals), 1e-6, 1.0, 0.0, ptr(ref), ws, nb, stream_ptr())
-        for _ in range(2):  # two calls in a row share (and reuse) the static scratch
+        side = torch.cuda.Stream()
+        for call in range(2):  # two calls in a row share (and reuse) the static scratch
             got = torch.full(shape, float("nan"), dtype=torch.float64, device="cuda")
-            _lib.call("pvl_line_velocity_noalloc", _lib.PVL_F64, mesh.n_points, mesh.n_lines, ptr(d["lines"]),
-                      ptr(pos), ptr(lg), 5000, ptr(pts), ptr(normals), 1e-6, 1.0, 0.0, ptr(got), stream_ptr())
             torch.cuda.synchronize()
+            free0, used0 = torch.cuda.mem_get_info()[0], torch.cuda.memory_allocated()
+            # the second call on a stream of the caller's own, not the default one
+            stream = stream_ptr() if call == 0 else side.cuda_stream
+            _lib.call("pvl_line_velocity_noalloc", _lib.PVL_F64, mesh.n_points, mesh.n_lines, ptr(d["lines"]),
+                      ptr(pos), ptr(lg), 5000, ptr(pts), ptr(normals), 1e-6, 1.0, 0.0, ptr(got), stream)
+            torch.cuda.synchronize()
+            if call:  # after the first call (its one-time set-up), a call allocates no device memory
+                assert torch.cuda.mem_get_info()[0] == free0
+            assert torch.cuda.memory_allocated() == used0
             err = (torch.linalg.norm(got - ref) / torch.linalg.norm(ref)).item()
             assert err <= 1e-12
 
