@@ -71,6 +71,8 @@ def parse():
                     help="flapping: the deforming wing (headline); batch: 256 ragged wings x 50 steps; "
                          "swept: pitching swept wing, 200 steps; sphere: closed 5120-ring sphere")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the batched-cases summary (bench.py --workload batch, run after the headline)")
     ap.add_argument("--profile-kernel", choices=["line_sum", "advect_f32", "wake_term", "body", "gemv", "lu", "lu32",
                                                  "mixed_step", "batch_step"],
                     default=None,
@@ -195,6 +197,21 @@ def run_reference(args) -> None:
         "e2e": {"value": sps, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "reference_step": detail,
     }), flush=True)
+
+
+def batch_summary() -> dict:
+    """Run the batched workload (256 ragged wings x 50 steps, bench.py --workload batch) in a
+    subprocess after the headline measurement and quote its main figures."""
+    cmd = [sys.executable, str(ROOT / "bench.py"), "--workload", "batch"]
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=1200, env=env)
+        d = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
+        keys = ("metric", "value", "unit", "ms_per_step", "config", "e2e", "roofline", "cpu_baseline",
+                "per_case_loop", "speedup_vs_per_case_loop", "accuracy", "gmres_failures", "cuda_graph", "clocks")
+        return {k: d.get(k) for k in keys}
+    except Exception as e:  # reported, never fatal for the headline
+        return {"failed": f"{type(e).__name__}: {e}"}
 
 
 def cpu_baseline() -> dict | None:
@@ -930,6 +947,10 @@ def main() -> None:
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline()
+    batch = None
+    if rank == 0 and world == 1 and not args.no_batch:
+        torch.cuda.empty_cache()
+        batch = batch_summary()
     if rank == 0:
         h2d = 2 * mesh.n_points * 3 * 8
         d2h = mesh.n_surfaces * 8
@@ -981,6 +1002,7 @@ def main() -> None:
                          "timed": "pvl_line_velocity: segment table, the sweep and the partial-sum reduction"},
             "rooflines_secondary": secondary,
             "cpu_baseline": base,
+            "batched_cases": batch,
             "gpu_launches": int(head["launches"]),
             "clocks": clocks,
         }), flush=True)

@@ -221,5 +221,160 @@ __device__ __forceinline__ void tile(Smem<BM, BN>& s, const double* A, uint32_t 
         atomicExch(flag, 1);
 }
 
+// ---------------------------------------------------------------- pipelined trailing update
+// C -= A B over a run of 64 x 64 tiles of one M x N block (A: M x 64 rows, B: 64 x N), tiles in
+// column-major order so that consecutive tiles of a CTA share their B block.  While tile t is
+// multiplied, tile t + 1's A block is already being copied into the other A buffer
+// (cp.async) and its C block is already being loaded into registers, so the loads of the next
+// tile overlap the MMAs of this one.  4 warps, warp tile 32 x 32.
+constexpr int kUpdTile = 64;
+struct UpdSmem {
+    double a[2][kUpdTile * kPad];
+    double b[K * kPad];
+};
+
+template <bool VEC>
+__device__ __forceinline__ void update_tiles(UpdSmem& s, double* __restrict__ Cm, uint32_t ld, uint32_t row0,
+                                             uint32_t col0, uint32_t m, uint32_t nn, uint32_t t_begin, uint32_t t_end)
+{
+    constexpr int MT = 2, NT = 4;  // warp tile 32 x 32
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t g = lane >> 2, t4 = lane & 3;
+    const uint32_t wm0 = (warp >> 1) * 32, wn0 = (warp & 1) * 32;
+    const uint32_t tiles_i = (m + kUpdTile - 1) / kUpdTile;
+    // A block: rows row0 + i * 64 .., columns col0 - 64 .. (the panel); B block: rows row0 - 64 ..
+    // (the panel's row block), columns col0 + j * 64 ..; C block: rows row0 + i * 64, columns col0 + j * 64
+    const uint32_t a_col = col0 - K, b_row = row0 - K;
+    auto coords = [&](uint32_t t, uint32_t& i0, uint32_t& j0, uint32_t& me, uint32_t& ne) {
+        i0 = (t % tiles_i) * kUpdTile;
+        j0 = (t / tiles_i) * kUpdTile;
+        me = min((uint32_t)kUpdTile, m - i0);
+        ne = min((uint32_t)kUpdTile, nn - j0);
+    };
+    auto load_c = [&](uint32_t t, double (&c)[MT][NT][4]) {
+        uint32_t i0, j0, me, ne;
+        coords(t, i0, j0, me, ne);
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < NT; ++j) {
+                const uint32_t col = wn0 + 8 * j + 2 * t4;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const uint32_t row = wm0 + 16 * i + g + 8 * h;
+                    c[i][j][2 * h] = c[i][j][2 * h + 1] = 0.0;
+                    if (row >= me)
+                        continue;
+                    const double* cp = Cm + (size_t)(row0 + i0 + row) * ld + col0 + j0 + col;
+                    if (VEC && col + 1 < ne) {
+                        const double2 v = *reinterpret_cast<const double2*>(cp);
+                        c[i][j][2 * h] = v.x;
+                        c[i][j][2 * h + 1] = v.y;
+                    } else {
+                        if (col < ne)
+                            c[i][j][2 * h] = cp[0];
+                        if (col + 1 < ne)
+                            c[i][j][2 * h + 1] = cp[1];
+                    }
+                }
+            }
+    };
+    auto stage_a = [&](uint32_t t, int buf) {
+        uint32_t i0, j0, me, ne;
+        coords(t, i0, j0, me, ne);
+        stage_rows<kUpdTile, VEC>(s.a[buf], Cm, ld, row0 + i0, row0 + i0 + me, a_col);
+    };
+    auto stage_b = [&](uint32_t t) {
+        uint32_t i0, j0, me, ne;
+        coords(t, i0, j0, me, ne);
+        stage_cols<kUpdTile, VEC>(s.b, Cm, ld, b_row, col0 + j0, col0 + j0 + ne);
+    };
+    auto commit = [] { asm volatile("cp.async.commit_group;" ::: "memory"); };
+    double cnext[MT][NT][4];
+    if (t_begin >= t_end)
+        return;
+    stage_a(t_begin, 0);
+    stage_b(t_begin);
+    commit();
+    load_c(t_begin, cnext);
+    for (uint32_t t = t_begin; t < t_end; ++t) {
+        const int cur = (int)((t - t_begin) & 1u);
+        double acc[MT][NT][4];
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < NT; ++j)
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    acc[i][j][q] = -cnext[i][j][q];
+        const bool more = t + 1 < t_end;
+        const bool same_b = more && (t + 1) / tiles_i == t / tiles_i;
+        if (same_b) {  // the next tile's A block into the other buffer while this one computes
+            stage_a(t + 1, cur ^ 1);
+            commit();
+        }
+        if (more)
+            load_c(t + 1, cnext);
+        if (same_b)
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        else
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        __syncthreads();
+#pragma unroll
+        for (int k0 = 0; k0 < K; k0 += 8) {
+            double af[MT][4], bf[NT][2];
+#pragma unroll
+            for (int i = 0; i < MT; ++i) {
+                const double* p = s.a[cur] + (wm0 + 16 * i + g) * kPad + k0 + t4;
+                af[i][0] = p[0];
+                af[i][1] = p[8 * kPad];
+                af[i][2] = p[4];
+                af[i][3] = p[8 * kPad + 4];
+            }
+#pragma unroll
+            for (int j = 0; j < NT; ++j) {
+                const double* p = s.b + (k0 + t4) * kPad + wn0 + 8 * j + g;
+                bf[j][0] = p[0];
+                bf[j][1] = p[4 * kPad];
+            }
+#pragma unroll
+            for (int i = 0; i < MT; ++i)
+#pragma unroll
+                for (int j = 0; j < NT; ++j)
+                    mma16x8x8(acc[i][j], af[i], bf[j]);
+        }
+        uint32_t i0, j0, me, ne;
+        coords(t, i0, j0, me, ne);
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < NT; ++j) {
+                const uint32_t col = wn0 + 8 * j + 2 * t4;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const uint32_t row = wm0 + 16 * i + g + 8 * h;
+                    if (row >= me)
+                        continue;
+                    double* cp = Cm + (size_t)(row0 + i0 + row) * ld + col0 + j0 + col;
+                    const double v0 = -acc[i][j][2 * h], v1 = -acc[i][j][2 * h + 1];
+                    if (VEC && col + 1 < ne) {
+                        *reinterpret_cast<double2*>(cp) = make_double2(v0, v1);
+                    } else {
+                        if (col < ne)
+                            cp[0] = v0;
+                        if (col + 1 < ne)
+                            cp[1] = v1;
+                    }
+                }
+            }
+        __syncthreads();  // both buffers and B are free for what follows
+        if (more && !same_b) {  // a new column of tiles: its B block and the next A block
+            stage_a(t + 1, cur ^ 1);
+            stage_b(t + 1);
+            commit();
+        }
+    }
+}
+
 }  // namespace dmma
 }  // namespace pvl

@@ -378,11 +378,23 @@ __global__ void __launch_bounds__(kTrsmCols, 1) trsm_kernel(uint32_t n, uint32_t
 //                       its row block and refactors the panel with explicit partial pivoting in
 //                       getf2 order, after which trsm_kernel applies the interchanges and forms
 //                       U12 by substitution;
-//   dmma_update_kernel  A22 -= L21 U12 on the FP64 tensor cores, two 128 x 64 tiles per SM.
+//   dmma_update_kernel  A22 -= L21 U12 on the FP64 tensor cores: 64 x 64 tiles, each CTA a
+//                       run of them with the next tile's operands loading during the MMAs.
 // Every product has K = 64, the panel width; the multipliers and U12 are the blocked forms of
 // getf2's and trsm's, equal to them up to rounding.
 constexpr int kTopThreads = 256;
+constexpr int kTopStride = NB + 1;
+constexpr size_t kTopSmem = 3 * (size_t)NB * kTopStride * sizeof(double) + NB * sizeof(double);
 
+// One CTA: the 64 x 64 diagonal block in shared memory (a partial block padded with identity),
+// factored without interchanges, together with L11^-1, then U11^-1.  Thread (r, g) owns row r
+// and columns 16 g .. 16 g + 15 (the four threads of a row are neighbouring lanes of one warp),
+// so a column step needs one barrier: row r's multiplier is read by its four threads, the
+// owner of column j writes it back after a warp-level sync, each thread updates its columns of
+// row r, and the thread that finishes the next pivot publishes its reciprocal.  X = L^-1 is
+// formed in the same steps (row j of X is final once step j begins); Y = U^-1 (unscaled rows,
+// 1 / U[q][q] applied at the end) takes 64 more steps from the last row up.  Loops, not
+// unrolled code: the kernel runs once per panel on one SM.
 __global__ void __launch_bounds__(kTopThreads) top_factor_kernel(uint32_t k0, uint32_t nb,
                                                                  const double* __restrict__ A, uint32_t lda,
                                                                  double* __restrict__ top_out,
@@ -390,71 +402,63 @@ __global__ void __launch_bounds__(kTopThreads) top_factor_kernel(uint32_t k0, ui
                                                                  double* __restrict__ uinv,
                                                                  int32_t* __restrict__ reject)
 {
-    __shared__ double T[NB][NB + 1];
+    extern __shared__ double top_smem[];
+    double(*T)[kTopStride] = reinterpret_cast<double(*)[kTopStride]>(top_smem);
+    double(*X)[kTopStride] = T + NB;
+    double(*Y)[kTopStride] = T + 2 * NB;
+    double* rd = top_smem + 3 * NB * kTopStride;  // 1 / U[q][q]
     const uint32_t tid = threadIdx.x;
     for (uint32_t e = tid; e < NB * NB; e += kTopThreads) {
         const uint32_t r = e / NB, c = e % NB;
         T[r][c] = (r < nb && c < nb) ? A[(size_t)(k0 + r) * lda + k0 + c] : (r == c ? 1.0 : 0.0);
+        X[r][c] = Y[r][c] = r == c ? 1.0 : 0.0;
     }
     __syncthreads();
+    const uint32_t row = tid >> 2, g = tid & 3u, c0 = 16 * g, c1 = c0 + 16;
+    if (tid == 0)
+        rd[0] = 1.0 / T[0][0];
     bool bad = false;
-    const uint32_t tx = tid & 15, ty = tid >> 4;  // 16 x 16 threads for the rank-1 updates
+    __syncthreads();
 #pragma unroll 1
     for (uint32_t j = 0; j < NB; ++j) {
-        const double piv = T[j][j];
-        if (tid == 0)
-            bad |= !(fabs(piv) > 0.0);  // zero or NaN pivot
-        const double rcp = 1.0 / piv;   // getf2 scales by the reciprocal of the pivot
-        if (tid > j && tid < NB) {
-            const double l = T[tid][j] * rcp;
-            bad |= !(fabs(l) < pvl::dmma::kMultLimit);
-            T[tid][j] = l;
-        }
-        __syncthreads();
-        for (uint32_t i = j + 1 + ty; i < NB; i += 16) {
-            const double l = T[i][j];
-            for (uint32_t c = j + 1 + tx; c < NB; c += 16)
-                T[i][c] = fma(-l, T[j][c], T[i][c]);
+        if (row == j && g == j / 16)
+            bad |= !(fabs(T[j][j]) > 0.0);  // zero or NaN pivot
+        if (row > j) {
+            const double l = T[row][j] * rd[j];  // getf2 scales by the reciprocal of the pivot
+            __syncwarp();
+            if (j >= c0 && j < c1) {
+                bad |= !(fabs(l) < pvl::dmma::kMultLimit);
+                T[row][j] = l;
+            }
+            for (uint32_t c = max(c0, j + 1); c < c1; ++c)
+                T[row][c] = fma(-l, T[j][c], T[row][c]);
+            for (uint32_t c = c0; c < c1 && c <= j; ++c)  // X = L^-1, column step j
+                X[row][c] = fma(-l, X[j][c], X[row][c]);
+            if (row == j + 1 && j + 1 >= c0 && j + 1 < c1)
+                rd[j + 1] = 1.0 / T[j + 1][j + 1];  // the next pivot is final now
+        } else {
+            __syncwarp();
         }
         __syncthreads();
     }
     if (__syncthreads_or(bad) && tid == 0)
         atomicExch(reject, 1);
+#pragma unroll 1
+    for (uint32_t t = 0; t < NB; ++t) {  // Y: step q eliminates column q above U[q][q]
+        const uint32_t q = NB - 1 - t;
+        if (row < q) {
+            const double u = T[row][q] * rd[q];
+            for (uint32_t c = max(c0, q); c < c1; ++c)
+                Y[row][c] = fma(-u, Y[q][c], Y[row][c]);
+        }
+        __syncthreads();
+    }
     for (uint32_t e = tid; e < NB * NB; e += kTopThreads) {
         const uint32_t r = e / NB, c = e % NB;
         if (r < nb && c < nb)
             top_out[(size_t)r * NB + c] = T[r][c];
-    }
-    // inverses: threads 0..63 column c of L11^-1 (unit lower), threads 64..127 column c of U11^-1
-    if (tid < 2 * NB) {
-        const bool lower = tid < NB;
-        const int c = (int)(tid & (NB - 1));
-        double y[NB];
-#pragma unroll
-        for (int r = 0; r < NB; ++r)
-            y[r] = r == c ? 1.0 : 0.0;
-        if (lower) {
-#pragma unroll
-            for (int q = 0; q < NB - 1; ++q) {
-                const double yq = y[q];
-#pragma unroll
-                for (int r = q + 1; r < NB; ++r)
-                    y[r] = fma(-T[r][q], yq, y[r]);
-            }
-        } else {
-#pragma unroll
-            for (int q = NB - 1; q >= 0; --q) {
-                const double yq = y[q] / T[q][q];
-                y[q] = yq;
-#pragma unroll
-                for (int r = 0; r < q; ++r)
-                    y[r] = fma(-T[r][q], yq, y[r]);
-            }
-        }
-        double* out = lower ? linv : uinv;
-#pragma unroll
-        for (int r = 0; r < NB; ++r)
-            out[(size_t)r * NB + c] = y[r];
+        linv[(size_t)r * NB + c] = X[r][c];
+        uinv[(size_t)r * NB + c] = Y[r][c] * rd[r];
     }
 }
 
@@ -491,19 +495,21 @@ __global__ void __launch_bounds__(pvl::dmma::kThreads) panel_apply_kernel(uint32
     }
 }
 
-constexpr int kUpdM = 128, kUpdN = 64;  // trailing-update tile; two CTAs per SM
-
+// A22 -= L21 U12: the (below x below) trailing block as 64 x 64 tiles, each CTA a contiguous
+// run of them in column-major order (dmma.cuh update_tiles: the next tile's operands load
+// while this one multiplies), two CTAs per SM.
 template <bool VEC>
 __global__ void __launch_bounds__(pvl::dmma::kThreads, 2) dmma_update_kernel(uint32_t n, uint32_t k0,
-                                                                             double* __restrict__ A, uint32_t lda)
+                                                                             double* __restrict__ A, uint32_t lda,
+                                                                             uint32_t per_cta)
 {
-    using namespace pvl::dmma;
     extern __shared__ __align__(16) double upd_smem[];
-    auto& sm = *reinterpret_cast<Smem<kUpdM, kUpdN>*>(upd_smem);
-    const uint32_t base = k0 + NB;
-    const uint32_t i0 = base + blockIdx.y * kUpdM, j0 = base + blockIdx.x * kUpdN;
-    tile<kUpdM, kUpdN, kUpdate, VEC>(sm, A, lda, i0, k0, A, lda, k0, j0, A, lda, i0, j0, min((uint32_t)kUpdM, n - i0),
-                                     min((uint32_t)kUpdN, n - j0), nullptr, 0, 0, 0, nullptr);
+    auto& sm = *reinterpret_cast<pvl::dmma::UpdSmem*>(upd_smem);
+    const uint32_t base = k0 + NB, m = n - base;
+    const uint32_t tiles = ((m + pvl::dmma::kUpdTile - 1) / pvl::dmma::kUpdTile) *
+                           ((m + pvl::dmma::kUpdTile - 1) / pvl::dmma::kUpdTile);
+    const uint32_t t0 = blockIdx.x * per_cta, t1 = min(tiles, t0 + per_cta);
+    pvl::dmma::update_tiles<VEC>(sm, A, lda, base, base, m, m, t0, t1);
 }
 
 // ---------------------------------------------------------------- diagonal-block inverses
@@ -637,13 +643,17 @@ extern "C" int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv,
     cudaStream_t st = (cudaStream_t)stream;
     LuWs w = carve(ws, n);
     const size_t trsm_smem = (size_t)(NB * (NB + 1) + NB * (kTrsmCols + 1)) * sizeof(double);
-    const size_t upd_smem = sizeof(pvl::dmma::Smem<kUpdM, kUpdN>);
+    const size_t upd_smem = sizeof(pvl::dmma::UpdSmem);
+    int dev = 0, sms = 0;
+    PVL_CUDA_CHECK(cudaGetDevice(&dev));
+    PVL_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     // 16-byte operand copies and stores need even row strides and an even width
     const bool vec = (lda % 2 == 0) && (n % 2 == 0) && (((uintptr_t)A & 15u) == 0);
     const void* apply_fn = vec ? (const void*)panel_apply_kernel<true> : (const void*)panel_apply_kernel<false>;
     const void* upd_fn = vec ? (const void*)dmma_update_kernel<true> : (const void*)dmma_update_kernel<false>;
     PVL_SMEM_OPTIN(trsm_kernel<double>, trsm_smem);
     PVL_SMEM_OPTIN(apply_fn, kApplySmem);
+    PVL_SMEM_OPTIN(top_factor_kernel, kTopSmem);
     PVL_SMEM_OPTIN(upd_fn, upd_smem);
     int32_t* perm = ipiv + n;
     PVL_CUDA_CHECK(cudaMemsetAsync(info, 0, sizeof(int32_t), st));
@@ -655,7 +665,7 @@ extern "C" int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv,
         const uint32_t k0 = p * NB;
         const uint32_t nb = std::min<uint32_t>(NB, n - k0);
         const uint32_t below = n - k0 - nb;  // nonzero only for full panels (nb == NB)
-        top_factor_kernel<<<1, kTopThreads, 0, st>>>(k0, nb, A, lda, w.top_out, w.linv, w.uinv, w.reject + p);
+        top_factor_kernel<<<1, kTopThreads, kTopSmem, st>>>(k0, nb, A, lda, w.top_out, w.linv, w.uinv, w.reject + p);
         PVL_LAUNCH_CHECK();
         if (below > 0) {
             const uint32_t nl = blocks_for(below, kApplyRows), nu = blocks_for(below, kApplyCols);
@@ -679,9 +689,12 @@ extern "C" int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv,
         }
         if (below > 0) {
             uint32_t kk = k0;
-            void* args[] = {(void*)&n, (void*)&kk, (void*)&A, (void*)&lda};
-            const dim3 g(blocks_for(below, kUpdN), blocks_for(below, kUpdM));
-            PVL_CUDA_CHECK(cudaLaunchKernel(upd_fn, g, dim3(pvl::dmma::kThreads), args, upd_smem, st));
+            const uint32_t tpd = blocks_for(below, pvl::dmma::kUpdTile), tiles = tpd * tpd;
+            const uint32_t slots = 2u * (uint32_t)sms;  // two CTAs per SM
+            uint32_t per = blocks_for(tiles, slots);
+            const uint32_t grid = blocks_for(tiles, per);
+            void* args[] = {(void*)&n, (void*)&kk, (void*)&A, (void*)&lda, (void*)&per};
+            PVL_CUDA_CHECK(cudaLaunchKernel(upd_fn, dim3(grid), dim3(pvl::dmma::kThreads), args, upd_smem, st));
             pvl_count_launch();
         }
     }

@@ -7,10 +7,10 @@
 //                      (previous circulation + one Jacobi correction of the new system);
 //   forward_tc_kernel -- inference on the tensor cores (tcgen05.mma kind::f16, BF16 operands,
 //                      FP32 accumulators in tensor memory), one 128-panel tile per CTA;
-//   train_kernel    -- forward + backward of the mean squared error over a batch, persistent
-//                      CTAs, each accumulating its gradient in shared memory (FP32) and
-//                      writing one partial gradient row; reduce_kernel sums the rows in a
-//                      fixed order (deterministic);
+//   train_tc_kernel -- forward + backward of the mean squared error over a batch on the tensor
+//                      cores, persistent CTAs of 128-sample tiles, the layer-2 weight gradient
+//                      accumulated in tensor memory; each CTA writes one partial gradient row
+//                      and reduce_kernel sums the rows in a fixed order (deterministic);
 //   adam_kernel     -- Adam (Kingma & Ba, 2015) on the FP32 master copy, refreshing the BF16
 //                      working copy.
 // Parameter vector (FP32 master and BF16 copy alike): W1 (128 x 12), b1 (128), W2 (128 x 128),
@@ -27,108 +27,14 @@ namespace {
 
 constexpr int kIn = 12;
 constexpr int kH = 128;
-constexpr int kTile = 32;     // panels per tile of training
-constexpr int kThreads = kH;
 constexpr int oW1 = 0, oB1 = oW1 + kH * kIn, oW2 = oB1 + kH, oB2 = oW2 + kH * kH, oW3 = oB2 + kH, oB3 = oW3 + kH;
 constexpr int kParams = oB3 + 1;
-static_assert(oW2 % 8 == 0 && kH % 8 == 0 && kThreads == kH, "W2 is staged in 16-byte vectors, a row per thread");
-constexpr int kDW2Stride = kH + 1;  // padded rows of the W2 gradient (conflict-free row-per-thread updates)
+static_assert(oW2 % 8 == 0 && kH % 8 == 0, "W2 rows are read as 16-byte vectors");
 
 inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
 __device__ __forceinline__ float bf(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 __device__ __forceinline__ float ldb(const __nv_bfloat16* p) { return __bfloat162float(*p); }
-
-template <int T> struct FwdSmemT {
-    __nv_bfloat16 w2t[kH][kH];  // w2t[k][j] = W2[j][k]
-    float x[T][kIn];
-    float h1[T][kH];
-    float red[kThreads / 32][T];
-};
-using FwdSmem = FwdSmemT<kTile>;
-
-// Layers 1 and 2 for one tile; returns h2[s] (BF16-rounded) for this thread's unit j in h2.
-template <int T>
-__device__ __forceinline__ void tile_forward(const FwdSmemT<T>& sm, float (&h1s)[T][kH], const float (&w1)[kIn],
-                                             float b1, float b2, int ns, float (&h2)[T])
-{
-    const int j = threadIdx.x;
-    for (int s = 0; s < T; ++s) {
-        float a = b1;
-#pragma unroll
-        for (int i = 0; i < kIn; ++i)
-            a = fmaf(w1[i], sm.x[s][i], a);
-        h1s[s][j] = s < ns ? bf(fmaxf(a, 0.0f)) : 0.0f;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int s = 0; s < T; ++s)
-        h2[s] = b2;
-    for (int k = 0; k < kH; k += 4) {
-        float w[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-            w[q] = __bfloat162float(sm.w2t[k + q][j]);
-#pragma unroll
-        for (int s = 0; s < T; ++s) {
-            const float4 h = *reinterpret_cast<const float4*>(&h1s[s][k]);
-            h2[s] = fmaf(w[0], h.x, fmaf(w[1], h.y, fmaf(w[2], h.z, fmaf(w[3], h.w, h2[s]))));
-        }
-    }
-#pragma unroll
-    for (int s = 0; s < T; ++s)
-        h2[s] = bf(fmaxf(h2[s], 0.0f));
-}
-
-// y[s] = b3 + sum_j w3[j] h2[s][j] for the tile (all threads take part; result in red[0][s]).
-template <int T>
-__device__ __forceinline__ void tile_output(FwdSmemT<T>& sm, float w3, const float (&h2)[T])
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int s = 0; s < T; ++s) {
-        float v = w3 * h2[s];
-        for (int o = 16; o > 0; o >>= 1)
-            v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0)
-            sm.red[warp][s] = v;
-    }
-    __syncthreads();
-}
-
-template <int T>
-__device__ __forceinline__ void load_x_tile(FwdSmemT<T>& sm, const float* __restrict__ X, uint64_t s0, int ns)
-{
-    for (int e = threadIdx.x; e < T * kIn; e += kThreads) {
-        const int s = e / kIn, i = e % kIn;
-        sm.x[s][i] = s < ns ? bf(X[(s0 + s) * kIn + i]) : 0.0f;
-    }
-}
-
-// W2 into shared memory, transposed: thread j loads row j of W2 as sixteen 16-byte vectors,
-// eight in flight before their stores (the 32 KB arrive in two rounds of L2 latency), and
-// writes column j of w2t: the 32 lanes of a store write 32 consecutive entries of one row.
-template <int T>
-__device__ __forceinline__ void load_w2t(FwdSmemT<T>& sm, const __nv_bfloat16* __restrict__ P)
-{
-    constexpr int kVec = 8, kBatch = 8, kPer = kH / kVec;  // 16 vectors per row
-    const int j = threadIdx.x;
-    const uint4* __restrict__ row = reinterpret_cast<const uint4*>(P + oW2) + j * kPer;  // oW2 % 8 == 0
-#pragma unroll
-    for (int b0 = 0; b0 < kPer; b0 += kBatch) {
-        uint4 q[kBatch];
-#pragma unroll
-        for (int b = 0; b < kBatch; ++b)
-            q[b] = __ldg(row + b0 + b);
-#pragma unroll
-        for (int b = 0; b < kBatch; ++b) {
-            const __nv_bfloat16* w = reinterpret_cast<const __nv_bfloat16*>(&q[b]);
-#pragma unroll
-            for (int i = 0; i < kVec; ++i)
-                sm.w2t[(b0 + b) * kVec + i][j] = w[i];
-        }
-    }
-}
 
 // ---------------------------------------------------------------- inference on the tensor cores
 // One CTA of 128 threads per 128-panel tile (the tiles strided over the CTAs).  Layer 1:
@@ -285,127 +191,332 @@ __global__ void __launch_bounds__(kTcTile) forward_tc_kernel(uint32_t n, const f
         um::tmem_dealloc(tmem, 2 * kH);
 }
 
-struct TrainSmem {
-    FwdSmem f;
-    __nv_bfloat16 w2[kH][kH];  // row-major W2 for the input gradient
-    float dh2[kTile][kH];
-    float dy[kTile];
-    float dW2[kH][kDW2Stride];
-    float loss[kThreads / 32];
+// ---------------------------------------------------------------- training on the tensor cores
+// Forward + backward of mean((y - t)^2) over 128-sample tiles, persistent CTAs of 128 threads
+// (thread s = sample s of the tile = TMEM lane s).  Per tile, three rounds of tcgen05.mma
+// kind::f16 (BF16 operands, FP32 accumulators in tensor memory):
+//   1. acc1 = X W1^T (K = 16: the 12 inputs, zero-padded)          -> h1 = bf16(relu(acc1 + b1))
+//   2. acc2 = H1 W2^T (K = 128)                                     -> h2, y, dy = 2 (y - t) / n,
+//      dh2 = [h2 > 0] dy w3 (rounded to BF16 as an MMA operand)
+//   3. dH1 = dH2 W2 (K = 128, into acc1's columns)  and  dW2 += dH2^T H1 (K = 128 samples,
+//      accumulated in TMEM over all tiles of the CTA).
+// The operands of round 3 need H1 and dH2 also transposed (samples along K): the epilogue
+// threads write both layouts.  db2 and dw3 are per-unit sums over samples: warp reductions
+// (halving exchange, 16 shuffles per 16 columns) then a fixed-order sum over the 4 warps;
+// db1 and dW1 = sum_s dh1[s][k] x[s][i] on CUDA cores from dh1 staged in shared memory, a
+// unit per thread.  Every sum runs in a fixed order: the same data give the same gradient bit
+// for bit.  Shared memory is time-shared: X then dH2 in r1, H1 then dH2^T in r2, H1^T in r3,
+// and r2 + r3 hold dh1 (FP32) for the CUDA-core phase.  Waits are bounded; one that runs out
+// poisons the partial gradient with NaN (training then stops on the loss).
+struct TrainTcSmem {
+    unsigned char w1[kH * 128];        // W1: N = 128 units x K (12 used)
+    unsigned char w2[2][kH * 128];     // W2: N = j x K = k (round 2's B)
+    unsigned char w2t[2][kH * 128];    // W2^T: N = k x K = j (round 3's B for dH1)
+    unsigned char r1[2][kTcTile * 128];
+    unsigned char r2[2][kTcTile * 128];
+    unsigned char r3[2][kH * 128];
+    float xs[kTcTile][kIn];            // the tile's inputs, BF16-rounded
+    float b1[kH], b2[kH], w3[kH];
+    float red[4][2 * kH];              // per-warp dw3 | db2 partials
+    float lred[4];
+    uint64_t bar[3];
+    uint32_t tmem;
 };
+static_assert(sizeof(TrainTcSmem) + 1024 <= 227 * 1024, "training tile fits one CTA's shared memory");
 
-// Forward + backward of mean((y - t)^2) over samples [0, n) (normalised by n_total, so that
-// batches can be split over launches), CTAs striding over 32-sample tiles.  Each CTA writes
-// its partial gradient to part[blockIdx.x * kParams + p] and its partial loss to
-// part_loss[blockIdx.x].
-__global__ void __launch_bounds__(kThreads, 1) train_kernel(uint32_t n, double n_total, const float* __restrict__ X,
-                                                            const float* __restrict__ T,
-                                                            const __nv_bfloat16* __restrict__ P,
-                                                            float* __restrict__ part, float* __restrict__ part_loss)
+// Sum of v[0..15] over the warp's 32 lanes by halving exchanges; lane l ends with the sum for
+// column (l >> 1) & 15 (lanes l and l ^ 1 alike).
+__device__ __forceinline__ float warp_sum16(float (&v)[16], uint32_t lane)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    TrainSmem& sm = *reinterpret_cast<TrainSmem*>(smem_raw);
-    const int j = threadIdx.x, lane = j & 31, warp = j >> 5;
-    load_w2t(sm.f, P);
-    for (int e = j; e < kH * kH; e += kThreads)
-        sm.w2[e / kH][e % kH] = P[oW2 + e];
-    for (int e = j; e < kH * kDW2Stride; e += kThreads)
-        (&sm.dW2[0][0])[e] = 0.0f;
-    float w1[kIn], dW1[kIn];
 #pragma unroll
-    for (int i = 0; i < kIn; ++i) {
-        w1[i] = ldb(P + oW1 + j * kIn + i);
-        dW1[i] = 0.0f;
+    for (int h = 8, o = 16; h >= 1; h >>= 1, o >>= 1) {
+#pragma unroll
+        for (int i = 0; i < h; ++i) {
+            const bool up = (lane & (uint32_t)o) != 0;
+            const float send = up ? v[i] : v[i + h];
+            const float keep = up ? v[i + h] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
     }
-    const float b1 = ldb(P + oB1 + j), b2 = ldb(P + oB2 + j), w3 = ldb(P + oW3 + j), b3 = ldb(P + oB3);
-    float db1 = 0.0f, db2 = 0.0f, dw3 = 0.0f, db3 = 0.0f, loss = 0.0f;
+    return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+
+// element (row, k) of a BF16 K-major SW128 tile made of 64-wide column blocks of `rows` rows
+__device__ __forceinline__ void st_bf16(unsigned char* tile, uint32_t rows, uint32_t row, uint32_t k, float v)
+{
+    unsigned char* blk = tile + (size_t)(k >> 6) * rows * 128u;
+    *reinterpret_cast<__nv_bfloat16*>(blk + pvl::umma::sw128(row, (k & 63u) >> 3) + (k & 7u) * 2u) =
+        __float2bfloat16_rn(v);
+}
+
+__global__ void __launch_bounds__(kTcTile, 1) train_tc_kernel(uint32_t n, double n_total, const float* __restrict__ X,
+                                                              const float* __restrict__ T,
+                                                              const __nv_bfloat16* __restrict__ P,
+                                                              float* __restrict__ part, float* __restrict__ part_loss)
+{
+    namespace um = pvl::umma;
+    extern __shared__ __align__(1024) unsigned char tr_raw[];
+    TrainTcSmem& sm = *reinterpret_cast<TrainTcSmem*>(tr_raw + ((1024u - (um::smem_u32(tr_raw) & 1023u)) & 1023u));
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // weights: W1 and W2 rows as they are (unit j = N index), W2^T row k = column k of W2
+    for (uint32_t e = tid; e < kH * 8; e += kTcTile) {
+        const uint32_t j = e >> 3, c = e & 7u;
+        uint32_t w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint32_t k0 = c * 8 + 2 * q;
+            const float a = k0 < kIn ? __bfloat162float(P[oW1 + j * kIn + k0]) : 0.0f;
+            const float b = k0 + 1 < kIn ? __bfloat162float(P[oW1 + j * kIn + k0 + 1]) : 0.0f;
+            w[q] = pack_bf16x2(a, b);
+        }
+        *reinterpret_cast<uint4*>(sm.w1 + um::sw128(j, c)) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    for (uint32_t e = tid; e < kH * 16; e += kTcTile) {
+        const uint32_t j = e >> 4, c = e & 15u;
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(P + oW2 + j * kH + c * 8));
+        *reinterpret_cast<uint4*>(sm.w2[c >> 3] + um::sw128(j, c & 7u)) = v;
+    }
+    for (uint32_t e = tid; e < kH * kH; e += kTcTile) {  // W2^T[k][j] = W2[j][k]
+        const uint32_t j = e / kH, k = e % kH;
+        const float v = __bfloat162float(P[oW2 + e]);
+        st_bf16(&sm.w2t[0][0], kH, k, j, v);
+    }
+    sm.b1[tid] = ldb(P + oB1 + tid);
+    sm.b2[tid] = ldb(P + oB2 + tid);
+    sm.w3[tid] = ldb(P + oW3 + tid);
+    const float b3 = ldb(P + oB3);
+    if (tid == 0)
+        for (int i = 0; i < 3; ++i)
+            um::mbar_init(um::smem_u32(&sm.bar[i]), 1);
+    if (warp == 0)
+        um::tmem_alloc(&sm.tmem, 512);
+    um::fence_proxy_async();
+    um::fence_before_sync();
+    __syncthreads();
+    um::fence_after_sync();
+    const uint32_t tmem = sm.tmem;
+    const uint32_t lane_base = (32u * warp) << 16;
+    constexpr uint32_t kId = pvl::umma::idesc_bf16(kTcTile, kH);
     const float inv_n = (float)(2.0 / n_total);
-    for (uint64_t s0 = (uint64_t)blockIdx.x * kTile; s0 < n; s0 += (uint64_t)gridDim.x * kTile) {
-        const int ns = (int)(n - s0 < (uint64_t)kTile ? n - s0 : (uint64_t)kTile);
-        __syncthreads();
-        load_x_tile(sm.f, X, s0, ns);
-        __syncthreads();
-        float h2[kTile];
-        tile_forward(sm.f, sm.f.h1, w1, b1, b2, ns, h2);
-        tile_output(sm.f, w3, h2);
-        if (j < kTile) {
-            float d = 0.0f;
-            if (j < ns) {
-                float y = b3;
-                for (int w = 0; w < kThreads / 32; ++w)
-                    y += sm.f.red[w][j];
-                const float r = y - T[s0 + j];
-                loss += r * r;
-                d = r * inv_n;
+    float dW1[kIn], db1 = 0.0f, acc_dw3[8], acc_db2[8], loss = 0.0f, db3 = 0.0f;
+#pragma unroll
+    for (int i = 0; i < kIn; ++i)
+        dW1[i] = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        acc_dw3[i] = acc_db2[i] = 0.0f;
+    bool ok = true;
+    uint32_t ti = 0;
+    for (uint64_t s0 = (uint64_t)blockIdx.x * kTcTile; s0 < n; s0 += (uint64_t)gridDim.x * kTcTile, ++ti) {
+        const uint32_t ph = ti & 1u;
+        const uint64_t smp = s0 + tid;
+        const bool valid = smp < n;
+        // ---- inputs: BF16 into X (r1) and as FP32 values for dW1
+        {
+            float f[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                f[i] = (i < kIn && valid) ? bf(X[smp * kIn + i]) : 0.0f;
+                if (i < kIn)
+                    sm.xs[tid][i] = f[i];
             }
-            sm.dy[j] = d;
+            uint32_t w[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                w[q] = pack_bf16x2(f[2 * q], f[2 * q + 1]);
+            *reinterpret_cast<uint4*>(sm.r1[0] + um::sw128(tid, 0)) = make_uint4(w[0], w[1], w[2], w[3]);
+            *reinterpret_cast<uint4*>(sm.r1[0] + um::sw128(tid, 1)) = make_uint4(w[4], w[5], w[6], w[7]);
         }
+        um::fence_proxy_async();
+        um::fence_before_sync();
         __syncthreads();
-        // output layer and the gradient at h2 (unit j; kept in registers and shared)
-        float dh2[kTile];
-#pragma unroll
-        for (int s = 0; s < kTile; ++s) {
-            const float d = sm.dy[s];
-            if (j == 0)
-                db3 += d;
-            dw3 = fmaf(d, h2[s], dw3);
-            const float g = h2[s] > 0.0f ? d * w3 : 0.0f;
-            dh2[s] = g;
-            sm.dh2[s][j] = g;
-            db2 += g;
+        if (tid == 0) {
+            um::fence_after_sync();
+            um::mma<false>(tmem, um::sw128_desc(um::smem_u32(sm.r1[0])), um::sw128_desc(um::smem_u32(sm.w1)), kId, 0u);
+            um::commit(um::smem_u32(&sm.bar[0]));
         }
+        ok = um::mbar_wait(um::smem_u32(&sm.bar[0]), ph) && ok;
+        um::fence_after_sync();
+        // ---- h1 = bf16(relu(acc1 + b1)) into H1 (r2, rows s) and H1^T (r3, rows k); its ReLU mask
+        uint32_t mask[4] = {0u, 0u, 0u, 0u};
+#pragma unroll 1
+        for (uint32_t c0 = 0; c0 < kH; c0 += 16) {
+            float v[16];
+            __syncwarp();
+            um::tmem_ld16(tmem + lane_base + c0, v);
+            uint32_t w[8];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                v[i] = bf(fmaxf(v[i] + sm.b1[c0 + i], 0.0f));
+                if (v[i] > 0.0f)
+                    mask[(c0 + i) >> 5] |= 1u << ((c0 + i) & 31u);
+                st_bf16(&sm.r3[0][0], kH, c0 + i, tid, v[i]);
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                w[q] = pack_bf16x2(v[2 * q], v[2 * q + 1]);
+            unsigned char* blk = sm.r2[c0 >> 6];
+            const uint32_t ch = (c0 & 63u) >> 3;
+            *reinterpret_cast<uint4*>(blk + um::sw128(tid, ch)) = make_uint4(w[0], w[1], w[2], w[3]);
+            *reinterpret_cast<uint4*>(blk + um::sw128(tid, ch + 1)) = make_uint4(w[4], w[5], w[6], w[7]);
+        }
+        um::fence_proxy_async();
+        um::fence_before_sync();
         __syncthreads();
-        // dW2[j][k] += sum_s dh2[s][j] h1[s][k]      (thread j owns row j)
-        for (int k = 0; k < kH; ++k) {
-            float g = 0.0f;
+        if (tid == 0) {
+            um::fence_after_sync();
 #pragma unroll
-            for (int s = 0; s < kTile; ++s)
-                g = fmaf(dh2[s], sm.f.h1[s][k], g);
-            sm.dW2[j][k] += g;
+            for (uint32_t ks = 0; ks < kH / 16; ++ks) {
+                const uint32_t blk = ks >> 2, step = 2u * (ks & 3u);
+                um::mma<false>(tmem + kH, um::sw128_desc(um::smem_u32(sm.r2[blk])) + step,
+                               um::sw128_desc(um::smem_u32(sm.w2[blk])) + step, kId, ks ? 1u : 0u);
+            }
+            um::commit(um::smem_u32(&sm.bar[1]));
         }
-        // dh1[s][k] = [h1 > 0] sum_j dh2[s][j] W2[j][k]  (thread k = j), then dW1, db1
-        float dh1[kTile];
+        ok = um::mbar_wait(um::smem_u32(&sm.bar[1]), ph) && ok;
+        um::fence_after_sync();
+        // ---- output, loss and dy
+        float y = b3;
+#pragma unroll 1
+        for (uint32_t c0 = 0; c0 < kH; c0 += 16) {
+            float v[16];
+            __syncwarp();
+            um::tmem_ld16(tmem + lane_base + kH + c0, v);
 #pragma unroll
-        for (int s = 0; s < kTile; ++s)
-            dh1[s] = 0.0f;
-        for (int q = 0; q < kH; ++q) {
-            const float w = __bfloat162float(sm.w2[q][j]);
-#pragma unroll
-            for (int s = 0; s < kTile; ++s)
-                dh1[s] = fmaf(sm.dh2[s][q], w, dh1[s]);
+            for (int i = 0; i < 16; ++i)
+                y = fmaf(sm.w3[c0 + i], bf(fmaxf(v[i] + sm.b2[c0 + i], 0.0f)), y);
         }
+        float dy = 0.0f;
+        if (valid) {
+            const float r = y - T[smp];
+            loss += r * r;
+            dy = r * inv_n;
+        }
+        db3 += dy;
+        // ---- dh2 = [h2 > 0] dy w3 into dH2 (r1, rows s) and dH2^T (r2, rows j); dw3 and db2 sums
+#pragma unroll 1
+        for (uint32_t c0 = 0; c0 < kH; c0 += 16) {
+            float v[16], g[16], hv[16];
+            __syncwarp();
+            um::tmem_ld16(tmem + lane_base + kH + c0, v);
 #pragma unroll
-        for (int s = 0; s < kTile; ++s) {
-            const float g = sm.f.h1[s][j] > 0.0f ? dh1[s] : 0.0f;
+            for (int i = 0; i < 16; ++i) {
+                const float h2 = bf(fmaxf(v[i] + sm.b2[c0 + i], 0.0f));
+                g[i] = h2 > 0.0f ? dy * sm.w3[c0 + i] : 0.0f;
+                hv[i] = dy * h2;
+                st_bf16(&sm.r1[0][0], kTcTile, tid, c0 + i, g[i]);
+                st_bf16(&sm.r2[0][0], kH, c0 + i, tid, g[i]);
+            }
+            const uint32_t slot = c0 >> 4;
+            acc_dw3[slot] += warp_sum16(hv, lane);
+            acc_db2[slot] += warp_sum16(g, lane);
+        }
+        um::fence_proxy_async();
+        um::fence_before_sync();
+        __syncthreads();
+        if (tid == 0) {
+            um::fence_after_sync();
+#pragma unroll
+            for (uint32_t ks = 0; ks < kH / 16; ++ks) {  // dH1 = dH2 W2 (acc1's columns)
+                const uint32_t blk = ks >> 2, step = 2u * (ks & 3u);
+                um::mma<false>(tmem, um::sw128_desc(um::smem_u32(sm.r1[blk])) + step,
+                               um::sw128_desc(um::smem_u32(sm.w2t[blk])) + step, kId, ks ? 1u : 0u);
+            }
+#pragma unroll
+            for (uint32_t ks = 0; ks < kTcTile / 16; ++ks) {  // dW2 += dH2^T H1 over the tile's samples
+                const uint32_t blk = ks >> 2, step = 2u * (ks & 3u);
+                um::mma<false>(tmem + 2 * kH, um::sw128_desc(um::smem_u32(sm.r2[blk])) + step,
+                               um::sw128_desc(um::smem_u32(sm.r3[blk])) + step, kId, (ti | ks) ? 1u : 0u);
+            }
+            um::commit(um::smem_u32(&sm.bar[2]));
+        }
+        ok = um::mbar_wait(um::smem_u32(&sm.bar[2]), ph) && ok;
+        um::fence_after_sync();
+        // ---- dh1 = [h1 > 0] dH1, staged FP32 (r2 + r3, 16-byte chunks XOR-swizzled by row)
+        float* D = reinterpret_cast<float*>(sm.r2);
+#pragma unroll 1
+        for (uint32_t c0 = 0; c0 < kH; c0 += 16) {
+            float v[16];
+            __syncwarp();
+            um::tmem_ld16(tmem + lane_base + c0, v);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                float4 o;
+                float* op = &o.x;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const uint32_t k = c0 + 4 * q + i;
+                    op[i] = (mask[k >> 5] >> (k & 31u)) & 1u ? v[4 * q + i] : 0.0f;
+                }
+                const uint32_t chunk = ((c0 >> 2) + q) ^ (tid & 31u);
+                *reinterpret_cast<float4*>(D + tid * kH + chunk * 4) = o;
+            }
+        }
+        um::fence_before_sync();
+        __syncthreads();
+        // ---- unit k = tid: db1, dW1 over the tile's samples
+        for (uint32_t s_ = 0; s_ < (uint32_t)kTcTile; ++s_) {
+            const float g = D[s_ * kH + ((((tid >> 2) ^ (s_ & 31u)) << 2) | (tid & 3u))];
             db1 += g;
 #pragma unroll
             for (int i = 0; i < kIn; ++i)
-                dW1[i] = fmaf(g, sm.f.x[s][i], dW1[i]);
+                dW1[i] = fmaf(g, sm.xs[s_][i], dW1[i]);
         }
+        __syncthreads();  // r1..r3 and xs are rewritten by the next tile
+    }
+    // ---- this CTA's partial gradient
+    um::fence_after_sync();
+    float* g = part + (size_t)blockIdx.x * kParams;
+    if (ti > 0) {
+#pragma unroll 1
+        for (uint32_t c0 = 0; c0 < kH; c0 += 16) {  // dW2 row j = tid (TMEM lane)
+            float v[16];
+            __syncwarp();
+            um::tmem_ld16(tmem + lane_base + 2 * kH + c0, v);
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                g[oW2 + tid * kH + c0 + i] = ok ? v[i] : __int_as_float(0x7FC00000);
+        }
+    } else {
+        for (uint32_t k = 0; k < kH; ++k)
+            g[oW2 + tid * kH + k] = 0.0f;
+    }
+    if ((lane & 1u) == 0)
+#pragma unroll
+        for (int slot = 0; slot < 8; ++slot) {
+            sm.red[warp][slot * 16 + ((lane >> 1) & 15u)] = acc_dw3[slot];
+            sm.red[warp][kH + slot * 16 + ((lane >> 1) & 15u)] = acc_db2[slot];
+        }
+    float lsum = loss, d3 = db3;
+    for (int o = 16; o > 0; o >>= 1) {
+        lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+        d3 += __shfl_xor_sync(0xffffffffu, d3, o);
     }
     __syncthreads();
-    float* g = part + (size_t)blockIdx.x * kParams;
+    const float dw3 = ((sm.red[0][tid] + sm.red[1][tid]) + sm.red[2][tid]) + sm.red[3][tid];
+    const float db2 = ((sm.red[0][kH + tid] + sm.red[1][kH + tid]) + sm.red[2][kH + tid]) + sm.red[3][kH + tid];
+    const float bad = ok ? 0.0f : __int_as_float(0x7FC00000);
 #pragma unroll
     for (int i = 0; i < kIn; ++i)
-        g[oW1 + j * kIn + i] = dW1[i];
-    g[oB1 + j] = db1;
-    for (int k = 0; k < kH; ++k)
-        g[oW2 + j * kH + k] = sm.dW2[j][k];
-    g[oB2 + j] = db2;
-    g[oW3 + j] = dw3;
-    if (j == 0)
-        g[oB3] = db3;
-    for (int o = 16; o > 0; o >>= 1)
-        loss += __shfl_xor_sync(0xffffffffu, loss, o);
-    if (lane == 0)
-        sm.loss[warp] = loss;
+        g[oW1 + tid * kIn + i] = dW1[i] + bad;
+    g[oB1 + tid] = db1 + bad;
+    g[oB2 + tid] = db2 + bad;
+    g[oW3 + tid] = dw3 + bad;
     __syncthreads();
-    if (j == 0) {
-        float t = 0.0f;
-        for (int w = 0; w < kThreads / 32; ++w)
-            t += sm.loss[w];
-        part_loss[blockIdx.x] = t;
+    if (lane == 0) {
+        sm.red[warp][0] = lsum;
+        sm.red[warp][1] = d3;
     }
+    __syncthreads();
+    if (tid == 0) {
+        g[oB3] = ((sm.red[0][1] + sm.red[1][1]) + sm.red[2][1]) + sm.red[3][1] + bad;
+        part_loss[blockIdx.x] = ((sm.red[0][0] + sm.red[1][0]) + sm.red[2][0]) + sm.red[3][0] + bad;
+    }
+    um::fence_before_sync();
+    __syncthreads();
+    um::fence_after_sync();
+    if (warp == 0)
+        um::tmem_dealloc(tmem, 512);
 }
 
 // grad[p] = sum over CTAs of part[c * kParams + p], in CTA order; loss likewise (thread 0).
@@ -499,7 +610,7 @@ __global__ void features_kernel(uint32_t n, const double* __restrict__ g0, const
 int set_attrs()
 {
     PVL_SMEM_OPTIN(forward_tc_kernel, sizeof(FwdTcSmem) + 1024);
-    PVL_SMEM_OPTIN(train_kernel, sizeof(TrainSmem));
+    PVL_SMEM_OPTIN(train_tc_kernel, sizeof(TrainTcSmem) + 1024);
     return PVL_OK;
 }
 
@@ -564,10 +675,9 @@ extern "C" int pvl_mlp_gradient(uint32_t n, const float* X, const float* T, cons
     cudaStream_t st = (cudaStream_t)stream;
     float* part = static_cast<float*>(ws);
     float* part_loss = part + (size_t)n_ctas * kParams;
-    const unsigned grid = (unsigned)std::min<uint64_t>(n_ctas, blocks_for(n, kTile));
-    train_kernel<<<grid, kThreads, sizeof(TrainSmem), st>>>(n, (double)n, X, T,
-                                                            static_cast<const __nv_bfloat16*>(params_bf16), part,
-                                                            part_loss);
+    const unsigned grid = (unsigned)std::min<uint64_t>(n_ctas, blocks_for(n, kTcTile));
+    train_tc_kernel<<<grid, kTcTile, sizeof(TrainTcSmem) + 1024, st>>>(
+        n, (double)n, X, T, static_cast<const __nv_bfloat16*>(params_bf16), part, part_loss);
     PVL_LAUNCH_CHECK();
     reduce_kernel<<<blocks_for(kParams, 256), 256, 0, st>>>(grid, part, part_loss, (double)n, grad, loss);
     PVL_LAUNCH_CHECK();

@@ -417,13 +417,15 @@ class SolverEngine:
                       ptr(self.rhs), ws, nb, s)
 
     def solve(self) -> None:
-        s = stream_ptr()
         ws, nb = ptr(self.ws), self._ws_bytes
-        _lib.call("pvl_lu_factor", self.N, ptr(self.A), self.N, ptr(self.ipiv), ptr(self.info), ws, nb, s)
-        _lib.call("pvl_lu_solve", self.N, ptr(self.A), self.N, ptr(self.ipiv), ptr(self.rhs), ptr(self.err), ws, nb, s)
+        # the factorisation's ~5 launches per 64-column panel run as one captured graph (fixed buffers)
+        self.captured(("lu", ws, nb), lambda: _lib.call("pvl_lu_factor", self.N, ptr(self.A), self.N, ptr(self.ipiv),
+                                                        ptr(self.info), ws, nb, stream_ptr()))
+        _lib.call("pvl_lu_solve", self.N, ptr(self.A), self.N, ptr(self.ipiv), ptr(self.rhs), ptr(self.err), ws, nb,
+                  stream_ptr())
         self.gamma.copy_(self.rhs[: self.P])
         if self.m:
-            _lib.call("pvl_group_mean_remove", self.m, ptr(self.goff), ptr(self.gamma), s)
+            _lib.call("pvl_group_mean_remove", self.m, ptr(self.goff), ptr(self.gamma), stream_ptr())
 
     def wake_update(self, time: float) -> None:
         """Advance the wake to `time` (wake_models.py:111-157)."""

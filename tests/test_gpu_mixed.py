@@ -207,27 +207,34 @@ def test_mixed_closed_sphere_judged():
 
 
 def test_mixed_trajectory_tracks_plain():
-    """Whole trajectories: the FP32 far-field terms perturb the wake slightly; the
-    circulation histories of the mixed and the plain engine stay close."""
+    """Whole trajectories, held to the mixed path's 1e-10: the flapping wing (64 x 16) flown
+    from t = 0 for 250 steps by the plain FP64 engine and by the mixed engine with its default
+    precision bands (FP64 wake term, FP32 advection beyond the first 8 node rows); the wake
+    grows to its 100 rows and is then truncated for 150 steps.  Every step's circulation of the
+    mixed run is within 1e-10 of the plain run's."""
     from pyvl_b200.cvl import Mesh
-    from pyvl_b200.engine import SolverEngine, wake_spec_from_te
+    from pyvl_b200.engine import MixedSolverEngine, SolverEngine, wake_spec_from_te
     from pyvl_b200.workloads import flapping
 
-    case = flapping(ns=64, nc=16, line_rows=40)
+    case = flapping(ns=64, nc=16, line_rows=100)
     mesh = Mesh(case.n_points, case.elements)
-    plain = SolverEngine(mesh, case.freestream, case.tol,
-                         wake_spec_from_te(mesh, case.te_node_pairs, case.line_rows, case.t0))
-    mixed = _mixed_engine(case, refresh=25, advect_near_rows=4)
+
+    def spec():
+        return wake_spec_from_te(mesh, case.te_node_pairs, case.line_rows, case.t0)
+
+    plain = SolverEngine(mesh, case.freestream, case.tol, spec())
+    mixed = MixedSolverEngine(mesh, case.freestream, case.tol, spec())
     worst = 0.0
-    for it in range(60):
+    for it in range(250):
         t = it * case.dt
         p, v = case.positions_at(t), case.velocities_at(t)
         plain.step(t, p, v)
         mixed.step(t, p, v)
         a, b = mixed.gamma_host(), plain.gamma_host()
         worst = max(worst, float(np.linalg.norm(a - b) / np.linalg.norm(b)))
-    print(f"max trajectory difference over 60 steps: {worst:.3e}")
-    assert worst <= 1e-8, worst
+    print(f"max trajectory difference over 250 steps: {worst:.3e}")
+    assert worst <= MIXED_TOL, worst
+    assert mixed.stats["fallbacks"] == 0
 
 
 def test_gmres_graph_replay_is_bitwise_identical():
