@@ -74,7 +74,7 @@ def parse():
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batched-cases summary (bench.py --workload batch, run after the headline)")
     ap.add_argument("--profile-kernel", choices=["line_sum", "advect_f32", "wake_term", "body", "gemv", "lu", "lu32",
-                                                 "mixed_step", "batch_step"],
+                                                 "mixed_step", "plain_step", "batch_step", "mlp"],
                     default=None,
                     help="set up the workload, launch only that kernel family twice and exit (for ncu captures)")
     ap.add_argument("--fraction", type=int, default=16,
@@ -299,6 +299,28 @@ def profile_kernel(args) -> None:
         for k in range(5):
             t = t0 + k * case.dt
             eng.step(t, case.positions_at(t), case.velocities_at(t))
+    elif args.profile_kernel == "plain_step":  # 3 + 2 whole plain FP64 steps
+        from pyvl_b200.engine import SolverEngine
+
+        plain = SolverEngine(mesh, case.freestream, case.tol, spec)
+        plain.set_wake_state(wpos, wcirc, step_count=case.line_rows + 1, time=t0 - case.dt)
+        plain.iteration = 1
+        for k in range(5):
+            t = t0 + k * case.dt
+            plain.step(t, case.positions_at(t), case.velocities_at(t))
+        plain.check_status()
+    elif args.profile_kernel == "mlp":  # warm-start network: two inference launches, two gradient launches
+        from pyvl_b200.learned import WarmStartMLP
+
+        mlp = WarmStartMLP(torch.device("cuda"), seed=0)
+        g = torch.Generator(device="cuda").manual_seed(0)
+        X = torch.randn(16384, 12, device="cuda", generator=g)
+        T = torch.randn(16384, device="cuda", generator=g)
+        base = torch.zeros(eng.P, dtype=torch.float64, device="cuda")
+        out = torch.zeros_like(base)
+        for _ in range(2):
+            mlp.predict(X[: eng.P], base, out)
+            mlp.gradient(X, T)
     else:  # the mixed path's preconditioner refresh (FP32 LU + inverse on the tensor cores)
         eng.assemble()
         for _ in range(2):

@@ -6,13 +6,15 @@ The library is compiled from pyvl_b200/csrc/*.cu and *.cpp with
 ``-gencode arch=compute_100a,code=sm_100a`` and lands next to this file, where the
 Python layer loads it.  nvcc cross-compiles without a GPU.  Beside it, libpvl_probe.so
 (pyvl_b200/probe: an FMA-throughput probe and test hooks) is built for benchmarks and tests;
-the product never loads it.
+the product never loads it.  Extra nvcc flags (e.g. a tuning define such as
+``-DPVL_UPD_WARPS=4``) can be passed in the environment variable PVL_NVCC_FLAGS.
 """
 
 from __future__ import annotations
 
 import argparse
 import os
+import shlex
 import shutil
 import subprocess
 import sys
@@ -67,7 +69,7 @@ def _build_lib(lib: Path, srcs: list[Path], prefix: str, verbose: bool, force: b
         return lib
     BUILD_DIR.mkdir(exist_ok=True)
     common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(HERE.parent / "include"), "-I", str(CSRC),
-              "-I", str(PROBE_SRC)]
+              "-I", str(PROBE_SRC), *shlex.split(os.environ.get("PVL_NVCC_FLAGS", ""))]
 
     def compile_one(src: Path) -> str:
         obj = BUILD_DIR / (prefix + src.name + ".o")

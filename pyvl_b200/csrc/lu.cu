@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(kTrsmCols, 1) trsm_kernel(uint32_t n, uint32_t
 // diagonal in column j exactly when no entry below it is larger in magnitude at that moment,
 // i.e. when every multiplier l_ij (i > j) has |l_ij| <= 1 (LAPACK's idamax returns the first
 // maximal entry, and the diagonal comes first).  The multipliers are formed by blocks:
-//   top_factor_kernel   L11 U11 = A11 (one CTA, the 64 x 64 diagonal block, in shared memory),
+//   top_factor_kernel   L11 U11 = A11 (one CTA, the 64 x 64 diagonal block, in registers),
 //                       the check inside the block, and L11^-1, U11^-1;
 //   panel_apply_kernel  L21 = A21 U11^-1 (with the check on every multiplier) and
 //                       U12 = L11^-1 A12, both as FP64 tensor-core tiles (dmma.cuh), the
@@ -382,19 +382,21 @@ __global__ void __launch_bounds__(kTrsmCols, 1) trsm_kernel(uint32_t n, uint32_t
 //                       run of them with the next tile's operands loading during the MMAs.
 // Every product has K = 64, the panel width; the multipliers and U12 are the blocked forms of
 // getf2's and trsm's, equal to them up to rounding.
-constexpr int kTopThreads = 256;
-constexpr int kTopStride = NB + 1;
-constexpr size_t kTopSmem = 3 * (size_t)NB * kTopStride * sizeof(double) + NB * sizeof(double);
+constexpr int kTopThreads = 256;  // 64 rows x 4 groups of 16 columns
+constexpr int kTopGs = 18;        // doubles per column group of a broadcast row: 144 B, so the four
+                                  // groups' 16-byte loads fall in distinct banks
 
-// One CTA: the 64 x 64 diagonal block in shared memory (a partial block padded with identity),
-// factored without interchanges, together with L11^-1, then U11^-1.  Thread (r, g) owns row r
-// and columns 16 g .. 16 g + 15 (the four threads of a row are neighbouring lanes of one warp),
-// so a column step needs one barrier: row r's multiplier is read by its four threads, the
-// owner of column j writes it back after a warp-level sync, each thread updates its columns of
-// row r, and the thread that finishes the next pivot publishes its reciprocal.  X = L^-1 is
-// formed in the same steps (row j of X is final once step j begins); Y = U^-1 (unscaled rows,
-// 1 / U[q][q] applied at the end) takes 64 more steps from the last row up.  Loops, not
-// unrolled code: the kernel runs once per panel on one SM.
+// One CTA: the 64 x 64 diagonal block (a partial block padded with identity) factored without
+// interchanges, with X = L11^-1 and Y = U11^-1 formed in the same 64 column steps.  Thread
+// (r, g) holds row r, columns 16 g .. 16 g + 15, of T, X and Y in registers (the four threads
+// of a row are neighbouring lanes); the column loop is unrolled by 16, so every register index
+// is a constant.  Step j: row j is final and sits in shared memory (published by its threads at
+// the end of step j - 1, double-buffered by parity, one barrier per step).  A row r > j takes
+// its multiplier l = T[r][j] / U[j][j] (getf2 scales by the reciprocal) from the thread that
+// holds column j, checks it, and applies T[r][c] -= l U[j][c] (c > j) and X[r] -= l X[j].  A row
+// r <= j finishes Y[r][j] = (delta_rj - sum_{k<j} Y[r][k] U[k][j]) / U[j][j] (the sum has been
+// accumulated in y by the earlier steps) and applies Y[r][c] -= Y[r][j] U[j][c] (c > j), the
+// same broadcast row.  The threads of row j + 1 then publish it with its pivot's reciprocal.
 __global__ void __launch_bounds__(kTopThreads) top_factor_kernel(uint32_t k0, uint32_t nb,
                                                                  const double* __restrict__ A, uint32_t lda,
                                                                  double* __restrict__ top_out,
@@ -402,63 +404,106 @@ __global__ void __launch_bounds__(kTopThreads) top_factor_kernel(uint32_t k0, ui
                                                                  double* __restrict__ uinv,
                                                                  int32_t* __restrict__ reject)
 {
-    extern __shared__ double top_smem[];
-    double(*T)[kTopStride] = reinterpret_cast<double(*)[kTopStride]>(top_smem);
-    double(*X)[kTopStride] = T + NB;
-    double(*Y)[kTopStride] = T + 2 * NB;
-    double* rd = top_smem + 3 * NB * kTopStride;  // 1 / U[q][q]
-    const uint32_t tid = threadIdx.x;
-    for (uint32_t e = tid; e < NB * NB; e += kTopThreads) {
-        const uint32_t r = e / NB, c = e % NB;
-        T[r][c] = (r < nb && c < nb) ? A[(size_t)(k0 + r) * lda + k0 + c] : (r == c ? 1.0 : 0.0);
-        X[r][c] = Y[r][c] = r == c ? 1.0 : 0.0;
+    __shared__ __align__(16) double prow[2][4][kTopGs];  // row j of T
+    __shared__ __align__(16) double xrow[2][4][kTopGs];  // row j of X
+    __shared__ double rd[NB];                            // 1 / U[q][q]
+    const uint32_t tid = threadIdx.x, row = tid >> 2, g = tid & 3u;
+    const int src = (int)(tid & 28u);  // lane of this row's group 0
+    double t[16], x[16], y[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        const uint32_t c = 16 * g + k;
+        t[k] = (row < nb && c < nb) ? A[(size_t)(k0 + row) * lda + k0 + c] : (row == c ? 1.0 : 0.0);
+        x[k] = y[k] = row == c ? 1.0 : 0.0;
+    }
+    bool bad = false;
+    if (row == 0) {
+#pragma unroll
+        for (int k = 0; k < 16; k += 2) {
+            *reinterpret_cast<double2*>(&prow[0][g][k]) = make_double2(t[k], t[k + 1]);
+            *reinterpret_cast<double2*>(&xrow[0][g][k]) = make_double2(x[k], x[k + 1]);
+        }
+        if (g == 0) {
+            bad |= !(fabs(t[0]) > 0.0);  // zero or NaN pivot
+            rd[0] = 1.0 / t[0];
+        }
     }
     __syncthreads();
-    const uint32_t row = tid >> 2, g = tid & 3u, c0 = 16 * g, c1 = c0 + 16;
-    if (tid == 0)
-        rd[0] = 1.0 / T[0][0];
-    bool bad = false;
-    __syncthreads();
 #pragma unroll 1
-    for (uint32_t j = 0; j < NB; ++j) {
-        if (row == j && g == j / 16)
-            bad |= !(fabs(T[j][j]) > 0.0);  // zero or NaN pivot
-        if (row > j) {
-            const double l = T[row][j] * rd[j];  // getf2 scales by the reciprocal of the pivot
-            __syncwarp();
-            if (j >= c0 && j < c1) {
-                bad |= !(fabs(l) < pvl::dmma::kMultLimit);
-                T[row][j] = l;
+    for (uint32_t gj = 0; gj < 4; ++gj) {
+#pragma unroll
+        for (int kj = 0; kj < 16; ++kj) {
+            const uint32_t j = 16 * gj + kj;
+            const int b = kj & 1;
+            const bool below = row > j;
+            const double a = __shfl_sync(0xffffffffu, below ? t[kj] : y[kj], src + (int)gj) * rd[j];
+            if (g == gj) {
+                if (below) {
+                    bad |= !(fabs(a) < pvl::dmma::kMultLimit);
+                    t[kj] = a;
+                } else {
+                    y[kj] = a;
+                }
             }
-            for (uint32_t c = max(c0, j + 1); c < c1; ++c)
-                T[row][c] = fma(-l, T[j][c], T[row][c]);
-            for (uint32_t c = c0; c < c1 && c <= j; ++c)  // X = L^-1, column step j
-                X[row][c] = fma(-l, X[j][c], X[row][c]);
-            if (row == j + 1 && j + 1 >= c0 && j + 1 < c1)
-                rd[j + 1] = 1.0 / T[j + 1][j + 1];  // the next pivot is final now
-        } else {
-            __syncwarp();
+            if (g >= gj) {  // columns right of j: k > kj in group gj, every k in later groups
+                const bool later = g > gj;
+                if (below) {
+#pragma unroll
+                    for (int k = 0; k < 16; k += 2) {
+                        const double2 p = *reinterpret_cast<const double2*>(&prow[b][g][k]);
+                        if (k > kj || later)
+                            t[k] = fma(-a, p.x, t[k]);
+                        if (k + 1 > kj || later)
+                            t[k + 1] = fma(-a, p.y, t[k + 1]);
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 16; k += 2) {
+                        const double2 p = *reinterpret_cast<const double2*>(&prow[b][g][k]);
+                        if (k > kj || later)
+                            y[k] = fma(-a, p.x, y[k]);
+                        if (k + 1 > kj || later)
+                            y[k + 1] = fma(-a, p.y, y[k + 1]);
+                    }
+                }
+            }
+            if (below && g <= gj) {  // X[j][c] = 0 for c > j
+#pragma unroll
+                for (int k = 0; k < 16; k += 2) {
+                    const double2 p = *reinterpret_cast<const double2*>(&xrow[b][g][k]);
+                    x[k] = fma(-a, p.x, x[k]);
+                    x[k + 1] = fma(-a, p.y, x[k + 1]);
+                }
+            }
+            if (row == j + 1) {  // row j + 1 is final: publish it (never true after the last step)
+                const int kn = (kj + 1) & 15;
+                const uint32_t gn = gj + (kj == 15 ? 1u : 0u);
+#pragma unroll
+                for (int k = 0; k < 16; k += 2) {
+                    *reinterpret_cast<double2*>(&prow[b ^ 1][g][k]) = make_double2(t[k], t[k + 1]);
+                    *reinterpret_cast<double2*>(&xrow[b ^ 1][g][k]) = make_double2(x[k], x[k + 1]);
+                }
+                if (g == gn) {
+                    bad |= !(fabs(t[kn]) > 0.0);
+                    rd[j + 1] = 1.0 / t[kn];
+                }
+            }
+            __syncthreads();
         }
-        __syncthreads();
     }
     if (__syncthreads_or(bad) && tid == 0)
         atomicExch(reject, 1);
-#pragma unroll 1
-    for (uint32_t t = 0; t < NB; ++t) {  // Y: step q eliminates column q above U[q][q]
-        const uint32_t q = NB - 1 - t;
-        if (row < q) {
-            const double u = T[row][q] * rd[q];
-            for (uint32_t c = max(c0, q); c < c1; ++c)
-                Y[row][c] = fma(-u, Y[q][c], Y[row][c]);
-        }
-        __syncthreads();
+    const size_t o = (size_t)row * NB + 16 * g;
+#pragma unroll
+    for (int k = 0; k < 16; k += 2) {
+        *reinterpret_cast<double2*>(linv + o + k) = make_double2(x[k], x[k + 1]);
+        *reinterpret_cast<double2*>(uinv + o + k) = make_double2(y[k], y[k + 1]);
     }
-    for (uint32_t e = tid; e < NB * NB; e += kTopThreads) {
-        const uint32_t r = e / NB, c = e % NB;
-        if (r < nb && c < nb)
-            top_out[(size_t)r * NB + c] = T[r][c];
-        linv[(size_t)r * NB + c] = X[r][c];
-        uinv[(size_t)r * NB + c] = Y[r][c] * rd[r];
+    if (row < nb) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+            if (16 * g + k < nb)
+                top_out[o + k] = t[k];
     }
 }
 
@@ -499,7 +544,7 @@ __global__ void __launch_bounds__(pvl::dmma::kThreads) panel_apply_kernel(uint32
 // run of them in column-major order (dmma.cuh update_tiles: the next tile's operands load
 // while this one multiplies), two CTAs per SM.
 template <bool VEC>
-__global__ void __launch_bounds__(pvl::dmma::kThreads, 2) dmma_update_kernel(uint32_t n, uint32_t k0,
+__global__ void __launch_bounds__(pvl::dmma::kUpdThreads, 2) dmma_update_kernel(uint32_t n, uint32_t k0,
                                                                              double* __restrict__ A, uint32_t lda,
                                                                              uint32_t per_cta)
 {
@@ -653,7 +698,6 @@ extern "C" int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv,
     const void* upd_fn = vec ? (const void*)dmma_update_kernel<true> : (const void*)dmma_update_kernel<false>;
     PVL_SMEM_OPTIN(trsm_kernel<double>, trsm_smem);
     PVL_SMEM_OPTIN(apply_fn, kApplySmem);
-    PVL_SMEM_OPTIN(top_factor_kernel, kTopSmem);
     PVL_SMEM_OPTIN(upd_fn, upd_smem);
     int32_t* perm = ipiv + n;
     PVL_CUDA_CHECK(cudaMemsetAsync(info, 0, sizeof(int32_t), st));
@@ -665,7 +709,7 @@ extern "C" int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv,
         const uint32_t k0 = p * NB;
         const uint32_t nb = std::min<uint32_t>(NB, n - k0);
         const uint32_t below = n - k0 - nb;  // nonzero only for full panels (nb == NB)
-        top_factor_kernel<<<1, kTopThreads, kTopSmem, st>>>(k0, nb, A, lda, w.top_out, w.linv, w.uinv, w.reject + p);
+        top_factor_kernel<<<1, kTopThreads, 0, st>>>(k0, nb, A, lda, w.top_out, w.linv, w.uinv, w.reject + p);
         PVL_LAUNCH_CHECK();
         if (below > 0) {
             const uint32_t nl = blocks_for(below, kApplyRows), nu = blocks_for(below, kApplyCols);
@@ -694,7 +738,7 @@ extern "C" int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv,
             uint32_t per = blocks_for(tiles, slots);
             const uint32_t grid = blocks_for(tiles, per);
             void* args[] = {(void*)&n, (void*)&kk, (void*)&A, (void*)&lda, (void*)&per};
-            PVL_CUDA_CHECK(cudaLaunchKernel(upd_fn, dim3(grid), dim3(pvl::dmma::kThreads), args, upd_smem, st));
+            PVL_CUDA_CHECK(cudaLaunchKernel(upd_fn, dim3(grid), dim3(pvl::dmma::kUpdThreads), args, upd_smem, st));
             pvl_count_launch();
         }
     }
