@@ -63,13 +63,14 @@ __device__ __forceinline__ void cp_async_wait_all()
 
 // rows x 64 block at (row0, col0) of a row-major matrix into sm[rows][kPad]; rows past
 // row_end read as zero.
+// NTHR threads copy, tid = 0 .. NTHR - 1 the caller's index among them.
 template <int ROWS, bool VEC, int NTHR = kThreads>
 __device__ __forceinline__ void stage_rows(double* sm, const double* __restrict__ g, uint32_t ld, uint32_t row0,
-                                           uint32_t row_end, uint32_t col0)
+                                           uint32_t row_end, uint32_t col0, uint32_t tid = threadIdx.x)
 {
     constexpr int PER = VEC ? 2 : 1;           // doubles per copy
     constexpr int CHUNKS = K / PER;            // copies per row
-    for (uint32_t e = threadIdx.x; e < (uint32_t)(ROWS * CHUNKS); e += NTHR) {
+    for (uint32_t e = tid; e < (uint32_t)(ROWS * CHUNKS); e += NTHR) {
         const uint32_t r = e / CHUNKS, c = (e % CHUNKS) * PER;
         const bool ok = row0 + r < row_end;
         const double* src = ok ? g + (size_t)(row0 + r) * ld + col0 + c : g;
@@ -80,11 +81,11 @@ __device__ __forceinline__ void stage_rows(double* sm, const double* __restrict_
 // 64 x COLS block at (row0, col0) into sm[64][kPad] (columns past col_end read as zero).
 template <int COLS, bool VEC, int NTHR = kThreads>
 __device__ __forceinline__ void stage_cols(double* sm, const double* __restrict__ g, uint32_t ld, uint32_t row0,
-                                           uint32_t col0, uint32_t col_end)
+                                           uint32_t col0, uint32_t col_end, uint32_t tid = threadIdx.x)
 {
     constexpr int PER = VEC ? 2 : 1;
     constexpr int CHUNKS = COLS / PER;
-    for (uint32_t e = threadIdx.x; e < (uint32_t)(K * CHUNKS); e += NTHR) {
+    for (uint32_t e = tid; e < (uint32_t)(K * CHUNKS); e += NTHR) {
         const uint32_t r = e / CHUNKS, c = (e % CHUNKS) * PER;
         const bool ok = col0 + c < col_end;  // col_end and c are even when VEC
         const double* src = ok ? g + (size_t)(row0 + r) * ld + col0 + c : g;
@@ -222,37 +223,45 @@ __device__ __forceinline__ void tile(Smem<BM, BN>& s, const double* A, uint32_t 
 }
 
 // ---------------------------------------------------------------- pipelined trailing update
-// C -= A B over a run of 64 x 64 tiles of one M x N block (A: M x 64 rows, B: 64 x N), tiles in
-// column-major order so that consecutive tiles of a CTA share their B block.  While tile t is
-// multiplied, tile t + 1's A block is already being copied into the other A buffer
-// (cp.async) and its C block is already being loaded into registers, so the loads of the next
-// tile overlap the MMAs of this one.  kUpdWarps warps: 4 (warp tile 32 x 32) or 8 (32 x 16);
-// two CTAs per SM either way.
+// C -= A B over a run of 64 x 64 tiles of one M x N block C (rows row0.., columns col0..),
+// A: the 64 columns a_col.. of C's rows, B: the 64 rows b_row.. of C's columns.  Tiles in
+// column-major order, so that consecutive tiles of a run share their B block.  While tile t is
+// multiplied, tile t + 1's A block is already being copied into the other A buffer (cp.async)
+// and its C block is already being loaded into registers, so the loads of the next tile
+// overlap the MMAs of this one.  One tile group = kUpdWarps warps (8: warp tile 32 x 16; 4:
+// 32 x 32) with its own shared memory and named barrier; a CTA of the update kernel holds two
+// groups, each running its own tiles, and fills one SM.
 #ifndef PVL_UPD_WARPS
 #define PVL_UPD_WARPS 8
 #endif
 constexpr int kUpdTile = 64;
 constexpr int kUpdWarps = PVL_UPD_WARPS;
-constexpr int kUpdThreads = 32 * kUpdWarps;
+constexpr int kUpdThreads = 32 * kUpdWarps;  // one tile group
 static_assert(kUpdWarps == 4 || kUpdWarps == 8, "2 x 2 or 2 x 4 warps over a 64 x 64 tile");
 struct UpdSmem {
     double a[2][kUpdTile * kPad];
     double b[K * kPad];
 };
 
+// Barrier `id` (1, 2, ...; 0 is __syncthreads) over the kUpdThreads threads of one tile group.
+__device__ __forceinline__ void group_sync(uint32_t id)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(kUpdThreads) : "memory");
+}
+
 template <bool VEC>
 __device__ __forceinline__ void update_tiles(UpdSmem& s, double* __restrict__ Cm, uint32_t ld, uint32_t row0,
-                                             uint32_t col0, uint32_t m, uint32_t nn, uint32_t t_begin, uint32_t t_end)
+                                             uint32_t col0, uint32_t m, uint32_t nn, uint32_t a_col, uint32_t b_row,
+                                             uint32_t t_begin, uint32_t t_end, uint32_t gtid, uint32_t bar)
 {
     constexpr int WN = kUpdWarps / 2;     // warps along N
     constexpr int MT = 2, NT = 8 / WN;    // warp tile 32 x (64 / WN)
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lane = gtid & 31, warp = gtid >> 5;
     const uint32_t g = lane >> 2, t4 = lane & 3;
     const uint32_t wm0 = (warp / WN) * 32, wn0 = (warp % WN) * (8 * NT);
     const uint32_t tiles_i = (m + kUpdTile - 1) / kUpdTile;
-    // A block: rows row0 + i * 64 .., columns col0 - 64 .. (the panel); B block: rows row0 - 64 ..
-    // (the panel's row block), columns col0 + j * 64 ..; C block: rows row0 + i * 64, columns col0 + j * 64
-    const uint32_t a_col = col0 - K, b_row = row0 - K;
+    // A block: rows row0 + i * 64 .., columns a_col ..; B block: rows b_row .., columns
+    // col0 + j * 64 ..; C block: rows row0 + i * 64 .., columns col0 + j * 64 ..
     auto coords = [&](uint32_t t, uint32_t& i0, uint32_t& j0, uint32_t& me, uint32_t& ne) {
         i0 = (t % tiles_i) * kUpdTile;
         j0 = (t / tiles_i) * kUpdTile;
@@ -290,12 +299,12 @@ __device__ __forceinline__ void update_tiles(UpdSmem& s, double* __restrict__ Cm
     auto stage_a = [&](uint32_t t, int buf) {
         uint32_t i0, j0, me, ne;
         coords(t, i0, j0, me, ne);
-        stage_rows<kUpdTile, VEC, kUpdThreads>(s.a[buf], Cm, ld, row0 + i0, row0 + i0 + me, a_col);
+        stage_rows<kUpdTile, VEC, kUpdThreads>(s.a[buf], Cm, ld, row0 + i0, row0 + i0 + me, a_col, gtid);
     };
     auto stage_b = [&](uint32_t t) {
         uint32_t i0, j0, me, ne;
         coords(t, i0, j0, me, ne);
-        stage_cols<kUpdTile, VEC, kUpdThreads>(s.b, Cm, ld, b_row, col0 + j0, col0 + j0 + ne);
+        stage_cols<kUpdTile, VEC, kUpdThreads>(s.b, Cm, ld, b_row, col0 + j0, col0 + j0 + ne, gtid);
     };
     auto commit = [] { asm volatile("cp.async.commit_group;" ::: "memory"); };
     double cnext[MT][NT][4];
@@ -327,7 +336,7 @@ __device__ __forceinline__ void update_tiles(UpdSmem& s, double* __restrict__ Cm
             asm volatile("cp.async.wait_group 1;" ::: "memory");
         else
             asm volatile("cp.async.wait_group 0;" ::: "memory");
-        __syncthreads();
+        group_sync(bar);
 #pragma unroll
         for (int k0 = 0; k0 < K; k0 += 8) {
             double af[MT][4], bf[NT][2];
@@ -375,7 +384,7 @@ __device__ __forceinline__ void update_tiles(UpdSmem& s, double* __restrict__ Cm
                     }
                 }
             }
-        __syncthreads();  // both buffers and B are free for what follows
+        group_sync(bar);  // both buffers and B are free for what follows
         if (more && !same_b) {  // a new column of tiles: its B block and the next A block
             stage_a(t + 1, cur ^ 1);
             stage_b(t + 1);

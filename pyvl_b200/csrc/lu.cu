@@ -540,21 +540,72 @@ __global__ void __launch_bounds__(pvl::dmma::kThreads) panel_apply_kernel(uint32
     }
 }
 
-// A22 -= L21 U12: the (below x below) trailing block as 64 x 64 tiles, each CTA a contiguous
-// run of them in column-major order (dmma.cuh update_tiles: the next tile's operands load
-// while this one multiplies), two CTAs per SM.
+// One rectangle of the trailing update A22 -= L21 U12: C = rows row0 .. row0 + m, columns
+// col0 .. col0 + nn; A = the panel's L21 (columns a_col ..) on C's rows, B = its U12 (rows
+// b_row ..) on C's columns.  `slots` runs of `per` 64 x 64 tiles.
+struct UpdRect {
+    uint32_t row0, col0, m, nn, a_col, b_row, per, slots;
+};
+
+UpdRect upd_rect(uint32_t row0, uint32_t col0, uint32_t m, uint32_t nn, uint32_t k0, uint32_t max_slots)
+{
+    const uint32_t tiles = blocks_for(m, pvl::dmma::kUpdTile) * blocks_for(nn, pvl::dmma::kUpdTile);
+    UpdRect r{row0, col0, m, nn, k0, k0, 0, 0};
+    r.per = tiles ? blocks_for(tiles, std::max(1u, max_slots)) : 1;
+    r.slots = blocks_for(tiles, r.per);
+    return r;
+}
+
+// Two tile groups per CTA, each with its own shared memory and barrier (dmma.cuh update_tiles:
+// the next tile's operands load while this one multiplies); a CTA fills one SM.  Group slot
+// s = 2 blockIdx.x + group runs tiles [s per, (s + 1) per) of r0, the slots after r0's those
+// of r1 (each rectangle's tiles in column-major order).
 template <bool VEC>
-__global__ void __launch_bounds__(pvl::dmma::kUpdThreads, 2) dmma_update_kernel(uint32_t n, uint32_t k0,
-                                                                             double* __restrict__ A, uint32_t lda,
-                                                                             uint32_t per_cta)
+__global__ void __launch_bounds__(2 * pvl::dmma::kUpdThreads, 1) dmma_update_kernel(double* __restrict__ A,
+                                                                                 uint32_t lda, UpdRect r0,
+                                                                                 UpdRect r1)
 {
     extern __shared__ __align__(16) double upd_smem[];
-    auto& sm = *reinterpret_cast<pvl::dmma::UpdSmem*>(upd_smem);
-    const uint32_t base = k0 + NB, m = n - base;
-    const uint32_t tiles = ((m + pvl::dmma::kUpdTile - 1) / pvl::dmma::kUpdTile) *
-                           ((m + pvl::dmma::kUpdTile - 1) / pvl::dmma::kUpdTile);
-    const uint32_t t0 = blockIdx.x * per_cta, t1 = min(tiles, t0 + per_cta);
-    pvl::dmma::update_tiles<VEC>(sm, A, lda, base, base, m, m, t0, t1);
+    const uint32_t grp = threadIdx.x / pvl::dmma::kUpdThreads, gtid = threadIdx.x % pvl::dmma::kUpdThreads;
+    auto& sm = reinterpret_cast<pvl::dmma::UpdSmem*>(upd_smem)[grp];
+    uint32_t slot = 2 * blockIdx.x + grp;
+    const bool first = slot < r0.slots;
+    const UpdRect r = first ? r0 : r1;
+    if (!first)
+        slot -= r0.slots;
+    if (slot >= r.slots)
+        return;  // the whole group: its barrier counts only its own threads
+    constexpr uint32_t T = pvl::dmma::kUpdTile;
+    const uint32_t tiles = ((r.m + T - 1) / T) * ((r.nn + T - 1) / T);
+    const uint32_t t0 = slot * r.per, t1 = min(tiles, t0 + r.per);
+    pvl::dmma::update_tiles<VEC>(sm, A, lda, r.row0, r.col0, r.m, r.nn, r.a_col, r.b_row, t0, t1, gtid, 1 + grp);
+}
+
+// SMs left free while the bulk of a panel's trailing update runs on the side stream: the next
+// panel's top block, apply and pivot kernels run there meanwhile.
+constexpr int kLookaheadSms = 8;
+
+// A second stream and two events per thread and device for the look-ahead fork and join (a
+// stream may take part in one capture at a time: per thread, since captures here are
+// thread-local).  Created once, never destroyed.
+struct SideStream {
+    cudaStream_t s = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+
+int side_stream(int dev, SideStream*& out)
+{
+    thread_local SideStream cache[64];
+    if (dev < 0 || dev >= 64)
+        return pvl_fail(PVL_ERR_ARG, "pvl_lu_factor: device %d out of range", dev);
+    SideStream& c = cache[dev];
+    if (!c.s) {
+        PVL_CUDA_CHECK(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
+        PVL_CUDA_CHECK(cudaEventCreateWithFlags(&c.fork, cudaEventDisableTiming));
+        PVL_CUDA_CHECK(cudaEventCreateWithFlags(&c.join, cudaEventDisableTiming));
+    }
+    out = &c;
+    return PVL_OK;
 }
 
 // ---------------------------------------------------------------- diagonal-block inverses
@@ -688,10 +739,13 @@ extern "C" int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv,
     cudaStream_t st = (cudaStream_t)stream;
     LuWs w = carve(ws, n);
     const size_t trsm_smem = (size_t)(NB * (NB + 1) + NB * (kTrsmCols + 1)) * sizeof(double);
-    const size_t upd_smem = sizeof(pvl::dmma::UpdSmem);
+    const size_t upd_smem = 2 * sizeof(pvl::dmma::UpdSmem);
     int dev = 0, sms = 0;
     PVL_CUDA_CHECK(cudaGetDevice(&dev));
     PVL_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    SideStream* side = nullptr;
+    if (int rc = side_stream(dev, side))
+        return rc;
     // 16-byte operand copies and stores need even row strides and an even width
     const bool vec = (lda % 2 == 0) && (n % 2 == 0) && (((uintptr_t)A & 15u) == 0);
     const void* apply_fn = vec ? (const void*)panel_apply_kernel<true> : (const void*)panel_apply_kernel<false>;
@@ -699,12 +753,31 @@ extern "C" int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv,
     PVL_SMEM_OPTIN(trsm_kernel<double>, trsm_smem);
     PVL_SMEM_OPTIN(apply_fn, kApplySmem);
     PVL_SMEM_OPTIN(upd_fn, upd_smem);
+    auto update = [&](cudaStream_t s, const UpdRect& r0, const UpdRect& r1) -> int {
+        const uint32_t ctas = blocks_for(r0.slots + r1.slots, 2);
+        if (ctas == 0)
+            return PVL_OK;
+        void* args[] = {(void*)&A, (void*)&lda, (void*)&r0, (void*)&r1};
+        PVL_CUDA_CHECK(cudaLaunchKernel(upd_fn, dim3(ctas), dim3(2 * pvl::dmma::kUpdThreads), args, upd_smem, s));
+        pvl_count_launch();
+        return PVL_OK;
+    };
+    const UpdRect none{0, 0, 0, 0, 0, 0, 1, 0};
+    const uint32_t all_slots = 2u * (uint32_t)sms;
+    const uint32_t bulk_slots = 2u * (uint32_t)std::max(1, sms - kLookaheadSms);
     int32_t* perm = ipiv + n;
     PVL_CUDA_CHECK(cudaMemsetAsync(info, 0, sizeof(int32_t), st));
     init_perm_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, perm);
     PVL_LAUNCH_CHECK();
     const uint32_t n_panels = (n + NB - 1) / NB;
     PVL_CUDA_CHECK(cudaMemsetAsync(w.reject, 0, sizeof(int32_t) * (n_panels + 1), st));
+    // Look-ahead: panel p's trailing update is split into the next panel's column and row
+    // blocks (the L shape next to this panel, on `st`) and the rest (on the side stream, on all
+    // but kLookaheadSms SMs).  Panel p + 1's top block, apply and pivot kernels touch only its
+    // own columns and row block, so they run on `st` while the rest of panel p's update is in
+    // flight; its trsm kernel (whose fallback interchanges reach every column) and everything
+    // after wait for it.
+    bool pending = false;
     for (uint32_t p = 0; p < n_panels; ++p) {
         const uint32_t k0 = p * NB;
         const uint32_t nb = std::min<uint32_t>(NB, n - k0);
@@ -726,21 +799,38 @@ extern "C" int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv,
         panel_pivot_kernel<double><<<1, 1024, 0, st>>>(n, k0, nb, A, lda, w.backup, w.top_out, w.reject, w.ok, p, ipiv,
                                                        perm, info, below > 0 ? w.backup_row : nullptr);
         PVL_LAUNCH_CHECK();
+        if (pending) {  // the rest of the previous panel's update
+            PVL_CUDA_CHECK(cudaEventRecord(side->join, side->s));
+            PVL_CUDA_CHECK(cudaStreamWaitEvent(st, side->join, 0));
+            pending = false;
+        }
         if (n > nb) {
             trsm_kernel<double><<<blocks_for(n - nb, kTrsmCols), kTrsmCols, trsm_smem, st>>>(n, k0, nb, A, lda, w.ok, p,
                                                                                            ipiv, 1);
             PVL_LAUNCH_CHECK();
         }
-        if (below > 0) {
-            uint32_t kk = k0;
-            const uint32_t tpd = blocks_for(below, pvl::dmma::kUpdTile), tiles = tpd * tpd;
-            const uint32_t slots = 2u * (uint32_t)sms;  // two CTAs per SM
-            uint32_t per = blocks_for(tiles, slots);
-            const uint32_t grid = blocks_for(tiles, per);
-            void* args[] = {(void*)&n, (void*)&kk, (void*)&A, (void*)&lda, (void*)&per};
-            PVL_CUDA_CHECK(cudaLaunchKernel(upd_fn, dim3(grid), dim3(pvl::dmma::kUpdThreads), args, upd_smem, st));
-            pvl_count_launch();
+        if (below == 0)
+            continue;
+        const uint32_t base = k0 + NB;
+        if (below <= (uint32_t)pvl::dmma::kUpdTile) {  // one tile column: no look-ahead split
+            if (int rc = update(st, upd_rect(base, base, below, below, k0, all_slots), none))
+                return rc;
+            continue;
         }
+        const uint32_t step = pvl::dmma::kUpdTile;
+        if (int rc = update(st, upd_rect(base, base, below, step, k0, all_slots),
+                            upd_rect(base, base + step, step, below - step, k0, all_slots)))
+            return rc;
+        PVL_CUDA_CHECK(cudaEventRecord(side->fork, st));
+        PVL_CUDA_CHECK(cudaStreamWaitEvent(side->s, side->fork, 0));
+        if (int rc = update(side->s, upd_rect(base + step, base + step, below - step, below - step, k0, bulk_slots),
+                            none))
+            return rc;
+        pending = true;
+    }
+    if (pending) {
+        PVL_CUDA_CHECK(cudaEventRecord(side->join, side->s));
+        PVL_CUDA_CHECK(cudaStreamWaitEvent(st, side->join, 0));
     }
     diag_inverse_kernel<double><<<(n + kRB - 1) / kRB, 2 * kRB, 0, st>>>(n, A, lda, w.inv);
     PVL_LAUNCH_CHECK();
