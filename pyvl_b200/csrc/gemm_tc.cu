@@ -15,10 +15,11 @@
 //   warp 1       allocates 256 TMEM columns (two 128 x 128 FP32 accumulators) and issues the
 //                MMAs (four K = 8 steps per slice) from one thread, each slice's commit freeing
 //                its stage, each tile's commit handing its accumulator to the epilogue;
-//   warps 2..5   epilogue: the accumulator's rows through tcgen05.ld into a shared staging
-//                tile (the TMEM buffer is released at once, so the next tile's MMAs run
-//                during the rest of the epilogue), then C read and written in 512-byte
-//                coalesced rows.
+//   warps 2..5   epilogue: each thread first requests its 32 four-float pieces of the tile's
+//                C (kept in registers: one memory round trip per tile), then moves the
+//                accumulator's rows through tcgen05.ld into a shared staging tile (the TMEM
+//                buffer is released at once, so the next tile's MMAs run during the rest of
+//                the epilogue) and writes C in 512-byte coalesced rows.
 // Every wait is bounded.  A wait that runs out sets *err and stops the CTA's roles; before
 // the CTA frees its tensor memory it waits (bounded) for its own copies and MMAs in flight.
 // A TMA load never reads another GPU's memory here and none uses cluster multicast.
@@ -195,6 +196,20 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tf32_kernel(const __grid_con
         uint32_t ti = 0;
         for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x, ++ti) {
             const uint32_t a = ti & 1u;
+            const uint32_t m0 = (t / tiles_n) * kTile, n0 = (t % tiles_n) * kTile;
+            const uint32_t col = n0 + 4 * lane;
+            // this thread's 32 four-float pieces of C (rows ew, ew + 4, ...), all requested
+            // before the accumulator is awaited, so that one memory round trip per tile (not
+            // one per row) overlaps the tile's MMAs
+            float4 cin[kTile / 4];
+            const bool full_cols = col + 4 <= N;
+#pragma unroll
+            for (int i = 0; i < kTile / 4; ++i) {
+                const uint32_t grow = m0 + ew + 4u * i;
+                cin[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (beta != 0.0f && full_cols && grow < M)
+                    cin[i] = *reinterpret_cast<const float4*>(C + (size_t)grow * ldc + col);
+            }
             const bool ok = umma::mbar_wait(umma::smem_u32(&s.acc_full[a]), (ti >> 1) & 1u, wait_limit);
             if (!ok)
                 set_fail(s, err);
@@ -217,17 +232,15 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tf32_kernel(const __grid_con
             epi_sync();
             if (ew == 0 && lane == 0)
                 mbar_arrive(umma::smem_u32(&s.acc_empty[a]));  // the accumulator may take the next tile
-            const uint32_t m0 = (t / tiles_n) * kTile, n0 = (t % tiles_n) * kTile;
-            const uint32_t col = n0 + 4 * lane;
-#pragma unroll 1
-            for (uint32_t r = ew; r < (uint32_t)kTile; r += 4) {
-                const uint32_t grow = m0 + r;
+#pragma unroll
+            for (int i = 0; i < kTile / 4; ++i) {
+                const uint32_t r = ew + 4u * i, grow = m0 + r;
                 if (grow >= M || col >= N)
                     continue;
                 const float4 v = *reinterpret_cast<const float4*>(s.out + r * kTile + ((lane ^ (r & 7u)) << 2));
                 float* crow = C + (size_t)grow * ldc + col;
-                if (col + 4 <= N) {
-                    float4 o = beta == 0.0f ? make_float4(0.f, 0.f, 0.f, 0.f) : *reinterpret_cast<const float4*>(crow);
+                if (full_cols) {
+                    float4 o = cin[i];
                     o.x = alpha * v.x + beta * o.x;
                     o.y = alpha * v.y + beta * o.y;
                     o.z = alpha * v.z + beta * o.z;
@@ -235,8 +248,8 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tf32_kernel(const __grid_con
                     *reinterpret_cast<float4*>(crow) = o;
                 } else {
                     const float av[4] = {v.x, v.y, v.z, v.w};
-                    for (uint32_t i = 0; i < 4 && col + i < N; ++i)
-                        crow[i] = alpha * av[i] + (beta == 0.0f ? 0.0f : beta * crow[i]);
+                    for (uint32_t e = 0; e < 4 && col + e < N; ++e)
+                        crow[e] = alpha * av[e] + (beta == 0.0f ? 0.0f : beta * crow[e]);
                 }
             }
             epi_sync();  // the staging tile is free for the next tile

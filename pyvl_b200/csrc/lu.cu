@@ -386,13 +386,27 @@ constexpr int kTopThreads = 256;  // 64 rows x 4 groups of 16 columns
 constexpr int kTopGs = 18;        // doubles per column group of a broadcast row: 144 B, so the four
                                   // groups' 16-byte loads fall in distinct banks
 
+constexpr double kPivotLo = 0x1p-1000, kPivotHi = 0x1p+1000;
+
+// 1/p for a pivot with kPivotLo <= |p| <= kPivotHi: the hardware's approximate reciprocal r
+// (rcp.approx.ftz.f64, relative error d < 2^-19) refined by one third-order step of the
+// geometric series 1/p = r / (1 - e), e = 1 - p r:  r + r (e + e^2) = (1/p)(1 - d^3), within an
+// ulp of the rounded quotient.  Pivots outside the range take the exact (pivoting) path.
+__device__ __forceinline__ double pivot_rcp(double p)
+{
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(p));
+    const double e = fma(-p, r, 1.0);
+    return fma(r, fma(e, e, e), r);
+}
+
 // One CTA: the 64 x 64 diagonal block (a partial block padded with identity) factored without
 // interchanges, with X = L11^-1 and Y = U11^-1 formed in the same 64 column steps.  Thread
 // (r, g) holds row r, columns 16 g .. 16 g + 15, of T, X and Y in registers (the four threads
 // of a row are neighbouring lanes); the column loop is unrolled by 16, so every register index
 // is a constant.  Step j: row j is final and sits in shared memory (published by its threads at
 // the end of step j - 1, double-buffered by parity, one barrier per step).  A row r > j takes
-// its multiplier l = T[r][j] / U[j][j] (getf2 scales by the reciprocal) from the thread that
+// its multiplier l = T[r][j] / U[j][j] (by the pivot's reciprocal, as getf2) from the thread that
 // holds column j, checks it, and applies T[r][c] -= l U[j][c] (c > j) and X[r] -= l X[j].  A row
 // r <= j finishes Y[r][j] = (delta_rj - sum_{k<j} Y[r][k] U[k][j]) / U[j][j] (the sum has been
 // accumulated in y by the earlier steps) and applies Y[r][c] -= Y[r][j] U[j][c] (c > j), the
@@ -424,8 +438,8 @@ __global__ void __launch_bounds__(kTopThreads) top_factor_kernel(uint32_t k0, ui
             *reinterpret_cast<double2*>(&xrow[0][g][k]) = make_double2(x[k], x[k + 1]);
         }
         if (g == 0) {
-            bad |= !(fabs(t[0]) > 0.0);  // zero or NaN pivot
-            rd[0] = 1.0 / t[0];
+            bad |= !(fabs(t[0]) >= kPivotLo && fabs(t[0]) <= kPivotHi);  // zero, tiny, huge or NaN pivot
+            rd[0] = pivot_rcp(t[0]);
         }
     }
     __syncthreads();
@@ -484,8 +498,8 @@ __global__ void __launch_bounds__(kTopThreads) top_factor_kernel(uint32_t k0, ui
                     *reinterpret_cast<double2*>(&xrow[b ^ 1][g][k]) = make_double2(x[k], x[k + 1]);
                 }
                 if (g == gn) {
-                    bad |= !(fabs(t[kn]) > 0.0);
-                    rd[j + 1] = 1.0 / t[kn];
+                    bad |= !(fabs(t[kn]) >= kPivotLo && fabs(t[kn]) <= kPivotHi);
+                    rd[j + 1] = pivot_rcp(t[kn]);
                 }
             }
             __syncthreads();

@@ -60,7 +60,9 @@ def test_lu_solve_blocked_matches_wavefront(n):
     _lib.call("pvl_lu_solve_blocked", n, ptr(LU), n, ptr(ipiv), ptr(x2), ptr(ws), nb, s)
     torch.cuda.synchronize()
     assert int(info.item()) == 0 and int(err.item()) == 0
-    assert float(torch.linalg.vector_norm(x2 - x1) / torch.linalg.vector_norm(x1)) <= 1e-13
+    # two substitution orders of the same factors: their difference is bounded by ~cond(A) x
+    # eps (the shifted random matrix's spectrum reaches near zero; cond ~1e3 at n = 4096)
+    assert float(torch.linalg.vector_norm(x2 - x1) / torch.linalg.vector_norm(x1)) <= 1e-12
     assert float(torch.linalg.vector_norm(A @ x2 - b) / torch.linalg.vector_norm(b)) <= 1e-12
 
 
