@@ -225,124 +225,112 @@ __device__ __forceinline__ void tile(Smem<BM, BN>& s, const double* A, uint32_t 
 // ---------------------------------------------------------------- pipelined trailing update
 // C -= A B over a run of 64 x 64 tiles of one M x N block C (rows row0.., columns col0..),
 // A: the 64 columns a_col.. of C's rows, B: the 64 rows b_row.. of C's columns.  Tiles in
-// column-major order, so that consecutive tiles of a run share their B block.  While tile t is
-// multiplied, tile t + 1's A block is already being copied into the other A buffer (cp.async)
-// and its C block is already being loaded into registers, so the loads of the next tile
-// overlap the MMAs of this one.  One tile group = kUpdWarps warps (8: warp tile 32 x 16; 4:
-// 32 x 32) with its own shared memory and named barrier; a CTA of the update kernel holds two
-// groups, each running its own tiles, and fills one SM.
+// column-major order, so that consecutive tiles of a run share their B block.  One CTA of
+// kUpdWarps warps (8: warp tile 32 x 16; 4: 32 x 32) per SM.  The C and A blocks of each tile
+// stream into a two-deep ring of shared memory by cp.async, issued one whole tile ahead: while
+// tile t is multiplied, tile t + 1's blocks are already there and tile t + 2's are in flight;
+// the accumulators start from -C (shared memory) and the result goes from registers to global
+// memory.  So every tile costs its MMAs, two barriers and a few shared loads, and the HBM
+// traffic (C in and out) runs underneath.
 #ifndef PVL_UPD_WARPS
 #define PVL_UPD_WARPS 8
 #endif
 constexpr int kUpdTile = 64;
 constexpr int kUpdWarps = PVL_UPD_WARPS;
-constexpr int kUpdThreads = 32 * kUpdWarps;  // one tile group
+constexpr int kUpdThreads = 32 * kUpdWarps;
 static_assert(kUpdWarps == 4 || kUpdWarps == 8, "2 x 2 or 2 x 4 warps over a 64 x 64 tile");
 struct UpdSmem {
     double a[2][kUpdTile * kPad];
+    double c[2][kUpdTile * kPad];
     double b[K * kPad];
 };
 
-// Barrier `id` (1, 2, ...; 0 is __syncthreads) over the kUpdThreads threads of one tile group.
-__device__ __forceinline__ void group_sync(uint32_t id)
+// ROWS x COLS block at (row0, col0) of a row-major matrix into sm[ROWS][kPad]; rows past
+// row_end and columns past col_end are not copied (their contents are never used).
+template <int ROWS, int COLS, bool VEC, int NTHR>
+__device__ __forceinline__ void stage_tile(double* sm, const double* __restrict__ g, uint32_t ld, uint32_t row0,
+                                           uint32_t row_end, uint32_t col0, uint32_t col_end, uint32_t tid)
 {
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(kUpdThreads) : "memory");
+    constexpr int PER = VEC ? 2 : 1;
+    constexpr int CHUNKS = COLS / PER;
+    for (uint32_t e = tid; e < (uint32_t)(ROWS * CHUNKS); e += NTHR) {
+        const uint32_t r = e / CHUNKS, c = (e % CHUNKS) * PER;
+        if (row0 + r < row_end && col0 + c < col_end)  // col_end and c are even when VEC
+            cp_async<8 * PER>(sm + r * kPad + c, g + (size_t)(row0 + r) * ld + col0 + c, true);
+    }
 }
 
 template <bool VEC>
 __device__ __forceinline__ void update_tiles(UpdSmem& s, double* __restrict__ Cm, uint32_t ld, uint32_t row0,
                                              uint32_t col0, uint32_t m, uint32_t nn, uint32_t a_col, uint32_t b_row,
-                                             uint32_t t_begin, uint32_t t_end, uint32_t gtid, uint32_t bar)
+                                             uint32_t t_begin, uint32_t t_end)
 {
     constexpr int WN = kUpdWarps / 2;     // warps along N
     constexpr int MT = 2, NT = 8 / WN;    // warp tile 32 x (64 / WN)
-    const uint32_t lane = gtid & 31, warp = gtid >> 5;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t g = lane >> 2, t4 = lane & 3;
     const uint32_t wm0 = (warp / WN) * 32, wn0 = (warp % WN) * (8 * NT);
     const uint32_t tiles_i = (m + kUpdTile - 1) / kUpdTile;
-    // A block: rows row0 + i * 64 .., columns a_col ..; B block: rows b_row .., columns
-    // col0 + j * 64 ..; C block: rows row0 + i * 64 .., columns col0 + j * 64 ..
+    if (t_begin >= t_end)
+        return;
     auto coords = [&](uint32_t t, uint32_t& i0, uint32_t& j0, uint32_t& me, uint32_t& ne) {
         i0 = (t % tiles_i) * kUpdTile;
         j0 = (t / tiles_i) * kUpdTile;
         me = min((uint32_t)kUpdTile, m - i0);
         ne = min((uint32_t)kUpdTile, nn - j0);
     };
-    auto load_c = [&](uint32_t t, double (&c)[MT][NT][4]) {
+    // tile t's A block (rows of C, the panel's columns) and C block into ring slot `buf`
+    auto stage_ac = [&](uint32_t t, int buf) {
         uint32_t i0, j0, me, ne;
         coords(t, i0, j0, me, ne);
-#pragma unroll
-        for (int i = 0; i < MT; ++i)
-#pragma unroll
-            for (int j = 0; j < NT; ++j) {
-                const uint32_t col = wn0 + 8 * j + 2 * t4;
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const uint32_t row = wm0 + 16 * i + g + 8 * h;
-                    c[i][j][2 * h] = c[i][j][2 * h + 1] = 0.0;
-                    if (row >= me)
-                        continue;
-                    const double* cp = Cm + (size_t)(row0 + i0 + row) * ld + col0 + j0 + col;
-                    if (VEC && col + 1 < ne) {
-                        const double2 v = *reinterpret_cast<const double2*>(cp);
-                        c[i][j][2 * h] = v.x;
-                        c[i][j][2 * h + 1] = v.y;
-                    } else {
-                        if (col < ne)
-                            c[i][j][2 * h] = cp[0];
-                        if (col + 1 < ne)
-                            c[i][j][2 * h + 1] = cp[1];
-                    }
-                }
-            }
-    };
-    auto stage_a = [&](uint32_t t, int buf) {
-        uint32_t i0, j0, me, ne;
-        coords(t, i0, j0, me, ne);
-        stage_rows<kUpdTile, VEC, kUpdThreads>(s.a[buf], Cm, ld, row0 + i0, row0 + i0 + me, a_col, gtid);
+        stage_tile<kUpdTile, K, VEC, kUpdThreads>(s.a[buf], Cm, ld, row0 + i0, row0 + i0 + me, a_col, a_col + K, tid);
+        stage_tile<kUpdTile, kUpdTile, VEC, kUpdThreads>(s.c[buf], Cm, ld, row0 + i0, row0 + i0 + me, col0 + j0,
+                                                         col0 + j0 + ne, tid);
     };
     auto stage_b = [&](uint32_t t) {
         uint32_t i0, j0, me, ne;
         coords(t, i0, j0, me, ne);
-        stage_cols<kUpdTile, VEC, kUpdThreads>(s.b, Cm, ld, b_row, col0 + j0, col0 + j0 + ne, gtid);
+        stage_cols<kUpdTile, VEC, kUpdThreads>(s.b, Cm, ld, b_row, col0 + j0, col0 + j0 + ne, tid);
     };
     auto commit = [] { asm volatile("cp.async.commit_group;" ::: "memory"); };
-    double cnext[MT][NT][4];
-    if (t_begin >= t_end)
-        return;
-    stage_a(t_begin, 0);
+    // prologue: {B, A/C of the first tile}, {A/C of the second} -- one commit group each
     stage_b(t_begin);
+    stage_ac(t_begin, 0);
     commit();
-    load_c(t_begin, cnext);
+    if (t_begin + 1 < t_end)
+        stage_ac(t_begin + 1, 1);
+    commit();
+    bool b_new = false;  // the most recent group holds a new B block
     for (uint32_t t = t_begin; t < t_end; ++t) {
         const int cur = (int)((t - t_begin) & 1u);
+        // this tile's group is the second most recent, unless the most recent one holds its B
+        if (b_new)
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        else
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        __syncthreads();
+        uint32_t i0, j0, me, ne;
+        coords(t, i0, j0, me, ne);
         double acc[MT][NT][4];
+        const double* cs = s.c[cur];
 #pragma unroll
         for (int i = 0; i < MT; ++i)
 #pragma unroll
             for (int j = 0; j < NT; ++j)
 #pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    acc[i][j][q] = -cnext[i][j][q];
-        const bool more = t + 1 < t_end;
-        const bool same_b = more && (t + 1) / tiles_i == t / tiles_i;
-        if (same_b) {  // the next tile's A block into the other buffer while this one computes
-            stage_a(t + 1, cur ^ 1);
-            commit();
-        }
-        if (more)
-            load_c(t + 1, cnext);
-        if (same_b)
-            asm volatile("cp.async.wait_group 1;" ::: "memory");
-        else
-            asm volatile("cp.async.wait_group 0;" ::: "memory");
-        group_sync(bar);
+                for (int h = 0; h < 2; ++h) {
+                    const uint32_t row = wm0 + 16 * i + g + 8 * h, col = wn0 + 8 * j + 2 * t4;
+                    const double2 v = *reinterpret_cast<const double2*>(cs + row * kPad + col);
+                    acc[i][j][2 * h] = -v.x;  // rows / columns outside the block: never stored
+                    acc[i][j][2 * h + 1] = -v.y;
+                }
+        const double* as = s.a[cur];
 #pragma unroll
         for (int k0 = 0; k0 < K; k0 += 8) {
             double af[MT][4], bf[NT][2];
 #pragma unroll
             for (int i = 0; i < MT; ++i) {
-                const double* p = s.a[cur] + (wm0 + 16 * i + g) * kPad + k0 + t4;
+                const double* p = as + (wm0 + 16 * i + g) * kPad + k0 + t4;
                 af[i][0] = p[0];
                 af[i][1] = p[8 * kPad];
                 af[i][2] = p[4];
@@ -360,8 +348,6 @@ __device__ __forceinline__ void update_tiles(UpdSmem& s, double* __restrict__ Cm
                 for (int j = 0; j < NT; ++j)
                     mma16x8x8(acc[i][j], af[i], bf[j]);
         }
-        uint32_t i0, j0, me, ne;
-        coords(t, i0, j0, me, ne);
 #pragma unroll
         for (int i = 0; i < MT; ++i)
 #pragma unroll
@@ -384,13 +370,15 @@ __device__ __forceinline__ void update_tiles(UpdSmem& s, double* __restrict__ Cm
                     }
                 }
             }
-        group_sync(bar);  // both buffers and B are free for what follows
-        if (more && !same_b) {  // a new column of tiles: its B block and the next A block
-            stage_a(t + 1, cur ^ 1);
+        __syncthreads();  // slot `cur` (and B, if the next tile starts a column) may be refilled
+        b_new = t + 1 < t_end && (t + 1) / tiles_i != t / tiles_i;
+        if (b_new)
             stage_b(t + 1);
-            commit();
-        }
+        if (t + 2 < t_end)
+            stage_ac(t + 2, cur);
+        commit();
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");  // nothing in flight when the CTA exits
 }
 
 }  // namespace dmma

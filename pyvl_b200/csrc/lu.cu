@@ -382,9 +382,17 @@ __global__ void __launch_bounds__(kTrsmCols, 1) trsm_kernel(uint32_t n, uint32_t
 //                       run of them with the next tile's operands loading during the MMAs.
 // Every product has K = 64, the panel width; the multipliers and U12 are the blocked forms of
 // getf2's and trsm's, equal to them up to rounding.
-constexpr int kTopThreads = 256;  // 64 rows x 4 groups of 16 columns
-constexpr int kTopGs = 18;        // doubles per column group of a broadcast row: 144 B, so the four
-                                  // groups' 16-byte loads fall in distinct banks
+// Columns per thread of the top-block kernel: 16 (256 threads), 8 (512) or 4 (1024); more
+// threads shorten each column step's chain of dependent instructions per warp.
+#ifndef PVL_TOP_CPT
+#define PVL_TOP_CPT 16
+#endif
+constexpr int kTopCpt = PVL_TOP_CPT;
+constexpr int kTopGroups = NB / kTopCpt;          // threads per row (neighbouring lanes)
+constexpr int kTopThreads = NB * kTopGroups;
+constexpr int kTopGs = kTopCpt + 2;               // doubles per column group of a broadcast row:
+                                                  // the groups' 16-byte loads fall in distinct banks
+static_assert(kTopCpt == 16 || kTopCpt == 8 || kTopCpt == 4, "16, 8 or 4 columns per thread");
 
 constexpr double kPivotLo = 0x1p-1000, kPivotHi = 0x1p+1000;
 
@@ -402,15 +410,16 @@ __device__ __forceinline__ double pivot_rcp(double p)
 
 // One CTA: the 64 x 64 diagonal block (a partial block padded with identity) factored without
 // interchanges, with X = L11^-1 and Y = U11^-1 formed in the same 64 column steps.  Thread
-// (r, g) holds row r, columns 16 g .. 16 g + 15, of T, X and Y in registers (the four threads
-// of a row are neighbouring lanes); the column loop is unrolled by 16, so every register index
-// is a constant.  Step j: row j is final and sits in shared memory (published by its threads at
-// the end of step j - 1, double-buffered by parity, one barrier per step).  A row r > j takes
-// its multiplier l = T[r][j] / U[j][j] (by the pivot's reciprocal, as getf2) from the thread that
-// holds column j, checks it, and applies T[r][c] -= l U[j][c] (c > j) and X[r] -= l X[j].  A row
-// r <= j finishes Y[r][j] = (delta_rj - sum_{k<j} Y[r][k] U[k][j]) / U[j][j] (the sum has been
-// accumulated in y by the earlier steps) and applies Y[r][c] -= Y[r][j] U[j][c] (c > j), the
-// same broadcast row.  The threads of row j + 1 then publish it with its pivot's reciprocal.
+// (r, g) holds row r, columns C g .. C g + C - 1 (C = kTopCpt), of T, X and Y in registers (the
+// threads of a row are neighbouring lanes); the column loop is unrolled by C, so every register
+// index is a constant.  Step j: row j is final and sits in shared memory (published by its
+// threads at the end of step j - 1, double-buffered by parity, one barrier per step).  A row
+// r > j takes its multiplier l = T[r][j] / U[j][j] (by the pivot's reciprocal, as getf2) from
+// the thread that holds column j, checks it, and applies T[r][c] -= l U[j][c] (c > j) and
+// X[r] -= l X[j].  A row r <= j finishes Y[r][j] = (delta_rj - sum_{k<j} Y[r][k] U[k][j]) /
+// U[j][j] (the sum has been accumulated in y by the earlier steps) and applies
+// Y[r][c] -= Y[r][j] U[j][c] (c > j), the same broadcast row.  The threads of row j + 1 then
+// publish it with its pivot's reciprocal.
 __global__ void __launch_bounds__(kTopThreads) top_factor_kernel(uint32_t k0, uint32_t nb,
                                                                  const double* __restrict__ A, uint32_t lda,
                                                                  double* __restrict__ top_out,
@@ -418,22 +427,23 @@ __global__ void __launch_bounds__(kTopThreads) top_factor_kernel(uint32_t k0, ui
                                                                  double* __restrict__ uinv,
                                                                  int32_t* __restrict__ reject)
 {
-    __shared__ __align__(16) double prow[2][4][kTopGs];  // row j of T
-    __shared__ __align__(16) double xrow[2][4][kTopGs];  // row j of X
+    constexpr int C = kTopCpt, G = kTopGroups;
+    __shared__ __align__(16) double prow[2][G][kTopGs];  // row j of T
+    __shared__ __align__(16) double xrow[2][G][kTopGs];  // row j of X
     __shared__ double rd[NB];                            // 1 / U[q][q]
-    const uint32_t tid = threadIdx.x, row = tid >> 2, g = tid & 3u;
-    const int src = (int)(tid & 28u);  // lane of this row's group 0
-    double t[16], x[16], y[16];
+    const uint32_t tid = threadIdx.x, row = tid / G, g = tid % G;
+    const int src = (int)(tid & 31u & ~(uint32_t)(G - 1));  // lane of this row's group 0
+    double t[C], x[C], y[C];
 #pragma unroll
-    for (int k = 0; k < 16; ++k) {
-        const uint32_t c = 16 * g + k;
+    for (int k = 0; k < C; ++k) {
+        const uint32_t c = C * g + k;
         t[k] = (row < nb && c < nb) ? A[(size_t)(k0 + row) * lda + k0 + c] : (row == c ? 1.0 : 0.0);
         x[k] = y[k] = row == c ? 1.0 : 0.0;
     }
     bool bad = false;
     if (row == 0) {
 #pragma unroll
-        for (int k = 0; k < 16; k += 2) {
+        for (int k = 0; k < C; k += 2) {
             *reinterpret_cast<double2*>(&prow[0][g][k]) = make_double2(t[k], t[k + 1]);
             *reinterpret_cast<double2*>(&xrow[0][g][k]) = make_double2(x[k], x[k + 1]);
         }
@@ -444,10 +454,10 @@ __global__ void __launch_bounds__(kTopThreads) top_factor_kernel(uint32_t k0, ui
     }
     __syncthreads();
 #pragma unroll 1
-    for (uint32_t gj = 0; gj < 4; ++gj) {
+    for (uint32_t gj = 0; gj < (uint32_t)G; ++gj) {
 #pragma unroll
-        for (int kj = 0; kj < 16; ++kj) {
-            const uint32_t j = 16 * gj + kj;
+        for (int kj = 0; kj < C; ++kj) {
+            const uint32_t j = C * gj + kj;
             const int b = kj & 1;
             const bool below = row > j;
             const double a = __shfl_sync(0xffffffffu, below ? t[kj] : y[kj], src + (int)gj) * rd[j];
@@ -463,7 +473,7 @@ __global__ void __launch_bounds__(kTopThreads) top_factor_kernel(uint32_t k0, ui
                 const bool later = g > gj;
                 if (below) {
 #pragma unroll
-                    for (int k = 0; k < 16; k += 2) {
+                    for (int k = 0; k < C; k += 2) {
                         const double2 p = *reinterpret_cast<const double2*>(&prow[b][g][k]);
                         if (k > kj || later)
                             t[k] = fma(-a, p.x, t[k]);
@@ -472,7 +482,7 @@ __global__ void __launch_bounds__(kTopThreads) top_factor_kernel(uint32_t k0, ui
                     }
                 } else {
 #pragma unroll
-                    for (int k = 0; k < 16; k += 2) {
+                    for (int k = 0; k < C; k += 2) {
                         const double2 p = *reinterpret_cast<const double2*>(&prow[b][g][k]);
                         if (k > kj || later)
                             y[k] = fma(-a, p.x, y[k]);
@@ -483,17 +493,17 @@ __global__ void __launch_bounds__(kTopThreads) top_factor_kernel(uint32_t k0, ui
             }
             if (below && g <= gj) {  // X[j][c] = 0 for c > j
 #pragma unroll
-                for (int k = 0; k < 16; k += 2) {
+                for (int k = 0; k < C; k += 2) {
                     const double2 p = *reinterpret_cast<const double2*>(&xrow[b][g][k]);
                     x[k] = fma(-a, p.x, x[k]);
                     x[k + 1] = fma(-a, p.y, x[k + 1]);
                 }
             }
             if (row == j + 1) {  // row j + 1 is final: publish it (never true after the last step)
-                const int kn = (kj + 1) & 15;
-                const uint32_t gn = gj + (kj == 15 ? 1u : 0u);
+                const int kn = (kj + 1) % C;
+                const uint32_t gn = gj + (kj == C - 1 ? 1u : 0u);
 #pragma unroll
-                for (int k = 0; k < 16; k += 2) {
+                for (int k = 0; k < C; k += 2) {
                     *reinterpret_cast<double2*>(&prow[b ^ 1][g][k]) = make_double2(t[k], t[k + 1]);
                     *reinterpret_cast<double2*>(&xrow[b ^ 1][g][k]) = make_double2(x[k], x[k + 1]);
                 }
@@ -507,16 +517,16 @@ __global__ void __launch_bounds__(kTopThreads) top_factor_kernel(uint32_t k0, ui
     }
     if (__syncthreads_or(bad) && tid == 0)
         atomicExch(reject, 1);
-    const size_t o = (size_t)row * NB + 16 * g;
+    const size_t o = (size_t)row * NB + C * g;
 #pragma unroll
-    for (int k = 0; k < 16; k += 2) {
+    for (int k = 0; k < C; k += 2) {
         *reinterpret_cast<double2*>(linv + o + k) = make_double2(x[k], x[k + 1]);
         *reinterpret_cast<double2*>(uinv + o + k) = make_double2(y[k], y[k + 1]);
     }
     if (row < nb) {
 #pragma unroll
-        for (int k = 0; k < 16; ++k)
-            if (16 * g + k < nb)
+        for (int k = 0; k < C; ++k)
+            if (C * g + k < nb)
                 top_out[o + k] = t[k];
     }
 }
@@ -570,29 +580,26 @@ UpdRect upd_rect(uint32_t row0, uint32_t col0, uint32_t m, uint32_t nn, uint32_t
     return r;
 }
 
-// Two tile groups per CTA, each with its own shared memory and barrier (dmma.cuh update_tiles:
-// the next tile's operands load while this one multiplies); a CTA fills one SM.  Group slot
-// s = 2 blockIdx.x + group runs tiles [s per, (s + 1) per) of r0, the slots after r0's those
-// of r1 (each rectangle's tiles in column-major order).
+// One CTA per SM, each a run of tiles (dmma.cuh update_tiles: C and A blocks stream into shared
+// memory one tile ahead of the MMAs).  CTA s < r0.slots runs tiles [s per, (s + 1) per) of r0,
+// the CTAs after them those of r1 (each rectangle's tiles in column-major order).
 template <bool VEC>
-__global__ void __launch_bounds__(2 * pvl::dmma::kUpdThreads, 1) dmma_update_kernel(double* __restrict__ A,
-                                                                                 uint32_t lda, UpdRect r0,
-                                                                                 UpdRect r1)
+__global__ void __launch_bounds__(pvl::dmma::kUpdThreads, 1) dmma_update_kernel(double* __restrict__ A, uint32_t lda,
+                                                                            UpdRect r0, UpdRect r1)
 {
     extern __shared__ __align__(16) double upd_smem[];
-    const uint32_t grp = threadIdx.x / pvl::dmma::kUpdThreads, gtid = threadIdx.x % pvl::dmma::kUpdThreads;
-    auto& sm = reinterpret_cast<pvl::dmma::UpdSmem*>(upd_smem)[grp];
-    uint32_t slot = 2 * blockIdx.x + grp;
+    auto& sm = *reinterpret_cast<pvl::dmma::UpdSmem*>(upd_smem);
+    uint32_t slot = blockIdx.x;
     const bool first = slot < r0.slots;
     const UpdRect r = first ? r0 : r1;
     if (!first)
         slot -= r0.slots;
     if (slot >= r.slots)
-        return;  // the whole group: its barrier counts only its own threads
+        return;
     constexpr uint32_t T = pvl::dmma::kUpdTile;
     const uint32_t tiles = ((r.m + T - 1) / T) * ((r.nn + T - 1) / T);
     const uint32_t t0 = slot * r.per, t1 = min(tiles, t0 + r.per);
-    pvl::dmma::update_tiles<VEC>(sm, A, lda, r.row0, r.col0, r.m, r.nn, r.a_col, r.b_row, t0, t1, gtid, 1 + grp);
+    pvl::dmma::update_tiles<VEC>(sm, A, lda, r.row0, r.col0, r.m, r.nn, r.a_col, r.b_row, t0, t1);
 }
 
 // SMs left free while the bulk of a panel's trailing update runs on the side stream: the next
@@ -753,7 +760,7 @@ extern "C" int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv,
     cudaStream_t st = (cudaStream_t)stream;
     LuWs w = carve(ws, n);
     const size_t trsm_smem = (size_t)(NB * (NB + 1) + NB * (kTrsmCols + 1)) * sizeof(double);
-    const size_t upd_smem = 2 * sizeof(pvl::dmma::UpdSmem);
+    const size_t upd_smem = sizeof(pvl::dmma::UpdSmem);
     int dev = 0, sms = 0;
     PVL_CUDA_CHECK(cudaGetDevice(&dev));
     PVL_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -768,17 +775,17 @@ extern "C" int pvl_lu_factor(uint32_t n, double* A, uint32_t lda, int32_t* ipiv,
     PVL_SMEM_OPTIN(apply_fn, kApplySmem);
     PVL_SMEM_OPTIN(upd_fn, upd_smem);
     auto update = [&](cudaStream_t s, const UpdRect& r0, const UpdRect& r1) -> int {
-        const uint32_t ctas = blocks_for(r0.slots + r1.slots, 2);
+        const uint32_t ctas = r0.slots + r1.slots;
         if (ctas == 0)
             return PVL_OK;
         void* args[] = {(void*)&A, (void*)&lda, (void*)&r0, (void*)&r1};
-        PVL_CUDA_CHECK(cudaLaunchKernel(upd_fn, dim3(ctas), dim3(2 * pvl::dmma::kUpdThreads), args, upd_smem, s));
+        PVL_CUDA_CHECK(cudaLaunchKernel(upd_fn, dim3(ctas), dim3(pvl::dmma::kUpdThreads), args, upd_smem, s));
         pvl_count_launch();
         return PVL_OK;
     };
     const UpdRect none{0, 0, 0, 0, 0, 0, 1, 0};
-    const uint32_t all_slots = 2u * (uint32_t)sms;
-    const uint32_t bulk_slots = 2u * (uint32_t)std::max(1, sms - kLookaheadSms);
+    const uint32_t all_slots = (uint32_t)sms;  // one CTA per SM
+    const uint32_t bulk_slots = (uint32_t)std::max(1, sms - kLookaheadSms);
     int32_t* perm = ipiv + n;
     PVL_CUDA_CHECK(cudaMemsetAsync(info, 0, sizeof(int32_t), st));
     init_perm_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, perm);
