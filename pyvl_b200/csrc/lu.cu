@@ -608,8 +608,10 @@ constexpr int kLookaheadSms = 8;
 
 // A second stream and two events per thread and device for the look-ahead fork and join (a
 // stream may take part in one capture at a time: per thread, since captures here are
-// thread-local).  Created once, never destroyed.
+// thread-local).  Created on first use in a context and kept; a new context (after a device
+// reset) gets new ones.
 struct SideStream {
+    void* ctx = nullptr;
     cudaStream_t s = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
 };
@@ -619,11 +621,16 @@ int side_stream(int dev, SideStream*& out)
     thread_local SideStream cache[64];
     if (dev < 0 || dev >= 64)
         return pvl_fail(PVL_ERR_ARG, "pvl_lu_factor: device %d out of range", dev);
+    void* ctx = nullptr;
+    if (int rc = pvl_current_context(&ctx))
+        return rc;
     SideStream& c = cache[dev];
-    if (!c.s) {
+    if (!c.s || c.ctx != ctx) {
+        c = SideStream{};
         PVL_CUDA_CHECK(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
         PVL_CUDA_CHECK(cudaEventCreateWithFlags(&c.fork, cudaEventDisableTiming));
         PVL_CUDA_CHECK(cudaEventCreateWithFlags(&c.join, cudaEventDisableTiming));
+        c.ctx = ctx;
     }
     out = &c;
     return PVL_OK;

@@ -42,21 +42,6 @@ struct ScratchAddr {
 ScratchAddr g_scratch[kMaxDevices] = {};
 std::mutex g_scratch_mutex;
 
-// The driver's cuCtxGetCurrent, reached through the runtime (the library links no libcuda).
-using CtxGetCurrent = CUresult (*)(CUcontext*);
-CtxGetCurrent ctx_get_current()
-{
-    static CtxGetCurrent fn = [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess)
-            p = nullptr;
-        return reinterpret_cast<CtxGetCurrent>(p);
-    }();
-    return fn;
-}
-
 // Device address of g_noalloc_scratch on the current device, looked up once per device and
 // context (the caller has made the device current, so the runtime's context is current too).
 int scratch_for_current_device(void** out)
@@ -65,12 +50,10 @@ int scratch_for_current_device(void** out)
     PVL_CUDA_CHECK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices)
         return pvl_fail(PVL_ERR_ARG, "pvl_line_velocity_noalloc: device index %d out of range", dev);
-    CtxGetCurrent get = ctx_get_current();
-    if (!get)
-        return pvl_fail(PVL_ERR_CUDA, "pvl_line_velocity_noalloc: cuCtxGetCurrent is not available");
-    CUcontext ctx = nullptr;
-    if (get(&ctx) != CUDA_SUCCESS)
-        return pvl_fail(PVL_ERR_CUDA, "pvl_line_velocity_noalloc: cuCtxGetCurrent failed");
+    void* cur = nullptr;
+    if (int rc = pvl_current_context(&cur))
+        return rc;
+    CUcontext ctx = static_cast<CUcontext>(cur);
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
     ScratchAddr& s = g_scratch[dev];
     if (!s.addr || !ctx || s.ctx != ctx) {
@@ -79,8 +62,13 @@ int scratch_for_current_device(void** out)
         if (e != cudaSuccess || !p)
             return pvl_fail(PVL_ERR_CUDA, "pvl_line_velocity_noalloc: cudaGetSymbolAddress failed: %s",
                             cudaGetErrorString(e));
-        if (!ctx && (get(&ctx) != CUDA_SUCCESS || !ctx))
-            return pvl_fail(PVL_ERR_CUDA, "pvl_line_velocity_noalloc: no current CUDA context");
+        if (!ctx) {
+            if (int rc = pvl_current_context(&cur))
+                return rc;
+            ctx = static_cast<CUcontext>(cur);
+            if (!ctx)
+                return pvl_fail(PVL_ERR_CUDA, "pvl_line_velocity_noalloc: no current CUDA context");
+        }
         s.ctx = ctx;
         s.addr = p;
     }

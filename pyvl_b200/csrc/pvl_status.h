@@ -8,6 +8,10 @@ int pvl_fail(int code, const char* fmt, ...);
 
 #include <stddef.h>
 
+// The calling thread's current CUDA context (the runtime's primary context once a runtime call
+// has run on the device).  Returns PVL_OK or PVL_ERR_CUDA with the message set.
+int pvl_current_context(void** ctx);
+
 // Opt the kernel `fn` in to `bytes` of dynamic shared memory on the current device (once per
 // kernel and device; thread-safe).  Returns PVL_OK or a PVL_ERR_* code with the message set.
 int pvl_smem_optin(const void* fn, size_t bytes);

@@ -5,6 +5,7 @@
 #include <mutex>
 #include <utility>
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "pvl_status.h"
@@ -25,6 +26,27 @@ int pvl_fail(int code, const char* fmt, ...)
 extern "C" const char* pvl_last_error(void) { return g_last_error; }
 
 extern "C" int pvl_version(void) { return 100; }
+
+// The driver's cuCtxGetCurrent, reached through the runtime (the library links no libcuda).
+int pvl_current_context(void** ctx)
+{
+    using CtxGetCurrent = CUresult (*)(CUcontext*);
+    static CtxGetCurrent fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<CtxGetCurrent>(p);
+    }();
+    if (!fn)
+        return pvl_fail(PVL_ERR_CUDA, "cuCtxGetCurrent is not available");
+    CUcontext c = nullptr;
+    if (fn(&c) != CUDA_SUCCESS)
+        return pvl_fail(PVL_ERR_CUDA, "cuCtxGetCurrent failed");
+    *ctx = c;
+    return PVL_OK;
+}
 
 // cudaFuncSetAttribute(MaxDynamicSharedMemorySize) is a per-device setting of a kernel: keep
 // the largest value set for each (kernel, device) and call the runtime only when a launch on
