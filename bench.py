@@ -74,7 +74,7 @@ def parse():
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batched-cases summary (bench.py --workload batch, run after the headline)")
     ap.add_argument("--profile-kernel", choices=["line_sum", "advect_f32", "wake_term", "body", "gemv", "lu", "lu32",
-                                                 "mixed_step", "plain_step", "batch_step", "mlp"],
+                                                 "mixed_step", "plain_step", "batch_step", "mlp", "gemm4096"],
                     default=None,
                     help="set up the workload, launch only that kernel family twice and exit (for ncu captures)")
     ap.add_argument("--fraction", type=int, default=16,
@@ -242,6 +242,29 @@ def profile_kernel(args) -> None:
     mixed_step / batch_step: a few whole steps (launch lists)."""
     import torch
 
+    if args.profile_kernel == "gemm4096":  # the TF32 tensor-core GEMM on a compute-bound 4096^3 product
+        from pyvl_b200 import _lib
+        from pyvl_b200.device import ptr, stream_ptr
+
+        n = 4096
+        g = torch.Generator(device="cuda").manual_seed(0)
+        A = torch.randn(n, n, device="cuda", generator=g)
+        Bt = torch.randn(n, n, device="cuda", generator=g)
+        C = torch.zeros(n, n, device="cuda")
+        err = torch.zeros(1, dtype=torch.int32, device="cuda")
+        ms = []
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            _lib.call("pvl_gemm_tf32", n, n, n, 1.0, ptr(A), n, ptr(Bt), n, 0.0, ptr(C), n, ptr(err), stream_ptr())
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        want = A.double() @ Bt.double().t()
+        rel = float((torch.linalg.norm(C.double() - want) / torch.linalg.norm(want)).item())
+        print(f"profile-kernel done gemm4096 ms={min(ms[1:]):.4f} tflops={2 * n ** 3 / (min(ms[1:]) * 1e-3) / 1e12:.1f} "
+              f"rel_err={rel:.2e} err={int(err.item())}")
+        return
     if args.profile_kernel == "batch_step":
         from pyvl_b200.batch import BatchEngine
         from pyvl_b200.workloads import batch_wings
