@@ -128,18 +128,30 @@ def _lu_roundtrip(torch, A, b):
 
 
 @pytest.mark.parametrize("n,kind", [(64, "dominant"), (200, "dominant"), (1000, "dominant"), (333, "general"),
-                                    (130, "general"), (777, "singular_last")])
+                                    (130, "general"), (777, "singular_last"), (1000, "mixed"), (1600, "mixed")])
 def test_lu_matches_lapack(torch_cuda, n, kind):
     rng = np.random.default_rng(n)
     A = rng.normal(size=(n, n))
-    if kind == "dominant":
+    if kind in ("dominant", "mixed"):
         A = A * 1e-3 - 2 * np.pi * np.eye(n)
+    if kind == "mixed":
+        # the diagonal blocks of panels 5 and 11 (64 columns each) are permuted (antidiagonal, a
+        # random permutation): those two panels interchange rows inside their own row block and
+        # take the pivoting fallback, every other panel the speculative path -- the fallback runs
+        # while the look-ahead's bulk update of the panel before it is in flight
+        for p, perm in ((5, np.arange(63, -1, -1)), (11, rng.permutation(64))):
+            c0 = 64 * p
+            A[c0:c0 + 64, c0:c0 + 64] = rng.normal(size=(64, 64)) * 1e-3
+            A[c0 + perm, c0 + np.arange(64)] -= 2 * np.pi
     if kind == "singular_last":
         A[:, -1] = 0.0
     b = rng.normal(size=n)
     LU, ipiv, info, err, x = _lu_roundtrip(torch_cuda, A, b)
     assert err == 0
     lu_ref, piv_ref = la.lu_factor(A)
+    if kind == "mixed":
+        moved = np.nonzero(piv_ref != np.arange(n))[0] // 64
+        assert sorted(set(moved.tolist())) == [5, 11]
     assert np.array_equal(ipiv[:n], piv_ref)
     assert rel(LU, lu_ref) <= 1e-13
     if kind == "singular_last":
