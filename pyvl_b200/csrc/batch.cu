@@ -26,6 +26,7 @@
 #include <cstdint>
 
 #include "pvl_common.cuh"
+#include "sweep.cuh"
 
 using pvl::Segment;
 using pvl::Vec3;
@@ -215,6 +216,10 @@ __global__ void __launch_bounds__(128) batched_ring_tile_kernel(
 }
 
 // ------------------------------------------------------------------ sweep jobs
+// The single-case sweep's pair arithmetic (sweep.cuh): each work item's segments are staged in
+// Pluecker form about the centroid of the item's points (one case's points, so neighbours),
+// and a thread evaluates them at its PPT points -- two segments per iteration when it holds
+// one point, one segment at PPT points otherwise (PPT independent chains).
 template <int THREADS, int PPT>
 __global__ void __launch_bounds__(THREADS) batched_sweep_kernel(const SweepJob* __restrict__ jobs,
                                                                 const uint32_t* __restrict__ job_item,
@@ -229,8 +234,12 @@ __global__ void __launch_bounds__(THREADS) batched_sweep_kernel(const SweepJob* 
                                                                 double* __restrict__ part)
 {
     constexpr uint32_t kPts = THREADS * PPT;
-    __shared__ Segment<double> s_seg[kSegTile];
+    __shared__ pvl::SweepSeg s_seg[kSegTile + 1];
+    __shared__ double s_red[THREADS / 32][4];
+    __shared__ double s_o[3];
     __shared__ uint32_t s_item;
+    if (threadIdx.x == 0)
+        s_seg[kSegTile] = pvl::SweepSeg{};  // the partner of an odd last segment: d = 0, nothing induced
     for (;;) {
         if (threadIdx.x == 0)
             s_item = atomicAdd(counter, 1u);
@@ -258,6 +267,7 @@ __global__ void __launch_bounds__(THREADS) batched_sweep_kernel(const SweepJob* 
         const uint32_t l_end = J.seg_begin + min(seg_count, (split + 1) * J.per);  // may be <= l_begin: zeros
         double px[PPT], py[PPT], pz[PPT];
         Vec3<double> acc[PPT];
+        double cx = 0.0, cy = 0.0, cz = 0.0, cn = 0.0;
 #pragma unroll
         for (int t = 0; t < PPT; ++t) {
             const uint32_t p = p0 + t * THREADS + threadIdx.x;
@@ -266,20 +276,44 @@ __global__ void __launch_bounds__(THREADS) batched_sweep_kernel(const SweepJob* 
             px[t] = ok ? pts[3 * q] : 0.0;
             py[t] = ok ? pts[3 * q + 1] : 0.0;
             pz[t] = ok ? pts[3 * q + 2] : 0.0;
+            cx += px[t];
+            cy += py[t];
+            cz += pz[t];
+            cn += ok ? 1.0 : 0.0;
             acc[t] = Vec3<double>{0.0, 0.0, 0.0};
+        }
+        pvl::cta_centroid<THREADS>(cx, cy, cz, cn, s_red, s_o);  // px.. are 0 for absent points
+#pragma unroll
+        for (int t = 0; t < PPT; ++t) {
+            px[t] -= s_o[0];
+            py[t] -= s_o[1];
+            pz[t] -= s_o[2];
         }
         for (uint32_t l0 = l_begin; l0 < l_end; l0 += kSegTile) {
             for (uint32_t e = threadIdx.x; e < kSegTile; e += THREADS)
                 if (l0 + e < l_end)
-                    s_seg[e] = seg[l0 + e];
+                    s_seg[e] = pvl::sweep_seg(seg[l0 + e], s_o);
             __syncthreads();
             const int cnt = (int)min((uint32_t)kSegTile, l_end - l0);
+            if (PPT == 1) {
 #pragma unroll 1
-            for (int k = 0; k < cnt; ++k) {
-                const Segment<double> s = s_seg[k];
+                for (int k = 0; k < cnt; k += 2) {  // k + 1 <= cnt: a segment, or the zero one at the tile end
+                    const pvl::SweepSeg a = s_seg[k], b = s_seg[k + 1 < cnt ? k + 1 : kSegTile];
+                    const pvl::SweepGeo ga = pvl::sweep_geo(a, px[0], py[0], pz[0]);
+                    const pvl::SweepGeo gb = pvl::sweep_geo(b, px[0], py[0], pz[0]);
+                    pvl::sweep_add(a, ga, tol2, acc[0]);
+                    pvl::sweep_add(b, gb, tol2, acc[0]);
+                }
+            } else {
+#pragma unroll 1
+                for (int k = 0; k < cnt; ++k) {
+                    const pvl::SweepSeg a = s_seg[k];
 #pragma unroll
-                for (int t = 0; t < PPT; ++t)
-                    pvl::segment_induction<double, true>(s, px[t], py[t], pz[t], tol2, s.gamma, acc[t]);
+                    for (int t = 0; t < PPT; ++t) {
+                        const pvl::SweepGeo ga = pvl::sweep_geo(a, px[t], py[t], pz[t]);
+                        pvl::sweep_add(a, ga, tol2, acc[t]);
+                    }
+                }
             }
             __syncthreads();
         }

@@ -84,6 +84,9 @@ __global__ void __launch_bounds__(kThreads) wavefront_kernel(uint32_t n, const d
     };
     if (n_dep > 0)
         load_block(0, cur);
+    // this block's own right-hand side: no other block writes it, so it is read now and not on
+    // the chain after the last dependency
+    const double rhs_own = threadIdx.x < rows ? __ldcg(x + r0 + threadIdx.x) : 0.0;
     __syncthreads();
     for (uint32_t step = 0; step < n_dep; ++step) {
         if (step + 1 < n_dep)
@@ -131,7 +134,7 @@ __global__ void __launch_bounds__(kThreads) wavefront_kernel(uint32_t n, const d
     }
     __syncthreads();
     if (threadIdx.x < kRB)
-        s_r[threadIdx.x] = threadIdx.x < rows ? __ldcg(x + r0 + threadIdx.x) - s_acc[threadIdx.x] : 0.0;
+        s_r[threadIdx.x] = threadIdx.x < rows ? rhs_own - s_acc[threadIdx.x] : 0.0;
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
