@@ -54,15 +54,22 @@ template <typename T> struct Vec3 { T x, y, z; };
 // Closer pairs (larger w, or x <= 0) take the atan2 form.
 // Comparisons of non-negative values (or +NaN) through their bit patterns: for IEEE numbers of
 // one sign, the order of the bit patterns is the order of the values, and the integer compare
-// runs on the ALU pipe instead of the FP64 pipe that bounds the FP64 sweeps.  le_nn(a, b):
-// a <= b; lt_nn(a, b): a < b; pos(x): x > +0 (a +NaN counts as positive, and then fails the
-// far-field test that follows).
+// runs on the ALU pipe instead of the FP64 pipe that bounds the FP64 sweeps.  lt_nn(a, b):
+// a < b, exactly (the cut-off).
 __device__ __forceinline__ bool lt_nn(double a, double b) { return __double_as_longlong(a) < __double_as_longlong(b); }
-__device__ __forceinline__ bool le_nn(double a, double b) { return __double_as_longlong(a) <= __double_as_longlong(b); }
-__device__ __forceinline__ bool pos(double x) { return __double_as_longlong(x) > 0; }
+// Threshold tests that only choose between two evaluations that are both accurate near the
+// threshold (far-field series or atan2, which series tier) compare the high 32 bits (sign,
+// exponent, 20 mantissa bits): one integer compare instead of two.  A value above the threshold
+// by less than 2^-20 of it may take the series tier meant for the threshold, whose truncation
+// bound then grows by less than 2e-5 of itself (still below 1.2e-17).  The cut-off test stays
+// exact (lt_nn).  pos_hi(x): x > +0 with at least one bit in the high word (a smaller positive
+// x takes the atan2 form; a +NaN counts as positive and then fails the far-field test).
+__device__ __forceinline__ int hi32(double a) { return (int)(__double_as_longlong(a) >> 32); }
+__device__ __forceinline__ bool le_hi(double a, double b) { return hi32(a) <= hi32(b); }
+__device__ __forceinline__ bool pos_hi(double x) { return hi32(x) > 0; }
+__device__ __forceinline__ bool le_hi(float a, float b) { return a <= b; }
+__device__ __forceinline__ bool pos_hi(float x) { return x > 0.0f; }
 __device__ __forceinline__ bool lt_nn(float a, float b) { return a < b; }
-__device__ __forceinline__ bool le_nn(float a, float b) { return a <= b; }
-__device__ __forceinline__ bool pos(float x) { return x > 0.0f; }
 
 template <typename T> struct FarSeries;
 template <> struct FarSeries<double> {
@@ -84,12 +91,12 @@ template <> struct FarSeries<double> {
     static __device__ __forceinline__ double sum(double w)
     {
         double s;
-        if (le_nn(w, 1e-4)) {  // most pairs of a wake sweep: four terms, 1e-4^4 / 9 < 1.2e-17
+        if (le_hi(w, 1e-4)) {  // most pairs of a wake sweep: four terms, 1e-4^4 / 9 < 1.2e-17
             s = -1.0 / 7.0;
             s = fma(s, w, 1.0 / 5.0);
             s = fma(s, w, -1.0 / 3.0);
             return fma(s, w, 1.0);
-        } else if (le_nn(w, 0.01)) {  // eight terms: 0.01^8 / 17 < 1e-17
+        } else if (le_hi(w, 0.01)) {  // eight terms: 0.01^8 / 17 < 1e-17
             s = -1.0 / 15.0;
             s = fma(s, w, 1.0 / 13.0);
             s = fma(s, w, -1.0 / 11.0);
@@ -119,9 +126,9 @@ template <> struct FarSeries<double> {
     static __device__ __forceinline__ double sum_uniform(double w)
     {
         const unsigned m = __activemask();
-        if (__any_sync(m, !le_nn(w, 0.01)))
+        if (__any_sync(m, !le_hi(w, 0.01)))
             return sum_tier<16>(w);
-        if (__any_sync(m, !le_nn(w, 1e-4)))
+        if (__any_sync(m, !le_hi(w, 1e-4)))
             return sum_tier<8>(w);
         return sum_tier<4>(w);
     }
@@ -179,7 +186,7 @@ __device__ __forceinline__ void segment_induction(const Segment<T>& s, T px, T p
     const T r = FarSeries<T>::rcp(x);  // wasted only on the rare near pairs
     const T w = hsq * s.len2 * (r * r);  // >= +0, or +NaN
     T mag;
-    if (pos(x) && le_nn(w, FarSeries<T>::kW)) {
+    if (pos_hi(x) && le_hi(w, FarSeries<T>::kW)) {
         const T S = UNIFORM ? FarSeries<T>::sum_uniform(w) : FarSeries<T>::sum(w);
         mag = (GAMMA ? -s.glen : -scale * s.len) * r * S;
     } else {

@@ -66,7 +66,7 @@ __device__ __forceinline__ SweepGeo sweep_geo(const SweepSeg& s, double px, doub
 __device__ __forceinline__ void sweep_add(const SweepSeg& s, const SweepGeo& g, double tol2, Vec3<double>& acc)
 {
     const bool ok = !lt_nn(g.hsq, tol2);
-    const bool far = ok && pos(g.x) && le_nn(g.w, FarSeries<double>::kW);
+    const bool far = ok && pos_hi(g.x) && le_hi(g.w, FarSeries<double>::kW);
     double mag = far ? -s.glen * g.r * FarSeries<double>::sum(g.w) : 0.0;
     if (ok && !far) {
         const double rh = rsqrt(g.hsq);
