@@ -193,14 +193,14 @@ __global__ void __launch_bounds__(kTcTile) forward_tc_kernel(uint32_t n, const f
 
 // ---------------------------------------------------------------- training on the tensor cores
 // Forward + backward of mean((y - t)^2) over 128-sample tiles, persistent CTAs of 128 threads
-// (thread s = sample s of the tile = TMEM lane s).  Per tile, three rounds of tcgen05.mma
+// (thread s = sample s of the tile = TMEM lane s).  Per tile, three stages of tcgen05.mma
 // kind::f16 (BF16 operands, FP32 accumulators in tensor memory):
 //   1. acc1 = X W1^T (K = 16: the 12 inputs, zero-padded)          -> h1 = bf16(relu(acc1 + b1))
 //   2. acc2 = H1 W2^T (K = 128)                                     -> h2, y, dy = 2 (y - t) / n,
 //      dh2 = [h2 > 0] dy w3 (rounded to BF16 as an MMA operand)
 //   3. dH1 = dH2 W2 (K = 128, into acc1's columns)  and  dW2 += dH2^T H1 (K = 128 samples,
 //      accumulated in TMEM over all tiles of the CTA).
-// The operands of round 3 need H1 and dH2 also transposed (samples along K): the epilogue
+// The operands of stage 3 need H1 and dH2 also transposed (samples along K): the epilogue
 // threads write both layouts.  db2 and dw3 are per-unit sums over samples: warp reductions
 // (halving exchange, 16 shuffles per 16 columns) then a fixed-order sum over the 4 warps;
 // db1 and dW1 = sum_s dh1[s][k] x[s][i] on CUDA cores from dh1 staged in shared memory, a
@@ -210,8 +210,8 @@ __global__ void __launch_bounds__(kTcTile) forward_tc_kernel(uint32_t n, const f
 // poisons the partial gradient with NaN (training then stops on the loss).
 struct TrainTcSmem {
     unsigned char w1[kH * 128];        // W1: N = 128 units x K (12 used)
-    unsigned char w2[2][kH * 128];     // W2: N = j x K = k (round 2's B)
-    unsigned char w2t[2][kH * 128];    // W2^T: N = k x K = j (round 3's B for dH1)
+    unsigned char w2[2][kH * 128];     // W2: N = j x K = k (stage 2's B)
+    unsigned char w2t[2][kH * 128];    // W2^T: N = k x K = j (stage 3's B for dH1)
     unsigned char r1[2][kTcTile * 128];
     unsigned char r2[2][kTcTile * 128];
     unsigned char r3[2][kH * 128];
