@@ -239,6 +239,26 @@ int pvl_wake_node_velocity_cols(int precision, uint32_t n_points, uint32_t n_lin
                                 double ux, double uy, double uz, double tol, double* node_vel, void* ws,
                                 size_t ws_bytes, void* stream);
 
+/* pvl_wake_node_velocity_cols for rows row_begin + k * row_step, k < row_count (each < complete_rows)
+ * of the n_cols node columns; output at the same rows of node_vel.  Workspace:
+ * pvl_line_velocity_workspace(n_lines, n_cols row_count, precision).  Used with
+ * pvl_wake_interp_rows for the far wake rows, whose body-induced velocity varies slowly along a
+ * node column.  No reference counterpart. */
+int pvl_wake_node_velocity_rows(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
+                                const double* positions, const double* line_gamma, uint32_t n_shed,
+                                uint32_t line_rows, uint32_t complete_rows, uint32_t row_begin,
+                                uint32_t row_count, uint32_t row_step, uint32_t n_cols, const uint32_t* cols,
+                                const double* wake_pos, double ux, double uy, double uz, double tol,
+                                double* node_vel, void* ws, size_t ws_bytes, void* stream);
+
+/* node_vel (n_cols, complete_rows, 3): rows row_first, row_first + 2, ... <= row_last of every
+ * column set to the midpoint value of the cubic through the same column's rows -3, -1, +1 and +3
+ * away ((9 (v[-1] + v[+1]) - (v[-3] + v[+3])) / 16); needs row_first >= 3 and
+ * row_last + 3 < complete_rows.  The mixed path's far-row advection (no reference
+ * counterpart: the reference evaluates every node). */
+int pvl_wake_interp_rows(uint32_t n_cols, uint32_t complete_rows, uint32_t row_first, uint32_t row_last,
+                         double* node_vel, void* stream);
+
 /* Advance wake node rows (explicit Euler) from `old_pos` into `new_pos` (both
  * (n_shed, 2, line_rows + 1, 3)): new[:, :, i+1] = old[:, :, i] + node_vel[:, :, i] * dt for
  * i < complete_rows; row 0 pinned to the bordering body nodes; rows beyond complete_rows

@@ -57,6 +57,9 @@ SIGNATURES = {
     "pvl_wake_node_velocity": (_I, [_I, _U, _U, _P, _P, _P, _U, _U, _U, _P, _D, _D, _D, _D, _P, _P, _Z, _P]),
     "pvl_wake_node_velocity_cols": (_I, [_I, _U, _U, _P, _P, _P, _U, _U, _U, _U, _U, _U, _P, _P, _D, _D, _D, _D, _P,
                                          _P, _Z, _P]),
+    "pvl_wake_node_velocity_rows": (_I, [_I, _U, _U, _P, _P, _P, _U, _U, _U, _U, _U, _U, _U, _P, _P, _D, _D, _D, _D,
+                                         _P, _P, _Z, _P]),
+    "pvl_wake_interp_rows": (_I, [_U, _U, _U, _U, _P, _P]),
     "pvl_wake_fold_implicit": (_I, [_U, _U, _P, _P, _P, _U, _P]),
     "pvl_wake_fold_implicit_distinct": (_I, [_U, _U, _P, _P, _P, _U, _P]),
     "pvl_wake_advect": (_I, [_U, _U, _U, _P, _P, _D, _P, _P, _P, _P]),

@@ -209,19 +209,20 @@ __global__ void __launch_bounds__(kRingThreads) line_matrix_kernel(uint32_t n_li
     }
 }
 
-// Point p of a sweep is pts[col(p / group) * stride + p % group + in_off] with col(c) =
-// cols ? cols[c] : c: group == stride == n_pts is a plain array; group = a range of wake
-// rows, stride = rows + 1, in_off = first row walks those rows of the listed wake node
-// columns (strip side s * 2 + side).  A listed column at or past col_limit is no point.
+// Point p of a sweep is pts[col(p / group) * stride + (p % group) * row_step + in_off] with
+// col(c) = cols ? cols[c] : c: group == stride == n_pts, row_step 1 is a plain array; group = a
+// set of wake rows, stride = rows + 1, in_off = first row, row_step = the rows' spacing walks
+// those rows of the listed wake node columns (strip side s * 2 + side).  A listed column at or
+// past col_limit is no point.
 __device__ __forceinline__ bool sweep_point(uint32_t p, uint32_t n_pts, uint32_t group, uint32_t stride,
-                                            uint32_t in_off, const uint32_t* __restrict__ cols, uint32_t col_limit,
-                                            size_t& q)
+                                            uint32_t in_off, uint32_t row_step, const uint32_t* __restrict__ cols,
+                                            uint32_t col_limit, size_t& q)
 {
     bool ok = p < n_pts;
     uint32_t col = ok ? (cols ? cols[p / group] : p / group) : 0;
     if (col >= col_limit)
         ok = false;
-    q = ok ? (size_t)col * stride + p % group + in_off : 0;
+    q = ok ? (size_t)col * stride + (size_t)(p % group) * row_step + in_off : 0;
     return ok;
 }
 
@@ -232,7 +233,8 @@ __device__ __forceinline__ bool sweep_point(uint32_t p, uint32_t n_pts, uint32_t
 __global__ void __launch_bounds__(kSumThreads, 8) line_sum_f64_kernel(
     const Segment<double>* __restrict__ seg, uint32_t n_lines, uint32_t lines_per_split,
     const double* __restrict__ pts, uint32_t n_pts, uint32_t group, uint32_t stride, uint32_t in_off,
-    const uint32_t* __restrict__ cols, uint32_t col_limit, double tol2, double* __restrict__ partial)
+    uint32_t row_step, const uint32_t* __restrict__ cols, uint32_t col_limit, double tol2,
+    double* __restrict__ partial)
 {
     __shared__ SweepSeg s_seg[kSegTile + 1];
     __shared__ double s_red[kSumThreads / 32][4];
@@ -242,7 +244,7 @@ __global__ void __launch_bounds__(kSumThreads, 8) line_sum_f64_kernel(
     const uint32_t l_end = min(n_lines, l_begin + lines_per_split);
     const uint32_t p = blockIdx.x * kSumThreads + threadIdx.x;
     size_t q;
-    const bool ok = sweep_point(p, n_pts, group, stride, in_off, cols, col_limit, q);
+    const bool ok = sweep_point(p, n_pts, group, stride, in_off, row_step, cols, col_limit, q);
     double px = ok ? pts[3 * q] : 0.0, py = ok ? pts[3 * q + 1] : 0.0, pz = ok ? pts[3 * q + 2] : 0.0;
     pvl::cta_centroid<kSumThreads>(px, py, pz, ok ? 1.0 : 0.0, s_red, s_o);  // px.. are 0 when !ok
     px -= s_o[0];
@@ -325,6 +327,7 @@ __global__ void __launch_bounds__(kSumThreads, 12) line_sum_f32x2_kernel(const S
                                                                      uint32_t n_lines, uint32_t lines_per_split,
                                                                      const double* __restrict__ pts, uint32_t n_pts,
                                                                      uint32_t group, uint32_t stride, uint32_t in_off,
+                                                                     uint32_t row_step,
                                                                      const uint32_t* __restrict__ cols,
                                                                      uint32_t col_limit, float tol2,
                                                                      float* __restrict__ partial)
@@ -343,7 +346,7 @@ __global__ void __launch_bounds__(kSumThreads, 12) line_sum_f32x2_kernel(const S
         const uint32_t p = blockIdx.x * (kSumThreads * 2) + t * kSumThreads + threadIdx.x;
         pid[t] = p;
         size_t q;
-        const bool ok = sweep_point(p, n_pts, group, stride, in_off, cols, col_limit, q);
+        const bool ok = sweep_point(p, n_pts, group, stride, in_off, row_step, cols, col_limit, q);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             pv[t][c] = ok ? pts[3 * q + c] : 0.0;
@@ -422,7 +425,8 @@ __global__ void __launch_bounds__(kSumThreads, 12) line_sum_f32x2_kernel(const S
 template <typename T>
 __global__ void __launch_bounds__(kReducePts * kReduceGroups) reduce_partials_kernel(
     uint32_t n_pts, uint32_t n_split, const T* __restrict__ partial, const double* __restrict__ normals, double alpha,
-    double beta, double ux, double uy, double uz, uint32_t group, uint32_t out_stride, uint32_t out_off,
+    double beta, double ux, double uy, double uz, uint32_t group, uint32_t row_step, uint32_t out_stride,
+    uint32_t out_off,
     double* __restrict__ out)
 {
     // kReducePts consecutive points per CTA (their partials are contiguous for every split, so a
@@ -451,7 +455,7 @@ __global__ void __launch_bounds__(kReducePts * kReduceGroups) reduce_partials_ke
         vy += s_v[g][tx][1];
         vz += s_v[g][tx][2];
     }
-    const size_t op = (size_t)(p / group) * out_stride + p % group + out_off;
+    const size_t op = (size_t)(p / group) * out_stride + (size_t)(p % group) * row_step + out_off;
     if (normals) {
         const double v = vx * normals[3 * (size_t)p] + vy * normals[3 * (size_t)p + 1] + vz * normals[3 * (size_t)p + 2];
         out[p] = beta == 0.0 ? alpha * v : beta * out[p] + alpha * v;
@@ -882,7 +886,8 @@ namespace {
 // Shared driver of the N-body sweep: segment table, split sweep, deterministic reduction.
 int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines, const double* positions,
                  const double* line_gamma, uint32_t n_pts, const double* pts, uint32_t group, uint32_t stride,
-                 uint32_t in_off, const uint32_t* cols, uint32_t col_limit, uint32_t out_stride, uint32_t out_off,
+                 uint32_t in_off, uint32_t row_step, const uint32_t* cols, uint32_t col_limit, uint32_t out_stride,
+                 uint32_t out_off,
                  const double* normals, double tol,
                  double alpha, double beta, double ux, double uy, double uz, double* out, void* ws, size_t ws_bytes,
                  cudaStream_t st, const char* who)
@@ -891,7 +896,7 @@ int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint3
         return pvl_fail(PVL_ERR_ARG, "%s: unknown precision %d", who, precision);
     if (n_lines == 0) {
         reduce_partials_kernel<double><<<blocks_for(n_pts, kReducePts), kReducePts * kReduceGroups, 0, st>>>(
-            n_pts, 0, nullptr, normals, alpha, beta, ux, uy, uz, group, out_stride, out_off, out);
+            n_pts, 0, nullptr, normals, alpha, beta, ux, uy, uz, group, row_step, out_stride, out_off, out);
         PVL_LAUNCH_CHECK();
         return PVL_OK;
     }
@@ -910,21 +915,22 @@ int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint3
         auto* part = reinterpret_cast<double*>(base + pvl_segments_workspace(n_lines, PVL_F64));
         if (int r = prep_segments<double>(n_points, n_lines, lines, positions, line_gamma, tol, seg, st))
             return r;
-        line_sum_f64_kernel<<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off, cols,
-                                                          col_limit, pvl::cutoff2<double>(tol), part);
+        line_sum_f64_kernel<<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off,
+                                                          row_step, cols, col_limit, pvl::cutoff2<double>(tol), part);
         PVL_LAUNCH_CHECK();
         reduce_partials_kernel<double><<<blocks_for(n_pts, kReducePts), kReducePts * kReduceGroups, 0, st>>>(
-            n_pts, n_split_used, part, normals, alpha, beta, ux, uy, uz, group, out_stride, out_off, out);
+            n_pts, n_split_used, part, normals, alpha, beta, ux, uy, uz, group, row_step, out_stride, out_off, out);
     } else {
         auto* seg = reinterpret_cast<Segment<float>*>(base);
         auto* part = reinterpret_cast<float*>(base + pvl_segments_workspace(n_lines, PVL_F32));
         if (int r = prep_segments<float>(n_points, n_lines, lines, positions, line_gamma, tol, seg, st))
             return r;
         line_sum_f32x2_kernel<<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off,
-                                                               cols, col_limit, pvl::cutoff2<float>(tol), part);
+                                                               row_step, cols, col_limit, pvl::cutoff2<float>(tol),
+                                                               part);
         PVL_LAUNCH_CHECK();
         reduce_partials_kernel<float><<<blocks_for(n_pts, kReducePts), kReducePts * kReduceGroups, 0, st>>>(
-            n_pts, n_split_used, part, normals, alpha, beta, ux, uy, uz, group, out_stride, out_off, out);
+            n_pts, n_split_used, part, normals, alpha, beta, ux, uy, uz, group, row_step, out_stride, out_off, out);
     }
     PVL_LAUNCH_CHECK();
     return PVL_OK;
@@ -940,7 +946,7 @@ extern "C" int pvl_line_velocity(int precision, uint32_t n_points, uint32_t n_li
     if (n_pts == 0)
         return PVL_OK;
     PVL_REQUIRE(pts); PVL_REQUIRE(out);
-    return run_line_sum(precision, n_points, n_lines, lines, positions, line_gamma, n_pts, pts, n_pts, n_pts, 0,
+    return run_line_sum(precision, n_points, n_lines, lines, positions, line_gamma, n_pts, pts, n_pts, n_pts, 0, 1,
                         nullptr, 0xFFFFFFFFu, n_pts, 0, normals, tol, alpha, beta, 0.0, 0.0, 0.0, out, ws, ws_bytes, (cudaStream_t)stream,
                         "pvl_line_velocity");
 }
@@ -951,6 +957,35 @@ extern "C" size_t pvl_wake_node_velocity_workspace(uint32_t n_lines, uint32_t n_
     return pvl_line_velocity_workspace(n_lines, 2 * n_shed * complete_rows, precision);
 }
 
+extern "C" int pvl_wake_node_velocity_rows(int precision, uint32_t n_points, uint32_t n_lines,
+                                           const uint32_t* lines, const double* positions, const double* line_gamma,
+                                           uint32_t n_shed, uint32_t line_rows, uint32_t complete_rows,
+                                           uint32_t row_begin, uint32_t row_count, uint32_t row_step, uint32_t n_cols,
+                                           const uint32_t* cols, const double* wake_pos, double ux, double uy,
+                                           double uz, double tol, double* node_vel, void* ws, size_t ws_bytes,
+                                           void* stream)
+{
+    if (complete_rows > line_rows)
+        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity: complete_rows %u > line_rows %u", complete_rows,
+                        line_rows);
+    if (row_count > 0 && (row_step == 0 ||
+                          (uint64_t)row_begin + (uint64_t)(row_count - 1) * row_step >= (uint64_t)complete_rows))
+        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity_rows: rows %u + k * %u (k < %u) outside [0, %u)",
+                        row_begin, row_step, row_count, complete_rows);
+    if (!cols && n_cols != 2 * n_shed)
+        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity_cols: without a column list n_cols must be 2 n_shed");
+    if (n_cols == 0 || row_count == 0)
+        return PVL_OK;
+    PVL_REQUIRE(wake_pos); PVL_REQUIRE(node_vel);
+    const uint64_t n_pts = (uint64_t)n_cols * row_count;
+    if (n_pts > 0xFFFFFFFFull)
+        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity: too many nodes");
+    return run_line_sum(precision, n_points, n_lines, lines, positions, line_gamma, (uint32_t)n_pts, wake_pos,
+                        row_count, line_rows + 1, row_begin, row_step, cols, 2 * n_shed, complete_rows, row_begin,
+                        nullptr, tol, 1.0, 0.0, ux, uy, uz, node_vel, ws, ws_bytes, (cudaStream_t)stream,
+                        "pvl_wake_node_velocity");
+}
+
 extern "C" int pvl_wake_node_velocity_cols(int precision, uint32_t n_points, uint32_t n_lines,
                                            const uint32_t* lines, const double* positions, const double* line_gamma,
                                            uint32_t n_shed, uint32_t line_rows, uint32_t complete_rows,
@@ -959,24 +994,12 @@ extern "C" int pvl_wake_node_velocity_cols(int precision, uint32_t n_points, uin
                                            double uz, double tol, double* node_vel, void* ws, size_t ws_bytes,
                                            void* stream)
 {
-    if (complete_rows > line_rows)
-        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity: complete_rows %u > line_rows %u", complete_rows,
-                        line_rows);
     if (row_begin > row_end || row_end > complete_rows)
         return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity_cols: rows [%u, %u) outside [0, %u)", row_begin, row_end,
                         complete_rows);
-    if (!cols && n_cols != 2 * n_shed)
-        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity_cols: without a column list n_cols must be 2 n_shed");
-    if (n_cols == 0 || row_end == row_begin)
-        return PVL_OK;
-    PVL_REQUIRE(wake_pos); PVL_REQUIRE(node_vel);
-    const uint32_t group = row_end - row_begin;
-    const uint64_t n_pts = (uint64_t)n_cols * group;
-    if (n_pts > 0xFFFFFFFFull)
-        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity: too many nodes");
-    return run_line_sum(precision, n_points, n_lines, lines, positions, line_gamma, (uint32_t)n_pts, wake_pos, group,
-                        line_rows + 1, row_begin, cols, 2 * n_shed, complete_rows, row_begin, nullptr, tol, 1.0, 0.0, ux, uy, uz,
-                        node_vel, ws, ws_bytes, (cudaStream_t)stream, "pvl_wake_node_velocity");
+    return pvl_wake_node_velocity_rows(precision, n_points, n_lines, lines, positions, line_gamma, n_shed, line_rows,
+                                       complete_rows, row_begin, row_end - row_begin, 1, n_cols, cols, wake_pos, ux,
+                                       uy, uz, tol, node_vel, ws, ws_bytes, stream);
 }
 
 extern "C" int pvl_wake_node_velocity(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines,

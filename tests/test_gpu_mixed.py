@@ -159,6 +159,35 @@ def test_wake_node_velocity_column_and_row_split():
     torch.cuda.synchronize()
     want = full.reshape(2 * S, complete, 3)[torch.as_tensor(cols.astype(np.int64), device="cuda")]
     assert torch.allclose(dedup, want, rtol=1e-13, atol=1e-13)
+    # every other row (pvl_wake_node_velocity_rows, step 2): those rows as in the full sweep,
+    # the rows between untouched
+    stepped = torch.full_like(full, float("nan"))
+    count = (complete - 5 + 1) // 2
+    _lib.call("pvl_wake_node_velocity_rows", _lib.PVL_F64, mesh.n_points, mesh.n_lines, ptr(d["lines"]), ptr(pos),
+              ptr(lg), S, R, complete, 5, count, 2, 2 * S, None, ptr(wp), float(u[0]), float(u[1]), float(u[2]),
+              case.tol, ptr(stepped), ptr(ws), nb, s)
+    torch.cuda.synchronize()
+    assert torch.allclose(stepped[:, :, 5::2], full[:, :, 5::2], rtol=1e-13, atol=1e-13)
+    assert torch.isnan(stepped[:, :, 6::2]).all() and torch.isnan(stepped[:, :, :5]).all()
+    with pytest.raises(ValueError):  # the last listed row must lie below complete_rows
+        _lib.call("pvl_wake_node_velocity_rows", _lib.PVL_F64, mesh.n_points, mesh.n_lines, ptr(d["lines"]),
+                  ptr(pos), ptr(lg), S, R, complete, 5, count + 1, 2, 2 * S, None, ptr(wp), float(u[0]),
+                  float(u[1]), float(u[2]), case.tol, ptr(stepped), ptr(ws), nb, s)
+    # the rows between from their column's neighbours 1 and 3 rows away (pvl_wake_interp_rows)
+    interp = full.clone()
+    last = complete - 4 if (complete - 4) % 2 == 1 else complete - 5
+    _lib.call("pvl_wake_interp_rows", 2 * S, complete, 7, last, ptr(interp), s)
+    torch.cuda.synchronize()
+    f = full.reshape(2 * S, complete, 3)
+    i = torch.arange(7, last + 1, 2, device="cuda")
+    want = (9.0 * (f[:, i - 1] + f[:, i + 1]) - (f[:, i - 3] + f[:, i + 3])) / 16.0
+    got = interp.reshape(2 * S, complete, 3)
+    assert torch.allclose(got[:, i], want, rtol=1e-15, atol=1e-15)
+    keep = torch.ones(complete, dtype=torch.bool, device="cuda")
+    keep[i] = False
+    assert torch.equal(got[:, keep], f[:, keep])
+    with pytest.raises(ValueError):  # an interpolated row needs the rows 3 above it
+        _lib.call("pvl_wake_interp_rows", 2 * S, complete, 7, complete - 3, ptr(interp), s)
 
 
 def _mixed_engine(case, **kw):
@@ -235,6 +264,37 @@ def test_mixed_trajectory_tracks_plain():
     print(f"max trajectory difference over 250 steps: {worst:.3e}")
     assert worst <= MIXED_TOL, worst
     assert mixed.stats["fallbacks"] == 0
+
+
+def test_mixed_trajectory_with_interpolated_far_rows():
+    """As test_mixed_trajectory_tracks_plain, with the advection of every other node row from
+    row 48 on interpolated (advect_interp_row=48; 52 of the 100 rows): every step's circulation
+    is still within 1e-10 of the plain FP64 run's."""
+    from pyvl_b200.cvl import Mesh
+    from pyvl_b200.engine import MixedSolverEngine, SolverEngine, wake_spec_from_te
+    from pyvl_b200.workloads import flapping
+
+    case = flapping(ns=64, nc=16, line_rows=100)
+    mesh = Mesh(case.n_points, case.elements)
+
+    def spec():
+        return wake_spec_from_te(mesh, case.te_node_pairs, case.line_rows, case.t0)
+
+    plain = SolverEngine(mesh, case.freestream, case.tol, spec())
+    mixed = MixedSolverEngine(mesh, case.freestream, case.tol, spec(), advect_interp_row=48)
+    worst = 0.0
+    for it in range(250):
+        t = it * case.dt
+        p, v = case.positions_at(t), case.velocities_at(t)
+        plain.step(t, p, v)
+        mixed.step(t, p, v)
+        a, b = mixed.gamma_host(), plain.gamma_host()
+        worst = max(worst, float(np.linalg.norm(a - b) / np.linalg.norm(b)))
+    print(f"max trajectory difference over 250 steps: {worst:.3e}")
+    assert worst <= MIXED_TOL, worst
+    assert mixed.stats["fallbacks"] == 0
+    with pytest.raises(ValueError):
+        MixedSolverEngine(mesh, case.freestream, case.tol, spec(), advect_interp_row=47)
 
 
 def test_gmres_graph_replay_is_bitwise_identical():
