@@ -758,7 +758,7 @@ def main() -> None:
             if record is not None:
                 warm = WarmStart(eng, None, record=True)
         else:
-            eng = MixedSolverEngine(mesh, case.freestream, case.tol, spec())
+            eng = MixedSolverEngine(mesh, case.freestream, case.tol, spec(), cp_patches=case.smooth_patches)
             warm = {"learned": lambda: WarmStart(eng, mlp), "jacobi": lambda: WarmStart(eng, jacobi=True),
                     "previous": lambda: None}[seed_mode]()
         end = n_steps if last is None else last
@@ -1031,7 +1031,11 @@ def main() -> None:
                                   "refreshes_in_window": mx["refreshes_in_window"],
                                   "refresh_failures": mx["refresh_failures"],
                                   "initial_rel_residual_median": mx["initial_rel_residual_median"],
-                                  "warm_start_training": train_info},
+                                  "warm_start_training": train_info,
+                                  "far_wake": "explicit wake term of rows >= 64 at every other chordwise control "
+                                              "point, of rows >= 192 every other spanwise too (quintic midpoint "
+                                              "rule within each half wing); advection FP32 from row 8, every other "
+                                              "row from row 128 (cubic midpoint); error: trajectory"},
                 "speedup_mixed_over_plain": results["plain"]["ms"] / mx["ms"],
             },
             "warm_start": {**seed_arms,

@@ -259,6 +259,23 @@ int pvl_wake_node_velocity_rows(int precision, uint32_t n_points, uint32_t n_lin
 int pvl_wake_interp_rows(uint32_t n_cols, uint32_t complete_rows, uint32_t row_first, uint32_t row_last,
                          double* node_vel, void* stream);
 
+/* out[k] = pts[index[k]] (3 doubles each) for k < n; an index outside [0, n_pts) writes NaN.
+ * Gathers the control points at which the mixed path evaluates the far wake term.  No
+ * reference counterpart. */
+int pvl_gather_points(uint32_t n, const uint32_t* index, uint32_t n_pts, const double* pts, double* out,
+                      void* stream);
+
+/* out[p] += n_p . sum_{k in [offsets[p], offsets[p+1])} weights[k] values[entries[k]] for p < n_cp:
+ * velocities (values, (n_values, 3)) known at some points, interpolated to every control point
+ * by a stencil and projected on its normal (normals (n_cp, 3)), terms summed in stored order.
+ * offsets has n_cp + 1 entries, entries and weights n_entries; a range outside [0, n_entries)
+ * or an entry outside [0, n_values) makes the point's result NaN.  The mixed path's far wake
+ * term (the reference evaluates the wake at every control point,
+ * python/pyvl/wake_models.py:219-223). */
+int pvl_stencil_normal_add(uint32_t n_cp, const uint32_t* offsets, uint32_t n_entries, const uint32_t* entries,
+                           const double* weights, uint32_t n_values, const double* values, const double* normals,
+                           double* out, void* stream);
+
 /* Advance wake node rows (explicit Euler) from `old_pos` into `new_pos` (both
  * (n_shed, 2, line_rows + 1, 3)): new[:, :, i+1] = old[:, :, i] + node_vel[:, :, i] * dt for
  * i < complete_rows; row 0 pinned to the bordering body nodes; rows beyond complete_rows

@@ -186,6 +186,79 @@ __global__ void interp_rows_kernel(uint32_t n_cols, uint32_t complete, uint32_t 
     col[(size_t)i * 3] = (9.0 * (b + d) - (a + f)) * 0.0625;
 }
 
+// out[k] = pts[index[k]] (3 doubles); an index outside [0, n_pts) gives NaN.
+__global__ void gather_points_kernel(uint32_t n, const uint32_t* __restrict__ index, uint32_t n_pts,
+                                     const double* __restrict__ pts, double* __restrict__ out)
+{
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (uint64_t)n * 3)
+        return;
+    const uint32_t k = (uint32_t)(e / 3), c = (uint32_t)(e % 3);
+    const uint32_t i = index[k];
+    out[e] = i < n_pts ? pts[(size_t)i * 3 + c] : __longlong_as_double(0x7FF8000000000000ll);
+}
+
+// out[p] += n_p . sum_k weights[k] values[entries[k]] over k in [offsets[p], offsets[p+1]);
+// one thread per point, terms summed in stored order.  A range outside [0, n_entries) or an
+// entry outside [0, n_values) makes the point's sum NaN (nothing outside the arrays is read).
+__global__ void stencil_normal_add_kernel(uint32_t n_cp, const uint32_t* __restrict__ offsets, uint32_t n_entries,
+                                          const uint32_t* __restrict__ entries, const double* __restrict__ weights,
+                                          uint32_t n_values, const double* __restrict__ values,
+                                          const double* __restrict__ normals, double* __restrict__ out)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n_cp)
+        return;
+    double vx = 0.0, vy = 0.0, vz = 0.0;
+    const uint32_t k0 = offsets[p], k1 = offsets[p + 1];
+    if (k0 > k1 || k1 > n_entries) {
+        out[p] = __longlong_as_double(0x7FF8000000000000ll);
+        return;
+    }
+    for (uint32_t k = k0; k < k1; ++k) {
+        const uint32_t j = entries[k];
+        const double w = weights[k];
+        if (j >= n_values) {
+            vx = __longlong_as_double(0x7FF8000000000000ll);
+            continue;
+        }
+        const double* v = values + (size_t)j * 3;
+        vx = fma(w, v[0], vx);
+        vy = fma(w, v[1], vy);
+        vz = fma(w, v[2], vz);
+    }
+    const double* n = normals + (size_t)p * 3;
+    out[p] += n[0] * vx + n[1] * vy + n[2] * vz;
+}
+
+extern "C" int pvl_gather_points(uint32_t n, const uint32_t* index, uint32_t n_pts, const double* pts, double* out,
+                                 void* stream)
+{
+    if (n == 0)
+        return PVL_OK;
+    PVL_REQUIRE(index); PVL_REQUIRE(pts); PVL_REQUIRE(out);
+    gather_points_kernel<<<blocks_for((uint64_t)n * 3, 256), 256, 0, (cudaStream_t)stream>>>(n, index, n_pts, pts,
+                                                                                             out);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_stencil_normal_add(uint32_t n_cp, const uint32_t* offsets, uint32_t n_entries,
+                                      const uint32_t* entries, const double* weights, uint32_t n_values,
+                                      const double* values, const double* normals, double* out, void* stream)
+{
+    if (n_cp == 0)
+        return PVL_OK;
+    PVL_REQUIRE(offsets); PVL_REQUIRE(normals); PVL_REQUIRE(out);
+    if (n_entries) {
+        PVL_REQUIRE(entries); PVL_REQUIRE(weights); PVL_REQUIRE(values);
+    }
+    stencil_normal_add_kernel<<<blocks_for(n_cp, 128), 128, 0, (cudaStream_t)stream>>>(
+        n_cp, offsets, n_entries, entries, weights, n_values, values, normals, out);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
 extern "C" int pvl_wake_fold_implicit(uint32_t n_cp, uint32_t n_shed, const double* implicit, const uint32_t* adjacent,
                                       double* A, uint32_t lda, void* stream)
 {

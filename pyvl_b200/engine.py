@@ -100,6 +100,67 @@ def wake_node_columns(bordering_nodes):
     return rep, cols.astype(np.uint32), slot.astype(np.uint32)
 
 
+# midpoint value of the quintic through six equally spaced samples at -5, -3, -1, +1, +3, +5
+_MID6 = ((-5, 3.0 / 256), (-3, -25.0 / 256), (-1, 150.0 / 256), (1, 150.0 / 256), (3, -25.0 / 256), (5, 3.0 / 256))
+
+
+def _midpoint_rules(n: int) -> list:
+    """Per sample of a smooth run of n: [(sample, weight), ...].  Odd samples with five samples
+    on either side take the quintic midpoint rule of their even neighbours, the rest are
+    evaluated ([(itself, 1.0)])."""
+    return [[(j + o, w) for o, w in _MID6] if j % 2 and 5 <= j <= n - 6 else [(j, 1.0)] for j in range(n)]
+
+
+def far_wake_stencil(n_rings: int, patches) -> dict:
+    """Where the far wake term is evaluated and how the other control points get it.
+
+    ``patches``: (ring0, n_span, n_chord) blocks of rings ring0 + i * n_chord + j whose control
+    points (and normals) are smooth functions of (i, j) — a kink, e.g. a twist linear in |y|,
+    splits a wing into two patches.  Rings outside every patch are always evaluated.  Two
+    bands: in the chord band a point takes its chordwise rule (``_midpoint_rules`` along j), in
+    the span band the product of its spanwise and chordwise rules.  Returns ``index`` (rings to
+    gather: the span band's evaluated rings first, n_span_eval of them, then the rest of the
+    chord band's, n_chord_eval in all) and the CSR stencil (offsets, entries, weights) over the
+    values [chord band at the n_chord_eval points; span band at the first n_span_eval]: ring p
+    receives sum_k weights[k] values[entries[k]] in both bands together.
+    """
+    chord_rule = [[(p, 1.0)] for p in range(n_rings)]
+    span_rule = [[(p, 1.0)] for p in range(n_rings)]
+    owner = np.full(n_rings, -1, np.int64)
+    for k, (r0, ns, nc) in enumerate(patches):
+        r0, ns, nc = int(r0), int(ns), int(nc)
+        if r0 < 0 or ns <= 0 or nc <= 0 or r0 + ns * nc > n_rings:
+            raise ValueError(f"patch {k} ({r0}, {ns}, {nc}) outside the {n_rings} rings")
+        blk = owner[r0:r0 + ns * nc]
+        if (blk >= 0).any():
+            raise ValueError(f"patch {k} overlaps another patch")
+        blk[:] = k
+        cr, sr = _midpoint_rules(nc), _midpoint_rules(ns)
+        for i in range(ns):
+            for j in range(nc):
+                p = r0 + i * nc + j
+                chord_rule[p] = [(r0 + i * nc + jj, w) for jj, w in cr[j]]
+                span_rule[p] = [(r0 + ii * nc + j, w) for ii, w in sr[i]]
+    chord_eval = np.array([len(r) == 1 for r in chord_rule])
+    both_eval = chord_eval & np.array([len(r) == 1 for r in span_rule])
+    index = np.concatenate([np.nonzero(both_eval)[0], np.nonzero(chord_eval & ~both_eval)[0]])
+    pos = np.full(n_rings, -1, np.int64)
+    pos[index] = np.arange(index.size)
+    n_chord, n_span = int(index.size), int(both_eval.sum())
+    offsets = np.zeros(n_rings + 1, np.int64)
+    entries, weights = [], []
+    for p in range(n_rings):
+        terms = [(int(pos[q]), w) for q, w in chord_rule[p]]
+        for q, ws in span_rule[p]:
+            terms += [(n_chord + int(pos[qq]), ws * wc) for qq, wc in chord_rule[q]]
+        entries += [e for e, _ in terms]
+        weights += [w for _, w in terms]
+        offsets[p + 1] = len(entries)
+    return {"index": index.astype(np.uint32), "n_chord_eval": n_chord, "n_span_eval": n_span,
+            "offsets": offsets.astype(np.uint32), "entries": np.asarray(entries, np.uint32),
+            "weights": np.asarray(weights, np.float64)}
+
+
 def _node_velocity_workspace(n_lines: int, n_cols: int, rows: int, precision: int) -> int:
     """Largest sweep workspace over every row count 1..rows the growing wake passes through."""
     return max(_lib.query("pvl_line_velocity_workspace", n_lines, n_cols * c, precision) for c in range(1, rows + 1))
@@ -196,6 +257,7 @@ class SolverEngine:
                 raise ValueError("closed groups must be contiguous ranges of rings")
             self.goff = to_device_u32(goff, self.dev)
         self.wake = None
+        self._far = None  # far-wake stencil of the explicit wake term (MixedSolverEngine cp_patches)
         if wake is not None:
             self._init_wake(wake)
         self._ws_bytes = self._workspace_bytes()
@@ -386,7 +448,9 @@ class SolverEngine:
         strip, in strip order) at the control points, folded into the columns of the rings
         that shed them; the explicit term sweeps the lines of the rows shed so far with the
         line circulations of rows >= 1, in FP64 for the first ``n_near_lines`` lines and in
-        FP32 beyond (all FP64 unless a subclass says otherwise, or with ``fp64_only``)."""
+        FP32 beyond (all FP64 unless a subclass says otherwise, or with ``fp64_only``).  With a
+        far-wake stencil (``_far``, the mixed engine's ``cp_patches``) and not ``fp64_only``, the
+        rows from its chord row on are evaluated at part of the control points only."""
         s = stream_ptr()
         w = self.wake
         S, R = w["S"], w["R"]
@@ -407,6 +471,10 @@ class SolverEngine:
         lg = w["rm_line_gamma"]
         _lib.call("pvl_line_circulation", rm.n_lines, ptr(d["map_offsets"]), ptr(d["map_entries"]), ptr(crs), 0,
                   ptr(lg), s)
+        far = None if fp64_only else self._far
+        if far is not None and min(w["step_count"], R) > far["chord_row"]:
+            self._far_wake_term(active, lg, wpos, s)
+            return
         near = active if fp64_only else min(self.n_near_lines, active)
         lines = d["lines"]
         _lib.call("pvl_line_velocity", _lib.PVL_F64, rm.n_points, near, ptr(lines), ptr(wpos), ptr(lg), self.P,
@@ -415,6 +483,32 @@ class SolverEngine:
             _lib.call("pvl_line_velocity", _lib.PVL_F32, rm.n_points, active - near, lines.data_ptr() + 8 * near,
                       ptr(wpos), lg.data_ptr() + 8 * near, self.P, ptr(self.cps), ptr(self.nrm), self.tol, 1.0, 1.0,
                       ptr(self.rhs), ws, nb, s)
+
+    def _far_wake_term(self, active: int, lg: torch.Tensor, wpos: torch.Tensor, s) -> None:
+        """The explicit wake term with the far rows interpolated across the control points.
+
+        Rows below the chord row: every control point, into the RHS.  Rows from the chord row to
+        the span row: velocities at the chord band's evaluated points; rows beyond: at the span
+        band's (a prefix of the same gathered points); then every RHS entry takes its stencil of
+        the two (pvl_stencil_normal_add)."""
+        f, w = self._far, self.wake
+        rm, d = w["rm"], w["rm_d"]
+        lines, up = d["lines"], w["lines_upto"]
+        a = up[f["chord_row"]]
+        b = active if f["span_row"] is None else max(a, min(up[f["span_row"]], active))
+        ws, nb = ptr(self.ws), self._ws_bytes
+        n_c, n_s = f["n_chord_eval"], f["n_span_eval"]
+        pts, vals = f["pts"], f["vals"]
+        _lib.call("pvl_line_velocity", _lib.PVL_F64, rm.n_points, a, ptr(lines), ptr(wpos), ptr(lg), self.P,
+                  ptr(self.cps), ptr(self.nrm), self.tol, 1.0, 1.0, ptr(self.rhs), ws, nb, s)
+        _lib.call("pvl_gather_points", n_c, ptr(f["index"]), self.P, ptr(self.cps), ptr(pts), s)
+        _lib.call("pvl_line_velocity", _lib.PVL_F64, rm.n_points, b - a, lines.data_ptr() + 8 * a, ptr(wpos),
+                  lg.data_ptr() + 8 * a, n_c, ptr(pts), None, self.tol, 1.0, 0.0, ptr(vals), ws, nb, s)
+        _lib.call("pvl_line_velocity", _lib.PVL_F64, rm.n_points, active - b, lines.data_ptr() + 8 * b, ptr(wpos),
+                  lg.data_ptr() + 8 * b, n_s, ptr(pts), None, self.tol, 1.0, 0.0, vals.data_ptr() + 24 * n_c,
+                  ws, nb, s)
+        _lib.call("pvl_stencil_normal_add", self.P, ptr(f["offsets"]), f["entries"].numel(), ptr(f["entries"]),
+                  ptr(f["weights"]), n_c + n_s, ptr(vals), ptr(self.nrm), ptr(self.rhs), s)
 
     def solve(self) -> None:
         ws, nb = ptr(self.ws), self._ws_bytes
@@ -591,6 +685,16 @@ class MixedSolverEngine(SolverEngine):
       slowly along a node column.  On the 128x32 flapping wing, 2000 steps, interpolating from
       row 128 keeps every step's circulation within 1.4e-11 of the plain FP64 run (from row 64:
       5.6e-11; row 32: 1.4e-10, over the 1e-10 bar).
+    * With ``cp_patches`` (smooth (ring0, n_span, n_chord) blocks of the body's ring grid,
+      ``far_wake_stencil``) the explicit wake term of the rows from ``wake_chord_row`` on is
+      evaluated at every other chordwise control point (plus those within five of a patch
+      edge) and interpolated between them by the quintic midpoint rule, and from
+      ``wake_span_row`` on (None: never) at every other spanwise one too: seen from the body,
+      wake rows four or more chords away vary slowly across a patch.  On the 128x32 flapping
+      wing (two patches, split at the root where the twist has its kink), 2000 steps, every
+      step's circulation stays within 1.4e-11 of the plain FP64 run with the chordwise rule
+      from row 64 and within 1.0e-11 with both from row 192; the cubic rule, the product
+      rule from row 64, or a patch across the kink go over the 1e-10 bar.  Default off.
     ``judge()`` re-assembles the step's system entirely in FP64 and solves it with the FP64
     factorisation, which is how the mixed answer's error is measured.
     """
@@ -599,7 +703,8 @@ class MixedSolverEngine(SolverEngine):
                  refresh: int | None = None, near_rows: int | None = None, advect_near_rows: int = 8,
                  gmres_tol: float = 1e-12, max_iter: int = 20, async_refresh: bool = True,
                  refresh_on_iters: int = 5, use_graphs: bool = True, wake_self_induction: bool = False,
-                 device_solve: bool = True, refresh_excess: int = 128, advect_interp_row: int | None = 128):
+                 device_solve: bool = True, refresh_excess: int = 128, advect_interp_row: int | None = 128,
+                 cp_patches=None, wake_chord_row: int = 64, wake_span_row: int | None = 192):
         super().__init__(mesh, freestream, tol, wake, closed_groups, wake_self_induction)
         if advect_interp_row is not None and (int(advect_interp_row) < 4 or int(advect_interp_row) % 2):
             raise ValueError("advect_interp_row must be even and at least 4 (or None)")
@@ -667,6 +772,8 @@ class MixedSolverEngine(SolverEngine):
         need = 0
         if self.wake is not None:
             need = max(need, self._init_row_major_wake(near_rows, advect_near_rows))
+            if cp_patches is not None:
+                need = max(need, self._init_far_stencil(cp_patches, wake_chord_row, wake_span_row))
         if need + 256 > self._ws_bytes:
             self._ws_bytes = need + 256
             self.ws = torch.empty(self._ws_bytes, dtype=torch.uint8, device=self.dev)
@@ -692,6 +799,32 @@ class MixedSolverEngine(SolverEngine):
             if c > nr:
                 need.append(_lib.query("pvl_line_velocity_workspace", L, nc * (c - nr), _lib.PVL_F32))
         return max(need)
+
+    def _init_far_stencil(self, patches, chord_row: int, span_row: int | None) -> int:
+        """Device copy of far_wake_stencil(patches) and the workspace of its two sweeps."""
+        w = self.wake
+        R = w["R"]
+        if self.near_rows < R:
+            raise ValueError("cp_patches needs the explicit wake term in FP64 (near_rows None)")
+        chord_row = int(chord_row)
+        if chord_row < 1 or (span_row is not None and int(span_row) < chord_row):
+            raise ValueError("need 1 <= wake_chord_row <= wake_span_row")
+        span_row = None if span_row is None else min(int(span_row), R)
+        chord_row = min(chord_row, R)
+        plan = far_wake_stencil(self.P, patches)
+        n_c, n_s = plan["n_chord_eval"], plan["n_span_eval"]
+        f64 = dict(dtype=torch.float64, device=self.dev)
+        self._far = {
+            "chord_row": chord_row, "span_row": span_row, "n_chord_eval": n_c, "n_span_eval": n_s,
+            "index": to_device_u32(plan["index"], self.dev), "offsets": to_device_u32(plan["offsets"], self.dev),
+            "entries": to_device_u32(plan["entries"], self.dev),
+            "weights": torch.as_tensor(plan["weights"]).to(self.dev),
+            "pts": torch.zeros((max(n_c, 1), 3), **f64), "vals": torch.zeros((max(n_c + n_s, 1), 3), **f64),
+        }
+        up, n_all = w["lines_upto"], w["rm"].n_lines
+        b = n_all if span_row is None else up[span_row]
+        return max(_lib.query("pvl_line_velocity_workspace", max(b - up[chord_row], 1), max(n_c, 1), _lib.PVL_F64),
+                   _lib.query("pvl_line_velocity_workspace", max(n_all - b, 1), max(n_s, 1), _lib.PVL_F64))
 
     # ------------------------------------------------------------------ preconditioner
     def refresh_preconditioner(self, wait: bool = True) -> None:

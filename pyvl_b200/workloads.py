@@ -155,6 +155,9 @@ class Case:
     s_ref: float = 1.0                           # reference area for CL
     t0: float = 0.0                              # wake model start time (first dt)
     meta: dict = field(default_factory=dict)
+    # (ring0, n_span, n_chord) blocks of rings ring0 + i * n_chord + j over which the control
+    # points are smooth in (i, j) (MixedSolverEngine cp_patches); empty: not a structured grid
+    smooth_patches: tuple = ()
 
     @property
     def n_points(self) -> int:
@@ -194,6 +197,15 @@ def _grid_wing(xs: npt.NDArray, ys: npt.NDArray) -> tuple:
     loops = np.stack([n00, n00 + nc1, n00 + nc1 + 1, n00 + 1], axis=1).astype(np.uint32)
     te = np.stack([np.arange(ns) * nc1 + nc, (np.arange(ns) + 1) * nc1 + nc], axis=1)
     return pos, [loops[k] for k in range(loops.shape[0])], te.astype(np.uint32)
+
+
+def _root_split(ns: int, nc: int) -> tuple:
+    """The two half wings of a _grid_wing whose shape or motion depends on |y| (a kink at the
+    root, y = 0, between strips ns/2 - 1 and ns/2); one patch for an odd strip count."""
+    if ns % 2:
+        return ((0, ns, nc),)
+    h = ns // 2
+    return ((0, h, nc), (h * nc, h, nc))
 
 
 def flat_wing(ns: int = 16, nc: int = 4, span: float = 8.0, chord: float = 1.0,
@@ -239,6 +251,7 @@ def swept_pitching(ns: int = 64, nc: int = 16, seed: int = 1, span: float = 8.0,
         positions=pos, elements=elements, kinematics=kin,
         freestream=np.array([1.0, 0.0, 0.0]), dt=dt, nt=nt, line_rows=line_rows,
         te_node_pairs=te, s_ref=s_ref, t0=-dt, meta={"k": k, "seed": seed},
+        smooth_patches=_root_split(ns, nc),
     )
 
 
@@ -262,7 +275,7 @@ def flapping(ns: int = 128, nc: int = 32, span: float = 8.0, chord: float = 1.0,
         positions=pos, elements=elements, kinematics=kin,
         freestream=np.array([np.cos(a), 0.0, np.sin(a)]), dt=dt, nt=nt,
         line_rows=line_rows, te_node_pairs=te, s_ref=span * chord, t0=-dt,
-        meta={"k": k},
+        meta={"k": k}, smooth_patches=_root_split(ns, nc),
     )
 
 

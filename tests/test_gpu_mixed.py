@@ -297,6 +297,108 @@ def test_mixed_trajectory_with_interpolated_far_rows():
         MixedSolverEngine(mesh, case.freestream, case.tol, spec(), advect_interp_row=47)
 
 
+def test_far_stencil_kernels_match_numpy():
+    """pvl_gather_points and pvl_stencil_normal_add against numpy on seeded data (bit-exact
+    gather; the stencil's sums to rounding), out-of-range indices giving NaN."""
+    import torch
+
+    from pyvl_b200 import _lib
+    from pyvl_b200.device import ptr, stream_ptr, to_device_u32
+
+    rng = np.random.default_rng(7)
+    n_pts, n = 300, 257
+    pts = rng.normal(size=(n_pts, 3))
+    index = rng.integers(0, n_pts, n).astype(np.uint32)
+    index[5] = n_pts  # out of range
+    # every device array held by a name until the results are read back: a temporary freed
+    # before the launch would hand its block to the next allocation
+    d_pts = torch.tensor(pts, device="cuda")
+    d_out = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    d_index = to_device_u32(index)
+    _lib.call("pvl_gather_points", n, ptr(d_index), n_pts, ptr(d_pts), ptr(d_out), stream_ptr())
+    got = d_out.cpu().numpy()
+    ok = np.arange(n) != 5
+    assert np.array_equal(got[ok], pts[index[ok].astype(np.int64)])
+    assert np.isnan(got[5]).all()
+
+    n_cp, n_val = 500, 120
+    counts = rng.integers(0, 43, n_cp)
+    offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint32)
+    entries = rng.integers(0, n_val, int(offsets[-1])).astype(np.uint32)
+    entries[offsets[3]] = n_val if counts[3] else entries[offsets[3]]
+    weights = rng.normal(size=int(offsets[-1]))
+    vals, nrm, out0 = rng.normal(size=(n_val, 3)), rng.normal(size=(n_cp, 3)), rng.normal(size=n_cp)
+    d_o = torch.tensor(out0, device="cuda")
+    d_off, d_ent = to_device_u32(offsets), to_device_u32(entries)
+    d_w, d_v, d_n = (torch.tensor(a, device="cuda") for a in (weights, vals, nrm))
+    _lib.call("pvl_stencil_normal_add", n_cp, ptr(d_off), entries.size, ptr(d_ent), ptr(d_w), n_val, ptr(d_v),
+              ptr(d_n), ptr(d_o), stream_ptr())
+    got = d_o.cpu().numpy()
+    # offsets past the entries: NaN for the points concerned, nothing read outside the arrays
+    bad_off = offsets.copy()
+    bad_off[7:] += 5
+    d_bad = to_device_u32(bad_off)
+    d_o2 = torch.zeros(n_cp, dtype=torch.float64, device="cuda")
+    _lib.call("pvl_stencil_normal_add", n_cp, ptr(d_bad), entries.size, ptr(d_ent), ptr(d_w), n_val, ptr(d_v),
+              ptr(d_n), ptr(d_o2), stream_ptr())
+    got2 = d_o2.cpu().numpy()
+    past = bad_off[1:] > entries.size
+    assert np.isnan(got2[past]).all() and past.any()
+    want = out0.copy()
+    for p in range(n_cp):
+        k = slice(int(offsets[p]), int(offsets[p + 1]))
+        e = entries[k].astype(np.int64)
+        if (e >= n_val).any():
+            want[p] = np.nan
+            continue
+        want[p] += nrm[p] @ (weights[k, None] * vals[e]).sum(0)
+    bad = np.isnan(want)
+    assert bad[3] == bool(counts[3]) and np.isnan(got[bad]).all()
+    np.testing.assert_allclose(got[~bad], want[~bad], rtol=1e-12, atol=1e-12)
+
+
+def test_mixed_trajectory_with_far_wake_stencil():
+    """As test_mixed_trajectory_tracks_plain, with the explicit wake term of the far rows
+    evaluated at part of the control points and interpolated across each half wing
+    (cp_patches; 200 wake rows, chordwise from row 64 = 4 chords, spanwise too from row 160 =
+    10 chords, where the coarser 64 x 16 grid's spacing relative to the distance matches the
+    128 x 32 wing's from row 192): every step's circulation is still within 1e-10 of the plain
+    FP64 run's, and the judged step (everything re-assembled in FP64) agrees with the
+    interpolated one to the same bar."""
+    from pyvl_b200.cvl import Mesh
+    from pyvl_b200.engine import MixedSolverEngine, SolverEngine, wake_spec_from_te
+    from pyvl_b200.workloads import flapping
+
+    case = flapping(ns=64, nc=16, line_rows=200)
+    mesh = Mesh(case.n_points, case.elements)
+
+    def spec():
+        return wake_spec_from_te(mesh, case.te_node_pairs, case.line_rows, case.t0)
+
+    plain = SolverEngine(mesh, case.freestream, case.tol, spec())
+    mixed = MixedSolverEngine(mesh, case.freestream, case.tol, spec(), cp_patches=case.smooth_patches,
+                              wake_chord_row=64, wake_span_row=160)
+    assert mixed._far["n_chord_eval"] < mixed.P
+    worst = 0.0
+    for it in range(250):
+        t = it * case.dt
+        p, v = case.positions_at(t), case.velocities_at(t)
+        plain.step(t, p, v)
+        mixed.step(t, p, v)
+        a, b = mixed.gamma_host(), plain.gamma_host()
+        worst = max(worst, float(np.linalg.norm(a - b) / np.linalg.norm(b)))
+    print(f"max trajectory difference over 250 steps: {worst:.3e}")
+    assert worst <= MIXED_TOL, worst
+    assert mixed.stats["fallbacks"] == 0
+    t = 250 * case.dt
+    assert mixed.step_judged(t, case.positions_at(t), case.velocities_at(t)) <= MIXED_TOL
+    with pytest.raises(ValueError):
+        MixedSolverEngine(mesh, case.freestream, case.tol, spec(), cp_patches=case.smooth_patches, near_rows=10)
+    with pytest.raises(ValueError):
+        MixedSolverEngine(mesh, case.freestream, case.tol, spec(), cp_patches=case.smooth_patches,
+                          wake_chord_row=80, wake_span_row=40)
+
+
 def test_gmres_graph_replay_is_bitwise_identical():
     """The GMRES pieces replayed as captured CUDA graphs give the same circulations, bit for
     bit, as launching them directly."""
