@@ -758,7 +758,8 @@ def main() -> None:
             if record is not None:
                 warm = WarmStart(eng, None, record=True)
         else:
-            eng = MixedSolverEngine(mesh, case.freestream, case.tol, spec(), cp_patches=case.smooth_patches)
+            eng = MixedSolverEngine(mesh, case.freestream, case.tol, spec(), cp_patches=case.smooth_patches,
+                                    wake_col_runs=case.wake_col_runs)
             warm = {"learned": lambda: WarmStart(eng, mlp), "jacobi": lambda: WarmStart(eng, jacobi=True),
                     "previous": lambda: None}[seed_mode]()
         end = n_steps if last is None else last
@@ -1035,7 +1036,9 @@ def main() -> None:
                                   "far_wake": "explicit wake term of rows >= 64 at every other chordwise control "
                                               "point, of rows >= 192 every other spanwise too (quintic midpoint "
                                               "rule within each half wing); advection FP32 from row 8, every other "
-                                              "row from row 128 (cubic midpoint); error: trajectory"},
+                                              "node column from row 64 (quintic midpoint rule within each half "
+                                              "wing), every other row from row 128 (cubic midpoint); error: "
+                                              "trajectory"},
                 "speedup_mixed_over_plain": results["plain"]["ms"] / mx["ms"],
             },
             "warm_start": {**seed_arms,

@@ -259,6 +259,18 @@ int pvl_wake_node_velocity_rows(int precision, uint32_t n_points, uint32_t n_lin
 int pvl_wake_interp_rows(uint32_t n_cols, uint32_t complete_rows, uint32_t row_first, uint32_t row_last,
                          double* node_vel, void* stream);
 
+/* node_vel[c, r] = sum_{k in [offsets[c], offsets[c+1])} weights[k] sub_vel[entries[k], r] for the
+ * rows r in [row_begin, row_end) of every column c < n_cols; node_vel is (n_cols, complete_rows, 3)
+ * and sub_vel (n_sub, complete_rows, 3), the velocities of the wake nodes of some columns (from
+ * pvl_wake_node_velocity_rows with those columns' list).  offsets has n_cols + 1 entries, entries
+ * and weights n_entries; a range outside [0, n_entries) or an entry outside [0, n_sub) writes NaN.
+ * The mixed path's advection of far rows at every other node column (no reference counterpart:
+ * the reference evaluates every node). */
+int pvl_wake_interp_cols(uint32_t n_cols, uint32_t complete_rows, uint32_t row_begin, uint32_t row_end,
+                         const uint32_t* offsets, uint32_t n_entries, const uint32_t* entries,
+                         const double* weights, uint32_t n_sub, const double* sub_vel, double* node_vel,
+                         void* stream);
+
 /* out[k] = pts[index[k]] (3 doubles each) for k < n; an index outside [0, n_pts) writes NaN.
  * Gathers the control points at which the mixed path evaluates the far wake term.  No
  * reference counterpart. */

@@ -231,6 +231,36 @@ __global__ void stencil_normal_add_kernel(uint32_t n_cp, const uint32_t* __restr
     out[p] += n[0] * vx + n[1] * vy + n[2] * vz;
 }
 
+// node_vel[c, r] = sum_k weights[k] sub_vel[entries[k], r] over k in [offsets[c], offsets[c+1])
+// for rows r in [row_begin, row_end) of every column c; both arrays (columns, complete, 3).  A
+// range outside [0, n_entries) or an entry outside [0, n_sub) gives NaN.
+__global__ void interp_cols_kernel(uint32_t n_cols, uint32_t complete, uint32_t row_begin, uint32_t n_rows,
+                                   const uint32_t* __restrict__ offsets, uint32_t n_entries,
+                                   const uint32_t* __restrict__ entries, const double* __restrict__ weights,
+                                   uint32_t n_sub, const double* __restrict__ sub_vel, double* __restrict__ node_vel)
+{
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (uint64_t)n_cols * n_rows * 3)
+        return;
+    const uint32_t k = (uint32_t)(e % 3), r = row_begin + (uint32_t)((e / 3) % n_rows);
+    const uint32_t c = (uint32_t)(e / (3 * (uint64_t)n_rows));
+    const uint32_t k0 = offsets[c], k1 = offsets[c + 1];
+    double v = 0.0;
+    if (k0 > k1 || k1 > n_entries) {
+        v = __longlong_as_double(0x7FF8000000000000ll);
+    } else {
+        for (uint32_t q = k0; q < k1; ++q) {
+            const uint32_t j = entries[q];
+            if (j >= n_sub) {
+                v = __longlong_as_double(0x7FF8000000000000ll);
+                break;
+            }
+            v = fma(weights[q], sub_vel[((size_t)j * complete + r) * 3 + k], v);
+        }
+    }
+    node_vel[((size_t)c * complete + r) * 3 + k] = v;
+}
+
 extern "C" int pvl_gather_points(uint32_t n, const uint32_t* index, uint32_t n_pts, const double* pts, double* out,
                                  void* stream)
 {
@@ -255,6 +285,27 @@ extern "C" int pvl_stencil_normal_add(uint32_t n_cp, const uint32_t* offsets, ui
     }
     stencil_normal_add_kernel<<<blocks_for(n_cp, 128), 128, 0, (cudaStream_t)stream>>>(
         n_cp, offsets, n_entries, entries, weights, n_values, values, normals, out);
+    PVL_LAUNCH_CHECK();
+    return PVL_OK;
+}
+
+extern "C" int pvl_wake_interp_cols(uint32_t n_cols, uint32_t complete_rows, uint32_t row_begin, uint32_t row_end,
+                                    const uint32_t* offsets, uint32_t n_entries, const uint32_t* entries,
+                                    const double* weights, uint32_t n_sub, const double* sub_vel, double* node_vel,
+                                    void* stream)
+{
+    if (row_end > complete_rows || row_begin > row_end)
+        return pvl_fail(PVL_ERR_ARG, "pvl_wake_interp_cols: rows [%u, %u) outside [0, %u)", row_begin, row_end,
+                        complete_rows);
+    if (n_cols == 0 || row_end == row_begin)
+        return PVL_OK;
+    PVL_REQUIRE(offsets); PVL_REQUIRE(node_vel);
+    if (n_entries) {
+        PVL_REQUIRE(entries); PVL_REQUIRE(weights); PVL_REQUIRE(sub_vel);
+    }
+    const uint32_t n_rows = row_end - row_begin;
+    interp_cols_kernel<<<blocks_for((uint64_t)n_cols * n_rows * 3, 256), 256, 0, (cudaStream_t)stream>>>(
+        n_cols, complete_rows, row_begin, n_rows, offsets, n_entries, entries, weights, n_sub, sub_vel, node_vel);
     PVL_LAUNCH_CHECK();
     return PVL_OK;
 }

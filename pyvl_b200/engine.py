@@ -161,6 +161,41 @@ def far_wake_stencil(n_rings: int, patches) -> dict:
             "weights": np.asarray(weights, np.float64)}
 
 
+def column_stencil(n_cols: int, runs) -> dict:
+    """Which wake node columns the far-row advection evaluates and how the others get theirs.
+
+    ``runs``: (col0, n) runs of consecutive node columns (in the de-duplicated column order)
+    whose wake nodes are smooth functions of the column index; runs may share their end
+    columns only (the trailing-edge node at a kink).  Odd columns of a run with five columns
+    on either side take the quintic midpoint rule of their even neighbours (_midpoint_rules);
+    the rest are evaluated.  Returns ``sub`` (the evaluated columns, ascending) and the CSR
+    rule of every column over positions in ``sub`` (offsets, entries, weights)."""
+    count = np.zeros(n_cols, np.int64)
+    runs = [(int(c0), int(n)) for c0, n in runs]
+    for c0, n in runs:
+        if c0 < 0 or n <= 0 or c0 + n > n_cols:
+            raise ValueError(f"column run ({c0}, {n}) outside the {n_cols} node columns")
+        count[c0:c0 + n] += 1
+    rules = [[(c, 1.0)] for c in range(n_cols)]
+    for c0, n in runs:
+        for j, r in enumerate(_midpoint_rules(n)):
+            if len(r) > 1:
+                if count[c0 + j] > 1:
+                    raise ValueError(f"column runs overlap at column {c0 + j}, inside a run")
+                rules[c0 + j] = [(c0 + jj, w) for jj, w in r]
+    sub = np.array([c for c in range(n_cols) if len(rules[c]) == 1], np.int64)
+    pos = np.full(n_cols, -1, np.int64)
+    pos[sub] = np.arange(sub.size)
+    offsets = np.zeros(n_cols + 1, np.int64)
+    entries, weights = [], []
+    for c in range(n_cols):
+        entries += [int(pos[q]) for q, _ in rules[c]]
+        weights += [w for _, w in rules[c]]
+        offsets[c + 1] = len(entries)
+    return {"sub": sub, "offsets": offsets.astype(np.uint32), "entries": np.asarray(entries, np.uint32),
+            "weights": np.asarray(weights, np.float64)}
+
+
 def _node_velocity_workspace(n_lines: int, n_cols: int, rows: int, precision: int) -> int:
     """Largest sweep workspace over every row count 1..rows the growing wake passes through."""
     return max(_lib.query("pvl_line_velocity_workspace", n_lines, n_cols * c, precision) for c in range(1, rows + 1))
@@ -438,8 +473,22 @@ class SolverEngine:
         """The corrected system of this iteration (solver.py:194-220)."""
         self.assemble_body_only()
         if self.wake is not None and self.iteration > 0:
-            self._wake_corrections()
+            self._wake_terms()
         self.border()
+
+    def _wake_full(self) -> bool:
+        """The wake has all its rows: every launch of a wake phase then depends only on which
+        of the double-buffered positions and circulations are current."""
+        return self.capture_steps and self.wake["step_count"] >= self.wake["R"]
+
+    def _wake_terms(self) -> None:
+        """_wake_corrections, as a captured graph per (positions, circulations) buffer pair once
+        the wake is full (while it grows every step has other sizes)."""
+        w = self.wake
+        if self._wake_full():
+            self.captured(("wake_terms", w["cur"], w["ccur"]), self._wake_corrections)
+        else:
+            self._wake_corrections()
 
     def _wake_corrections(self, fp64_only: bool = False) -> None:
         """Implicit first row into A, explicit rows into the RHS (wake_models.py:199-223).
@@ -704,11 +753,13 @@ class MixedSolverEngine(SolverEngine):
                  gmres_tol: float = 1e-12, max_iter: int = 20, async_refresh: bool = True,
                  refresh_on_iters: int = 5, use_graphs: bool = True, wake_self_induction: bool = False,
                  device_solve: bool = True, refresh_excess: int = 128, advect_interp_row: int | None = 128,
-                 cp_patches=None, wake_chord_row: int = 64, wake_span_row: int | None = 192):
+                 cp_patches=None, wake_chord_row: int = 64, wake_span_row: int | None = 192,
+                 wake_col_runs=None, advect_col_row: int = 64):
         super().__init__(mesh, freestream, tol, wake, closed_groups, wake_self_induction)
         if advect_interp_row is not None and (int(advect_interp_row) < 4 or int(advect_interp_row) % 2):
             raise ValueError("advect_interp_row must be even and at least 4 (or None)")
         self.advect_interp_row = None if advect_interp_row is None else int(advect_interp_row)
+        self._update_keys: set = set()  # captured wake_update graphs (full wake)
         self.refresh = None if refresh is None else int(refresh)
         self.refresh_excess = int(refresh_excess)
         self._iters_seen = 0      # solves the refresh policy has looked at
@@ -774,6 +825,9 @@ class MixedSolverEngine(SolverEngine):
             need = max(need, self._init_row_major_wake(near_rows, advect_near_rows))
             if cp_patches is not None:
                 need = max(need, self._init_far_stencil(cp_patches, wake_chord_row, wake_span_row))
+            self._cols = None  # node-column stencil of the far-row advection (wake_col_runs)
+            if wake_col_runs is not None:
+                self._init_col_stencil(wake_col_runs, advect_col_row)
         if need + 256 > self._ws_bytes:
             self._ws_bytes = need + 256
             self.ws = torch.empty(self._ws_bytes, dtype=torch.uint8, device=self.dev)
@@ -825,6 +879,23 @@ class MixedSolverEngine(SolverEngine):
         b = n_all if span_row is None else up[span_row]
         return max(_lib.query("pvl_line_velocity_workspace", max(b - up[chord_row], 1), max(n_c, 1), _lib.PVL_F64),
                    _lib.query("pvl_line_velocity_workspace", max(n_all - b, 1), max(n_s, 1), _lib.PVL_F64))
+
+    def _init_col_stencil(self, runs, col_row: int) -> None:
+        """Device copy of column_stencil(runs) and the velocity buffer of the evaluated columns."""
+        w = self.wake
+        col_row = max(int(col_row), self.advect_near_rows)
+        ri = self.advect_interp_row
+        if ri is not None and col_row > ri:
+            raise ValueError("advect_col_row must not exceed advect_interp_row")
+        plan = column_stencil(w["n_cols"], runs)
+        sub = plan["sub"]
+        cols = w["cols"].cpu().numpy().view(np.uint32)
+        self._cols = {
+            "row": col_row, "n_sub": int(sub.size), "ids": to_device_u32(cols[sub], self.dev),
+            "offsets": to_device_u32(plan["offsets"], self.dev), "entries": to_device_u32(plan["entries"], self.dev),
+            "weights": torch.as_tensor(plan["weights"]).to(self.dev),
+            "vel": torch.zeros((max(int(sub.size), 1), w["R"], 3), dtype=torch.float64, device=self.dev),
+        }
 
     # ------------------------------------------------------------------ preconditioner
     def refresh_preconditioner(self, wait: bool = True) -> None:
@@ -1140,7 +1211,7 @@ class MixedSolverEngine(SolverEngine):
     def assemble_rest(self) -> None:
         """The wake corrections and the closed-body border, the body part already in place."""
         if self.wake is not None and self.iteration > 0:
-            self._wake_corrections()
+            self._wake_terms()
         self.border()
 
     def begin_step(self, positions, velocities) -> None:
@@ -1189,15 +1260,32 @@ class MixedSolverEngine(SolverEngine):
 
     def wake_update(self, time: float) -> None:
         """As the plain update, with the advection sweep split into FP64 near rows and FP32 far rows."""
-        s = stream_ptr()
         w = self.wake
-        S, R = w["S"], w["R"]
+        R = w["R"]
         dt = float(time) - w["time"]
         w["time"] = float(time)
         if w["step_count"] == 0:
             self._advect(0, 0.0)
             w["step_count"] = 1
         complete = min(w["step_count"], R)
+        cur, c = w["cur"], w["ccur"]
+        key = ("wake_update", cur, c, dt)
+        if self._wake_full() and (key in self._update_keys or len(self._update_keys) < 8):
+            # one graph per buffer pair and time step (a few distinct dt at most)
+            self._update_keys.add(key)
+            self.captured(key, lambda: self._update_launches(complete, dt, cur, c))
+        else:
+            self._update_launches(complete, dt, cur, c)
+        w["cur"], w["ccur"] = 1 - cur, 1 - c
+        w["step_count"] += 1
+
+    def _update_launches(self, complete: int, dt: float, cur: int, c: int) -> None:
+        """The launches of wake_update from positions pos[cur] and circulations circ[c] into the
+        other buffers (no host state changes: they may be captured once and replayed)."""
+        s = stream_ptr()
+        w = self.wake
+        S, R = w["S"], w["R"]
+        wpos = w["pos"][cur]
         msh, d = self.mesh, self.d_body
         _lib.call("pvl_line_circulation", msh.n_lines, ptr(d["map_offsets"]), ptr(d["map_entries"]), ptr(self.gamma), 0,
                   ptr(self.body_line_gamma), s)
@@ -1209,21 +1297,31 @@ class MixedSolverEngine(SolverEngine):
         interp = ri is not None and ri >= nr and complete >= ri + 8
         mid = ri if interp else complete
         tail = (complete - 4) | 1 if interp else complete  # first odd row without 3 rows above it
-        bands = [(_lib.PVL_F64, 0, nr, 1), (_lib.PVL_F32, nr, mid - nr, 1)]  # (precision, row, count, step)
+        # rows from ac on: the evaluated node columns only (into the column buffer), the rest
+        # from the column rule (pvl_wake_interp_cols) before the odd rows are interpolated
+        cs = self._cols
+        ac = cs["row"] if cs is not None and complete > cs["row"] else complete  # ac <= mid
+        far = [(_lib.PVL_F32, ac, mid - ac, 1)] if ac < complete else []
         if interp:
-            bands += [(_lib.PVL_F32, ri, (complete - ri + 1) // 2, 2), (_lib.PVL_F32, tail, complete - tail, 1)]
-        for prec, r0, count, step in bands:
+            far += [(_lib.PVL_F32, ri, (tail - ri + 1) // 2, 2), (_lib.PVL_F32, tail, complete - tail, 1)]
+        # (precision, row, count, step, columns, column list, output)
+        all_cols = (w["n_cols"], w["cols"], w["node_vel"])
+        bands = [(_lib.PVL_F64, 0, nr, 1) + all_cols, (_lib.PVL_F32, nr, min(ac, mid) - nr, 1) + all_cols]
+        bands += [b + ((cs["n_sub"], cs["ids"], cs["vel"]) if ac < complete else all_cols) for b in far]
+        for prec, r0, count, step, n_c, col_list, out in bands:
             if count > 0:
                 _lib.call("pvl_wake_node_velocity_rows", prec, msh.n_points, msh.n_lines, ptr(d["lines"]),
-                          ptr(self.pos), ptr(self.body_line_gamma), S, R, complete, r0, count, step, w["n_cols"],
-                          ptr(w["cols"]), ptr(self.wake_positions), float(u[0]), float(u[1]), float(u[2]), self.tol,
-                          ptr(w["node_vel"]), ptr(self.ws), self._ws_bytes, s)
+                          ptr(self.pos), ptr(self.body_line_gamma), S, R, complete, r0, count, step, n_c,
+                          ptr(col_list), ptr(wpos), float(u[0]), float(u[1]), float(u[2]), self.tol,
+                          ptr(out), ptr(self.ws), self._ws_bytes, s)
+        if ac < complete:
+            _lib.call("pvl_wake_interp_cols", w["n_cols"], complete, ac, complete, ptr(cs["offsets"]),
+                      cs["entries"].numel(), ptr(cs["entries"]), ptr(cs["weights"]), cs["n_sub"], ptr(cs["vel"]),
+                      ptr(w["node_vel"]), s)
         if interp:
             _lib.call("pvl_wake_interp_rows", w["n_cols"], complete, ri + 1, tail - 2, ptr(w["node_vel"]), s)
         if self.wake_self_induction:
             self._add_wake_self_velocity(complete)
-        self._advect(complete, dt)
-        c = w["ccur"]
+        _lib.call("pvl_wake_advect_cols", S, R, complete, ptr(wpos), ptr(w["node_vel"]), ptr(w["slot"]), w["n_cols"],
+                  dt, ptr(self.pos), ptr(w["bn"]), ptr(w["pos"][1 - cur]), s)
         _lib.call("pvl_wake_shed", S, R, ptr(w["circ"][c]), ptr(w["adj"]), ptr(self.gamma), ptr(w["circ"][1 - c]), s)
-        w["ccur"] = 1 - c
-        w["step_count"] += 1

@@ -158,6 +158,9 @@ class Case:
     # (ring0, n_span, n_chord) blocks of rings ring0 + i * n_chord + j over which the control
     # points are smooth in (i, j) (MixedSolverEngine cp_patches); empty: not a structured grid
     smooth_patches: tuple = ()
+    # (col0, n) runs of wake node columns (trailing-edge nodes, in the engine's de-duplicated
+    # column order) along which the wake is smooth (MixedSolverEngine wake_col_runs)
+    wake_col_runs: tuple = ()
 
     @property
     def n_points(self) -> int:
@@ -208,6 +211,14 @@ def _root_split(ns: int, nc: int) -> tuple:
     return ((0, h, nc), (h * nc, h, nc))
 
 
+def _root_split_cols(ns: int) -> tuple:
+    """The trailing-edge node columns of _root_split's halves (sharing the root node ns/2)."""
+    if ns % 2:
+        return ((0, ns + 1),)
+    h = ns // 2
+    return ((0, h + 1), (h, h + 1))
+
+
 def flat_wing(ns: int = 16, nc: int = 4, span: float = 8.0, chord: float = 1.0,
               alpha_deg: float = 5.0, dt: float = 0.25, nt: int = 10,
               line_rows: int = 10) -> Case:
@@ -251,7 +262,7 @@ def swept_pitching(ns: int = 64, nc: int = 16, seed: int = 1, span: float = 8.0,
         positions=pos, elements=elements, kinematics=kin,
         freestream=np.array([1.0, 0.0, 0.0]), dt=dt, nt=nt, line_rows=line_rows,
         te_node_pairs=te, s_ref=s_ref, t0=-dt, meta={"k": k, "seed": seed},
-        smooth_patches=_root_split(ns, nc),
+        smooth_patches=_root_split(ns, nc), wake_col_runs=_root_split_cols(ns),
     )
 
 
@@ -275,7 +286,7 @@ def flapping(ns: int = 128, nc: int = 32, span: float = 8.0, chord: float = 1.0,
         positions=pos, elements=elements, kinematics=kin,
         freestream=np.array([np.cos(a), 0.0, np.sin(a)]), dt=dt, nt=nt,
         line_rows=line_rows, te_node_pairs=te, s_ref=span * chord, t0=-dt,
-        meta={"k": k}, smooth_patches=_root_split(ns, nc),
+        meta={"k": k}, smooth_patches=_root_split(ns, nc), wake_col_runs=_root_split_cols(ns),
     )
 
 

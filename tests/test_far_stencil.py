@@ -3,7 +3,7 @@ far_wake_stencil builds for smooth patches of the ring grid (no GPU)."""
 import numpy as np
 import pytest
 
-from pyvl_b200.engine import far_wake_stencil
+from pyvl_b200.engine import column_stencil, far_wake_stencil
 
 
 def _apply(plan, values):
@@ -72,3 +72,26 @@ def test_stencil_rejects_bad_patches():
     plan = far_wake_stencil(100, ())
     assert plan["n_chord_eval"] == plan["n_span_eval"] == 100
     assert (plan["weights"] == 1.0).all()
+
+
+def test_column_stencil_reproduces_quintics():
+    """129 trailing-edge node columns as two runs sharing the root column 64: 73 evaluated (the
+    even ones and those within five of a run end), every column of a quintic field exact."""
+    plan = column_stencil(129, ((0, 65), (64, 65)))
+    sub = plan["sub"]
+    assert sub.size == 73 and 64 in sub and 0 in sub and 128 in sub
+    c = np.arange(129, dtype=np.float64)
+    x = np.where(c <= 64, c, 128.0 - c)  # a kink at the shared column: each run smooth on its own
+    f = np.stack([1 + 0.01 * x - 1e-4 * x ** 3 + 1e-8 * x ** 5, np.ones(129), x ** 2], axis=1)
+    off, ent, w = plan["offsets"].astype(np.int64), plan["entries"].astype(np.int64), plan["weights"]
+    got = np.array([(w[off[k]:off[k + 1], None] * f[sub][ent[off[k]:off[k + 1]]]).sum(0) for k in range(129)])
+    np.testing.assert_allclose(got, f, rtol=0, atol=1e-9 * np.abs(f).max())
+
+
+def test_column_stencil_rejects_bad_runs():
+    with pytest.raises(ValueError):
+        column_stencil(20, ((0, 21),))
+    with pytest.raises(ValueError):  # column 15 inside both runs
+        column_stencil(40, ((0, 30), (10, 30)))
+    plan = column_stencil(12, ())
+    assert plan["sub"].size == 12 and (plan["weights"] == 1.0).all()

@@ -357,13 +357,52 @@ def test_far_stencil_kernels_match_numpy():
     np.testing.assert_allclose(got[~bad], want[~bad], rtol=1e-12, atol=1e-12)
 
 
+def test_wake_interp_cols_matches_numpy():
+    """pvl_wake_interp_cols against numpy: rows [4, 17) of 9 node columns from the 5 evaluated
+    ones by seeded rules; a rule past the entries gives NaN for its column only."""
+    import torch
+
+    from pyvl_b200 import _lib
+    from pyvl_b200.device import ptr, stream_ptr, to_device_u32
+
+    rng = np.random.default_rng(11)
+    n_cols, n_sub, complete = 9, 5, 20
+    counts = rng.integers(1, 7, n_cols)
+    offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint32)
+    entries = rng.integers(0, n_sub, int(offsets[-1])).astype(np.uint32)
+    weights = rng.normal(size=entries.size)
+    sub = rng.normal(size=(n_sub, complete, 3))
+    node0 = rng.normal(size=(n_cols, complete, 3))
+    d_off, d_ent = to_device_u32(offsets), to_device_u32(entries)
+    d_w, d_sub, d_node = (torch.tensor(a, device="cuda") for a in (weights, sub, node0))
+    _lib.call("pvl_wake_interp_cols", n_cols, complete, 4, 17, ptr(d_off), entries.size, ptr(d_ent), ptr(d_w),
+              n_sub, ptr(d_sub), ptr(d_node), stream_ptr())
+    got = d_node.cpu().numpy()
+    want = node0.copy()
+    for c in range(n_cols):
+        k = slice(int(offsets[c]), int(offsets[c + 1]))
+        want[c, 4:17] = (weights[k, None, None] * sub[entries[k].astype(np.int64), 4:17]).sum(0)
+    np.testing.assert_allclose(got, want, rtol=1e-13, atol=1e-13)
+    bad = offsets.copy()
+    bad[-1] += 3
+    d_bad = to_device_u32(bad)
+    _lib.call("pvl_wake_interp_cols", n_cols, complete, 0, complete, ptr(d_bad), entries.size, ptr(d_ent),
+              ptr(d_w), n_sub, ptr(d_sub), ptr(d_node), stream_ptr())
+    got = d_node.cpu().numpy()
+    assert np.isnan(got[-1]).all() and np.isfinite(got[:-1]).all()
+    with pytest.raises(ValueError):
+        _lib.call("pvl_wake_interp_cols", n_cols, complete, 3, complete + 1, ptr(d_off), entries.size, ptr(d_ent),
+                  ptr(d_w), n_sub, ptr(d_sub), ptr(d_node), stream_ptr())
+
+
 def test_mixed_trajectory_with_far_wake_stencil():
     """As test_mixed_trajectory_tracks_plain, with the explicit wake term of the far rows
     evaluated at part of the control points and interpolated across each half wing
     (cp_patches; 200 wake rows, chordwise from row 64 = 4 chords, spanwise too from row 160 =
     10 chords, where the coarser 64 x 16 grid's spacing relative to the distance matches the
-    128 x 32 wing's from row 192): every step's circulation is still within 1e-10 of the plain
-    FP64 run's, and the judged step (everything re-assembled in FP64) agrees with the
+    128 x 32 wing's from row 192) and the advection of the rows from 64 on evaluated at every
+    other node column (wake_col_runs): every step's circulation is still within 1e-10 of the
+    plain FP64 run's, and the judged step (everything re-assembled in FP64) agrees with the
     interpolated one to the same bar."""
     from pyvl_b200.cvl import Mesh
     from pyvl_b200.engine import MixedSolverEngine, SolverEngine, wake_spec_from_te
@@ -377,8 +416,9 @@ def test_mixed_trajectory_with_far_wake_stencil():
 
     plain = SolverEngine(mesh, case.freestream, case.tol, spec())
     mixed = MixedSolverEngine(mesh, case.freestream, case.tol, spec(), cp_patches=case.smooth_patches,
-                              wake_chord_row=64, wake_span_row=160)
-    assert mixed._far["n_chord_eval"] < mixed.P
+                              wake_chord_row=64, wake_span_row=160, wake_col_runs=case.wake_col_runs,
+                              advect_col_row=64)
+    assert mixed._far["n_chord_eval"] < mixed.P and mixed._cols["n_sub"] < mixed.wake["n_cols"]
     worst = 0.0
     for it in range(250):
         t = it * case.dt
@@ -397,6 +437,33 @@ def test_mixed_trajectory_with_far_wake_stencil():
     with pytest.raises(ValueError):
         MixedSolverEngine(mesh, case.freestream, case.tol, spec(), cp_patches=case.smooth_patches,
                           wake_chord_row=80, wake_span_row=40)
+
+
+def test_full_wake_graphs_match_direct_launches():
+    """Once the wake is full the wake terms and the wake update replay captured graphs (one per
+    buffer pair and time step); the circulations and the wake are bit-identical to an engine
+    that launches every kernel directly (capture_steps off)."""
+    import torch
+
+    from pyvl_b200.workloads import flapping
+
+    case = flapping(ns=32, nc=8, line_rows=24)
+    runs = []
+    for capture in (True, False):
+        eng = _mixed_engine(case, cp_patches=case.smooth_patches, wake_chord_row=8, wake_span_row=16,
+                            wake_col_runs=case.wake_col_runs, advect_col_row=8, advect_interp_row=12)
+        eng.capture_steps = capture
+        G = []
+        for it in range(40):
+            t = it * case.dt
+            eng.step(t, case.positions_at(t), case.velocities_at(t))
+            G.append(eng.gamma_host())
+        runs.append((np.array(G), eng.wake_positions.cpu().numpy(), eng.wake_circulation.cpu().numpy(),
+                     len(eng._update_keys), sum(1 for k in eng._step_graphs if k[0] == "wake_terms")))
+        torch.cuda.synchronize()
+    (g1, p1, c1, nu1, nt1), (g2, p2, c2, nu2, nt2) = runs
+    assert nu1 >= 2 and nt1 >= 2 and nu2 == 0 and nt2 == 0
+    assert np.array_equal(g1, g2) and np.array_equal(p1, p2) and np.array_equal(c1, c2)
 
 
 def test_gmres_graph_replay_is_bitwise_identical():
