@@ -630,10 +630,14 @@ inline uint32_t sweep_points_per_cta(int precision) { return precision == PVL_F3
 // over (32 per SM, so that the last resident wave is short), at least half a tile of segments
 // per range in FP64 (small point sets such as the near-row advection then still fill one
 // resident wave: 52 instead of 58 us for 1032 points) and two tiles in FP32.
+#ifndef PVL_SUM_CTAS_PER_SM
+#define PVL_SUM_CTAS_PER_SM 32  // CTAs per SM (148 SMs) the point tiles x line splits aim at
+#endif
+
 uint32_t sum_splits(uint32_t n_lines, uint32_t n_pts, int precision)
 {
     const uint64_t ctas_x = (n_pts + sweep_points_per_cta(precision) - 1) / sweep_points_per_cta(precision);
-    const uint64_t want = 148ull * 32;
+    const uint64_t want = 148ull * PVL_SUM_CTAS_PER_SM;
     uint64_t s = (want + ctas_x - 1) / std::max<uint64_t>(ctas_x, 1);
     const uint64_t min_range = precision == PVL_F32 ? 2 * kSegTile : kSegTile / 2;
     const uint64_t max_s = std::max<uint64_t>(1, (n_lines + min_range - 1) / min_range);

@@ -199,33 +199,56 @@ __global__ void gather_points_kernel(uint32_t n, const uint32_t* __restrict__ in
 }
 
 // out[p] += n_p . sum_k weights[k] values[entries[k]] over k in [offsets[p], offsets[p+1]);
-// one thread per point, terms summed in stored order.  A range outside [0, n_entries) or an
-// entry outside [0, n_values) makes the point's sum NaN (nothing outside the arrays is read).
+// kStencilLanes lanes per point, each summing every kStencilLanes-th term, then a butterfly
+// over the lanes (a fixed order: the result does not depend on the launch).  A range outside
+// [0, n_entries) or an entry outside [0, n_values) makes the point's sum NaN (nothing outside
+// the arrays is read).  Threads past the last point run the shuffles with no terms.
+constexpr unsigned kStencilLanes = 8;
+
 __global__ void stencil_normal_add_kernel(uint32_t n_cp, const uint32_t* __restrict__ offsets, uint32_t n_entries,
                                           const uint32_t* __restrict__ entries, const double* __restrict__ weights,
                                           uint32_t n_values, const double* __restrict__ values,
                                           const double* __restrict__ normals, double* __restrict__ out)
 {
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n_cp)
-        return;
-    double vx = 0.0, vy = 0.0, vz = 0.0;
-    const uint32_t k0 = offsets[p], k1 = offsets[p + 1];
-    if (k0 > k1 || k1 > n_entries) {
-        out[p] = __longlong_as_double(0x7FF8000000000000ll);
-        return;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t lane = (uint32_t)(t % kStencilLanes);
+    const uint64_t p = t / kStencilLanes;
+    const bool live = p < n_cp;
+    uint32_t k0 = 0, k1 = 0;
+    bool bad = false;
+    if (live) {
+        k0 = offsets[p];
+        k1 = offsets[p + 1];
+        bad = k0 > k1 || k1 > n_entries;
+        if (bad)
+            k1 = k0;
     }
-    for (uint32_t k = k0; k < k1; ++k) {
+    double vx = 0.0, vy = 0.0, vz = 0.0;
+    for (uint32_t k = k0 + lane; k < k1; k += kStencilLanes) {
         const uint32_t j = entries[k];
-        const double w = weights[k];
         if (j >= n_values) {
-            vx = __longlong_as_double(0x7FF8000000000000ll);
+            bad = true;
             continue;
         }
+        const double w = weights[k];
         const double* v = values + (size_t)j * 3;
         vx = fma(w, v[0], vx);
         vy = fma(w, v[1], vy);
         vz = fma(w, v[2], vz);
+    }
+    int any_bad = bad;
+#pragma unroll
+    for (unsigned o = kStencilLanes / 2; o > 0; o >>= 1) {
+        vx += __shfl_xor_sync(0xffffffffu, vx, o, kStencilLanes);
+        vy += __shfl_xor_sync(0xffffffffu, vy, o, kStencilLanes);
+        vz += __shfl_xor_sync(0xffffffffu, vz, o, kStencilLanes);
+        any_bad |= __shfl_xor_sync(0xffffffffu, any_bad, o, kStencilLanes);
+    }
+    if (!live || lane != 0)
+        return;
+    if (any_bad) {
+        out[p] = __longlong_as_double(0x7FF8000000000000ll);
+        return;
     }
     const double* n = normals + (size_t)p * 3;
     out[p] += n[0] * vx + n[1] * vy + n[2] * vz;
@@ -283,7 +306,7 @@ extern "C" int pvl_stencil_normal_add(uint32_t n_cp, const uint32_t* offsets, ui
     if (n_entries) {
         PVL_REQUIRE(entries); PVL_REQUIRE(weights); PVL_REQUIRE(values);
     }
-    stencil_normal_add_kernel<<<blocks_for(n_cp, 128), 128, 0, (cudaStream_t)stream>>>(
+    stencil_normal_add_kernel<<<blocks_for((uint64_t)n_cp * kStencilLanes, 128), 128, 0, (cudaStream_t)stream>>>(
         n_cp, offsets, n_entries, entries, weights, n_values, values, normals, out);
     PVL_LAUNCH_CHECK();
     return PVL_OK;
