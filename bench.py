@@ -283,7 +283,8 @@ def profile_kernel(args) -> None:
 
     case = workload()
     mesh, spec, wpos, wcirc, t0 = wake_setup(case)
-    eng = MixedSolverEngine(mesh, case.freestream, case.tol, spec)
+    eng = MixedSolverEngine(mesh, case.freestream, case.tol, spec, cp_patches=case.smooth_patches,
+                            wake_col_runs=case.wake_col_runs)
     eng.set_wake_state(wpos, wcirc, step_count=case.line_rows + 1, time=t0 - case.dt)
     eng.load_inputs(case.positions_at(t0), case.velocities_at(t0))
     eng.iteration = 1

@@ -251,6 +251,17 @@ int pvl_wake_node_velocity_rows(int precision, uint32_t n_points, uint32_t n_lin
                                 const double* wake_pos, double ux, double uy, double uz, double tol,
                                 double* node_vel, void* ws, size_t ws_bytes, void* stream);
 
+/* pvl_wake_node_velocity_rows for the rows listed in `rows` (device array of n_rows row
+ * indices; an entry at or past complete_rows is skipped, its nodes left as they are) of the n_cols
+ * listed node columns; output at the same rows of node_vel (n_cols, complete_rows, 3).
+ * Workspace: pvl_line_velocity_workspace(n_lines, n_cols n_rows, precision).  One sweep for rows
+ * that no single stride covers (the mixed path's far rows).  No reference counterpart. */
+int pvl_wake_node_velocity_list(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines,
+                                const double* positions, const double* line_gamma, uint32_t n_shed,
+                                uint32_t line_rows, uint32_t complete_rows, uint32_t n_rows, const uint32_t* rows,
+                                uint32_t n_cols, const uint32_t* cols, const double* wake_pos, double ux, double uy,
+                                double uz, double tol, double* node_vel, void* ws, size_t ws_bytes, void* stream);
+
 /* node_vel (n_cols, complete_rows, 3): rows row_first, row_first + 2, ... <= row_last of every
  * column set to the midpoint value of the cubic through the same column's rows -3, -1, +1 and +3
  * away ((9 (v[-1] + v[+1]) - (v[-3] + v[+3])) / 16); needs row_first >= 3 and

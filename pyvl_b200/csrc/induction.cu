@@ -209,20 +209,23 @@ __global__ void __launch_bounds__(kRingThreads) line_matrix_kernel(uint32_t n_li
     }
 }
 
-// Point p of a sweep is pts[col(p / group) * stride + (p % group) * row_step + in_off] with
-// col(c) = cols ? cols[c] : c: group == stride == n_pts, row_step 1 is a plain array; group = a
-// set of wake rows, stride = rows + 1, in_off = first row, row_step = the rows' spacing walks
-// those rows of the listed wake node columns (strip side s * 2 + side).  A listed column at or
-// past col_limit is no point.
+// Point p of a sweep is pts[col(p / group) * stride + row(p % group)] with col(c) = cols ? cols[c]
+// : c and row(k) = rows ? rows[k] : k * row_step + in_off: group == stride == n_pts, row_step 1
+// is a plain array; group = a set of wake rows, stride = rows + 1, in_off = first row, row_step =
+// the rows' spacing walks those rows of the listed wake node columns (strip side s * 2 + side);
+// a row list walks any rows.  A listed column at or past col_limit, or a listed row at or past
+// row_limit, is no point.
 __device__ __forceinline__ bool sweep_point(uint32_t p, uint32_t n_pts, uint32_t group, uint32_t stride,
                                             uint32_t in_off, uint32_t row_step, const uint32_t* __restrict__ cols,
-                                            uint32_t col_limit, size_t& q)
+                                            uint32_t col_limit, const uint32_t* __restrict__ rows, uint32_t row_limit,
+                                            size_t& q)
 {
     bool ok = p < n_pts;
-    uint32_t col = ok ? (cols ? cols[p / group] : p / group) : 0;
-    if (col >= col_limit)
+    const uint32_t col = ok ? (cols ? cols[p / group] : p / group) : 0;
+    const uint32_t row = ok ? (rows ? rows[p % group] : (p % group) * row_step + in_off) : 0;
+    if (col >= col_limit || (rows && row >= row_limit))
         ok = false;
-    q = ok ? (size_t)col * stride + (size_t)(p % group) * row_step + in_off : 0;
+    q = ok ? (size_t)col * stride + row : 0;
     return ok;
 }
 
@@ -233,8 +236,8 @@ __device__ __forceinline__ bool sweep_point(uint32_t p, uint32_t n_pts, uint32_t
 __global__ void __launch_bounds__(kSumThreads, 8) line_sum_f64_kernel(
     const Segment<double>* __restrict__ seg, uint32_t n_lines, uint32_t lines_per_split,
     const double* __restrict__ pts, uint32_t n_pts, uint32_t group, uint32_t stride, uint32_t in_off,
-    uint32_t row_step, const uint32_t* __restrict__ cols, uint32_t col_limit, double tol2,
-    double* __restrict__ partial)
+    uint32_t row_step, const uint32_t* __restrict__ cols, uint32_t col_limit, const uint32_t* __restrict__ rows,
+    uint32_t row_limit, double tol2, double* __restrict__ partial)
 {
     __shared__ SweepSeg s_seg[kSegTile + 1];
     __shared__ double s_red[kSumThreads / 32][4];
@@ -244,7 +247,7 @@ __global__ void __launch_bounds__(kSumThreads, 8) line_sum_f64_kernel(
     const uint32_t l_end = min(n_lines, l_begin + lines_per_split);
     const uint32_t p = blockIdx.x * kSumThreads + threadIdx.x;
     size_t q;
-    const bool ok = sweep_point(p, n_pts, group, stride, in_off, row_step, cols, col_limit, q);
+    const bool ok = sweep_point(p, n_pts, group, stride, in_off, row_step, cols, col_limit, rows, row_limit, q);
     double px = ok ? pts[3 * q] : 0.0, py = ok ? pts[3 * q + 1] : 0.0, pz = ok ? pts[3 * q + 2] : 0.0;
     pvl::cta_centroid<kSumThreads>(px, py, pz, ok ? 1.0 : 0.0, s_red, s_o);  // px.. are 0 when !ok
     px -= s_o[0];
@@ -329,7 +332,9 @@ __global__ void __launch_bounds__(kSumThreads, 12) line_sum_f32x2_kernel(const S
                                                                      uint32_t group, uint32_t stride, uint32_t in_off,
                                                                      uint32_t row_step,
                                                                      const uint32_t* __restrict__ cols,
-                                                                     uint32_t col_limit, float tol2,
+                                                                     uint32_t col_limit,
+                                                                     const uint32_t* __restrict__ rows,
+                                                                     uint32_t row_limit, float tol2,
                                                                      float* __restrict__ partial)
 {
     __shared__ SweepSeg2 s_seg[kSegTile];
@@ -346,7 +351,7 @@ __global__ void __launch_bounds__(kSumThreads, 12) line_sum_f32x2_kernel(const S
         const uint32_t p = blockIdx.x * (kSumThreads * 2) + t * kSumThreads + threadIdx.x;
         pid[t] = p;
         size_t q;
-        const bool ok = sweep_point(p, n_pts, group, stride, in_off, row_step, cols, col_limit, q);
+        const bool ok = sweep_point(p, n_pts, group, stride, in_off, row_step, cols, col_limit, rows, row_limit, q);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             pv[t][c] = ok ? pts[3 * q + c] : 0.0;
@@ -426,7 +431,7 @@ template <typename T>
 __global__ void __launch_bounds__(kReducePts * kReduceGroups) reduce_partials_kernel(
     uint32_t n_pts, uint32_t n_split, const T* __restrict__ partial, const double* __restrict__ normals, double alpha,
     double beta, double ux, double uy, double uz, uint32_t group, uint32_t row_step, uint32_t out_stride,
-    uint32_t out_off,
+    uint32_t out_off, const uint32_t* __restrict__ rows, uint32_t row_limit,
     double* __restrict__ out)
 {
     // kReducePts consecutive points per CTA (their partials are contiguous for every split, so a
@@ -455,7 +460,10 @@ __global__ void __launch_bounds__(kReducePts * kReduceGroups) reduce_partials_ke
         vy += s_v[g][tx][1];
         vz += s_v[g][tx][2];
     }
-    const size_t op = (size_t)(p / group) * out_stride + (size_t)(p % group) * row_step + out_off;
+    const uint32_t row = rows ? rows[p % group] : (p % group) * row_step + out_off;
+    if (rows && row >= row_limit)
+        return;  // no point (the sweep skipped it too)
+    const size_t op = (size_t)(p / group) * out_stride + row;
     if (normals) {
         const double v = vx * normals[3 * (size_t)p] + vy * normals[3 * (size_t)p + 1] + vz * normals[3 * (size_t)p + 2];
         out[p] = beta == 0.0 ? alpha * v : beta * out[p] + alpha * v;
@@ -891,7 +899,7 @@ namespace {
 int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines, const double* positions,
                  const double* line_gamma, uint32_t n_pts, const double* pts, uint32_t group, uint32_t stride,
                  uint32_t in_off, uint32_t row_step, const uint32_t* cols, uint32_t col_limit, uint32_t out_stride,
-                 uint32_t out_off,
+                 uint32_t out_off, const uint32_t* rows, uint32_t row_limit,
                  const double* normals, double tol,
                  double alpha, double beta, double ux, double uy, double uz, double* out, void* ws, size_t ws_bytes,
                  cudaStream_t st, const char* who)
@@ -900,7 +908,8 @@ int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint3
         return pvl_fail(PVL_ERR_ARG, "%s: unknown precision %d", who, precision);
     if (n_lines == 0) {
         reduce_partials_kernel<double><<<blocks_for(n_pts, kReducePts), kReducePts * kReduceGroups, 0, st>>>(
-            n_pts, 0, nullptr, normals, alpha, beta, ux, uy, uz, group, row_step, out_stride, out_off, out);
+            n_pts, 0, nullptr, normals, alpha, beta, ux, uy, uz, group, row_step, out_stride, out_off, rows, row_limit,
+            out);
         PVL_LAUNCH_CHECK();
         return PVL_OK;
     }
@@ -920,21 +929,24 @@ int run_line_sum(int precision, uint32_t n_points, uint32_t n_lines, const uint3
         if (int r = prep_segments<double>(n_points, n_lines, lines, positions, line_gamma, tol, seg, st))
             return r;
         line_sum_f64_kernel<<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off,
-                                                          row_step, cols, col_limit, pvl::cutoff2<double>(tol), part);
+                                                          row_step, cols, col_limit, rows, row_limit,
+                                                          pvl::cutoff2<double>(tol), part);
         PVL_LAUNCH_CHECK();
         reduce_partials_kernel<double><<<blocks_for(n_pts, kReducePts), kReducePts * kReduceGroups, 0, st>>>(
-            n_pts, n_split_used, part, normals, alpha, beta, ux, uy, uz, group, row_step, out_stride, out_off, out);
+            n_pts, n_split_used, part, normals, alpha, beta, ux, uy, uz, group, row_step, out_stride, out_off, rows,
+            row_limit, out);
     } else {
         auto* seg = reinterpret_cast<Segment<float>*>(base);
         auto* part = reinterpret_cast<float*>(base + pvl_segments_workspace(n_lines, PVL_F32));
         if (int r = prep_segments<float>(n_points, n_lines, lines, positions, line_gamma, tol, seg, st))
             return r;
         line_sum_f32x2_kernel<<<grid, kSumThreads, 0, st>>>(seg, n_lines, per, pts, n_pts, group, stride, in_off,
-                                                               row_step, cols, col_limit, pvl::cutoff2<float>(tol),
-                                                               part);
+                                                               row_step, cols, col_limit, rows, row_limit,
+                                                               pvl::cutoff2<float>(tol), part);
         PVL_LAUNCH_CHECK();
         reduce_partials_kernel<float><<<blocks_for(n_pts, kReducePts), kReducePts * kReduceGroups, 0, st>>>(
-            n_pts, n_split_used, part, normals, alpha, beta, ux, uy, uz, group, row_step, out_stride, out_off, out);
+            n_pts, n_split_used, part, normals, alpha, beta, ux, uy, uz, group, row_step, out_stride, out_off, rows,
+            row_limit, out);
     }
     PVL_LAUNCH_CHECK();
     return PVL_OK;
@@ -951,7 +963,7 @@ extern "C" int pvl_line_velocity(int precision, uint32_t n_points, uint32_t n_li
         return PVL_OK;
     PVL_REQUIRE(pts); PVL_REQUIRE(out);
     return run_line_sum(precision, n_points, n_lines, lines, positions, line_gamma, n_pts, pts, n_pts, n_pts, 0, 1,
-                        nullptr, 0xFFFFFFFFu, n_pts, 0, normals, tol, alpha, beta, 0.0, 0.0, 0.0, out, ws, ws_bytes, (cudaStream_t)stream,
+                        nullptr, 0xFFFFFFFFu, n_pts, 0, nullptr, 0, normals, tol, alpha, beta, 0.0, 0.0, 0.0, out, ws, ws_bytes, (cudaStream_t)stream,
                         "pvl_line_velocity");
 }
 
@@ -961,6 +973,39 @@ extern "C" size_t pvl_wake_node_velocity_workspace(uint32_t n_lines, uint32_t n_
     return pvl_line_velocity_workspace(n_lines, 2 * n_shed * complete_rows, precision);
 }
 
+namespace {
+
+// Sweep of the body's (or any) segments at wake nodes: rows row_begin + k * row_step (k < row_count)
+// or, with a row list, rows[k] (k < row_count; entries at or past complete_rows skipped) of the
+// n_cols listed node columns; node_vel (n_cols, complete_rows, 3) at the same rows.
+int node_velocity(int precision, uint32_t n_points, uint32_t n_lines, const uint32_t* lines, const double* positions,
+                  const double* line_gamma, uint32_t n_shed, uint32_t line_rows, uint32_t complete_rows,
+                  uint32_t row_begin, uint32_t row_count, uint32_t row_step, const uint32_t* rows, uint32_t n_cols,
+                  const uint32_t* cols, const double* wake_pos, double ux, double uy, double uz, double tol,
+                  double* node_vel, void* ws, size_t ws_bytes, void* stream, const char* who)
+{
+    if (complete_rows > line_rows)
+        return pvl_fail(PVL_ERR_ARG, "%s: complete_rows %u > line_rows %u", who, complete_rows, line_rows);
+    if (!rows && row_count > 0 &&
+        (row_step == 0 || (uint64_t)row_begin + (uint64_t)(row_count - 1) * row_step >= (uint64_t)complete_rows))
+        return pvl_fail(PVL_ERR_ARG, "%s: rows %u + k * %u (k < %u) outside [0, %u)", who, row_begin, row_step,
+                        row_count, complete_rows);
+    if (!cols && n_cols != 2 * n_shed)
+        return pvl_fail(PVL_ERR_ARG, "%s: without a column list n_cols must be 2 n_shed", who);
+    if (n_cols == 0 || row_count == 0)
+        return PVL_OK;
+    PVL_REQUIRE(wake_pos); PVL_REQUIRE(node_vel);
+    const uint64_t n_pts = (uint64_t)n_cols * row_count;
+    if (n_pts > 0xFFFFFFFFull)
+        return pvl_fail(PVL_ERR_ARG, "%s: too many nodes", who);
+    return run_line_sum(precision, n_points, n_lines, lines, positions, line_gamma, (uint32_t)n_pts, wake_pos,
+                        row_count, line_rows + 1, row_begin, row_step, cols, 2 * n_shed, complete_rows, row_begin,
+                        rows, complete_rows, nullptr, tol, 1.0, 0.0, ux, uy, uz, node_vel, ws, ws_bytes,
+                        (cudaStream_t)stream, who);
+}
+
+}  // namespace
+
 extern "C" int pvl_wake_node_velocity_rows(int precision, uint32_t n_points, uint32_t n_lines,
                                            const uint32_t* lines, const double* positions, const double* line_gamma,
                                            uint32_t n_shed, uint32_t line_rows, uint32_t complete_rows,
@@ -969,25 +1014,24 @@ extern "C" int pvl_wake_node_velocity_rows(int precision, uint32_t n_points, uin
                                            double uz, double tol, double* node_vel, void* ws, size_t ws_bytes,
                                            void* stream)
 {
-    if (complete_rows > line_rows)
-        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity: complete_rows %u > line_rows %u", complete_rows,
-                        line_rows);
-    if (row_count > 0 && (row_step == 0 ||
-                          (uint64_t)row_begin + (uint64_t)(row_count - 1) * row_step >= (uint64_t)complete_rows))
-        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity_rows: rows %u + k * %u (k < %u) outside [0, %u)",
-                        row_begin, row_step, row_count, complete_rows);
-    if (!cols && n_cols != 2 * n_shed)
-        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity_cols: without a column list n_cols must be 2 n_shed");
-    if (n_cols == 0 || row_count == 0)
-        return PVL_OK;
-    PVL_REQUIRE(wake_pos); PVL_REQUIRE(node_vel);
-    const uint64_t n_pts = (uint64_t)n_cols * row_count;
-    if (n_pts > 0xFFFFFFFFull)
-        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity: too many nodes");
-    return run_line_sum(precision, n_points, n_lines, lines, positions, line_gamma, (uint32_t)n_pts, wake_pos,
-                        row_count, line_rows + 1, row_begin, row_step, cols, 2 * n_shed, complete_rows, row_begin,
-                        nullptr, tol, 1.0, 0.0, ux, uy, uz, node_vel, ws, ws_bytes, (cudaStream_t)stream,
-                        "pvl_wake_node_velocity");
+    return node_velocity(precision, n_points, n_lines, lines, positions, line_gamma, n_shed, line_rows, complete_rows,
+                         row_begin, row_count, row_step, nullptr, n_cols, cols, wake_pos, ux, uy, uz, tol, node_vel,
+                         ws, ws_bytes, stream, "pvl_wake_node_velocity_rows");
+}
+
+extern "C" int pvl_wake_node_velocity_list(int precision, uint32_t n_points, uint32_t n_lines,
+                                           const uint32_t* lines, const double* positions, const double* line_gamma,
+                                           uint32_t n_shed, uint32_t line_rows, uint32_t complete_rows,
+                                           uint32_t n_rows, const uint32_t* rows, uint32_t n_cols,
+                                           const uint32_t* cols, const double* wake_pos, double ux, double uy,
+                                           double uz, double tol, double* node_vel, void* ws, size_t ws_bytes,
+                                           void* stream)
+{
+    if (n_rows && !rows)
+        return pvl_fail(PVL_ERR_ARG, "pvl_wake_node_velocity_list: rows is NULL");
+    return node_velocity(precision, n_points, n_lines, lines, positions, line_gamma, n_shed, line_rows, complete_rows,
+                         0, n_rows, 1, rows, n_cols, cols, wake_pos, ux, uy, uz, tol, node_vel, ws, ws_bytes, stream,
+                         "pvl_wake_node_velocity_list");
 }
 
 extern "C" int pvl_wake_node_velocity_cols(int precision, uint32_t n_points, uint32_t n_lines,

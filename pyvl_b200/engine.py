@@ -827,7 +827,7 @@ class MixedSolverEngine(SolverEngine):
                 need = max(need, self._init_far_stencil(cp_patches, wake_chord_row, wake_span_row))
             self._cols = None  # node-column stencil of the far-row advection (wake_col_runs)
             if wake_col_runs is not None:
-                self._init_col_stencil(wake_col_runs, advect_col_row)
+                need = max(need, self._init_col_stencil(wake_col_runs, advect_col_row))
         if need + 256 > self._ws_bytes:
             self._ws_bytes = need + 256
             self.ws = torch.empty(self._ws_bytes, dtype=torch.uint8, device=self.dev)
@@ -880,8 +880,9 @@ class MixedSolverEngine(SolverEngine):
         return max(_lib.query("pvl_line_velocity_workspace", max(b - up[chord_row], 1), max(n_c, 1), _lib.PVL_F64),
                    _lib.query("pvl_line_velocity_workspace", max(n_all - b, 1), max(n_s, 1), _lib.PVL_F64))
 
-    def _init_col_stencil(self, runs, col_row: int) -> None:
-        """Device copy of column_stencil(runs) and the velocity buffer of the evaluated columns."""
+    def _init_col_stencil(self, runs, col_row: int) -> int:
+        """Device copy of column_stencil(runs), the row lists and the velocity buffer of the
+        evaluated columns; returns the workspace of their sweeps."""
         w = self.wake
         col_row = max(int(col_row), self.advect_near_rows)
         ri = self.advect_interp_row
@@ -890,12 +891,25 @@ class MixedSolverEngine(SolverEngine):
         plan = column_stencil(w["n_cols"], runs)
         sub = plan["sub"]
         cols = w["cols"].cpu().numpy().view(np.uint32)
-        self._cols = {
-            "row": col_row, "n_sub": int(sub.size), "ids": to_device_u32(cols[sub], self.dev),
+        R = w["R"]
+        self._cols = {"row": col_row}
+        # the evaluated rows from col_row on for every row count 1..R: row k of ``lists``
+        lists = np.zeros((R + 1, R), np.uint32)
+        lens = [0] * (R + 1)
+        for c in range(1, R + 1):
+            rows = self._advect_schedule(c)[5]
+            lists[c, :len(rows)] = rows
+            lens[c] = len(rows)
+        self._cols.update({
+            "lists": to_device_u32(lists, self.dev), "list_len": lens,
+            "n_sub": int(sub.size), "ids": to_device_u32(cols[sub], self.dev),
             "offsets": to_device_u32(plan["offsets"], self.dev), "entries": to_device_u32(plan["entries"], self.dev),
             "weights": torch.as_tensor(plan["weights"]).to(self.dev),
-            "vel": torch.zeros((max(int(sub.size), 1), w["R"], 3), dtype=torch.float64, device=self.dev),
-        }
+            "vel": torch.zeros((max(int(sub.size), 1), R, 3), dtype=torch.float64, device=self.dev),
+        })
+        L = self.mesh.n_lines
+        return max(_lib.query("pvl_line_velocity_workspace", L, max(int(sub.size) * n, 1), _lib.PVL_F32)
+                   for n in set(lens))
 
     # ------------------------------------------------------------------ preconditioner
     def refresh_preconditioner(self, wait: bool = True) -> None:
@@ -1279,6 +1293,24 @@ class MixedSolverEngine(SolverEngine):
         w["cur"], w["ccur"] = 1 - cur, 1 - c
         w["step_count"] += 1
 
+    def _advect_schedule(self, complete: int):
+        """How the advection of a wake with ``complete`` rows is evaluated: rows below nr in
+        FP64, the rest in FP32; from ri (advect_interp_row, when interp) even rows only up to
+        the tail (the odd rows between from their neighbours), every row from tail on; from ac
+        (< complete when the column stencil applies) at the evaluated node columns only, whose
+        rows are then listed in ``rows`` (ascending).  Returns (nr, interp, mid, tail, ac, rows)."""
+        nr = min(self.advect_near_rows, complete)
+        ri = self.advect_interp_row
+        interp = ri is not None and ri >= nr and complete >= ri + 8
+        mid = ri if interp else complete
+        tail = (complete - 4) | 1 if interp else complete  # first odd row without 3 rows above it
+        cs = self._cols
+        ac = cs["row"] if cs is not None and complete > cs["row"] else complete  # ac <= mid
+        rows = []
+        if ac < complete:
+            rows = list(range(ac, mid)) + (list(range(ri, tail, 2)) + list(range(tail, complete)) if interp else [])
+        return nr, interp, mid, tail, ac, rows
+
     def _update_launches(self, complete: int, dt: float, cur: int, c: int) -> None:
         """The launches of wake_update from positions pos[cur] and circulations circ[c] into the
         other buffers (no host state changes: they may be captured once and replayed)."""
@@ -1290,24 +1322,15 @@ class MixedSolverEngine(SolverEngine):
         _lib.call("pvl_line_circulation", msh.n_lines, ptr(d["map_offsets"]), ptr(d["map_entries"]), ptr(self.gamma), 0,
                   ptr(self.body_line_gamma), s)
         u = self.u_inf
-        nr = min(self.advect_near_rows, complete)
-        # rows [ri, complete): even rows evaluated, odd rows interpolated, except the last few
-        # (an odd row needs rows 3 below and 3 above), which are evaluated too
+        nr, interp, mid, tail, ac, _ = self._advect_schedule(complete)
         ri = self.advect_interp_row
-        interp = ri is not None and ri >= nr and complete >= ri + 8
-        mid = ri if interp else complete
-        tail = (complete - 4) | 1 if interp else complete  # first odd row without 3 rows above it
-        # rows from ac on: the evaluated node columns only (into the column buffer), the rest
-        # from the column rule (pvl_wake_interp_cols) before the odd rows are interpolated
         cs = self._cols
-        ac = cs["row"] if cs is not None and complete > cs["row"] else complete  # ac <= mid
-        far = [(_lib.PVL_F32, ac, mid - ac, 1)] if ac < complete else []
-        if interp:
-            far += [(_lib.PVL_F32, ri, (tail - ri + 1) // 2, 2), (_lib.PVL_F32, tail, complete - tail, 1)]
-        # (precision, row, count, step, columns, column list, output)
+        # (precision, row, count, step, columns, column list, output) of the banded sweeps
         all_cols = (w["n_cols"], w["cols"], w["node_vel"])
         bands = [(_lib.PVL_F64, 0, nr, 1) + all_cols, (_lib.PVL_F32, nr, min(ac, mid) - nr, 1) + all_cols]
-        bands += [b + ((cs["n_sub"], cs["ids"], cs["vel"]) if ac < complete else all_cols) for b in far]
+        if ac == complete and interp:
+            bands += [(_lib.PVL_F32, ri, (tail - ri + 1) // 2, 2) + all_cols,
+                      (_lib.PVL_F32, tail, complete - tail, 1) + all_cols]
         for prec, r0, count, step, n_c, col_list, out in bands:
             if count > 0:
                 _lib.call("pvl_wake_node_velocity_rows", prec, msh.n_points, msh.n_lines, ptr(d["lines"]),
@@ -1315,6 +1338,13 @@ class MixedSolverEngine(SolverEngine):
                           ptr(col_list), ptr(wpos), float(u[0]), float(u[1]), float(u[2]), self.tol,
                           ptr(out), ptr(self.ws), self._ws_bytes, s)
         if ac < complete:
+            # every evaluated row from ac on, at the evaluated node columns, in one sweep (the row
+            # list of this row count, precomputed), then the other columns from their rule
+            n_list = cs["list_len"][complete]
+            _lib.call("pvl_wake_node_velocity_list", _lib.PVL_F32, msh.n_points, msh.n_lines, ptr(d["lines"]),
+                      ptr(self.pos), ptr(self.body_line_gamma), S, R, complete, n_list,
+                      cs["lists"].data_ptr() + 4 * R * complete, cs["n_sub"], ptr(cs["ids"]), ptr(wpos),
+                      float(u[0]), float(u[1]), float(u[2]), self.tol, ptr(cs["vel"]), ptr(self.ws), self._ws_bytes, s)
             _lib.call("pvl_wake_interp_cols", w["n_cols"], complete, ac, complete, ptr(cs["offsets"]),
                       cs["entries"].numel(), ptr(cs["entries"]), ptr(cs["weights"]), cs["n_sub"], ptr(cs["vel"]),
                       ptr(w["node_vel"]), s)

@@ -188,6 +188,21 @@ def test_wake_node_velocity_column_and_row_split():
     assert torch.equal(got[:, keep], f[:, keep])
     with pytest.raises(ValueError):  # an interpolated row needs the rows 3 above it
         _lib.call("pvl_wake_interp_rows", 2 * S, complete, 7, complete - 3, ptr(interp), s)
+    # listed rows (pvl_wake_node_velocity_list) of the de-duplicated columns: those rows as in the
+    # full sweep, a listed row at or past complete_rows skipped, the other rows untouched
+    rows = np.array([2, 3, 9, 10, 11, complete - 1, complete + 4], np.int32)
+    d_rows = torch.as_tensor(rows, device="cuda")
+    listed = torch.full((cols.size, complete, 3), float("nan"), dtype=torch.float64, device="cuda")
+    _lib.call("pvl_wake_node_velocity_list", _lib.PVL_F64, mesh.n_points, mesh.n_lines, ptr(d["lines"]), ptr(pos),
+              ptr(lg), S, R, complete, rows.size, ptr(d_rows), int(cols.size), ptr(dcols), ptr(wp), float(u[0]),
+              float(u[1]), float(u[2]), case.tol, ptr(listed), ptr(ws), nb, s)
+    torch.cuda.synchronize()
+    r_ok = torch.as_tensor(rows[:-1].astype(np.int64), device="cuda")
+    want = full.reshape(2 * S, complete, 3)[torch.as_tensor(cols.astype(np.int64), device="cuda")]
+    assert torch.allclose(listed[:, r_ok], want[:, r_ok], rtol=1e-13, atol=1e-13)
+    other = torch.ones(complete, dtype=torch.bool, device="cuda")
+    other[r_ok] = False
+    assert torch.isnan(listed[:, other]).all()
 
 
 def _mixed_engine(case, **kw):
