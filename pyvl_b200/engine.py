@@ -506,7 +506,8 @@ class SolverEngine:
         rm, d = w["rm"], w["rm_d"]
         wpos = self.wake_positions.reshape(-1, 3)
         ws, nb = ptr(self.ws), self._ws_bytes
-        _lib.call("pvl_induction_normal_tiled", rm.n_points, rm.n_lines, ptr(d["lines"]), ptr(wpos), S,
+        # the implicit block needs the segments of row 0's lines only (the first lines_upto[1])
+        _lib.call("pvl_induction_normal_tiled", rm.n_points, w["lines_upto"][1], ptr(d["lines"]), ptr(wpos), S,
                   ptr(d["offsets"]), ptr(d["surface_lines"]), ptr(d["tile_offsets"]), ptr(d["tile_lines"]),
                   ptr(d["sl_local"]), d["tile_max"], self.P, ptr(self.cps), ptr(self.nrm), self.tol,
                   ptr(w["implicit"]), S, ws, nb, s)
