@@ -29,8 +29,10 @@ Timed (K steps each, from step 1000 + W on, after 1000 + W untimed steps of the 
 * ``warm_start``: the same mixed engine seeded by the previous circulation, by the Jacobi
   correction the network starts from, and by the network, over the same timed window.
 * ``roofline``: the dominant kernel (the FP64 segment sweep of the explicit wake term) timed
-  live with CUDA events; 45 FLOP per segment-point pair (the reference kernel's arithmetic)
-  against the FP64 FMA throughput measured live by pvl_probe_fma on the same GPU.
+  live with CUDA events over the step's three row bands, as the mixed step launches it; 45 FLOP
+  per segment-point pair (the reference kernel's arithmetic) against the FP64 FMA throughput
+  measured live by pvl_probe_fma on the same GPU.  One sweep of every row at every point is
+  ``rooflines_secondary.wake_term_full_sweep``.
 * ``cpu_baseline``: the reference's own compiled kernels + LAPACK on the host cores, one whole
   full-wake step (oracle/refbench.py); ``--impl reference`` times K whole steps the same way.
 With --gpus N > 1 each rank flies an independent replica (the headline case does not shard)
@@ -73,7 +75,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batched-cases summary (bench.py --workload batch, run after the headline)")
-    ap.add_argument("--profile-kernel", choices=["line_sum", "advect_f32", "wake_term", "body", "gemv", "lu", "lu32",
+    ap.add_argument("--profile-kernel", choices=["line_sum", "advect_f32", "wake_term", "wake_bands", "body", "gemv",
+                                                 "lu", "lu32",
                                                  "mixed_step", "plain_step", "batch_step", "mlp", "gemm4096"],
                     default=None,
                     help="set up the workload, launch only that kernel family twice and exit (for ncu captures)")
@@ -237,6 +240,34 @@ def cpu_baseline() -> dict | None:
 
 
 # ------------------------------------------------------------------ our arm
+def wake_band_calls(eng, tol: float):
+    """The argument tuples of the mixed step's three FP64 sweeps of the explicit wake term on the
+    engine's current wake (every row shed), as MixedSolverEngine._far_wake_term issues them, and
+    their pair count; the stencil's points are gathered first."""
+    from pyvl_b200 import _lib
+    from pyvl_b200.device import ptr, stream_ptr
+
+    w, f = eng.wake, eng._far
+    rm, d = w["rm"], w["rm_d"]
+    up, n = w["lines_upto"], rm.n_lines
+    a = up[f["chord_row"]]
+    b = n if f["span_row"] is None else up[f["span_row"]]
+    n_c, n_s = f["n_chord_eval"], f["n_span_eval"]
+    wpos, lg, lines = eng.wake_positions.reshape(-1, 3), w["rm_line_gamma"], d["lines"]
+    s = stream_ptr()
+    _lib.call("pvl_gather_points", n_c, ptr(f["index"]), eng.P, ptr(eng.cps), ptr(f["pts"]), s)
+    ws = (ptr(eng.ws), eng._ws_bytes, s)
+    calls = [
+        (_lib.PVL_F64, rm.n_points, a, ptr(lines), ptr(wpos), ptr(lg), eng.P, ptr(eng.cps), ptr(eng.nrm), tol, 1.0,
+         1.0, ptr(eng.rhs)) + ws,
+        (_lib.PVL_F64, rm.n_points, b - a, lines.data_ptr() + 8 * a, ptr(wpos), lg.data_ptr() + 8 * a, n_c,
+         ptr(f["pts"]), None, tol, 1.0, 0.0, ptr(f["vals"])) + ws,
+        (_lib.PVL_F64, rm.n_points, n - b, lines.data_ptr() + 8 * b, ptr(wpos), lg.data_ptr() + 8 * b, n_s,
+         ptr(f["pts"]), None, tol, 1.0, 0.0, f["vals"].data_ptr() + 24 * n_c) + ws,
+    ]
+    return calls, a * eng.P + (b - a) * n_c + (n - b) * n_s
+
+
 def profile_kernel(args) -> None:
     """Two launches of one kernel family on the benchmark state, nothing else (ncu target);
     mixed_step / batch_step: a few whole steps (launch lists)."""
@@ -307,6 +338,12 @@ def profile_kernel(args) -> None:
             _lib.call("pvl_line_velocity", _lib.PVL_F64, rm.n_points, rm.n_lines, ptr(d["lines"]),
                       ptr(eng.wake_positions.reshape(-1, 3)), ptr(lg), eng.P, ptr(eng.cps), ptr(eng.nrm), case.tol,
                       1.0, 0.0, ptr(eng.rhs), ptr(eng.ws), eng._ws_bytes, stream_ptr())
+    elif args.profile_kernel == "wake_bands":  # the mixed step's three FP64 wake-term sweeps, twice
+        w["rm_line_gamma"].fill_(1e-3)
+        calls, _ = wake_band_calls(eng, case.tol)
+        for _ in range(2):
+            for c in calls:
+                _lib.call("pvl_line_velocity", *c)
     elif args.profile_kernel == "body":  # the body matrix (tiled ring kernel)
         for _ in range(2):
             eng.assemble_body_only()
@@ -898,10 +935,12 @@ def main() -> None:
     del Gp, Gm, seeds
     results["plain"].pop("G")
     results["mixed"].pop("G")
-    # ---------------- dominant kernel: the FP64 sweep of the explicit wake term, timed alone on a
-    # full-wake state (the seeded full wake that the kernel captures under ncu use as well)
+    # ---------------- dominant kernel: the FP64 sweeps of the explicit wake term, timed alone on a
+    # full-wake state (the seeded full wake that the kernel captures under ncu use as well): the
+    # headline's three row bands (wake_bands), and one sweep of every row at every point
     _, spec_full, wpos, wcirc, t0 = wake_setup(case, mesh)
-    eng = MixedSolverEngine(mesh, case.freestream, case.tol, spec_full)
+    eng = MixedSolverEngine(mesh, case.freestream, case.tol, spec_full, cp_patches=case.smooth_patches,
+                            wake_col_runs=case.wake_col_runs)
     eng.set_wake_state(wpos, wcirc, step_count=case.line_rows + 1, time=t0 - case.dt)
     eng.iteration = 1
     eng.load_inputs(case.positions_at(t0), case.velocities_at(t0))
@@ -923,8 +962,20 @@ def main() -> None:
         _lib.call("pvl_line_velocity", *kargs)
     k1.record()
     torch.cuda.synchronize()
+    full_ms = k0.elapsed_time(k1) / reps
+    full_pairs = rm.n_lines * eng.P
+    band_calls, pairs = wake_band_calls(eng, case.tol)
+    for _ in range(2):
+        for bc in band_calls:
+            _lib.call("pvl_line_velocity", *bc)
+    torch.cuda.synchronize()
+    k0.record()
+    for _ in range(reps):
+        for bc in band_calls:
+            _lib.call("pvl_line_velocity", *bc)
+    k1.record()
+    torch.cuda.synchronize()
     kms = k0.elapsed_time(k1) / reps
-    pairs = rm.n_lines * eng.P
     achieved = pairs * PAIR_FLOPS / (kms * 1e-3) / 1e12
     from pyvl_b200 import _probe
 
@@ -978,7 +1029,21 @@ def main() -> None:
     mp = ROOT / "MEASURED_PEAKS.json"
     if mp.exists():
         hbm_peak = json.loads(mp.read_text()).get("hbm_gbs")
+    traffic = traffic_full = None
+    prof = ROOT / "profiles" / "line_sum_f64_flapping_wake_term.md"
+    if prof.exists():
+        for line in prof.read_text().splitlines():
+            if line.startswith("traffic_bytes_per_launch:"):
+                traffic_full = float(line.split(":", 1)[1].split()[0])
+            if line.startswith("band_traffic_bytes_per_step:"):
+                traffic = float(line.split(":", 1)[1].split()[0])
     secondary = {
+        "wake_term_full_sweep": {"kernel": "line_sum_f64_kernel (every wake row at every control point)",
+                                 "ms_per_call": full_ms, "pairs": full_pairs,
+                                 "achieved": full_pairs * PAIR_FLOPS / (full_ms * 1e-3) / 1e12, "peak": peak,
+                                 "unit": "TFLOP/s",
+                                 "frac": full_pairs * PAIR_FLOPS / (full_ms * 1e-3) / 1e12 / peak,
+                                 "traffic": traffic_full},
         "advection_fp32x2": {"kernel": "line_sum_f32x2_kernel (wake rows %d..%d)" % (r_near, R - 1),
                              "ms_per_call": ams, "pairs": a_pairs,
                              "achieved": a_pairs * PAIR_FLOPS / (ams * 1e-3) / 1e12, "peak": peak32,
@@ -990,12 +1055,6 @@ def main() -> None:
                         "hbm_write_gbs": 8.0 * eng.P * eng.P / (bms * 1e-3) / 1e9, "hbm_peak_gbs": hbm_peak},
     }
     del eng
-    traffic = None
-    prof = ROOT / "profiles" / "line_sum_f64_flapping_wake_term.md"
-    if prof.exists():
-        for line in prof.read_text().splitlines():
-            if line.startswith("traffic_bytes_per_launch:"):
-                traffic = float(line.split(":", 1)[1].split()[0])
     head = results[args.path]
     sps = replica_throughput(K, head["ms"], world)
     sps_e2e = replica_throughput(K, head["ms_e2e"], world)
@@ -1058,9 +1117,11 @@ def main() -> None:
             "e2e": {"value": sps_e2e, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp64", "kernel": "line_sum_f64_kernel (explicit wake term)",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                         "traffic": traffic, "ms_per_launch": kms, "pairs_per_launch": pairs,
+                         "traffic": traffic, "ms_per_step": kms, "pairs_per_step": pairs, "launches_per_step": 3,
                          "peak_source": "FP64 FMA throughput measured live (pvl_probe_fma); 45 FLOP per pair",
-                         "timed": "pvl_line_velocity: segment table, the sweep and the partial-sum reduction"},
+                         "timed": "the step's three pvl_line_velocity calls of the explicit wake term (rows 1-63 "
+                                  "at every control point, 64-191 and 192-399 at the stencils' points): segment "
+                                  "tables, sweeps and partial-sum reductions; traffic: their three sweeps"},
             "rooflines_secondary": secondary,
             "cpu_baseline": base,
             "batched_cases": batch,
