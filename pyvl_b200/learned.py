@@ -122,9 +122,18 @@ class WarmStart:
     ``finish()`` runs after the solve and rotates the history.  With ``record=True`` the raw
     inputs and targets of every step are kept for training (``training_data``).  Open meshes
     only (the inputs are per panel; a bordered closed-body system keeps its multipliers).
+
+    The base the network corrects is one Jacobi correction of the circulation extrapolated
+    from the last steps by the polynomial of degree ``extrapolate`` (at most 3, and at most
+    the history there is; 0: the last circulation), which assumes equal time steps: on the
+    flapping wing (32 steps per chord) the cubic gives a relative residual of ~1e-8 and, after
+    the Jacobi correction, ~2e-12, against 2.7e-3 and 1.4e-6 from the last circulation.
     """
 
-    def __init__(self, engine, mlp: WarmStartMLP | None = None, record: bool = False, jacobi: bool = False):
+    _EXTRAPOLATION = {0: (1.0,), 1: (2.0, -1.0), 2: (3.0, -3.0, 1.0), 3: (4.0, -6.0, 4.0, -1.0)}
+
+    def __init__(self, engine, mlp: WarmStartMLP | None = None, record: bool = False, jacobi: bool = False,
+                 extrapolate: int = 3):
         if getattr(engine, "m", 0):
             raise ValueError("the learned warm start is for open meshes")
         if jacobi and (mlp is not None or record):
@@ -132,9 +141,13 @@ class WarmStart:
         self.eng = engine
         self.mlp = mlp
         self.jacobi = bool(jacobi)  # seed with the Jacobi correction alone (the method without the network)
+        if int(extrapolate) not in self._EXTRAPOLATION:
+            raise ValueError("extrapolate must be 0, 1, 2 or 3")
+        self.order = int(extrapolate)
         P, dev = engine.P, engine.dev
         f64 = dict(dtype=torch.float64, device=dev)
-        self.hist = [torch.zeros(P, **f64) for _ in range(2)]  # g0 (last step), g1
+        self.hist = [torch.zeros(P, **f64) for _ in range(4)]  # g0 (last step), g1, g2, g3
+        self.gext = torch.zeros(P, **f64)  # the extrapolated circulation
         self.rem = [torch.zeros(P, **f64) for _ in range(2)]   # gamma - base of the last two steps
         self.rhs_prev = torch.zeros(P, **f64)
         self.rhs_cur = torch.zeros(P, **f64)
@@ -165,24 +178,32 @@ class WarmStart:
         self.have_base = self.n_hist >= 1
         self.ready = self.n_hist >= 3  # g1, rem0 and rem1 hold real history
         infer = self.have_base and self.mlp is not None and not self.record and self.ready
-        run = lambda: self._prepare_ops(self.have_base, infer)
+        order = min(self.order, self.n_hist - 1) if self.have_base else 0
+        run = lambda: self._prepare_ops(self.have_base, infer, order)
         if self.record:
             run()
         else:  # fixed buffers: one captured graph per state (engine.captured)
             scale = self.mlp.out_scale if infer else 0.0  # a host value the graph keeps
-            eng.captured(("prepare", self.have_base, infer, scale), run, self._graphs)
+            eng.captured(("prepare", self.have_base, infer, scale, order), run, self._graphs)
         if self.jacobi and self.have_base:
             return self.base
         return self.seed if infer else None
 
-    def _prepare_ops(self, have_base: bool, infer: bool) -> None:
+    def _prepare_ops(self, have_base: bool, infer: bool, order: int) -> None:
         eng = self.eng
         P = eng.P
         self.rhs_cur.copy_(eng.rhs[:P])
         if not have_base:
             return
         s = stream_ptr()
-        g0, g1 = self.hist
+        g1 = self.hist[1]
+        g0 = self.hist[0]
+        if order:
+            w = self._EXTRAPOLATION[order]
+            torch.mul(self.hist[0], w[0], out=self.gext)
+            for c, g in zip(w[1:], self.hist[1:]):
+                self.gext.add_(g, alpha=c)
+            g0 = self.gext
         self.resid.copy_(self.rhs_cur)
         _lib.call("pvl_gemv_f64", P, P, -1.0, ptr(eng.A), eng.N, ptr(g0), 1.0, ptr(self.resid), s)
         _lib.call("pvl_normalize", P, ptr(self.resid), None, ptr(self.rnorm), s)
@@ -211,13 +232,15 @@ class WarmStart:
 
     def _finish_ops(self, have_base: bool) -> None:
         eng = self.eng
-        g0, g1 = self.hist
+        g0, g1, g2, g3 = self.hist
         r0, r1 = self.rem
         r1.copy_(r0)
         if have_base:
             torch.sub(eng.gamma, self.base, out=r0)
         else:
             r0.zero_()
+        g3.copy_(g2)
+        g2.copy_(g1)
         g1.copy_(g0)
         g0.copy_(eng.gamma)
         self.rhs_prev.copy_(self.rhs_cur)
