@@ -14,7 +14,7 @@ Both paths fly the whole run (plain FP64 first, then mixed + learned):
 * mixed (+ learned): FP64 assembly and wake terms, GMRES with FP64 residuals preconditioned by
   the inverse of an FP32 tensor-core LU rebuilt when it goes stale (engine.RefreshPolicy),
   seeded by the per-panel MLP, FP32 far-row advection.  The network is trained on the GPU,
-  between the two runs, on plain steps 200..263.
+  between the two runs, on plain steps 440..503 (full wake).
 
 Timed (K steps each, from step 1000 + W on, after 1000 + W untimed steps of the same run):
 * ``value``: steps/s with each step's body positions/velocities already in HBM.
