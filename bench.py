@@ -14,7 +14,7 @@ Both paths fly the whole run (plain FP64 first, then mixed + learned):
 * mixed (+ learned): FP64 assembly and wake terms, GMRES with FP64 residuals preconditioned by
   the inverse of an FP32 tensor-core LU rebuilt when it goes stale (engine.RefreshPolicy),
   seeded by the per-panel MLP, FP32 far-row advection.  The network is trained on the GPU,
-  between the two runs, on plain steps 440..503 (full wake).
+  between the two runs, on plain steps 440..943 (full wake, one flapping cycle).
 
 Timed (K steps each, from step 1000 + W on, after 1000 + W untimed steps of the same run):
 * ``value``: steps/s with each step's body positions/velocities already in HBM.
@@ -94,7 +94,7 @@ def workload():
 
 T_START_STEPS = 100  # the reference arm and the kernel timings use a seeded full wake at t = 100 dt
 T_TIMED = 1000       # our arm times steps from 1000 + W on of the run from t = 0 (wake full from step 400)
-TRAIN_STEPS = (440, 504)  # plain FP64 steps (full wake) whose inputs and circulations train the warm start
+TRAIN_STEPS = (440, 944)  # plain FP64 steps (full wake, one flapping cycle) whose inputs and circulations train the warm start
 REF_TIMED_BUDGET_S = 150.0  # the reference arm's timed whole CPU steps stop once they would exceed this
 
 
@@ -881,6 +881,9 @@ def main() -> None:
                         rec["refreshes_in_window"] = st["refreshes"] - refresh0
                 else:
                     rec["ms_e2e"] = ms
+                    if kind != "plain":
+                        st = eng.stats
+                        rec["gmres_iters_e2e"] = [int(i) for i in st["gmres_iters"][n_solves0 + K:n_solves0 + 2 * K]]
                     eng.check_status()
                 run0.record()
         run1.record()
@@ -1089,6 +1092,7 @@ def main() -> None:
                 "mixed_learned": {"steps_per_s": replica_throughput(K, mx["ms"], world), "ms_per_step": mx["ms"] / K,
                                   "e2e_steps_per_s": replica_throughput(K, mx["ms_e2e"], world),
                                   "gmres_iters_mean": float(np.mean(mx["gmres_iters"])),
+                                  "gmres_iters_mean_e2e": float(np.mean(mx["gmres_iters_e2e"])),
                                   "fallbacks": mx["fallbacks"], "preconditioner_refreshes": mx["refreshes"],
                                   "refreshes_in_window": mx["refreshes_in_window"],
                                   "refresh_failures": mx["refresh_failures"],
