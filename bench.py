@@ -95,6 +95,7 @@ def workload():
 T_START_STEPS = 100  # the reference arm and the kernel timings use a seeded full wake at t = 100 dt
 T_TIMED = 1000       # our arm times steps from 1000 + W on of the run from t = 0 (wake full from step 400)
 TRAIN_STEPS = (440, 944)  # plain FP64 steps (full wake, one flapping cycle) whose inputs and circulations train the warm start
+TRAIN_ITERS = 3000  # Adam iterations on 16 k-sample batches (2 M samples)
 REF_TIMED_BUDGET_S = 150.0  # the reference arm's timed whole CPU steps stop once they would exceed this
 
 
@@ -465,7 +466,7 @@ def train_warm_start(X, T, seed: int = 0):
 
     mlp = WarmStartMLP(torch.device("cuda"), seed=seed)
     Xn, Tn = mlp.fit_statistics(X, T)
-    losses = mlp.train(Xn, Tn, iters=600, batch=16384, lr=2e-3, seed=seed)
+    losses = mlp.train(Xn, Tn, iters=TRAIN_ITERS, batch=16384, lr=2e-3, seed=seed)
     return mlp, {"samples": int(X.shape[0]), "loss_first": losses[0], "loss_last": losses[-1]}
 
 

@@ -124,13 +124,18 @@ class WarmStart:
     only (the inputs are per panel; a bordered closed-body system keeps its multipliers).
 
     The base the network corrects is one Jacobi correction of the circulation extrapolated
-    from the last steps by the polynomial of degree ``extrapolate`` (at most 3, and at most
+    from the last steps by the polynomial of degree ``extrapolate`` (at most 4, and at most
     the history there is; 0: the last circulation), which assumes equal time steps: on the
     flapping wing (32 steps per chord) the cubic gives a relative residual of ~1e-8 and, after
-    the Jacobi correction, ~2e-12, against 2.7e-3 and 1.4e-6 from the last circulation.
+    the Jacobi correction, ~2e-12, the quartic ~1e-10 and ~4e-14, against 2.7e-3 and 1.4e-6
+    from the last circulation (higher degrees amplify the solves' own 1e-12 residuals).  The
+    default is the cubic: the network then still has a remainder worth predicting (7e-13 after
+    it); on the quartic base its correction no longer helps (2e-14 against 3.5e-14 at the
+    benchmark, worse than the Jacobi seed alone on a short 64 x 16 run).
     """
 
-    _EXTRAPOLATION = {0: (1.0,), 1: (2.0, -1.0), 2: (3.0, -3.0, 1.0), 3: (4.0, -6.0, 4.0, -1.0)}
+    _EXTRAPOLATION = {0: (1.0,), 1: (2.0, -1.0), 2: (3.0, -3.0, 1.0), 3: (4.0, -6.0, 4.0, -1.0),
+                      4: (5.0, -10.0, 10.0, -5.0, 1.0)}
 
     def __init__(self, engine, mlp: WarmStartMLP | None = None, record: bool = False, jacobi: bool = False,
                  extrapolate: int = 3):
@@ -142,11 +147,11 @@ class WarmStart:
         self.mlp = mlp
         self.jacobi = bool(jacobi)  # seed with the Jacobi correction alone (the method without the network)
         if int(extrapolate) not in self._EXTRAPOLATION:
-            raise ValueError("extrapolate must be 0, 1, 2 or 3")
+            raise ValueError("extrapolate must be 0, 1, 2, 3 or 4")
         self.order = int(extrapolate)
         P, dev = engine.P, engine.dev
         f64 = dict(dtype=torch.float64, device=dev)
-        self.hist = [torch.zeros(P, **f64) for _ in range(4)]  # g0 (last step), g1, g2, g3
+        self.hist = [torch.zeros(P, **f64) for _ in range(5)]  # g0 (last step), g1, ..., g4
         self.gext = torch.zeros(P, **f64)  # the extrapolated circulation
         self.rem = [torch.zeros(P, **f64) for _ in range(2)]   # gamma - base of the last two steps
         self.rhs_prev = torch.zeros(P, **f64)
@@ -232,17 +237,15 @@ class WarmStart:
 
     def _finish_ops(self, have_base: bool) -> None:
         eng = self.eng
-        g0, g1, g2, g3 = self.hist
         r0, r1 = self.rem
         r1.copy_(r0)
         if have_base:
             torch.sub(eng.gamma, self.base, out=r0)
         else:
             r0.zero_()
-        g3.copy_(g2)
-        g2.copy_(g1)
-        g1.copy_(g0)
-        g0.copy_(eng.gamma)
+        for older, newer in zip(self.hist[:0:-1], self.hist[-2::-1]):  # g4 <- g3, ..., g1 <- g0
+            older.copy_(newer)
+        self.hist[0].copy_(eng.gamma)
         self.rhs_prev.copy_(self.rhs_cur)
 
     def training_data(self) -> tuple[torch.Tensor, torch.Tensor]:
