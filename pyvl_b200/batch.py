@@ -86,6 +86,15 @@ def _splits(n_segments: int, n_points: int, pts_per_cta: int, target_ctas: int =
     return -(-n_segments // per), per
 
 
+# weights of (gamma, g0, g1, g2, g3) by the number of stored solutions: keep gamma, the last
+# solution, then the linear, quadratic and cubic extrapolations through 2, 3 and 4 of them
+_EXTRAP = [[1.0, 0.0, 0.0, 0.0, 0.0],
+           [0.0, 1.0, 0.0, 0.0, 0.0],
+           [0.0, 2.0, -1.0, 0.0, 0.0],
+           [0.0, 3.0, -3.0, 1.0, 0.0],
+           [0.0, 4.0, -6.0, 4.0, -1.0]]
+
+
 class BatchEngine:
     """Every case of ``cases`` stepped together on the device (see the module docstring)."""
 
@@ -280,6 +289,13 @@ class BatchEngine:
         self.nrm = torch.zeros((NR, 3), **f64)
         self.rhs = torch.zeros(NR, **f64)
         self.gamma = torch.zeros(NR, **f64)
+        # the GMRES start: the circulation extrapolated from the last solutions by the polynomial
+        # through up to four of them (equal steps within a case); row k of _EXTRAP holds the
+        # weights of (gamma, g0, g1, g2, g3) with k solutions stored, picked on the device so
+        # that the captured step graph ramps up by itself
+        self.ghist = torch.zeros((4, NR), **f64)
+        self.ghist_count = torch.zeros((), dtype=torch.int64, device=dev)
+        self.extrap_w = torch.tensor(_EXTRAP, **f64)
         self.A = torch.zeros(int(mat_off[-1]), **f64)
         self.implicit = torch.zeros(int(imp_off[-1]), **f64)
         self.seg_body = torch.empty(int(_lib.query("pvl_segments_workspace", max(NL, 1), _lib.PVL_F64)),
@@ -460,12 +476,28 @@ class BatchEngine:
         self.rows.zero_()
         self._advect()  # rows = 0: every row collapses onto the trailing edge
         self.rows.fill_(1)
+        self.ghist_count.zero_()
         self.iteration = 0
 
     def _step_body(self, with_wake: bool) -> None:
         self._assemble(with_wake)
+        self._seed()
         self._solve()
+        self._record_solution()
         self._wake_update()
+
+    def _seed(self) -> None:
+        """gamma <- the start of this step's GMRES: the previous solutions extrapolated."""
+        w = torch.index_select(self.extrap_w, 0, self.ghist_count.clamp(max=4).reshape(1))[0]
+        self.gamma.mul_(w[0])
+        for i in range(4):
+            self.gamma.addcmul_(self.ghist[i], w[i + 1])
+
+    def _record_solution(self) -> None:
+        for i in (3, 2, 1):
+            self.ghist[i].copy_(self.ghist[i - 1])
+        self.ghist[0].copy_(self.gamma)
+        self.ghist_count.add_(1).clamp_(max=4)
 
     def step(self) -> None:
         """One solver iteration of every case (static bodies: positions stay as loaded)."""
