@@ -270,6 +270,13 @@ int pvl_wake_node_velocity_list(int precision, uint32_t n_points, uint32_t n_lin
 int pvl_wake_interp_rows(uint32_t n_cols, uint32_t complete_rows, uint32_t row_first, uint32_t row_last,
                          double* node_vel, void* stream);
 
+/* pvl_wake_interp_rows at spacing `half` (> 0): rows row_first, row_first + 2 half, ... <= row_last
+ * from the same column's rows -3 half, -half, +half, +3 half away; needs row_first >= 3 half and
+ * row_last + 3 half < complete_rows.  With half = 2 it fills the rows midway between rows
+ * evaluated every fourth row, before the odd rows are filled with half = 1. */
+int pvl_wake_interp_rows_spaced(uint32_t n_cols, uint32_t complete_rows, uint32_t row_first, uint32_t row_last,
+                                uint32_t half, double* node_vel, void* stream);
+
 /* node_vel[c, r] = sum_{k in [offsets[c], offsets[c+1])} weights[k] sub_vel[entries[k], r] for the
  * rows r in [row_begin, row_end) of every column c < n_cols; node_vel is (n_cols, complete_rows, 3)
  * and sub_vel (n_sub, complete_rows, 3), the velocities of the wake nodes of some columns (from

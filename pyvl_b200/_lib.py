@@ -62,6 +62,7 @@ SIGNATURES = {
     "pvl_wake_node_velocity_list": (_I, [_I, _U, _U, _P, _P, _P, _U, _U, _U, _U, _P, _U, _P, _P, _D, _D, _D, _D,
                                          _P, _P, _Z, _P]),
     "pvl_wake_interp_rows": (_I, [_U, _U, _U, _U, _P, _P]),
+    "pvl_wake_interp_rows_spaced": (_I, [_U, _U, _U, _U, _U, _P, _P]),
     "pvl_wake_interp_cols": (_I, [_U, _U, _U, _U, _P, _U, _P, _P, _U, _P, _P, _P]),
     "pvl_gather_points": (_I, [_U, _P, _U, _P, _P, _P]),
     "pvl_stencil_normal_add": (_I, [_U, _P, _U, _P, _P, _U, _P, _P, _P, _P]),

@@ -168,21 +168,21 @@ int require(const void* p, const char* what)
             return _r;                   \
     } while (0)
 
-// node_vel (n_cols, complete, 3): rows row_first, row_first + 2, ... <= row_last of every column
-// from their neighbours at -3, -1, +1, +3 rows by the cubic that passes through the four
-// (v = (-v[-3] + 9 v[-1] + 9 v[+1] - v[+3]) / 16, the midpoint value of the interpolating cubic
+// node_vel (n_cols, complete, 3): rows row_first, row_first + 2h, ... <= row_last of every column
+// from their neighbours at -3h, -h, +h, +3h rows by the cubic that passes through the four
+// (v = (-v[-3h] + 9 v[-h] + 9 v[+h] - v[+3h]) / 16, the midpoint value of the interpolating cubic
 // of equally spaced samples).
 __global__ void interp_rows_kernel(uint32_t n_cols, uint32_t complete, uint32_t row_first, uint32_t n_rows,
-                                   double* __restrict__ node_vel)
+                                   uint32_t h, double* __restrict__ node_vel)
 {
     const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= (uint64_t)n_cols * n_rows * 3)
         return;
     const uint32_t k = (uint32_t)(e % 3), r = (uint32_t)((e / 3) % n_rows), c = (uint32_t)(e / (3 * (uint64_t)n_rows));
-    const uint32_t i = row_first + 2 * r;
+    const uint32_t i = row_first + 2 * h * r;
     double* col = node_vel + (size_t)c * complete * 3 + k;
-    const double a = col[(size_t)(i - 3) * 3], b = col[(size_t)(i - 1) * 3];
-    const double d = col[(size_t)(i + 1) * 3], f = col[(size_t)(i + 3) * 3];
+    const double a = col[(size_t)(i - 3 * h) * 3], b = col[(size_t)(i - h) * 3];
+    const double d = col[(size_t)(i + h) * 3], f = col[(size_t)(i + 3 * h) * 3];
     col[(size_t)i * 3] = (9.0 * (b + d) - (a + f)) * 0.0625;
 }
 
@@ -427,18 +427,27 @@ extern "C" int pvl_border_groups(uint32_t n, uint32_t m, const uint32_t* group_o
     return PVL_OK;
 }
 
-extern "C" int pvl_wake_interp_rows(uint32_t n_cols, uint32_t complete_rows, uint32_t row_first, uint32_t row_last,
-                                    double* node_vel, void* stream)
+extern "C" int pvl_wake_interp_rows_spaced(uint32_t n_cols, uint32_t complete_rows, uint32_t row_first,
+                                           uint32_t row_last, uint32_t half, double* node_vel, void* stream)
 {
+    if (half == 0)
+        return pvl_fail(PVL_ERR_ARG, "pvl_wake_interp_rows_spaced: half spacing 0");
     if (n_cols == 0 || row_last < row_first)
         return PVL_OK;
     PVL_REQUIRE(node_vel);
-    if (row_first < 3 || (uint64_t)row_last + 3 >= complete_rows)
-        return pvl_fail(PVL_ERR_ARG, "pvl_wake_interp_rows: rows %u..%u need rows 3 below and 3 above within [0, %u)",
-                        row_first, row_last, complete_rows);
-    const uint32_t n_rows = (row_last - row_first) / 2 + 1;
+    if ((uint64_t)row_first < 3ull * half || (uint64_t)row_last + 3ull * half >= complete_rows)
+        return pvl_fail(PVL_ERR_ARG,
+                        "pvl_wake_interp_rows: rows %u..%u need rows %u below and above within [0, %u)", row_first,
+                        row_last, 3 * half, complete_rows);
+    const uint32_t n_rows = (row_last - row_first) / (2 * half) + 1;
     interp_rows_kernel<<<blocks_for((uint64_t)n_cols * n_rows * 3, 256), 256, 0, (cudaStream_t)stream>>>(
-        n_cols, complete_rows, row_first, n_rows, node_vel);
+        n_cols, complete_rows, row_first, n_rows, half, node_vel);
     PVL_LAUNCH_CHECK();
     return PVL_OK;
+}
+
+extern "C" int pvl_wake_interp_rows(uint32_t n_cols, uint32_t complete_rows, uint32_t row_first, uint32_t row_last,
+                                    double* node_vel, void* stream)
+{
+    return pvl_wake_interp_rows_spaced(n_cols, complete_rows, row_first, row_last, 1, node_vel, stream);
 }

@@ -755,11 +755,15 @@ class MixedSolverEngine(SolverEngine):
                  refresh_on_iters: int = 5, use_graphs: bool = True, wake_self_induction: bool = False,
                  device_solve: bool = True, refresh_excess: int = 128, advect_interp_row: int | None = 128,
                  cp_patches=None, wake_chord_row: int = 64, wake_span_row: int | None = 192,
-                 wake_col_runs=None, advect_col_row: int = 64):
+                 wake_col_runs=None, advect_col_row: int = 64, advect_row4: int | None = 192):
         super().__init__(mesh, freestream, tol, wake, closed_groups, wake_self_induction)
         if advect_interp_row is not None and (int(advect_interp_row) < 4 or int(advect_interp_row) % 2):
             raise ValueError("advect_interp_row must be even and at least 4 (or None)")
         self.advect_interp_row = None if advect_interp_row is None else int(advect_interp_row)
+        self.advect_row4 = None if advect_row4 is None else int(advect_row4)
+        if self.advect_row4 is not None and (self.advect_row4 % 2 or self.advect_interp_row is None
+                                             or self.advect_row4 < self.advect_interp_row + 4):
+            raise ValueError("advect_row4 must be even and at least advect_interp_row + 4 (or None)")
         self._update_keys: set = set()  # captured wake_update graphs (full wake)
         self.refresh = None if refresh is None else int(refresh)
         self.refresh_excess = int(refresh_excess)
@@ -1299,7 +1303,11 @@ class MixedSolverEngine(SolverEngine):
         FP64, the rest in FP32; from ri (advect_interp_row, when interp) even rows only up to
         the tail (the odd rows between from their neighbours), every row from tail on; from ac
         (< complete when the column stencil applies) at the evaluated node columns only, whose
-        rows are then listed in ``rows`` (ascending).  Returns (nr, interp, mid, tail, ac, rows)."""
+        rows are then listed in ``rows`` (ascending).  With the column stencil and r4
+        (advect_row4, when four) every fourth row from r4 up to T, every row from T on (T a
+        multiple of 4, 5 to 8 rows below complete): the rows midway between from the rows 2 and
+        6 away, then the odd rows up to T - 1.  Returns (nr, interp, mid, tail, ac, rows, four,
+        T); the interpolated rows are ``_row_passes``."""
         nr = min(self.advect_near_rows, complete)
         ri = self.advect_interp_row
         interp = ri is not None and ri >= nr and complete >= ri + 8
@@ -1307,10 +1315,26 @@ class MixedSolverEngine(SolverEngine):
         tail = (complete - 4) | 1 if interp else complete  # first odd row without 3 rows above it
         cs = self._cols
         ac = cs["row"] if cs is not None and complete > cs["row"] else complete  # ac <= mid
+        r4 = self.advect_row4
+        T = ((complete - 5) // 4) * 4
+        four = interp and ac < complete and r4 is not None and T >= r4 + 8
         rows = []
         if ac < complete:
-            rows = list(range(ac, mid)) + (list(range(ri, tail, 2)) + list(range(tail, complete)) if interp else [])
-        return nr, interp, mid, tail, ac, rows
+            if four:
+                rows = list(range(ac, mid)) + list(range(ri, r4, 2)) + list(range(r4, T, 4)) + list(range(T, complete))
+            elif interp:
+                rows = list(range(ac, mid)) + list(range(ri, tail, 2)) + list(range(tail, complete))
+            else:
+                rows = list(range(ac, complete))
+        return nr, interp, mid, tail, ac, rows, four, T
+
+    def _row_passes(self, complete: int) -> list:
+        """(first row, last row, half spacing) of the row interpolations, in order."""
+        _, interp, _, tail, _, _, four, T = self._advect_schedule(complete)
+        ri = self.advect_interp_row
+        if four:
+            return [(self.advect_row4 + 2, T - 2, 2), (ri + 1, T - 1, 1)]
+        return [(ri + 1, tail - 2, 1)] if interp else []
 
     def _update_launches(self, complete: int, dt: float, cur: int, c: int) -> None:
         """The launches of wake_update from positions pos[cur] and circulations circ[c] into the
@@ -1323,7 +1347,7 @@ class MixedSolverEngine(SolverEngine):
         _lib.call("pvl_line_circulation", msh.n_lines, ptr(d["map_offsets"]), ptr(d["map_entries"]), ptr(self.gamma), 0,
                   ptr(self.body_line_gamma), s)
         u = self.u_inf
-        nr, interp, mid, tail, ac, _ = self._advect_schedule(complete)
+        nr, interp, mid, tail, ac, _, _, _ = self._advect_schedule(complete)
         ri = self.advect_interp_row
         cs = self._cols
         # (precision, row, count, step, columns, column list, output) of the banded sweeps
@@ -1349,8 +1373,8 @@ class MixedSolverEngine(SolverEngine):
             _lib.call("pvl_wake_interp_cols", w["n_cols"], complete, ac, complete, ptr(cs["offsets"]),
                       cs["entries"].numel(), ptr(cs["entries"]), ptr(cs["weights"]), cs["n_sub"], ptr(cs["vel"]),
                       ptr(w["node_vel"]), s)
-        if interp:
-            _lib.call("pvl_wake_interp_rows", w["n_cols"], complete, ri + 1, tail - 2, ptr(w["node_vel"]), s)
+        for first, last, half in self._row_passes(complete):
+            _lib.call("pvl_wake_interp_rows_spaced", w["n_cols"], complete, first, last, half, ptr(w["node_vel"]), s)
         if self.wake_self_induction:
             self._add_wake_self_velocity(complete)
         _lib.call("pvl_wake_advect_cols", S, R, complete, ptr(wpos), ptr(w["node_vel"]), ptr(w["slot"]), w["n_cols"],

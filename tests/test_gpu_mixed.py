@@ -188,6 +188,19 @@ def test_wake_node_velocity_column_and_row_split():
     assert torch.equal(got[:, keep], f[:, keep])
     with pytest.raises(ValueError):  # an interpolated row needs the rows 3 above it
         _lib.call("pvl_wake_interp_rows", 2 * S, complete, 7, complete - 3, ptr(interp), s)
+    # at spacing 2 (rows midway between every fourth row): rows 6, 10, 14 from rows +-2, +-6
+    spaced = full.clone()
+    _lib.call("pvl_wake_interp_rows_spaced", 2 * S, complete, 6, 14, 2, ptr(spaced), s)
+    torch.cuda.synchronize()
+    i2 = torch.arange(6, 15, 4, device="cuda")
+    want = (9.0 * (f[:, i2 - 2] + f[:, i2 + 2]) - (f[:, i2 - 6] + f[:, i2 + 6])) / 16.0
+    got = spaced.reshape(2 * S, complete, 3)
+    assert torch.allclose(got[:, i2], want, rtol=1e-15, atol=1e-15)
+    keep = torch.ones(complete, dtype=torch.bool, device="cuda")
+    keep[i2] = False
+    assert torch.equal(got[:, keep], f[:, keep])
+    with pytest.raises(ValueError):  # rows 6 above the last one needed
+        _lib.call("pvl_wake_interp_rows_spaced", 2 * S, complete, 6, complete - 6, 2, ptr(spaced), s)
     # listed rows (pvl_wake_node_velocity_list) of the de-duplicated columns: those rows as in the
     # full sweep, a listed row at or past complete_rows skipped, the other rows untouched
     rows = np.array([2, 3, 9, 10, 11, complete - 1, complete + 4], np.int32)
@@ -416,9 +429,9 @@ def test_mixed_trajectory_with_far_wake_stencil():
     (cp_patches; 200 wake rows, chordwise from row 64 = 4 chords, spanwise too from row 160 =
     10 chords, where the coarser 64 x 16 grid's spacing relative to the distance matches the
     128 x 32 wing's from row 192) and the advection of the rows from 64 on evaluated at every
-    other node column (wake_col_runs): every step's circulation is still within 1e-10 of the
-    plain FP64 run's, and the judged step (everything re-assembled in FP64) agrees with the
-    interpolated one to the same bar."""
+    other node column (wake_col_runs), from row 160 at every fourth row (advect_row4): every
+    step's circulation is still within 1e-10 of the plain FP64 run's, and the judged step
+    (everything re-assembled in FP64) agrees with the interpolated one to the same bar."""
     from pyvl_b200.cvl import Mesh
     from pyvl_b200.engine import MixedSolverEngine, SolverEngine, wake_spec_from_te
     from pyvl_b200.workloads import flapping
@@ -432,7 +445,7 @@ def test_mixed_trajectory_with_far_wake_stencil():
     plain = SolverEngine(mesh, case.freestream, case.tol, spec())
     mixed = MixedSolverEngine(mesh, case.freestream, case.tol, spec(), cp_patches=case.smooth_patches,
                               wake_chord_row=64, wake_span_row=160, wake_col_runs=case.wake_col_runs,
-                              advect_col_row=64)
+                              advect_col_row=64, advect_row4=160)
     assert mixed._far["n_chord_eval"] < mixed.P and mixed._cols["n_sub"] < mixed.wake["n_cols"]
     worst = 0.0
     for it in range(250):
@@ -462,14 +475,15 @@ def test_full_wake_graphs_match_direct_launches():
 
     from pyvl_b200.workloads import flapping
 
-    case = flapping(ns=32, nc=8, line_rows=24)
+    case = flapping(ns=32, nc=8, line_rows=32)
     runs = []
     for capture in (True, False):
         eng = _mixed_engine(case, cp_patches=case.smooth_patches, wake_chord_row=8, wake_span_row=16,
-                            wake_col_runs=case.wake_col_runs, advect_col_row=8, advect_interp_row=12)
+                            wake_col_runs=case.wake_col_runs, advect_col_row=8, advect_interp_row=12,
+                            advect_row4=16)
         eng.capture_steps = capture
         G = []
-        for it in range(40):
+        for it in range(50):
             t = it * case.dt
             eng.step(t, case.positions_at(t), case.velocities_at(t))
             G.append(eng.gamma_host())
