@@ -735,6 +735,13 @@ class MixedSolverEngine(SolverEngine):
       slowly along a node column.  On the 128x32 flapping wing, 2000 steps, interpolating from
       row 128 keeps every step's circulation within 1.4e-11 of the plain FP64 run (from row 64:
       5.6e-11; row 32: 1.4e-10, over the 1e-10 bar).
+    * With ``wake_col_runs`` (runs of smooth wake node columns, ``column_stencil``) the
+      advection of the rows from ``advect_col_row`` on is evaluated at every other node column
+      (plus those within five of a run end) and interpolated between them by the quintic
+      midpoint rule, and from ``advect_row4`` on (even, at least ``advect_interp_row`` + 4;
+      None: never) at every fourth row only, the rows between by the cubic midpoint rule at
+      spacing 2, then 1.  On the flapping wing, columns from row 64: 4.5e-11; every fourth row
+      from 192: no measurable change.  Default off (no runs given).
     * With ``cp_patches`` (smooth (ring0, n_span, n_chord) blocks of the body's ring grid,
       ``far_wake_stencil``) the explicit wake term of the rows from ``wake_chord_row`` on is
       evaluated at every other chordwise control point (plus those within five of a patch
