@@ -741,7 +741,7 @@ class MixedSolverEngine(SolverEngine):
       midpoint rule, and from ``advect_row4`` on (even, at least ``advect_interp_row`` + 4;
       None: never) at every fourth row only, the rows between by the cubic midpoint rule at
       spacing 2, then 1.  On the flapping wing, columns from row 64: 4.5e-11; every fourth row
-      from 192: no measurable change.  Default off (no runs given).
+      from 136 or 192: no measurable change (4.4e-11 overall).  Default off (no runs given).
     * With ``cp_patches`` (smooth (ring0, n_span, n_chord) blocks of the body's ring grid,
       ``far_wake_stencil``) the explicit wake term of the rows from ``wake_chord_row`` on is
       evaluated at every other chordwise control point (plus those within five of a patch
@@ -762,7 +762,7 @@ class MixedSolverEngine(SolverEngine):
                  refresh_on_iters: int = 5, use_graphs: bool = True, wake_self_induction: bool = False,
                  device_solve: bool = True, refresh_excess: int = 128, advect_interp_row: int | None = 128,
                  cp_patches=None, wake_chord_row: int = 64, wake_span_row: int | None = 192,
-                 wake_col_runs=None, advect_col_row: int = 64, advect_row4: int | None = 192):
+                 wake_col_runs=None, advect_col_row: int = 64, advect_row4: int | None = 136):
         super().__init__(mesh, freestream, tol, wake, closed_groups, wake_self_induction)
         if advect_interp_row is not None and (int(advect_interp_row) < 4 or int(advect_interp_row) % 2):
             raise ValueError("advect_interp_row must be even and at least 4 (or None)")
